@@ -1,0 +1,98 @@
+"""ctypes mirror of include/dgswem_cuda.h (the C-ABI of libdgswem_cuda.so).
+
+Loading fails loudly when the built library is missing: there is no CPU or
+Python fallback for the hydro step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libdgswem_cuda.so"
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class Setup(C.Structure):
+    """struct dgswem_cuda_setup (field order matters)."""
+
+    _fields_ = [
+        ("ne", C.c_int), ("np", C.c_int), ("dofh", C.c_int), ("nrk", C.c_int), ("nedges", C.c_int),
+        ("nieds", C.c_int), ("nleds", C.c_int), ("needs", C.c_int), ("nfeds", C.c_int), ("nreds", C.c_int),
+        ("nebseg", C.c_int), ("nibseg", C.c_int),
+        ("ics", C.c_int), ("nolifa", C.c_int), ("iflinbf", C.c_int), ("ifhybf", C.c_int), ("ifnlfa", C.c_int),
+        ("nramp", C.c_int), ("nws", C.c_int), ("rainfall", C.c_int), ("slopeflag", C.c_int),
+        ("load_manning", C.c_int),
+        ("nleq", C.c_double), ("leq", C.c_double), ("g", C.c_double), ("h0", C.c_double),
+        ("dtdp", C.c_double), ("statim", C.c_double), ("dramp", C.c_double),
+        ("cf", C.c_double), ("hbreak", C.c_double), ("ftheta", C.c_double), ("fgamma", C.c_double),
+        ("sfea0", C.c_double),
+        ("atvd", _dp), ("btvd", _dp), ("dtvd", _dp),
+        ("nm", _ip), ("x", _dp), ("y", _dp), ("dp", _dp),
+        ("nedno", _ip), ("nedel", _ip), ("nedsd", _ip), ("neled", _ip),
+        ("niedn", _ip), ("nledn", _ip), ("needn", _ip), ("nfedn", _ip), ("nredn", _ip), ("nebsegn", _ip),
+        ("nibsegn", _ip),
+        ("hb", _dp), ("cori_el", _dp), ("fric_el", _dp), ("manning", _dp),
+        ("ze", _dp), ("qx", _dp), ("qy", _dp), ("wdflg", _ip),
+        ("nbfr", C.c_int), ("amig", _dp), ("ff", _dp), ("face", _dp), ("per", _dp),
+        ("emo_dg", _dp), ("efa_dg", _dp),
+        ("nffr", C.c_int), ("famig", _dp), ("fff", _dp), ("fface", _dp), ("fper", _dp),
+        ("qnam_dg", _dp), ("qnph_dg", _dp),
+        ("ebht", _dp), ("ebcfsp", _dp), ("ibht", _dp), ("ibcfsb", _dp), ("ibcfsp", _dp),
+    ]
+
+
+# every entry point of the header: name -> (restype, argtypes)
+SIGNATURES = {
+    "dgswem_cuda_create": (C.c_int, [C.POINTER(Setup), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "dgswem_cuda_destroy": (None, [C.c_void_p]),
+    "dgswem_cuda_hydro_timestep": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dgswem_cuda_synchronize": (C.c_int, [C.c_void_p]),
+    "dgswem_cuda_upload_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
+    "dgswem_cuda_download_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
+    "dgswem_cuda_set_met": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "dgswem_cuda_modal2nodal": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
+    "dgswem_cuda_kernel_launches": (C.c_longlong, [C.c_void_p]),
+    "dgswem_cuda_last_error": (C.c_int, [C.c_char_p, C.c_int]),
+    "dgswem_cuda_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dgswem_cuda_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong)]),
+    "dgswem_deck_open": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "dgswem_deck_setup": (C.POINTER(Setup), [C.c_void_p]),
+    "dgswem_deck_int": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]),
+    "dgswem_deck_close": (None, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libdgswem_cuda.so from the package (build it with dgswem_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build the CUDA library with `python -m dgswem_b200.build`; "
+                "the DG hydro step has no CPU fallback")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class DgswemError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"libdgswem_cuda status {status}: {message}")
+        self.status = status
+
+
+def check(status: int) -> None:
+    if status != 0:
+        buf = C.create_string_buffer(1024)
+        load().dgswem_cuda_last_error(buf, len(buf))
+        raise DgswemError(status, buf.value.decode(errors="replace"))

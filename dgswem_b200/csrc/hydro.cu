@@ -1,0 +1,717 @@
+// hydro.cu -- libdgswem_cuda: device layout, launch sequence and C-ABI entry
+// points of the B200 DG hydro time step (declared in include/dgswem_cuda.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "abi_util.h"
+#include "dgswem_cuda.h"
+#include "hydro_kernels.cuh"
+
+namespace dgswem {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+#define DG_CUDA(call)                                                                     \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw Failure(DGSWEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// p=1 basis at the quadrature, edge and corner points (orthogonal_basis_v1.F
+// recurrences evaluated for D=1, with the |value| < 1e-15 -> 0 rule)
+static void p1_basis(double x, double y, double phi[3], double dr[3], double ds[3]) {
+  double v[3] = {1.0, (1.0 + 3.0 * y) / 2.0, (1.0 + 2.0 * x + y) / 2.0};
+  double a[3] = {0.0, 0.0, 1.0}, b[3] = {0.0, 3.0 / 2.0, 1.0 / 2.0};
+  for (int k = 0; k < 3; ++k) {
+    phi[k] = std::fabs(v[k]) < 1.0e-15 ? 0.0 : v[k];
+    if (dr) dr[k] = a[k];
+    if (ds) ds[k] = b[k];
+  }
+}
+
+static BasisP1 make_basis_p1() {
+  BasisP1 B{};
+  // 3-point area rule (quadrature_v1.F:255-260, 802-840)
+  const double A = 0.1666666666666666666666666666666666, W = 0.3333333333333333333333333333333333;
+  const double C = 1.0 - (A + A);
+  const double bary[3][3] = {{A, A, C}, {A, C, A}, {C, A, A}};
+  for (int i = 0; i < 3; ++i) {
+    const double x = -1.0 * bary[i][0] + 1.0 * bary[i][1] + -1.0 * bary[i][2];
+    const double y = -1.0 * bary[i][0] + -1.0 * bary[i][1] + 1.0 * bary[i][2];
+    double phi[3], dr[3], ds[3];
+    p1_basis(x, y, phi, dr, ds);
+    for (int k = 0; k < 3; ++k) {
+      B.phi_area[k][i] = phi[k];
+      B.drphi[k][i] = dr[k];
+      B.dsphi[k][i] = ds[k];
+    }
+    B.wagp[i] = 2.0 * W;
+    B.psi[0][i] = -1.0 / 2.0 * (x + y);
+    B.psi[1][i] = 1.0 / 2.0 * (x + 1.0);
+    B.psi[2][i] = 1.0 / 2.0 * (y + 1.0);
+  }
+  // 3-point Gauss-Lobatto edge rule (quad_rules_general.F)
+  B.xegp[0] = -1.0; B.xegp[1] = 0.0; B.xegp[2] = 1.0;
+  B.wegp[0] = 2.0 / ((1.0 + 1.0) * (1.0 + 2.0));
+  B.wegp[2] = B.wegp[0];
+  {
+    const double p2 = ((2.0 * 1.0 + 1.0) * 0.0 * 0.0 - 1.0 * 1.0) / (1.0 + 1.0);
+    B.wegp[1] = 2.0 / ((1.0 + 1.0) * (1.0 + 2.0) * p2 * p2);
+  }
+  // M_INV (prep_DG.F:712-721): (I,JJ) = (0,0),(0,1),(1,0)
+  B.m_inv[0] = (2.0 * 0 + 1.0) * (2.0 * 0 + 2.0 * 0 + 2.0) / 4.0;
+  B.m_inv[1] = (2.0 * 0 + 1.0) * (2.0 * 1 + 2.0 * 0 + 2.0) / 4.0;
+  B.m_inv[2] = (2.0 * 1 + 1.0) * (2.0 * 0 + 2.0 * 1 + 2.0) / 4.0;
+  // edge points: edge 1 (-x, x), edge 2 (-1, -x), edge 3 (x, -1)
+  for (int l = 0; l < 3; ++l)
+    for (int j = 0; j < 3; ++j) {
+      const double t = B.xegp[j];
+      const double px = l == 0 ? -t : (l == 1 ? -1.0 : t);
+      const double py = l == 0 ? t : (l == 1 ? -t : -1.0);
+      double phi[3];
+      p1_basis(px, py, phi, nullptr, nullptr);
+      for (int k = 0; k < 3; ++k) {
+        B.phi_edge[l][j][k] = phi[k];
+        B.edgeq[l][j][k] = 2.0 * B.m_inv[k] * phi[k] * B.wegp[j];
+      }
+    }
+  const double vx[3] = {-1.0, 1.0, -1.0}, vy[3] = {-1.0, -1.0, 1.0};
+  for (int v = 0; v < 3; ++v) p1_basis(vx[v], vy[v], B.phi_corner[v], nullptr, nullptr);
+  return B;
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) DG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const std::vector<T>& v) {
+    alloc(v.size());
+    if (n) DG_CUDA(cudaMemcpy(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { release(); }
+};
+
+}  // namespace dgswem
+
+using namespace dgswem;
+
+struct dgswem_cuda {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream the launches go to
+  cudaStream_t own_stream = nullptr;  // created with the context
+  int ne = 0, np = 0, nrk = 0;
+  // scalars kept from the setup
+  int nramp = 0, slopeflag = 0, nolifa = 0, nws = 0;
+  double dtdp = 0, statim = 0, dramp = 1;
+  std::vector<double> atvd, btvd, dtvd;
+  std::vector<double> amig, ff, face, per, famig, fff, fface, fper;
+  std::vector<char> keep_rhs;  // stage I's RHS is read by a later stage
+  Physics ph{};
+  MeshView mesh{};
+  // device arrays
+  DevBuf<double> x, y, dp, hb, cori, fric, manning, sfac_area, sfac_edge;
+  DevBuf<int> nm, link, star_ptr, star, ib_elem, ib_led;
+  DevBuf<unsigned> einfo;
+  DevBuf<double> emo_dg, efa_dg, qnam_dg, qnph_dg, ebht, ebcfsp, ibht, ibcfsb, ibcfsp;
+  DevBuf<double> wsx, wsy, pr, minmax, staging;
+  std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
+  std::vector<DevBuf<double>> rhs;  // nrk RHS buffers (allocated when kept)
+  DevBuf<int> wd, nodecode;
+  DevBuf<unsigned> err;
+  long long launches = 0;
+  // per-kernel event timing (dgswem_cuda_profile)
+  bool prof_on = false;
+  std::vector<cudaEvent_t> ev_pool;
+  struct Pending { int kind; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  double prof_ms[4] = {0, 0, 0, 0};
+  long long prof_n[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+void check_launch(dgswem_cuda* h) {
+  ++h->launches;
+  DG_CUDA(cudaPeekAtLastError());
+}
+
+cudaEvent_t take_event(dgswem_cuda* h) {
+  if (!h->ev_pool.empty()) {
+    cudaEvent_t e = h->ev_pool.back();
+    h->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  DG_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+void prof_flush(dgswem_cuda* h) {
+  if (h->pending.empty()) return;
+  DG_CUDA(cudaStreamSynchronize(h->stream));
+  for (auto& p : h->pending) {
+    float ms = 0.f;
+    DG_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+    h->prof_ms[p.kind] += ms;
+    h->prof_n[p.kind] += 1;
+    h->ev_pool.push_back(p.a);
+    h->ev_pool.push_back(p.b);
+  }
+  h->pending.clear();
+}
+
+// Records CUDA events around one launch on the launching stream when
+// profiling is on.
+struct LaunchTimer {
+  dgswem_cuda* h;
+  int kind;
+  cudaEvent_t a = nullptr;
+  LaunchTimer(dgswem_cuda* hh, int k) : h(hh), kind(k) {
+    if (h->prof_on) {
+      a = take_event(h);
+      DG_CUDA(cudaEventRecord(a, h->stream));
+    }
+  }
+  void done() {
+    check_launch(h);
+    if (a) {
+      cudaEvent_t b = take_event(h);
+      DG_CUDA(cudaEventRecord(b, h->stream));
+      h->pending.push_back({kind, a, b});
+      if (h->pending.size() > 2048) prof_flush(h);
+    }
+  }
+};
+
+unsigned grid_for(int n, int block) { return (unsigned)((n + block - 1) / block); }
+
+void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
+  const int ne = s->ne, np = s->np, ned = s->nedges;
+  auto need = [](bool ok, const char* what) {
+    if (!ok) throw Failure(DGSWEM_ERR_ARG, what);
+  };
+  need(s->nm && s->x && s->y && s->dp && s->neled && s->nedel && s->nedsd && s->hb, "setup lacks mesh arrays");
+  need(s->ze && s->qx && s->qy && s->wdflg, "setup lacks the initial state");
+  need(s->atvd && s->btvd && s->dtvd, "setup lacks RK tables");
+  // nodes, connectivity
+  std::vector<int> nm(3 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int v = 0; v < 3; ++v) {
+      int n = s->nm[e + (size_t)ne * v];
+      need(n >= 1 && n <= np, "NM refers to a node outside 1..NP");
+      nm[(size_t)v * ne + e] = n - 1;
+    }
+  // boundary membership of each edge: kind, list index, side
+  std::vector<int> bkind(ned + 1, -1), bidx(ned + 1, -1), bside(ned + 1, 0);
+  auto mark = [&](const int* list, int n, unsigned kind) {
+    for (int i = 0; i < n; ++i) {
+      int g = list[i];
+      need(g >= 1 && g <= ned, "boundary edge list refers to a missing edge");
+      need(bkind[g] < 0, "an edge appears in more than one boundary list");
+      bkind[g] = (int)kind;
+      bidx[g] = i;
+    }
+  };
+  if (s->needs) mark(s->needn, s->needs, kOcean);
+  if (s->nleds) mark(s->nledn, s->nleds, kLand);
+  if (s->nfeds) mark(s->nfedn, s->nfeds, kFlow);
+  if (s->nreds) mark(s->nredn, s->nreds, kRadiation);
+  if (s->nebseg) mark(s->nebsegn, s->nebseg, kEBarrier);
+  std::vector<int> ib_elem(2 * (size_t)std::max(s->nibseg, 1), 0), ib_led(2 * (size_t)std::max(s->nibseg, 1), 0);
+  for (int L = 0; L < s->nibseg; ++L) {
+    int gb = s->nibsegn[2 * L], gf = s->nibsegn[2 * L + 1];
+    if (gf == 0) continue;  // no opposite edge: the reference skips the segment
+    for (int side = 0; side < 2; ++side) {
+      int g = side == 0 ? gb : gf;
+      need(g >= 1 && g <= ned, "NIBSEGN refers to a missing edge");
+      need(bkind[g] < 0, "a barrier edge appears in more than one boundary list");
+      bkind[g] = kIBarrier;
+      bidx[g] = L;
+      bside[g] = side;
+      ib_elem[2 * L + side] = s->nedel[2 * (size_t)(g - 1)] - 1;
+      ib_led[2 * L + side] = s->nedsd[2 * (size_t)(g - 1)] - 1;
+    }
+  }
+  std::vector<int> link(3 * (size_t)ne, -1);
+  std::vector<unsigned> einfo(ne, 0u);
+  for (int e = 0; e < ne; ++e) {
+    unsigned info = 0u;
+    std::array<std::pair<long long, int>, 3> key;
+    for (int l = 0; l < 3; ++l) {
+      int g = s->neled[l + 3 * (size_t)e];
+      need(g >= 1 && g <= ned, "NELED refers to a missing edge");
+      int a = s->nedel[2 * (size_t)(g - 1)], b = s->nedel[2 * (size_t)(g - 1) + 1];
+      unsigned kind, flag = 0, nled = 0;
+      int lk;
+      if (a != 0 && b != 0) {
+        need(bkind[g] < 0, "an interior edge also appears in a boundary list");
+        bool first = a == e + 1;
+        need(first || b == e + 1, "NEDEL does not contain the element of NELED");
+        kind = kInterior;
+        flag = first ? 1u : 0u;
+        lk = (first ? b : a) - 1;
+        nled = (unsigned)(s->nedsd[2 * (size_t)(g - 1) + (first ? 1 : 0)] - 1);
+        key[l] = {(long long)8 << 40 | g, l};  // interior edges last, in edge-number order
+      } else if (bkind[g] >= 0) {
+        kind = (unsigned)bkind[g];
+        lk = bidx[g];
+        if (kind == kIBarrier) flag = bside[g] == 0 ? 1u : 0u;
+        key[l] = {(long long)kind << 40 | (long long)lk << 1 | (flag ? 0 : 1), l};
+      } else {
+        kind = kNone;
+        lk = -1;
+        key[l] = {(long long)9 << 40, l};
+      }
+      link[(size_t)l * ne + e] = lk;
+      info |= kind << (3 * l);
+      info |= flag << (9 + l);
+      info |= (nled & 3u) << (12 + 2 * l);
+    }
+    std::sort(key.begin(), key.end());
+    for (int slot = 0; slot < 3; ++slot) info |= (unsigned)key[slot].second << (18 + 2 * slot);
+    einfo[e] = info;
+  }
+  // node -> element star, element order
+  std::vector<int> sp(np + 1, 0), st(3 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int v = 0; v < 3; ++v) ++sp[nm[(size_t)v * ne + e] + 1];
+  for (int n = 0; n < np; ++n) sp[n + 1] += sp[n];
+  {
+    std::vector<int> cur(sp.begin(), sp.end() - 1);
+    for (int e = 0; e < ne; ++e)
+      for (int v = 0; v < 3; ++v) st[cur[nm[(size_t)v * ne + e]]++] = e;
+  }
+  h->nm.upload(nm);
+  h->link.upload(link);
+  h->einfo.upload(einfo);
+  h->star_ptr.upload(sp);
+  h->star.upload(st);
+  h->ib_elem.upload(ib_elem);
+  h->ib_led.upload(ib_led);
+  h->x.upload(std::vector<double>(s->x, s->x + np));
+  h->y.upload(std::vector<double>(s->y, s->y + np));
+  h->dp.upload(std::vector<double>(s->dp, s->dp + np));
+  std::vector<double> hb(3 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) hb[(size_t)k * ne + e] = s->hb[k + (size_t)s->dofh * e];
+  h->hb.upload(hb);
+  // per-element coefficients: a scalar when uniform
+  auto uniform = [&](const double* a, double* val) {
+    if (!a) { *val = 0.0; return true; }
+    for (int e = 1; e < ne; ++e)
+      if (a[e] != a[0]) return false;
+    *val = a[0];
+    return true;
+  };
+  double c0 = 0.0, f0 = s->cf;
+  if (!uniform(s->cori_el, &c0)) h->cori.upload(std::vector<double>(s->cori_el, s->cori_el + ne));
+  if (!uniform(s->fric_el, &f0)) h->fric.upload(std::vector<double>(s->fric_el, s->fric_el + ne));
+  h->ph.cori = c0;
+  h->ph.fric = f0;
+  if (s->load_manning) {
+    need(s->manning != nullptr, "load_manning set without ManningsN");
+    h->manning.upload(std::vector<double>(s->manning, s->manning + np));
+  }
+  if (s->ics == 2) {  // SFAC_ELEM / SFACED (prep_DG.F:1055-1100), host cos
+    const BasisP1 B = make_basis_p1();
+    const double R = 6378206.4;
+    std::vector<double> sa(3 * (size_t)ne), se(9 * (size_t)ne);
+    for (int e = 0; e < ne; ++e) {
+      const double y1 = s->y[nm[e]], y2 = s->y[nm[(size_t)ne + e]], y3 = s->y[nm[(size_t)2 * ne + e]];
+      const double yd[3] = {1.0 / 3.0 * (y1 + y2 + y3), -(1.0 / 6.0 * (y1 + y2)) + 1.0 / 3.0 * y3,
+                            -(0.5 * y1) + 0.5 * y2};
+      for (int i = 0; i < 3; ++i) {
+        double yel = 0.0;
+        for (int k = 0; k < 3; ++k) yel = yel + yd[k] * B.phi_area[k][i];
+        sa[(size_t)i * ne + e] = std::cos(s->sfea0) / std::cos(yel / R);
+      }
+      for (int l = 0; l < 3; ++l)
+        for (int i = 0; i < 3; ++i) {
+          double yed = 0.0;
+          for (int k = 0; k < 3; ++k) yed = yed + yd[k] * B.phi_edge[l][i][k];
+          se[(size_t)(l * 3 + i) * ne + e] = std::cos(s->sfea0) / std::cos(yed / R);
+        }
+    }
+    h->sfac_area.upload(sa);
+    h->sfac_edge.upload(se);
+  }
+  // boundary forcing tables (copied in the reference's Fortran layout)
+  const int nbfr = s->nbfr, nffr = s->nffr;
+  if (s->needs && nbfr) {
+    need(nbfr <= kMaxFreq, "too many open-boundary frequencies");
+    h->emo_dg.upload(std::vector<double>(s->emo_dg, s->emo_dg + (size_t)nbfr * s->needs * 2));
+    h->efa_dg.upload(std::vector<double>(s->efa_dg, s->efa_dg + (size_t)nbfr * s->needs * 2));
+    h->amig.assign(s->amig, s->amig + nbfr);
+    h->ff.assign(s->ff, s->ff + nbfr);
+    h->face.assign(s->face, s->face + nbfr);
+    h->per.assign(s->per, s->per + nbfr);
+  }
+  if (s->nfeds && nffr) {
+    need(nffr <= kMaxFreq, "too many flow-boundary frequencies");
+    h->qnam_dg.upload(std::vector<double>(s->qnam_dg, s->qnam_dg + (size_t)nffr * s->nfeds * 2));
+    h->qnph_dg.upload(std::vector<double>(s->qnph_dg, s->qnph_dg + (size_t)nffr * s->nfeds * 2));
+    h->famig.assign(s->famig, s->famig + nffr);
+    h->fff.assign(s->fff, s->fff + nffr);
+    h->fface.assign(s->fface, s->fface + nffr);
+    h->fper.assign(s->fper, s->fper + nffr);
+  }
+  if (s->nebseg) {
+    h->ebht.upload(std::vector<double>(s->ebht, s->ebht + s->nebseg));
+    h->ebcfsp.upload(std::vector<double>(s->ebcfsp, s->ebcfsp + s->nebseg));
+  }
+  if (s->nibseg) {
+    h->ibht.upload(std::vector<double>(s->ibht, s->ibht + s->nibseg));
+    h->ibcfsb.upload(std::vector<double>(s->ibcfsb, s->ibcfsb + s->nibseg));
+    h->ibcfsp.upload(std::vector<double>(s->ibcfsp, s->ibcfsp + s->nibseg));
+  }
+  MeshView& m = h->mesh;
+  m.ne = ne;
+  m.np = np;
+  m.x = h->x.p; m.y = h->y.p; m.dp = h->dp.p; m.nm = h->nm.p; m.link = h->link.p; m.einfo = h->einfo.p;
+  m.hb = h->hb.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
+  m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
+  m.star_ptr = h->star_ptr.p; m.star = h->star.p;
+  m.needs = s->needs; m.nfeds = s->nfeds; m.nebseg = s->nebseg; m.nibseg = s->nibseg;
+  m.nbfr = h->amig.empty() ? 0 : nbfr;
+  m.nffr = h->famig.empty() ? 0 : nffr;
+  m.emo_dg = h->emo_dg.p; m.efa_dg = h->efa_dg.p; m.qnam_dg = h->qnam_dg.p; m.qnph_dg = h->qnph_dg.p;
+  m.ebht = h->ebht.p; m.ebcfsp = h->ebcfsp.p;
+  m.ib_elem = h->ib_elem.p; m.ib_led = h->ib_led.p;
+  m.ibht = h->ibht.p; m.ibcfsb = h->ibcfsb.p; m.ibcfsp = h->ibcfsp.p;
+}
+
+void upload_state(dgswem_cuda* h, const double* ze, const double* qx, const double* qy, const int* wdflg) {
+  const int ne = h->ne;
+  h->staging.alloc(std::max(h->staging.n, 3 * (size_t)ne));
+  const double* src[3] = {ze, qx, qy};
+  for (int var = 0; var < 3; ++var) {
+    if (!src[var]) continue;
+    DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], 3 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice,
+                            h->stream));
+    fortran_to_soa<<<grid_for(ne, 256), 256, 0, h->stream>>>(h->staging.p, h->q[0].p, ne, var);
+    check_launch(h);
+  }
+  if (wdflg)
+    DG_CUDA(cudaMemcpyAsync(h->wd.p, wdflg, (size_t)ne * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  DG_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+void step(dgswem_cuda* h, int it) {
+  const int nrk = h->nrk, ne = h->ne;
+  const double itdt = it * h->dtdp;
+  const double time_a = itdt + h->statim * 86400.0;
+  for (int irk = 1; irk <= nrk; ++irk) {
+    StageArgs A{};
+    A.m = h->mesh;
+    A.ph = h->ph;
+    A.irk = irk;
+    A.qin = h->q[irk - 1].p;
+    A.qout = h->q[irk].p;
+    for (int I = 1; I <= irk; ++I) {
+      A.qhist[I - 1] = h->q[I - 1].p;
+      A.rhist[I - 1] = h->rhs[I - 1].p;
+      A.a[I - 1] = h->atvd[(size_t)(irk - 1) * nrk + (I - 1)];
+      A.b[I - 1] = h->btvd[(size_t)(irk - 1) * nrk + (I - 1)] * h->dtdp;
+    }
+    A.rout = h->keep_rhs[irk - 1] ? h->rhs[irk - 1].p : nullptr;
+    A.wd = h->wd.p;
+    // DG_hydro_timestep.F:79-100 (stage time and ramp)
+    const double dtvd = h->dtvd[irk - 1];
+    A.timedg = time_a - h->dtdp + dtvd * h->dtdp;
+    A.rampdg = 1.0;
+    if (h->nramp == 1 || h->nramp == 2) A.rampdg = std::tanh((2.0 * ((it - 1) + dtvd) * h->dtdp / 86400.0) / h->dramp);
+    // ocean_edge_hydro.F:148-160 / flow_edge_hydro.F:108-120 stage phases
+    for (size_t f = 0; f < h->amig.size(); ++f) {
+      const double ncyc = h->per[f] == 0.0 ? 0.0 : (double)(long long)(A.timedg / h->per[f]);
+      A.argj[f] = h->amig[f] * (A.timedg - ncyc * h->per[f]) + h->face[f];
+      A.rff[f] = h->ff[f] * A.rampdg;
+    }
+    for (size_t f = 0; f < h->famig.size(); ++f) {
+      const double ncyc = h->fper[f] == 0.0 ? 0.0 : (double)(long long)(A.timedg / h->fper[f]);
+      A.fargj[f] = h->famig[f] * (A.timedg - ncyc * h->fper[f]) + h->fface[f];
+      A.frff[f] = h->fff[f] * A.rampdg;
+    }
+    A.wsx = h->wsx.p;
+    A.wsy = h->wsy.p;
+    A.pr = h->pr.p;
+    A.err = h->err.p;
+    {
+      LaunchTimer t(h, 0);
+      if (h->ph.nleq == 1.0 && h->ph.leq == 0.0)
+        stage_p1<true><<<grid_for(ne, kStageBlock), kStageBlock, 0, h->stream>>>(A);
+      else
+        stage_p1<false><<<grid_for(ne, kStageBlock), kStageBlock, 0, h->stream>>>(A);
+      t.done();
+    }
+    const bool wetdry = h->nolifa >= 2;
+    if (h->slopeflag != 0 || wetdry) {
+      LimitArgs L{};
+      L.m = h->mesh;
+      L.ph = h->ph;
+      L.q = h->q[irk].p;
+      L.minmax = h->minmax.p;
+      L.wd = h->wd.p;
+      L.slopeflag = h->slopeflag;
+      L.wetdry = wetdry ? 1 : 0;
+      L.err = h->err.p;
+      if (h->slopeflag != 0) {
+        LaunchTimer t(h, 1);
+        node_minmax<<<grid_for(h->np, 256), 256, 0, h->stream>>>(L);
+        t.done();
+      }
+      LaunchTimer t(h, 2);
+      limit_wetdry<<<grid_for(ne, 256), 256, 0, h->stream>>>(L);
+      t.done();
+    }
+  }
+  std::swap(h->q[0], h->q[nrk]);  // stage NRK+1 becomes stage 1
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgswem_cuda_last_error(char* buf, int buflen) {
+  if (!buf || buflen <= 0) return DGSWEM_ERR_ARG;
+  std::strncpy(buf, g_last_error.c_str(), (size_t)buflen - 1);
+  buf[buflen - 1] = 0;
+  return DGSWEM_OK;
+}
+
+int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem_cuda** out) {
+  return guarded([&]() {
+    if (!s || !out) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (flags != 0) throw Failure(DGSWEM_ERR_ARG, "flags must be 0");
+    if (s->dofh != 3) throw Failure(DGSWEM_ERR_ARG, "only p=1 (DOFH=3) is implemented on the device");
+    if (s->ne <= 0 || s->np <= 0 || s->nedges <= 0) throw Failure(DGSWEM_ERR_ARG, "empty mesh");
+    if (s->nrk < 1 || s->nrk > kMaxStages) throw Failure(DGSWEM_ERR_ARG, "nrk out of range");
+    if (s->nws != 0 && s->nws != 1) throw Failure(DGSWEM_ERR_ARG, "only NWS=0/1 are supported");
+    if (s->nramp == 3) throw Failure(DGSWEM_ERR_ARG, "NRAMP = 3 not supported");
+    if (s->ics != 1 && s->ics != 2) throw Failure(DGSWEM_ERR_ARG, "ICS must be 1 or 2");
+    int ndev = 0;
+    DG_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) throw Failure(DGSWEM_ERR_ARG, "no such CUDA device");
+    DG_CUDA(cudaSetDevice(device));
+    std::unique_ptr<dgswem_cuda> h(new dgswem_cuda());
+    h->device = device;
+    h->ne = s->ne;
+    h->np = s->np;
+    h->nrk = s->nrk;
+    h->nramp = s->nramp;
+    h->slopeflag = s->slopeflag;
+    h->nolifa = s->nolifa;
+    h->nws = s->nws;
+    h->dtdp = s->dtdp;
+    h->statim = s->statim;
+    h->dramp = s->dramp;
+    h->atvd.assign(s->atvd, s->atvd + (size_t)s->nrk * s->nrk);
+    h->btvd.assign(s->btvd, s->btvd + (size_t)s->nrk * s->nrk);
+    h->dtvd.assign(s->dtvd, s->dtvd + s->nrk);
+    h->keep_rhs.assign(s->nrk, 0);
+    for (int I = 1; I <= s->nrk; ++I)
+      for (int irk = I + 1; irk <= s->nrk; ++irk)
+        if (h->btvd[(size_t)(irk - 1) * s->nrk + (I - 1)] != 0.0) h->keep_rhs[I - 1] = 1;
+    Physics& p = h->ph;
+    p.g = s->g;
+    p.h0 = s->h0;
+    p.dtdp = s->dtdp;
+    p.nleq = s->nleq;
+    p.leq = s->leq;
+    p.nleqg = s->nleq * s->g;
+    p.fg_l = s->leq * s->g;
+    p.cf = s->cf;
+    p.hbreak = s->hbreak;
+    p.ftheta = s->ftheta;
+    p.fgamma = s->fgamma;
+    p.iflinbf = s->iflinbf;
+    p.ifhybf = s->ifhybf;
+    p.ifnlfa = s->ifnlfa;
+    p.nws = s->nws;
+    p.rainfall = s->rainfall;
+    p.ics = s->ics;
+    DG_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    static bool basis_ready[64] = {false};
+    if (device < 64 && !basis_ready[device]) {
+      const BasisP1 B = make_basis_p1();
+      DG_CUDA(cudaMemcpyToSymbol(cBasis, &B, sizeof(B)));
+      basis_ready[device] = true;
+    }
+    build_layout(h.get(), s);
+    h->q.resize(s->nrk + 1);
+    for (auto& b : h->q) {
+      b.alloc(9 * (size_t)s->ne);
+      DG_CUDA(cudaMemset(b.p, 0, b.n * sizeof(double)));
+    }
+    h->rhs.resize(s->nrk);
+    for (int I = 0; I < s->nrk; ++I)
+      if (h->keep_rhs[I]) h->rhs[I].alloc(9 * (size_t)s->ne);
+    h->wd.alloc(s->ne);
+    h->nodecode.alloc(s->np);
+    h->minmax.alloc(6 * (size_t)s->np);
+    h->err.alloc(1);
+    DG_CUDA(cudaMemset(h->err.p, 0, sizeof(unsigned)));
+    if (s->nws == 1) {
+      h->wsx.alloc(s->np); h->wsy.alloc(s->np); h->pr.alloc(s->np);
+      DG_CUDA(cudaMemset(h->wsx.p, 0, s->np * sizeof(double)));
+      DG_CUDA(cudaMemset(h->wsy.p, 0, s->np * sizeof(double)));
+      DG_CUDA(cudaMemset(h->pr.p, 0, s->np * sizeof(double)));
+    }
+    upload_state(h.get(), s->ze, s->qx, s->qy, s->wdflg);
+    *out = h.release();
+  });
+}
+
+void dgswem_cuda_destroy(dgswem_cuda* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& p : h->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+int dgswem_cuda_hydro_timestep(dgswem_cuda* h, int it) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    step(h, it);
+  });
+}
+
+int dgswem_cuda_run(dgswem_cuda* h, int it0, int nsteps) {
+  return guarded([&]() {
+    if (!h || nsteps < 0) throw Failure(DGSWEM_ERR_ARG, "bad arguments");
+    DG_CUDA(cudaSetDevice(h->device));
+    for (int i = 0; i < nsteps; ++i) step(h, it0 + i);
+  });
+}
+
+int dgswem_cuda_synchronize(dgswem_cuda* h) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    unsigned e = 0;
+    DG_CUDA(cudaMemcpy(&e, h->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (e) throw Failure(DGSWEM_ERR_NUMERIC, "NaN in the state produced on the device");
+  });
+}
+
+int dgswem_cuda_upload_state(dgswem_cuda* h, const double* ze, const double* qx, const double* qy,
+                             const int* wdflg) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    upload_state(h, ze, qx, qy, wdflg);
+  });
+}
+
+int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* qy, int* wdflg) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    const int ne = h->ne;
+    h->staging.alloc(std::max(h->staging.n, 9 * (size_t)ne));
+    double* dst[3] = {ze, qx, qy};
+    for (int var = 0; var < 3; ++var) {
+      if (!dst[var]) continue;
+      soa_to_fortran<<<grid_for(ne, 256), 256, 0, h->stream>>>(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var);
+      check_launch(h);
+      DG_CUDA(cudaMemcpyAsync(dst[var], h->staging.p + (size_t)3 * ne * var, 3 * (size_t)ne * sizeof(double),
+                              cudaMemcpyDeviceToHost, h->stream));
+    }
+    if (wdflg)
+      DG_CUDA(cudaMemcpyAsync(wdflg, h->wd.p, (size_t)ne * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2, const double* pr2) {
+  return guarded([&]() {
+    if (!h || !wsx2 || !wsy2 || !pr2) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    if (h->nws != 1) throw Failure(DGSWEM_ERR_ARG, "met forcing needs NWS = 1");
+    DG_CUDA(cudaSetDevice(h->device));
+    const size_t bytes = (size_t)h->np * sizeof(double);
+    DG_CUDA(cudaMemcpyAsync(h->wsx.p, wsx2, bytes, cudaMemcpyHostToDevice, h->stream));
+    DG_CUDA(cudaMemcpyAsync(h->wsy.p, wsy2, bytes, cudaMemcpyHostToDevice, h->stream));
+    DG_CUDA(cudaMemcpyAsync(h->pr.p, pr2, bytes, cudaMemcpyHostToDevice, h->stream));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* vv2, int* nodecode) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    const int np = h->np;
+    h->staging.alloc(std::max(h->staging.n, 4 * (size_t)np));
+    double* d = h->staging.p;
+    modal2nodal_kernel<<<grid_for(np, 256), 256, 0, h->stream>>>(h->mesh, h->q[0].p, h->wd.p, h->ph.nleq,
+                                                                 h->ph.leq, d, d + np, d + 2 * (size_t)np,
+                                                                 h->nodecode.p);
+    check_launch(h);
+    if (eta2) DG_CUDA(cudaMemcpyAsync(eta2, d, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (uu2) DG_CUDA(cudaMemcpyAsync(uu2, d + np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (vv2) DG_CUDA(cudaMemcpyAsync(vv2, d + 2 * (size_t)np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (nodecode)
+      DG_CUDA(cudaMemcpyAsync(nodecode, h->nodecode.p, np * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+long long dgswem_cuda_kernel_launches(const dgswem_cuda* h) { return h ? h->launches : -1; }
+
+int dgswem_cuda_set_stream(dgswem_cuda* h, void* stream) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    prof_flush(h);
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  });
+}
+
+int dgswem_cuda_profile(dgswem_cuda* h, int enable) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    prof_flush(h);
+    for (int k = 0; k < 4; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
+    h->prof_on = enable != 0;
+  });
+}
+
+int dgswem_cuda_profile_read(dgswem_cuda* h, double* ms, long long* launches) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    prof_flush(h);
+    for (int k = 0; k < 4; ++k) {
+      if (ms) ms[k] = h->prof_ms[k];
+      if (launches) launches[k] = h->prof_n[k];
+    }
+  });
+}
+
+}  // extern "C"

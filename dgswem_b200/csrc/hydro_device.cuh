@@ -1,0 +1,120 @@
+// hydro_device.cuh -- device data layout and kernels of the p=1 DG hydro step.
+//
+// Layout in HBM (NE elements, NP nodes, all structure-of-arrays so a warp's
+// 32 consecutive elements make one coalesced transaction per field):
+//   state   q[c*NE + e], c = 3*var + k  (var: 0 zeta, 1 qx, 2 qy; k: mode)
+//   nm[v*NE + e]       0-based vertex node ids
+//   link[l*NE + e]     across local edge l: neighbour element (interior edge)
+//                      or index into the boundary list of that edge's kind
+//   einfo[e]           packed edge kinds, processing order, orientation bits
+//   hb[k*NE + e]       bathymetry modes HB(k,e)
+// Geometry (areas, Jacobian, edge lengths and normals) is recomputed from the
+// nodal coordinates each stage, with the reference's formulas, instead of
+// streaming the reference's per-element tables (XFAC/YFAC/SRFAC/BATHED: ~100
+// doubles per element).
+#pragma once
+
+#include <cstdint>
+
+namespace dgswem {
+
+constexpr int kMaxStages = 8;
+constexpr int kMaxFreq = 16;
+
+enum EdgeKind : unsigned {
+  kInterior = 0,
+  kOcean = 1,      // ocean_edge_hydro.F
+  kLand = 2,       // land_edge_hydro.F
+  kFlow = 3,       // flow_edge_hydro.F
+  kRadiation = 4,  // radiation_edge_hydro.F
+  kIBarrier = 5,   // ibarrier_edge_hydro.F
+  kEBarrier = 6,   // ebarrier_edge_hydro.F
+  kNone = 7        // boundary edge in no list: the reference skips it
+};
+
+// einfo bit fields
+__host__ __device__ inline unsigned ei_kind(unsigned info, int l) { return (info >> (3 * l)) & 7u; }
+__host__ __device__ inline unsigned ei_flag(unsigned info, int l) { return (info >> (9 + l)) & 1u; }
+__host__ __device__ inline unsigned ei_nled(unsigned info, int l) { return (info >> (12 + 2 * l)) & 3u; }
+__host__ __device__ inline unsigned ei_order(unsigned info, int s) { return (info >> (18 + 2 * s)) & 3u; }
+
+// p=1 basis tables (orthogonal_basis_v1.F, prep_DG.F:648-870), Lobatto edge
+// rule (quad_rules_general.F) and 3-point area rule (quadrature_v1.F:255-260)
+struct BasisP1 {
+  double phi_edge[3][3][3];  // [led][point][mode]
+  double edgeq[3][3][3];     // 2*M_INV*PHI_EDGE*WEGP
+  double phi_area[3][3];     // [mode][point]
+  double drphi[3][3], dsphi[3][3];
+  double phi_corner[3][3];   // [vertex][mode]
+  double psi[3][3];          // [vertex][area point] linear nodal basis
+  double m_inv[3], wagp[3], wegp[3], xegp[3];
+};
+
+struct MeshView {
+  int ne, np;
+  const double* __restrict__ x;
+  const double* __restrict__ y;
+  const double* __restrict__ dp;        // nodal depth
+  const int* __restrict__ nm;
+  const int* __restrict__ link;
+  const unsigned* __restrict__ einfo;
+  const double* __restrict__ hb;
+  const double* __restrict__ cori;      // per element, or null (uniform)
+  const double* __restrict__ fric;      // per element, or null (uniform)
+  const double* __restrict__ manning;   // nodal, or null
+  const double* __restrict__ sfac_area; // [i*NE+e] (ics=2) or null
+  const double* __restrict__ sfac_edge; // [(l*3+i)*NE+e] (ics=2) or null
+  const int* __restrict__ star_ptr;     // node -> element star (CSR)
+  const int* __restrict__ star;
+  // boundary lists
+  int needs, nfeds, nebseg, nibseg, nbfr, nffr;
+  const double* __restrict__ emo_dg;    // EMO_DG(NBFR,NEEDS,2)
+  const double* __restrict__ efa_dg;
+  const double* __restrict__ qnam_dg;   // QNAM_DG(NFFR,NFEDS,2)
+  const double* __restrict__ qnph_dg;
+  const double* __restrict__ ebht;
+  const double* __restrict__ ebcfsp;
+  const int* __restrict__ ib_elem;      // [2*L + side] element of back/front edge
+  const int* __restrict__ ib_led;       // [2*L + side] local edge
+  const double* __restrict__ ibht;
+  const double* __restrict__ ibcfsb;
+  const double* __restrict__ ibcfsp;
+};
+
+struct Physics {
+  double g, h0, dtdp, nleq, leq, nleqg, fg_l;
+  double cori, fric, cf, hbreak, ftheta, fgamma;
+  int iflinbf, ifhybf, ifnlfa, nws, rainfall, ics;
+};
+
+struct StageArgs {
+  MeshView m;
+  Physics ph;
+  int irk;                                  // 1-based stage
+  const double* __restrict__ qin;           // state of stage irk (edges read it)
+  double* qout;                             // state of stage irk+1
+  const double* qhist[kMaxStages];          // state of stage I, I=1..irk
+  const double* rhist[kMaxStages];          // RHS of stage I<irk (if needed)
+  double* rout;                             // this stage's RHS, or null
+  double a[kMaxStages], b[kMaxStages];      // ATVD(irk,I), BTVD(irk,I)*DT
+  const int* __restrict__ wd;               // WDFLG (read)
+  double timedg, rampdg;
+  double argj[kMaxFreq], rff[kMaxFreq];     // ocean harmonic phase and ramped amplitude
+  double fargj[kMaxFreq], frff[kMaxFreq];   // flow boundary equivalents
+  const double* __restrict__ wsx;           // nodal met forcing (already ramped), or null
+  const double* __restrict__ wsy;
+  const double* __restrict__ pr;
+  unsigned* err;                            // device error word
+};
+
+struct LimitArgs {
+  MeshView m;
+  Physics ph;
+  double* q;                 // stage output, limited / wet-dried in place
+  double* minmax;            // [6*NP]: zmin zmax qxmin qxmax qymin qymax
+  int* wd;                   // WDFLG (read + write)
+  int slopeflag, wetdry;
+  unsigned* err;
+};
+
+}  // namespace dgswem

@@ -1,0 +1,166 @@
+/*
+ * dgswem_cuda.h -- C-ABI of the B200 DG hydro time step (drop-in boundary).
+ *
+ * The Fortran host replaces `CALL DG_HYDRO_TIMESTEP(IT)` (reference
+ * src/DG_timestep.F:30) by `dgswem_cuda_hydro_timestep(h, IT)` through an
+ * iso_c_binding interface, in the style of the reference's own C binding
+ * (src/c_interface.F90:1-23, src/count_edges.cpp:324-354): plain pointers and
+ * sizes, `int` scalars by value, no C++ or torch types.
+ *
+ * Array conventions follow the reference's Fortran declarations so a host
+ * passes its module arrays unchanged (c_loc of the first element):
+ *   - column-major, 1-based ids (node, element and edge numbers start at 1);
+ *   - NM(NE,3)        -> nm[e + ne*v]
+ *   - NEDNO(2,NEDGES) -> nedno[s + 2*ed]   (NEDEL, NEDSD likewise)
+ *   - NELED(3,NE)     -> neled[l + 3*e]
+ *   - ZE(DOFH,NE)     -> ze[k + dofh*e]    (one RK stage slice; QX, QY, HB)
+ *   - EMO_DG(NBFR,NEEDS,2) -> emo_dg[f + nbfr*(l + needs*ipt)]
+ * All reals are REAL(SZ) with SZ=8 (double).  Every entry point returns 0 on
+ * success and a nonzero status otherwise; the library never aborts the
+ * process; dgswem_cuda_last_error() gives the message.  There is no CPU
+ * fallback: without a usable GPU, dgswem_cuda_create() fails.
+ */
+#ifndef DGSWEM_CUDA_H
+#define DGSWEM_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGSWEM_CUDA_ABI_VERSION 1
+
+enum {
+  DGSWEM_OK = 0,
+  DGSWEM_ERR_ARG = 1,      /* invalid argument or unsupported configuration */
+  DGSWEM_ERR_CUDA = 2,     /* CUDA runtime error */
+  DGSWEM_ERR_IO = 3,       /* input deck could not be read */
+  DGSWEM_ERR_NUMERIC = 4   /* NaN / negative depth detected on the device */
+};
+
+/*
+ * Setup data: what PREP_DG (reference src/prep_DG.F:25-1539) leaves in the
+ * GLOBAL/DG/NodalAttributes modules, restricted to what the hydro step reads.
+ * Pointers are only read during dgswem_cuda_create(); they are not retained.
+ */
+typedef struct dgswem_cuda_setup {
+  /* sizes */
+  int ne, np;              /* elements, nodes                              */
+  int dofh;                /* modes per variable: 3 (p=1)                  */
+  int nrk;                 /* RK stages (RK_STAGE)                         */
+  int nedges;              /* NEDGES                                       */
+  int nieds, nleds, needs, nfeds, nreds, nebseg, nibseg;
+  /* switches (read_input.F, dgswem.F:131-170, fort.dg) */
+  int ics;                 /* 1 Cartesian, 2 spherical (CPP)               */
+  int nolifa;              /* >=2 enables WETDRY                           */
+  int iflinbf, ifhybf;     /* friction form flags                          */
+  int ifnlfa;              /* finite amplitude flag                        */
+  int nramp;               /* ramp option                                  */
+  int nws;                 /* 0 or 1 (met forcing via dgswem_cuda_set_met) */
+  int rainfall;            /* 0 or 1                                       */
+  int slopeflag;           /* 0 off, otherwise SLOPELIMITER5               */
+  int load_manning;        /* ManningsN from fort.13                       */
+  double nleq, leq;        /* nonlinear / linear switches                  */
+  double g, h0, dtdp, statim, dramp;
+  double cf, hbreak, ftheta, fgamma;
+  double sfea0;            /* radians (ics=2)                              */
+  /* SSP-RK coefficients (RK_TIME, prep_DG.F:1551-1990), row-major nrk*nrk:
+   * atvd[(irk-1)*nrk + (i-1)] = ATVD(IRK,I); dtvd[irk-1] = DTVD(IRK)      */
+  const double *atvd, *btvd, *dtvd;
+  /* mesh */
+  const int* nm;           /* NM(NE,3)                                     */
+  const double *x, *y;     /* nodal coordinates (CPP metres if ics=2)      */
+  const double* dp;        /* nodal depth after the H0 clamp               */
+  /* edge graph (create_edge_data.F) */
+  const int *nedno, *nedel, *nedsd, *neled;
+  const int *niedn, *nledn, *needn, *nfedn, *nredn, *nebsegn;
+  const int* nibsegn;      /* NIBSEGN(2,NIBSEG)                            */
+  /* element data */
+  const double* hb;        /* HB(DOFH,NE) bathymetry modes                 */
+  const double* cori_el;   /* CORI_EL(NE)                                  */
+  const double* fric_el;   /* FRIC_EL(NE)                                  */
+  const double* manning;   /* ManningsN(NP) or NULL                        */
+  /* initial state (stage 1 slice) */
+  const double *ze, *qx, *qy;
+  const int* wdflg;
+  /* open-ocean harmonic forcing (prep_DG.F:180-205) */
+  int nbfr;
+  const double *amig, *ff, *face, *per;
+  const double *emo_dg, *efa_dg;
+  /* flow boundaries (prep_DG.F:208-245) */
+  int nffr;
+  const double *famig, *fff, *fface, *fper;
+  const double *qnam_dg, *qnph_dg;   /* QNAM_DG(NFFR,NFEDS,2)              */
+  /* barriers (read_input.F:2668-2685) */
+  const double *ebht, *ebcfsp;       /* per external-barrier segment       */
+  const double *ibht, *ibcfsb, *ibcfsp; /* per internal-barrier segment    */
+} dgswem_cuda_setup;
+
+typedef struct dgswem_cuda dgswem_cuda;
+
+/* Copies the setup to GPU `device` and builds the device layout.
+ * Replaces the state the reference keeps in module arrays after PREP_DG
+ * (src/dgswem.F:196).  flags: reserved, pass 0. */
+int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
+                       dgswem_cuda** out);
+void dgswem_cuda_destroy(dgswem_cuda* h);
+
+/* One DG_HYDRO_TIMESTEP(IT) (src/DG_hydro_timestep.F:24-744): all RK stages,
+ * slope limiter, wet/dry, stage copy.  Asynchronous on the library stream. */
+int dgswem_cuda_hydro_timestep(dgswem_cuda* h, int it);
+/* Steps it0 .. it0+nsteps-1 (one call per host loop, fewer launches). */
+int dgswem_cuda_run(dgswem_cuda* h, int it0, int nsteps);
+/* Waits for queued steps and reports device-side numeric errors. */
+int dgswem_cuda_synchronize(dgswem_cuda* h);
+
+/* Stage-1 state ZE/QX/QY(DOFH,NE) and WDFLG(NE), host memory.  Download is
+ * the sync point, like `!$acc wait` at src/DG_timestep.F:32. */
+int dgswem_cuda_upload_state(dgswem_cuda* h, const double* ze, const double* qx,
+                             const double* qy, const int* wdflg);
+int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* qy,
+                               int* wdflg);
+
+/* NWS=1: nodal WSX2/WSY2/PR2 (src/met_forcing.F:49-66); applied every stage
+ * times RAMPDG.  Arrays of NP doubles. */
+int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2,
+                        const double* pr2);
+
+/* modal2nodal (src/write_results.F:14-170) on the device; results copied to
+ * host arrays of NP entries (any may be NULL).  nodecode: 1 where a wet
+ * element touches the node (the value WETDRY leaves in NODECODE). */
+int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* vv2,
+                            int* nodecode);
+
+/* Number of kernels the library launched since create (for accounting). */
+long long dgswem_cuda_kernel_launches(const dgswem_cuda* h);
+
+/* Launch on the caller's CUDA stream (a cudaStream_t passed as void*; NULL
+ * restores the library's own stream).  Lets a host time the step with its
+ * own events or order it after its own work.  No counterpart in the
+ * reference (its OpenACC regions run on async queue 1). */
+int dgswem_cuda_set_stream(dgswem_cuda* h, void* stream);
+
+/* Per-kernel timing with CUDA events recorded around every launch on the
+ * launching stream.  enable != 0 starts accumulating (and resets); read
+ * returns, per kernel kind (0 stage, 1 node_minmax, 2 limit_wetdry,
+ * 3 other), the summed milliseconds and launch counts (arrays of 4). */
+int dgswem_cuda_profile(dgswem_cuda* h, int enable);
+int dgswem_cuda_profile_read(dgswem_cuda* h, double* ms, long long* launches);
+
+/* Last error message of the calling thread (NUL-terminated, truncated). */
+int dgswem_cuda_last_error(char* buf, int buflen);
+
+/* ---- standalone input path (no Fortran host) ------------------------------
+ * Reads fort.14, fort.15, fort.dg (and fort.13 when NWP>0) from `dir` and runs
+ * the setup the reference does in READ_INPUT + PREP_DG, producing a
+ * dgswem_cuda_setup.  The deck owns all arrays the setup points to. */
+typedef struct dgswem_deck dgswem_deck;
+int dgswem_deck_open(const char* dir, dgswem_deck** out);
+const dgswem_cuda_setup* dgswem_deck_setup(const dgswem_deck* d);
+/* nt, nspoolge, ntcysge, ntcyfge, noutge (integer run controls) */
+int dgswem_deck_int(const dgswem_deck* d, const char* key, int* value);
+void dgswem_deck_close(dgswem_deck* d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGSWEM_CUDA_H */

@@ -864,7 +864,7 @@ void Model::create_edge_data() {
   }
   for (int i = 0; i < NEDGES; ++i)
     if (ncount[i] < 0) NLEDN.push_back(i);
-  NEDSD.assign(2 * (size_t)NEDGES, 0);
+  NEDSD.assign(2 * (size_t)NEDGES, -1);  // NEDSD(:,:) = 0 for a missing side
   for (int i = 0; i < NEDGES; ++i)
     for (int s = 0; s < 2; ++s) {
       int el = NEDEL[2 * i + s];

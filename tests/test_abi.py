@@ -1,0 +1,58 @@
+"""The C-ABI library without a GPU: it loads, exports every entry point
+include/dgswem_cuda.h declares, and a create call on a machine without a GPU
+fails with a status code instead of aborting."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from dgswem_b200 import _abi, Deck, decks
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "dgswem_cuda.h"
+
+
+def declared_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(dgswem_(?:cuda|deck)_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(built):
+    lib = _abi.load()
+    names = declared_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _abi.SIGNATURES, f"{name} missing from the ctypes mirror"
+
+
+def test_setup_struct_mirror_matches_header(built):
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    body = text[text.index("typedef struct dgswem_cuda_setup {"):text.index("} dgswem_cuda_setup;")]
+    fields = []
+    for decl in body.split(";")[:-1]:
+        decl = decl.split("{")[-1].strip()
+        names = [n.strip().lstrip("*") for n in re.sub(r"^(const\s+)?(int|double)\s*\*?", "", decl).split(",")]
+        fields += [n for n in names if n]
+    assert fields == [f[0] for f in _abi.Setup._fields_]
+
+
+def test_create_without_gpu_returns_status(built, scratch):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    path = decks.quarter_annulus(scratch / "qa_nogpu", nr=2, nth=4, nsteps=1)
+    d = Deck(path)
+    h = C.c_void_p()
+    rc = _abi.load().dgswem_cuda_create(d.setup, 0, 0, C.byref(h))
+    assert rc == 2 and not h.value  # DGSWEM_ERR_CUDA, no handle, process alive
+    buf = C.create_string_buffer(256)
+    _abi.load().dgswem_cuda_last_error(buf, 256)
+    assert buf.value
+
+
+def test_bad_arguments(built):
+    lib = _abi.load()
+    h = C.c_void_p()
+    assert lib.dgswem_cuda_create(None, 0, 0, C.byref(h)) == 1
+    assert lib.dgswem_cuda_hydro_timestep(None, 1) == 1

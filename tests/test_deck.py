@@ -1,0 +1,66 @@
+"""The library's standalone input path (READ_INPUT + PREP_DG restated in
+dgswem_b200/csrc/deck.cpp) against the oracle: integer edge tables are
+compared bit for bit, real setup arrays exactly."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, golden_dir
+from dgswem_b200 import Deck, decks
+from oracle_lib import Oracle
+
+
+def _decks(scratch):
+    out = [golden_dir(c) for c in GOLDEN_CASES]
+    out.append(decks.quarter_annulus(scratch / "qa_small", nr=8, nth=16, nsteps=20))
+    out.append(decks.sloping_beach(scratch / "sb_small", nx=40, ny=8, nsteps=20))
+    return out
+
+
+def test_edge_tables_bit_exact(built, scratch):
+    for path in _decks(scratch):
+        d = Deck(path)
+        o = Oracle(path)
+        s = d.s
+        ned, ne = s.nedges, s.ne
+        assert ned == o.info("nedges"), path
+        for name, n in [("nedno", 2 * ned), ("nedel", 2 * ned), ("nedsd", 2 * ned)]:
+            np.testing.assert_array_equal(d.int_array(name, n), o.int_table(name.upper()), err_msg=f"{path} {name}")
+        # NELED(3,NE) is stored [l + 3*e] in both
+        np.testing.assert_array_equal(d.int_array("neled", 3 * ne), o.int_table("NELED"))
+        for name, cnt in [("niedn", s.nieds), ("nledn", s.nleds), ("needn", s.needs), ("nfedn", s.nfeds),
+                          ("nredn", s.nreds), ("nebsegn", s.nebseg), ("nibsegn", 2 * s.nibseg)]:
+            np.testing.assert_array_equal(d.int_array(name, cnt), o.int_table(name.upper()),
+                                          err_msg=f"{path} {name}")
+        ze0, _, _, wd0 = o.state()
+        np.testing.assert_array_equal(d.int_array("wdflg", ne), wd0)
+        np.testing.assert_array_equal(d.real_array("ze", 3 * ne), ze0.ravel())
+        np.testing.assert_array_equal(d.real_array("dp", s.np), o.real_table("DP"))
+        np.testing.assert_array_equal(d.real_array("x", s.np), o.real_table("X"))
+        np.testing.assert_array_equal(d.real_array("y", s.np), o.real_table("Y"))
+        np.testing.assert_array_equal(d.real_array("hb", 3 * ne), o.real_table("HB"))
+        assert s.nrk == o.info("nrk")
+        d.close()
+        o.close()
+
+
+def test_wetdry_golden_deck_contents(built):
+    d = Deck(golden_dir("wetdry"))
+    s = d.s
+    # wetdry golden: external barriers (type 3) and internal barriers (type 24)
+    assert s.nebseg > 0 and s.nibseg > 0 and s.needs > 0
+    assert s.nolifa == 2 and s.nrk == 5 and s.ifhybf == 1
+    assert d.control("nspoolge") == 100 and d.control("nt") == 1728
+
+
+def test_deck_errors_are_status_codes(built, scratch):
+    from dgswem_b200._abi import DgswemError
+    with pytest.raises(DgswemError, match="cannot open"):
+        Deck(scratch / "does_not_exist")
+    bad = decks.quarter_annulus(scratch / "qa_cw", nr=2, nth=2, nsteps=1)
+    text = (bad / "fort.14").read_text().split("\n")
+    # flip the first element to clockwise order (read_input.F:1408-1419 stops)
+    parts = text[2 + 9].split()
+    text[2 + 9] = " ".join([parts[0], parts[1], parts[2], parts[4], parts[3]])
+    (bad / "fort.14").write_text("\n".join(text))
+    with pytest.raises(DgswemError, match="clockwise"):
+        Deck(bad)
