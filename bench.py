@@ -213,7 +213,9 @@ def main(argv=None):
     deck = Deck(path)
     hs = HydroStep(deck, device=local)
     ne, nrk = hs.ne, hs.nrk
-    stream = torch.cuda.current_stream()
+    # all work on one dedicated stream; the events below are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     hs.set_stream(stream.cuda_stream)
 
     # warm-up

@@ -20,8 +20,11 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIBNAME = "libdgswem_cuda.so"
-SOURCES = ["hydro.cu", "deck.cpp"]
-HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "abi_util.h"]
+# (source, extra nvcc flags): the strict kernel variant is compiled without
+# fused multiply-add contraction
+SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_strict.cu", ["-fmad=false"]),
+           ("deck.cpp", [])]
+HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
@@ -49,15 +52,15 @@ def _stale(target: Path, inputs) -> bool:
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     LIBDIR.mkdir(exist_ok=True)
     out = LIBDIR / LIBNAME
-    inputs = [CSRC / s for s in SOURCES + HEADERS] + [ROOT / "include" / "dgswem_cuda.h"]
+    inputs = [CSRC / s for s, _ in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "dgswem_cuda.h"]
     if not force and not _stale(out, inputs):
         return out
     objs = []
     build = PKG / "_build"
     build.mkdir(exist_ok=True)
-    for src in SOURCES:
+    for src, extra in SOURCES:
         obj = build / (Path(src).stem + ".o")
-        cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, *ARCH, "-I", str(ROOT / "include"), "-I", str(CSRC),
+        cmd = [nvcc(), "-ccbin", host_cxx(), *NVCC_FLAGS, *extra, *ARCH, "-I", str(ROOT / "include"), "-I", str(CSRC),
                "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

@@ -11,7 +11,7 @@
 
 #include "abi_util.h"
 #include "dgswem_cuda.h"
-#include "hydro_kernels.cuh"
+#include "hydro_device.cuh"
 
 namespace dgswem {
 
@@ -88,14 +88,33 @@ static BasisP1 make_basis_p1() {
   return B;
 }
 
+// Owning device allocation; movable, not copyable (a copy would free the
+// buffer twice).
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
   void alloc(size_t count) {
     release();
     n = count;
     if (count) DG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void ensure(size_t count) {  // grow only
+    if (count > n) alloc(count);
   }
   void upload(const std::vector<T>& v) {
     alloc(v.size());
@@ -109,12 +128,41 @@ struct DevBuf {
   ~DevBuf() { release(); }
 };
 
+// Launchers of one compilation variant (kernels_fast.cu / kernels_strict.cu).
+struct Variant {
+  void (*set_basis)(const BasisP1&);
+  void (*stage)(const StageArgs&, bool, unsigned, cudaStream_t);
+  void (*node_minmax)(const LimitArgs&, unsigned, cudaStream_t);
+  void (*limit_wetdry)(const LimitArgs&, unsigned, cudaStream_t);
+  void (*modal2nodal)(const MeshView&, const double*, const int*, double, double, double*, double*,
+                      double*, int*, unsigned, cudaStream_t);
+  void (*f2s)(const double*, double*, int, int, unsigned, cudaStream_t);
+  void (*s2f)(const double*, double*, int, int, unsigned, cudaStream_t);
+};
+
+static const Variant kFast = {fast::set_basis, fast::launch_stage, fast::launch_node_minmax,
+                              fast::launch_limit_wetdry, fast::launch_modal2nodal,
+                              fast::launch_fortran_to_soa, fast::launch_soa_to_fortran};
+static const Variant kStrict = {strict::set_basis, strict::launch_stage, strict::launch_node_minmax,
+                                strict::launch_limit_wetdry, strict::launch_modal2nodal,
+                                strict::launch_fortran_to_soa, strict::launch_soa_to_fortran};
+
 }  // namespace dgswem
 
 using namespace dgswem;
 
 struct dgswem_cuda {
   int device = 0;
+  const Variant* v = &kFast;
+  // per-stage boundary forcing computed on the host (ocean EMO*RFF*COS,
+  // flow QNAM*RFF*COS), uploaded once per chunk of steps
+  size_t forcing_per_stage = 0;
+  int chunk_steps = 0;
+  double* forcing_host = nullptr;   // pinned, chunk_steps*nrk*forcing_per_stage
+  DevBuf<double> forcing_dev;
+  cudaEvent_t forcing_copied = nullptr;
+  std::vector<double> emo_h, efa_h, qnam_h, qnph_h;
+  int needs = 0, nfeds = 0;
   cudaStream_t stream = nullptr;      // stream the launches go to
   cudaStream_t own_stream = nullptr;  // created with the context
   int ne = 0, np = 0, nrk = 0;
@@ -148,9 +196,11 @@ struct dgswem_cuda {
 
 namespace {
 
-void check_launch(dgswem_cuda* h) {
+void check_launch(dgswem_cuda* h, const char* what = "kernel") {
   ++h->launches;
-  DG_CUDA(cudaPeekAtLastError());
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw Failure(DGSWEM_ERR_CUDA, std::string("launch of ") + what + ": " + cudaGetErrorString(e));
 }
 
 cudaEvent_t take_event(dgswem_cuda* h) {
@@ -184,6 +234,7 @@ struct LaunchTimer {
   dgswem_cuda* h;
   int kind;
   cudaEvent_t a = nullptr;
+  static constexpr const char* kNames[4] = {"stage_p1", "node_minmax", "limit_wetdry", "other"};
   LaunchTimer(dgswem_cuda* hh, int k) : h(hh), kind(k) {
     if (h->prof_on) {
       a = take_event(h);
@@ -191,7 +242,7 @@ struct LaunchTimer {
     }
   }
   void done() {
-    check_launch(h);
+    check_launch(h, kNames[kind]);
     if (a) {
       cudaEvent_t b = take_event(h);
       DG_CUDA(cudaEventRecord(b, h->stream));
@@ -356,18 +407,12 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   // boundary forcing tables (copied in the reference's Fortran layout)
   const int nbfr = s->nbfr, nffr = s->nffr;
   if (s->needs && nbfr) {
-    need(nbfr <= kMaxFreq, "too many open-boundary frequencies");
-    h->emo_dg.upload(std::vector<double>(s->emo_dg, s->emo_dg + (size_t)nbfr * s->needs * 2));
-    h->efa_dg.upload(std::vector<double>(s->efa_dg, s->efa_dg + (size_t)nbfr * s->needs * 2));
     h->amig.assign(s->amig, s->amig + nbfr);
     h->ff.assign(s->ff, s->ff + nbfr);
     h->face.assign(s->face, s->face + nbfr);
     h->per.assign(s->per, s->per + nbfr);
   }
   if (s->nfeds && nffr) {
-    need(nffr <= kMaxFreq, "too many flow-boundary frequencies");
-    h->qnam_dg.upload(std::vector<double>(s->qnam_dg, s->qnam_dg + (size_t)nffr * s->nfeds * 2));
-    h->qnph_dg.upload(std::vector<double>(s->qnph_dg, s->qnph_dg + (size_t)nffr * s->nfeds * 2));
     h->famig.assign(s->famig, s->famig + nffr);
     h->fff.assign(s->fff, s->fff + nffr);
     h->fface.assign(s->fface, s->fface + nffr);
@@ -400,89 +445,141 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
 
 void upload_state(dgswem_cuda* h, const double* ze, const double* qx, const double* qy, const int* wdflg) {
   const int ne = h->ne;
-  h->staging.alloc(std::max(h->staging.n, 3 * (size_t)ne));
+  h->staging.ensure(3 * (size_t)ne);
   const double* src[3] = {ze, qx, qy};
   for (int var = 0; var < 3; ++var) {
     if (!src[var]) continue;
     DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], 3 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice,
                             h->stream));
-    fortran_to_soa<<<grid_for(ne, 256), 256, 0, h->stream>>>(h->staging.p, h->q[0].p, ne, var);
-    check_launch(h);
+    h->v->f2s(h->staging.p, h->q[0].p, ne, var, grid_for(ne, kPointBlock), h->stream);
+    check_launch(h, "fortran_to_soa");
   }
   if (wdflg)
     DG_CUDA(cudaMemcpyAsync(h->wd.p, wdflg, (size_t)ne * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   DG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
-void step(dgswem_cuda* h, int it) {
-  const int nrk = h->nrk, ne = h->ne;
+// DG_hydro_timestep.F:79-100: stage time and ramp
+void stage_clock(const dgswem_cuda* h, int it, int irk, double* timedg, double* rampdg) {
   const double itdt = it * h->dtdp;
   const double time_a = itdt + h->statim * 86400.0;
-  for (int irk = 1; irk <= nrk; ++irk) {
-    StageArgs A{};
-    A.m = h->mesh;
-    A.ph = h->ph;
-    A.irk = irk;
-    A.qin = h->q[irk - 1].p;
-    A.qout = h->q[irk].p;
-    for (int I = 1; I <= irk; ++I) {
-      A.qhist[I - 1] = h->q[I - 1].p;
-      A.rhist[I - 1] = h->rhs[I - 1].p;
-      A.a[I - 1] = h->atvd[(size_t)(irk - 1) * nrk + (I - 1)];
-      A.b[I - 1] = h->btvd[(size_t)(irk - 1) * nrk + (I - 1)] * h->dtdp;
-    }
-    A.rout = h->keep_rhs[irk - 1] ? h->rhs[irk - 1].p : nullptr;
-    A.wd = h->wd.p;
-    // DG_hydro_timestep.F:79-100 (stage time and ramp)
-    const double dtvd = h->dtvd[irk - 1];
-    A.timedg = time_a - h->dtdp + dtvd * h->dtdp;
-    A.rampdg = 1.0;
-    if (h->nramp == 1 || h->nramp == 2) A.rampdg = std::tanh((2.0 * ((it - 1) + dtvd) * h->dtdp / 86400.0) / h->dramp);
-    // ocean_edge_hydro.F:148-160 / flow_edge_hydro.F:108-120 stage phases
-    for (size_t f = 0; f < h->amig.size(); ++f) {
-      const double ncyc = h->per[f] == 0.0 ? 0.0 : (double)(long long)(A.timedg / h->per[f]);
-      A.argj[f] = h->amig[f] * (A.timedg - ncyc * h->per[f]) + h->face[f];
-      A.rff[f] = h->ff[f] * A.rampdg;
-    }
-    for (size_t f = 0; f < h->famig.size(); ++f) {
-      const double ncyc = h->fper[f] == 0.0 ? 0.0 : (double)(long long)(A.timedg / h->fper[f]);
-      A.fargj[f] = h->famig[f] * (A.timedg - ncyc * h->fper[f]) + h->fface[f];
-      A.frff[f] = h->fff[f] * A.rampdg;
-    }
-    A.wsx = h->wsx.p;
-    A.wsy = h->wsy.p;
-    A.pr = h->pr.p;
-    A.err = h->err.p;
-    {
-      LaunchTimer t(h, 0);
-      if (h->ph.nleq == 1.0 && h->ph.leq == 0.0)
-        stage_p1<true><<<grid_for(ne, kStageBlock), kStageBlock, 0, h->stream>>>(A);
-      else
-        stage_p1<false><<<grid_for(ne, kStageBlock), kStageBlock, 0, h->stream>>>(A);
-      t.done();
-    }
-    const bool wetdry = h->nolifa >= 2;
-    if (h->slopeflag != 0 || wetdry) {
-      LimitArgs L{};
-      L.m = h->mesh;
-      L.ph = h->ph;
-      L.q = h->q[irk].p;
-      L.minmax = h->minmax.p;
-      L.wd = h->wd.p;
-      L.slopeflag = h->slopeflag;
-      L.wetdry = wetdry ? 1 : 0;
-      L.err = h->err.p;
-      if (h->slopeflag != 0) {
-        LaunchTimer t(h, 1);
-        node_minmax<<<grid_for(h->np, 256), 256, 0, h->stream>>>(L);
-        t.done();
+  const double dtvd = h->dtvd[irk - 1];
+  *timedg = time_a - h->dtdp + dtvd * h->dtdp;
+  *rampdg = 1.0;
+  if (h->nramp == 1 || h->nramp == 2) *rampdg = std::tanh((2.0 * ((it - 1) + dtvd) * h->dtdp / 86400.0) / h->dramp);
+}
+
+// Host part of the boundary forcing of one stage: the ocean harmonic
+// endpoint values (ocean_edge_hydro.F:148-177) and the flow boundary normal
+// flux terms (flow_edge_hydro.F:108-125), with the host's cos.
+void stage_forcing(const dgswem_cuda* h, double timedg, double rampdg, double* out) {
+  const int nbfr = (int)h->amig.size(), nffr = (int)h->famig.size();
+  const int needs = h->needs, nfeds = h->nfeds;
+  for (int f = 0; f < nbfr; ++f) {
+    const double ncyc = h->per[f] == 0.0 ? 0.0 : (double)(long long)(timedg / h->per[f]);
+    const double argj = h->amig[f] * (timedg - ncyc * h->per[f]) + h->face[f];
+    const double rff = h->ff[f] * rampdg;
+    for (int l = 0; l < needs; ++l)
+      for (int ipt = 0; ipt < 2; ++ipt) {
+        const size_t at = f + (size_t)nbfr * (l + (size_t)needs * ipt);
+        out[((size_t)f * needs + l) * 2 + ipt] = h->emo_h[at] * rff * std::cos(argj - h->efa_h[at]);
       }
-      LaunchTimer t(h, 2);
-      limit_wetdry<<<grid_for(ne, 256), 256, 0, h->stream>>>(L);
-      t.done();
+  }
+  double* fq = out + (size_t)nbfr * needs * 2;
+  const double xegp[3] = {-1.0, 0.0, 1.0};
+  for (int f = 0; f < nffr; ++f) {
+    const double ncyc = h->fper[f] == 0.0 ? 0.0 : (double)(long long)(timedg / h->fper[f]);
+    const double argj = h->famig[f] * (timedg - ncyc * h->fper[f]) + h->fface[f];
+    const double rff = h->fff[f] * rampdg;
+    for (int l = 0; l < nfeds; ++l) {
+      const size_t a0 = f + (size_t)nffr * l, a1 = f + (size_t)nffr * (l + (size_t)nfeds);
+      for (int j = 0; j < 3; ++j) {
+        const double qa = 0.5 * (h->qnam_h[a0] + h->qnam_h[a1]) + 0.5 * (h->qnam_h[a1] - h->qnam_h[a0]) * xegp[j];
+        const double qp = 0.5 * (h->qnph_h[a0] + h->qnph_h[a1]) + 0.5 * (h->qnph_h[a1] - h->qnph_h[a0]) * xegp[j];
+        fq[((size_t)f * nfeds + l) * 3 + j] = qa * rff * std::cos(argj - qp);
+      }
     }
   }
-  std::swap(h->q[0], h->q[nrk]);  // stage NRK+1 becomes stage 1
+}
+
+void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
+  const int nrk = h->nrk, ne = h->ne;
+  StageArgs A{};
+  A.m = h->mesh;
+  A.ph = h->ph;
+  A.irk = irk;
+  A.qin = h->q[irk - 1].p;
+  A.qout = h->q[irk].p;
+  for (int I = 1; I <= irk; ++I) {
+    A.qhist[I - 1] = h->q[I - 1].p;
+    A.rhist[I - 1] = h->rhs[I - 1].p;
+    A.a[I - 1] = h->atvd[(size_t)(irk - 1) * nrk + (I - 1)];
+    A.b[I - 1] = h->btvd[(size_t)(irk - 1) * nrk + (I - 1)] * h->dtdp;
+  }
+  A.rout = h->keep_rhs[irk - 1] ? h->rhs[irk - 1].p : nullptr;
+  A.wd = h->wd.p;
+  stage_clock(h, it, irk, &A.timedg, &A.rampdg);
+  A.ocean_zg = forcing;
+  A.flow_qn = forcing ? forcing + (size_t)h->amig.size() * h->needs * 2 : nullptr;
+  A.wsx = h->wsx.p;
+  A.wsy = h->wsy.p;
+  A.pr = h->pr.p;
+  A.err = h->err.p;
+  {
+    LaunchTimer t(h, 0);
+    h->v->stage(A, h->ph.nleq == 1.0 && h->ph.leq == 0.0, grid_for(ne, kStageBlock), h->stream);
+    t.done();
+  }
+  const bool wetdry = h->nolifa >= 2;
+  if (h->slopeflag != 0 || wetdry) {
+    LimitArgs L{};
+    L.m = h->mesh;
+    L.ph = h->ph;
+    L.q = h->q[irk].p;
+    L.minmax = h->minmax.p;
+    L.wd = h->wd.p;
+    L.slopeflag = h->slopeflag;
+    L.wetdry = wetdry ? 1 : 0;
+    L.err = h->err.p;
+    if (h->slopeflag != 0) {
+      LaunchTimer t(h, 1);
+      h->v->node_minmax(L, grid_for(h->np, kPointBlock), h->stream);
+      t.done();
+    }
+    LaunchTimer t(h, 2);
+    h->v->limit_wetdry(L, grid_for(ne, kPointBlock), h->stream);
+    t.done();
+  }
+}
+
+// Steps it0 .. it0+n-1: the host forcing of each chunk of steps is computed
+// into pinned memory and copied with one transfer ahead of its kernels.
+void run_steps(dgswem_cuda* h, int it0, int n) {
+  const int nrk = h->nrk;
+  for (int done = 0; done < n;) {
+    const int m = std::min(n - done, h->chunk_steps > 0 ? h->chunk_steps : n);
+    const double* dev = nullptr;
+    if (h->forcing_per_stage) {
+      if (h->forcing_copied) DG_CUDA(cudaEventSynchronize(h->forcing_copied));  // pinned buffer free again
+      for (int i = 0; i < m; ++i)
+        for (int irk = 1; irk <= nrk; ++irk) {
+          double timedg, rampdg;
+          stage_clock(h, it0 + done + i, irk, &timedg, &rampdg);
+          stage_forcing(h, timedg, rampdg, h->forcing_host + ((size_t)i * nrk + (irk - 1)) * h->forcing_per_stage);
+        }
+      const size_t bytes = (size_t)m * nrk * h->forcing_per_stage * sizeof(double);
+      DG_CUDA(cudaMemcpyAsync(h->forcing_dev.p, h->forcing_host, bytes, cudaMemcpyHostToDevice, h->stream));
+      DG_CUDA(cudaEventRecord(h->forcing_copied, h->stream));
+      dev = h->forcing_dev.p;
+    }
+    for (int i = 0; i < m; ++i) {
+      const int it = it0 + done + i;
+      for (int irk = 1; irk <= nrk; ++irk)
+        launch_stage(h, it, irk, dev ? dev + ((size_t)i * nrk + (irk - 1)) * h->forcing_per_stage : nullptr);
+      std::swap(h->q[0], h->q[nrk]);  // stage NRK+1 becomes stage 1
+    }
+    done += m;
+  }
 }
 
 }  // namespace
@@ -500,7 +597,7 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
   return guarded([&]() {
     if (!s || !out) throw Failure(DGSWEM_ERR_ARG, "null argument");
     *out = nullptr;
-    if (flags != 0) throw Failure(DGSWEM_ERR_ARG, "flags must be 0");
+    if (flags & ~DGSWEM_CUDA_STRICT) throw Failure(DGSWEM_ERR_ARG, "unknown flags");
     if (s->dofh != 3) throw Failure(DGSWEM_ERR_ARG, "only p=1 (DOFH=3) is implemented on the device");
     if (s->ne <= 0 || s->np <= 0 || s->nedges <= 0) throw Failure(DGSWEM_ERR_ARG, "empty mesh");
     if (s->nrk < 1 || s->nrk > kMaxStages) throw Failure(DGSWEM_ERR_ARG, "nrk out of range");
@@ -509,10 +606,12 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
     if (s->ics != 1 && s->ics != 2) throw Failure(DGSWEM_ERR_ARG, "ICS must be 1 or 2");
     int ndev = 0;
     DG_CUDA(cudaGetDeviceCount(&ndev));
+    (void)cudaGetLastError();  // drop an error left by other code on this thread
     if (device < 0 || device >= ndev) throw Failure(DGSWEM_ERR_ARG, "no such CUDA device");
     DG_CUDA(cudaSetDevice(device));
     std::unique_ptr<dgswem_cuda> h(new dgswem_cuda());
     h->device = device;
+    h->v = (flags & DGSWEM_CUDA_STRICT) ? &kStrict : &kFast;
     h->ne = s->ne;
     h->np = s->np;
     h->nrk = s->nrk;
@@ -550,11 +649,11 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
     p.ics = s->ics;
     DG_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
-    static bool basis_ready[64] = {false};
-    if (device < 64 && !basis_ready[device]) {
+    {
       const BasisP1 B = make_basis_p1();
-      DG_CUDA(cudaMemcpyToSymbol(cBasis, &B, sizeof(B)));
-      basis_ready[device] = true;
+      kFast.set_basis(B);
+      kStrict.set_basis(B);
+      DG_CUDA(cudaGetLastError());
     }
     build_layout(h.get(), s);
     h->q.resize(s->nrk + 1);
@@ -576,6 +675,25 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
       DG_CUDA(cudaMemset(h->wsy.p, 0, s->np * sizeof(double)));
       DG_CUDA(cudaMemset(h->pr.p, 0, s->np * sizeof(double)));
     }
+    // host-side boundary forcing (ocean and flow harmonics)
+    h->needs = s->needs;
+    h->nfeds = s->nfeds;
+    if (!h->amig.empty()) {
+      h->emo_h.assign(s->emo_dg, s->emo_dg + (size_t)s->nbfr * s->needs * 2);
+      h->efa_h.assign(s->efa_dg, s->efa_dg + (size_t)s->nbfr * s->needs * 2);
+    }
+    if (!h->famig.empty()) {
+      h->qnam_h.assign(s->qnam_dg, s->qnam_dg + (size_t)s->nffr * s->nfeds * 2);
+      h->qnph_h.assign(s->qnph_dg, s->qnph_dg + (size_t)s->nffr * s->nfeds * 2);
+    }
+    h->forcing_per_stage = h->amig.size() * (size_t)s->needs * 2 + h->famig.size() * (size_t)s->nfeds * 3;
+    if (h->forcing_per_stage) {
+      const size_t per_step = h->forcing_per_stage * (size_t)s->nrk;
+      h->chunk_steps = (int)std::max<size_t>(1, std::min<size_t>(512, (size_t)(8u << 20) / (per_step * sizeof(double))));
+      DG_CUDA(cudaMallocHost(&h->forcing_host, per_step * h->chunk_steps * sizeof(double)));
+      h->forcing_dev.alloc(per_step * h->chunk_steps);
+      DG_CUDA(cudaEventCreateWithFlags(&h->forcing_copied, cudaEventDisableTiming));
+    }
     upload_state(h.get(), s->ze, s->qx, s->qy, s->wdflg);
     *out = h.release();
   });
@@ -587,6 +705,8 @@ void dgswem_cuda_destroy(dgswem_cuda* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (auto& p : h->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
   for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->forcing_copied) cudaEventDestroy(h->forcing_copied);
+  if (h->forcing_host) cudaFreeHost(h->forcing_host);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -595,7 +715,7 @@ int dgswem_cuda_hydro_timestep(dgswem_cuda* h, int it) {
   return guarded([&]() {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     DG_CUDA(cudaSetDevice(h->device));
-    step(h, it);
+    run_steps(h, it, 1);
   });
 }
 
@@ -603,7 +723,7 @@ int dgswem_cuda_run(dgswem_cuda* h, int it0, int nsteps) {
   return guarded([&]() {
     if (!h || nsteps < 0) throw Failure(DGSWEM_ERR_ARG, "bad arguments");
     DG_CUDA(cudaSetDevice(h->device));
-    for (int i = 0; i < nsteps; ++i) step(h, it0 + i);
+    run_steps(h, it0, nsteps);
   });
 }
 
@@ -632,12 +752,12 @@ int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* q
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     DG_CUDA(cudaSetDevice(h->device));
     const int ne = h->ne;
-    h->staging.alloc(std::max(h->staging.n, 9 * (size_t)ne));
+    h->staging.ensure(9 * (size_t)ne);
     double* dst[3] = {ze, qx, qy};
     for (int var = 0; var < 3; ++var) {
       if (!dst[var]) continue;
-      soa_to_fortran<<<grid_for(ne, 256), 256, 0, h->stream>>>(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var);
-      check_launch(h);
+      h->v->s2f(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var, grid_for(ne, kPointBlock), h->stream);
+      check_launch(h, "soa_to_fortran");
       DG_CUDA(cudaMemcpyAsync(dst[var], h->staging.p + (size_t)3 * ne * var, 3 * (size_t)ne * sizeof(double),
                               cudaMemcpyDeviceToHost, h->stream));
     }
@@ -665,12 +785,11 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     DG_CUDA(cudaSetDevice(h->device));
     const int np = h->np;
-    h->staging.alloc(std::max(h->staging.n, 4 * (size_t)np));
+    h->staging.ensure(4 * (size_t)np);
     double* d = h->staging.p;
-    modal2nodal_kernel<<<grid_for(np, 256), 256, 0, h->stream>>>(h->mesh, h->q[0].p, h->wd.p, h->ph.nleq,
-                                                                 h->ph.leq, d, d + np, d + 2 * (size_t)np,
-                                                                 h->nodecode.p);
-    check_launch(h);
+    h->v->modal2nodal(h->mesh, h->q[0].p, h->wd.p, h->ph.nleq, h->ph.leq, d, d + np, d + 2 * (size_t)np,
+                      h->nodecode.p, grid_for(np, kPointBlock), h->stream);
+    check_launch(h, "modal2nodal");
     if (eta2) DG_CUDA(cudaMemcpyAsync(eta2, d, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (uu2) DG_CUDA(cudaMemcpyAsync(uu2, d + np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (vv2) DG_CUDA(cudaMemcpyAsync(vv2, d + 2 * (size_t)np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -688,9 +807,11 @@ int dgswem_cuda_set_stream(dgswem_cuda* h, void* stream) {
     DG_CUDA(cudaSetDevice(h->device));
     prof_flush(h);
     DG_CUDA(cudaStreamSynchronize(h->stream));
-    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    h->stream = static_cast<cudaStream_t>(stream);
   });
 }
+
+void* dgswem_cuda_stream(const dgswem_cuda* h) { return h ? static_cast<void*>(h->stream) : nullptr; }
 
 int dgswem_cuda_profile(dgswem_cuda* h, int enable) {
   return guarded([&]() {

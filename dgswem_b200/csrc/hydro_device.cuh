@@ -16,10 +16,11 @@
 
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 namespace dgswem {
 
 constexpr int kMaxStages = 8;
-constexpr int kMaxFreq = 16;
 
 enum EdgeKind : unsigned {
   kInterior = 0,
@@ -99,8 +100,8 @@ struct StageArgs {
   double a[kMaxStages], b[kMaxStages];      // ATVD(irk,I), BTVD(irk,I)*DT
   const int* __restrict__ wd;               // WDFLG (read)
   double timedg, rampdg;
-  double argj[kMaxFreq], rff[kMaxFreq];     // ocean harmonic phase and ramped amplitude
-  double fargj[kMaxFreq], frff[kMaxFreq];   // flow boundary equivalents
+  const double* __restrict__ ocean_zg;      // [(f*NEEDS + L)*2 + ipt] EMO*RFF*COS(ARGJ-EFA)
+  const double* __restrict__ flow_qn;       // [(f*NFEDS + L)*3 + point] QNAM*RFF*COS(ARG)
   const double* __restrict__ wsx;           // nodal met forcing (already ramped), or null
   const double* __restrict__ wsy;
   const double* __restrict__ pr;
@@ -116,5 +117,29 @@ struct LimitArgs {
   int slopeflag, wetdry;
   unsigned* err;
 };
+
+// Kernel launchers, one set per compilation variant: `fast` lets the
+// compiler contract a*b+c into FMA; `strict` (-fmad=false) keeps every
+// product and sum separately rounded, the evaluation the FP64 oracle uses.
+#define DGSWEM_DECLARE_LAUNCHERS(NS)                                                           \
+  namespace NS {                                                                               \
+  void set_basis(const BasisP1& b);                                                            \
+  void launch_stage(const StageArgs& a, bool nonlin, unsigned grid, cudaStream_t s);            \
+  void launch_node_minmax(const LimitArgs& a, unsigned grid, cudaStream_t s);                  \
+  void launch_limit_wetdry(const LimitArgs& a, unsigned grid, cudaStream_t s);                 \
+  void launch_modal2nodal(const MeshView& m, const double* q, const int* wd, double nleq,      \
+                          double leq, double* eta2, double* uu2, double* vv2, int* nodecode,   \
+                          unsigned grid, cudaStream_t s);                                      \
+  void launch_fortran_to_soa(const double* f, double* q, int ne, int var, unsigned grid,       \
+                             cudaStream_t s);                                                  \
+  void launch_soa_to_fortran(const double* q, double* f, int ne, int var, unsigned grid,       \
+                             cudaStream_t s);                                                  \
+  }
+
+DGSWEM_DECLARE_LAUNCHERS(fast)
+DGSWEM_DECLARE_LAUNCHERS(strict)
+
+constexpr int kStageBlock = 128;
+constexpr int kPointBlock = 256;
 
 }  // namespace dgswem

@@ -11,7 +11,12 @@
 
 #include "hydro_device.cuh"
 
+#ifndef DGSWEM_VARIANT
+#error "define DGSWEM_VARIANT (fast or strict) before including hydro_kernels.cuh"
+#endif
+
 namespace dgswem {
+namespace DGSWEM_VARIANT {
 
 __constant__ BasisP1 cBasis;
 
@@ -161,13 +166,10 @@ __device__ __forceinline__ void edge_point(const StageArgs& A, const BasisP1& B,
   xx = xi;
   yx = yi;
   if (kind == kOcean) {  // ocean_edge_hydro.F:148-177, 255-259
+    // endpoint values EMO*RFF*COS(ARGJ-EFA) come from the host for this stage
     double zsum = 0.0;
     for (int f = 0; f < A.m.nbfr; ++f) {
-      double zg[2];
-      for (int ipt = 0; ipt < 2; ++ipt) {
-        const size_t at = f + (size_t)A.m.nbfr * (list + (size_t)A.m.needs * ipt);
-        zg[ipt] = A.m.emo_dg[at] * A.rff[f] * cos(A.argj[f] - A.m.efa_dg[at]);
-      }
+      const double* zg = A.ocean_zg + ((size_t)f * A.m.needs + list) * 2;
       zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * B.xegp[j]);
     }
     zx = zsum;
@@ -178,15 +180,12 @@ __device__ __forceinline__ void edge_point(const StageArgs& A, const BasisP1& B,
     xx = (ty * qne - ny * qte) * den;
     yx = (-tx * qne + nx * qte) * den;
   } else if (kind == kFlow) {  // flow_edge_hydro.F:126-150 (hb from HB modes, same value)
+    // per-point terms QNAM_GP*RFF*COS(ARG) come from the host for this stage
     double qne = 0.0;
     xx = 0.0;
     yx = 0.0;
     for (int f = 0; f < A.m.nffr; ++f) {
-      const size_t a0 = f + (size_t)A.m.nffr * (list + 0);
-      const size_t a1 = f + (size_t)A.m.nffr * (list + (size_t)A.m.nfeds);
-      const double qa = 0.5 * (A.m.qnam_dg[a0] + A.m.qnam_dg[a1]) + 0.5 * (A.m.qnam_dg[a1] - A.m.qnam_dg[a0]) * B.xegp[j];
-      const double qp = 0.5 * (A.m.qnph_dg[a0] + A.m.qnph_dg[a1]) + 0.5 * (A.m.qnph_dg[a1] - A.m.qnph_dg[a0]) * B.xegp[j];
-      qne = qne + qa * A.frff[f] * cos(A.fargj[f] - qp);
+      qne = qne + A.flow_qn[((size_t)f * A.m.nfeds + list) * 3 + j];
       xx = -(ty * qne - ny * 0.0) / (nx * ty - ny * tx);
       yx = -(-tx * qne + nx * 0.0) / (nx * ty - ny * tx);
     }
@@ -313,8 +312,6 @@ __device__ __noinline__ void ibarrier_side(const StageArgs& A, int seg, int side
     }
   }
 }
-
-constexpr int kStageBlock = 128;
 
 // One RK stage for one element: boundary edges, interior edges (fixed slot
 // order, no atomics), rain, volume integral with sources, SSP combination.
@@ -771,4 +768,5 @@ __global__ void soa_to_fortran(const double* __restrict__ q, double* __restrict_
   for (int k = 0; k < 3; ++k) f[(size_t)3 * e + k] = q[(size_t)(3 * var + k) * ne + e];
 }
 
+}  // namespace DGSWEM_VARIANT
 }  // namespace dgswem

@@ -76,14 +76,21 @@ class HydroStep:
     DG_HYDRO_TIMESTEP).  ``setup`` is a ``Deck`` or a pointer to a filled
     ``dgswem_cuda_setup``."""
 
-    def __init__(self, setup, device: int = 0):
+    STRICT = 1  # DGSWEM_CUDA_STRICT
+
+    def __init__(self, setup, device: int = 0, strict: bool = False):
+        """strict=True selects the kernels compiled without FMA contraction
+        (bitwise reproducible against the non-contracting FP64 oracle);
+        the default is the FMA-contracted fast form."""
         self._lib = _abi.load()
+        self.strict = bool(strict)
         self._deck = setup if isinstance(setup, Deck) else None
         sp = setup.setup if isinstance(setup, Deck) else setup
         s = sp.contents
         self.ne, self.np, self.dofh, self.nrk = s.ne, s.np, s.dofh, s.nrk
         h = C.c_void_p()
-        _abi.check(self._lib.dgswem_cuda_create(sp, int(device), 0, C.byref(h)))
+        flags = self.STRICT if strict else 0
+        _abi.check(self._lib.dgswem_cuda_create(sp, int(device), flags, C.byref(h)))
         self._h = h
 
     def close(self):
@@ -116,8 +123,13 @@ class HydroStep:
         return int(self._lib.dgswem_cuda_kernel_launches(self._h))
 
     def set_stream(self, stream_handle: int | None) -> None:
-        """Launch on a caller's cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+        """Launch on a caller's cudaStream_t, used as given (0 is the CUDA
+        default stream), e.g. ``torch.cuda.Stream().cuda_stream``."""
         _abi.check(self._lib.dgswem_cuda_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self._lib.dgswem_cuda_stream(self._h) or 0)
 
     KERNEL_KINDS = ("stage_p1", "node_minmax", "limit_wetdry", "other")
 
@@ -168,7 +180,7 @@ class HydroStep:
         return eta, uu, vv, nc
 
 
-def run_case(path, out=None, device: int = 0, nsteps: int | None = None):
+def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with
     DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  Returns the
     list of (it, eta2) snapshots; writes them to ``out`` when given."""
@@ -178,7 +190,7 @@ def run_case(path, out=None, device: int = 0, nsteps: int | None = None):
     noutge = deck.control("noutge")
     nolifa = deck.s.nolifa
     snaps = []
-    with HydroStep(deck, device) as hs:
+    with HydroStep(deck, device, strict=strict) as hs:
         count = 0
         for it in range(1, nt + 1):
             hs.timestep(it)

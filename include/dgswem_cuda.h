@@ -97,9 +97,16 @@ typedef struct dgswem_cuda_setup {
 
 typedef struct dgswem_cuda dgswem_cuda;
 
+/* dgswem_cuda_create flags.  Default (0): kernels compiled with fused
+ * multiply-add contraction, the fast form.  DGSWEM_CUDA_STRICT: kernels
+ * compiled with -fmad=false whose every product and sum is rounded
+ * separately in the reference's evaluation order (bitwise reproducible
+ * against a non-contracting FP64 CPU build except through pow()). */
+#define DGSWEM_CUDA_STRICT 1
+
 /* Copies the setup to GPU `device` and builds the device layout.
  * Replaces the state the reference keeps in module arrays after PREP_DG
- * (src/dgswem.F:196).  flags: reserved, pass 0. */
+ * (src/dgswem.F:196). */
 int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
                        dgswem_cuda** out);
 void dgswem_cuda_destroy(dgswem_cuda* h);
@@ -133,11 +140,14 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
 /* Number of kernels the library launched since create (for accounting). */
 long long dgswem_cuda_kernel_launches(const dgswem_cuda* h);
 
-/* Launch on the caller's CUDA stream (a cudaStream_t passed as void*; NULL
- * restores the library's own stream).  Lets a host time the step with its
- * own events or order it after its own work.  No counterpart in the
- * reference (its OpenACC regions run on async queue 1). */
+/* Launch on the caller's CUDA stream (a cudaStream_t passed as void*, used
+ * as given: NULL is the CUDA default stream).  dgswem_cuda_stream() returns
+ * the stream in use, so a caller can restore the library's own stream.
+ * Lets a host time the step with its own events or order it after its own
+ * work.  No counterpart in the reference (its OpenACC regions run on async
+ * queue 1). */
 int dgswem_cuda_set_stream(dgswem_cuda* h, void* stream);
+void* dgswem_cuda_stream(const dgswem_cuda* h);
 
 /* Per-kernel timing with CUDA events recorded around every launch on the
  * launching stream.  enable != 0 starts accumulating (and resets); read
