@@ -6,9 +6,11 @@ Python fallback for the hydro step.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libdgswem_cuda.so"
+# DGSWEM_CUDA_LIB points at another build of the same library
+LIB_PATH = Path(os.environ.get("DGSWEM_CUDA_LIB", Path(__file__).resolve().parent / "lib" / "libdgswem_cuda.so"))
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

@@ -131,7 +131,8 @@ struct DevBuf {
 // Launchers of one compilation variant (kernels_fast.cu / kernels_strict.cu).
 struct Variant {
   void (*set_basis)(const BasisP1&);
-  void (*stage)(const StageArgs&, bool, unsigned, cudaStream_t);
+  size_t (*stage_smem)(int);
+  void (*stage)(const StageArgs&, bool, unsigned, size_t, cudaStream_t);
   void (*node_minmax)(const LimitArgs&, unsigned, cudaStream_t);
   void (*limit_wetdry)(const LimitArgs&, unsigned, cudaStream_t);
   void (*modal2nodal)(const MeshView&, const double*, const int*, double, double, double*, double*,
@@ -140,10 +141,10 @@ struct Variant {
   void (*s2f)(const double*, double*, int, int, unsigned, cudaStream_t);
 };
 
-static const Variant kFast = {fast::set_basis, fast::launch_stage, fast::launch_node_minmax,
+static const Variant kFast = {fast::set_basis, fast::stage_smem, fast::launch_stage, fast::launch_node_minmax,
                               fast::launch_limit_wetdry, fast::launch_modal2nodal,
                               fast::launch_fortran_to_soa, fast::launch_soa_to_fortran};
-static const Variant kStrict = {strict::set_basis, strict::launch_stage, strict::launch_node_minmax,
+static const Variant kStrict = {strict::set_basis, strict::stage_smem, strict::launch_stage, strict::launch_node_minmax,
                                 strict::launch_limit_wetdry, strict::launch_modal2nodal,
                                 strict::launch_fortran_to_soa, strict::launch_soa_to_fortran};
 
@@ -163,6 +164,7 @@ struct dgswem_cuda {
   cudaEvent_t forcing_copied = nullptr;
   std::vector<double> emo_h, efa_h, qnam_h, qnph_h;
   int needs = 0, nfeds = 0;
+  int max_tasks = 0;  // largest edge-task list of a stage tile
   cudaStream_t stream = nullptr;      // stream the launches go to
   cudaStream_t own_stream = nullptr;  // created with the context
   int ne = 0, np = 0, nrk = 0;
@@ -339,6 +341,23 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     std::sort(key.begin(), key.end());
     for (int slot = 0; slot < 3; ++slot) info |= (unsigned)key[slot].second << (18 + 2 * slot);
     einfo[e] = info;
+  }
+  // tasks per stage tile (same ownership rule as stage_p1): boundary edges
+  // of the listed kinds, edges to another tile, shared edges once
+  for (int t0 = 0; t0 < ne; t0 += kStageBlock) {
+    const int t1 = std::min(ne, t0 + kStageBlock);
+    int n = 0;
+    for (int e = t0; e < t1; ++e)
+      for (int l = 0; l < 3; ++l) {
+        const unsigned kind = ei_kind(einfo[e], l);
+        if (kind == kNone || kind == kIBarrier) continue;
+        if (kind == kInterior) {
+          const int nb = link[(size_t)l * ne + e];
+          if (nb >= t0 && nb < t1 && !ei_flag(einfo[e], l)) continue;
+        }
+        ++n;
+      }
+    h->max_tasks = std::max(h->max_tasks, n);
   }
   // node -> element star, element order
   std::vector<int> sp(np + 1, 0), st(3 * (size_t)ne);
@@ -527,7 +546,8 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
   A.err = h->err.p;
   {
     LaunchTimer t(h, 0);
-    h->v->stage(A, h->ph.nleq == 1.0 && h->ph.leq == 0.0, grid_for(ne, kStageBlock), h->stream);
+    h->v->stage(A, h->ph.nleq == 1.0 && h->ph.leq == 0.0, grid_for(ne, kStageBlock),
+                h->v->stage_smem(h->max_tasks), h->stream);
     t.done();
   }
   const bool wetdry = h->nolifa >= 2;

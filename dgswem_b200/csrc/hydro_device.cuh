@@ -124,7 +124,8 @@ struct LimitArgs {
 #define DGSWEM_DECLARE_LAUNCHERS(NS)                                                           \
   namespace NS {                                                                               \
   void set_basis(const BasisP1& b);                                                            \
-  void launch_stage(const StageArgs& a, bool nonlin, unsigned grid, cudaStream_t s);            \
+  size_t stage_smem(int max_tasks);                                                            \
+  void launch_stage(const StageArgs& a, bool nonlin, unsigned grid, size_t smem, cudaStream_t s); \
   void launch_node_minmax(const LimitArgs& a, unsigned grid, cudaStream_t s);                  \
   void launch_limit_wetdry(const LimitArgs& a, unsigned grid, cudaStream_t s);                 \
   void launch_modal2nodal(const MeshView& m, const double* q, const int* wd, double nleq,      \

@@ -1,10 +1,10 @@
 // hydro_kernels.cuh -- sm_100a kernels of one RK stage of the p=1 DG hydro
-// step.  Per stage: stage_p1 (volume + all edge fluxes + SSP combination,
-// one thread per element, no atomics) -> node_minmax (slope limiter node
-// pass) -> limit_wetdry (limiter element pass + WETDRY).  Every arithmetic
-// sequence follows the reference routine named in its comment; the CUDA
-// compiler is allowed to contract a*b+c into FMA, so results agree with the
-// FP64 oracle to rounding, not bitwise.
+// step.  Per stage: stage_p1 (tile kernel: edge fluxes once per edge in
+// shared memory, volume integral, SSP combination; no atomics) ->
+// node_minmax (slope limiter node pass) -> limit_wetdry (limiter element
+// pass + WETDRY).  Every arithmetic sequence follows the reference routine
+// named in its comment.  Compiled twice (kernels_fast.cu with FMA
+// contraction, kernels_strict.cu without), see hydro_device.cuh.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -112,60 +112,19 @@ __device__ __forceinline__ void edge_trace(const BasisP1& B, const double* q, in
   v = q[6] + q[7] * p1 + q[8] * p2;
 }
 
-// Edge j-point state, in-side trace, neighbour or ghost exterior state,
-// LLF with the interior dry-side rules (internal_edge_hydro.F:212-302) or the
-// boundary's exterior state (land/ocean/flow/radiation/ebarrier files).
-template <bool kNonlin>
-__device__ __forceinline__ void edge_point(const StageArgs& A, const BasisP1& B, unsigned kind, int l,
-                                           int j, int list, const double* q, const double* qn, int nled,
-                                           int wde, int wdn, const double* hbe, const double* hbn,
-                                           double sfi, double sfx, double nx, double ny, double& F,
-                                           double& Gm, double& Hm) {
+// Exterior (ghost) state of a boundary edge point from the in-side trace
+// (land_edge_hydro.F:201-218, ocean_edge_hydro.F:148-177 and 255-259,
+// flow_edge_hydro.F:126-150, radiation_edge_hydro.F:173-193,
+// ebarrier_edge_hydro.F:120-160).  Point j of the edge, normal (nx, ny).
+__device__ __forceinline__ void ghost_state(const StageArgs& A, const BasisP1& B, unsigned kind, int list, int j,
+                                            double zi, double xi, double yi, double hbi, double nx, double ny,
+                                            double& zx, double& xx, double& yx) {
   const Physics& P = A.ph;
-  double zi, xi, yi;
-  edge_trace(B, q, l, j, zi, xi, yi);
-  const double hbi = hbe[0] + hbe[1] * B.phi_edge[l][j][1] + hbe[2] * B.phi_edge[l][j][2];
-  double zx, xx, yx, hbx = hbi;
   const double tx = -ny, ty = nx;
-  if (kind == kInterior) {
-    const int jn = 2 - j;
-    edge_trace(B, qn, nled, jn, zx, xx, yx);
-    hbx = hbn[0] + hbn[1] * B.phi_edge[nled][jn][1] + hbn[2] * B.phi_edge[nled][jn][2];
-    Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hbi, hbx, sfi, sfx, nx, ny, P.g);
-    F = f.f;
-    Gm = f.g;
-    Hm = f.h;
-    if (fabs(f.f) > 1.0e-8 && (wde == 0 || wdn == 0)) {
-      if (wde == 0) {
-        if (f.f > 0.0) {  // mass leaves the dry side: mirror the wet side
-          const double qne = xx * nx + yx * ny, qte = xx * tx + yx * ty;
-          const double qni = -qne, qti = qte, den = nx * ty - ny * tx;
-          const double qxi = (ty * qni - ny * qti) / den, qyi = (-tx * qni + nx * qti) / den;
-          Flux3 r = llf<kNonlin>(P, zx, zx, qxi, xx, qyi, yx, hbx, hbx, sfx, sfx, nx, ny, P.g);
-          F = r.f;
-          Gm = 0.0;
-          Hm = 0.0;
-        } else {          // mass enters the dry side: gravity off on this side
-          Flux3 r = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hbi, hbx, sfi, sfx, nx, ny, 0.0);
-          Gm = r.g;
-          Hm = r.h;
-        }
-      } else if (f.f < 0.0) {  // neighbour dry and pushing mass in: mirror this side
-        const double qni = xi * nx + yi * ny, qti = xi * tx + yi * ty;
-        const double qnx = -qni, qtx = qti, den = nx * ty - ny * tx;
-        const double qxe = (ty * qnx - ny * qtx) / den, qye = (-tx * qnx + nx * qtx) / den;
-        Flux3 r = llf<kNonlin>(P, zi, zi, xi, qxe, yi, qye, hbi, hbi, sfi, sfi, nx, ny, P.g);
-        F = r.f;
-        Gm = r.g;
-        Hm = r.h;
-      }
-    }
-    return;
-  }
   zx = zi;
   xx = xi;
   yx = yi;
-  if (kind == kOcean) {  // ocean_edge_hydro.F:148-177, 255-259
+  if (kind == kOcean) {
     // endpoint values EMO*RFF*COS(ARGJ-EFA) come from the host for this stage
     double zsum = 0.0;
     for (int f = 0; f < A.m.nbfr; ++f) {
@@ -173,13 +132,13 @@ __device__ __forceinline__ void edge_point(const StageArgs& A, const BasisP1& B,
       zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * B.xegp[j]);
     }
     zx = zsum;
-    if (zx * P.ifnlfa + hbx <= 0) zx = fabs(hbx) + P.h0;
-  } else if (kind == kLand) {  // land_edge_hydro.F:201-218
+    if (zx * P.ifnlfa + hbi <= 0) zx = fabs(hbi) + P.h0;
+  } else if (kind == kLand) {
     const double qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
     const double qne = -qn, qte = qt, den = 1.0 / (nx * ty - ny * tx);
     xx = (ty * qne - ny * qte) * den;
     yx = (-tx * qne + nx * qte) * den;
-  } else if (kind == kFlow) {  // flow_edge_hydro.F:126-150 (hb from HB modes, same value)
+  } else if (kind == kFlow) {
     // per-point terms QNAM_GP*RFF*COS(ARG) come from the host for this stage
     double qne = 0.0;
     xx = 0.0;
@@ -189,12 +148,12 @@ __device__ __forceinline__ void edge_point(const StageArgs& A, const BasisP1& B,
       xx = -(ty * qne - ny * 0.0) / (nx * ty - ny * tx);
       yx = -(-tx * qne + nx * 0.0) / (nx * ty - ny * tx);
     }
-  } else if (kind == kRadiation) {  // radiation_edge_hydro.F:173-193
+  } else if (kind == kRadiation) {
     const double qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
     const double qne = -qn + 2 * sqrt(P.g / (hbi + zi)) * zi, qte = qt, den = 1.0 / (nx * ty - ny * tx);
     xx = (ty * qne - ny * qte) * den;
     yx = (-tx * qne + nx * qte) * den;
-  } else if (kind == kEBarrier) {  // ebarrier_edge_hydro.F:120-160
+  } else if (kind == kEBarrier) {
     const double above = zi - A.m.ebht[list];
     const double subsup = 2.0 * above / 3.0;
     double qne, qte;
@@ -208,10 +167,6 @@ __device__ __forceinline__ void edge_point(const StageArgs& A, const BasisP1& B,
     xx = (ty * qne - ny * qte) / (nx * ty - ny * tx);
     yx = (-tx * qne + nx * qte) / (nx * ty - ny * tx);
   }
-  Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hbi, hbx, sfi, sfi, nx, ny, P.g);
-  F = f.f;
-  Gm = f.g;
-  Hm = f.h;
 }
 
 __device__ __forceinline__ void edge_geometry(const double* xs, const double* ys, int l, double& xlen,
@@ -313,113 +268,360 @@ __device__ __noinline__ void ibarrier_side(const StageArgs& A, int seg, int side
   }
 }
 
-// One RK stage for one element: boundary edges, interior edges (fixed slot
-// order, no atomics), rain, volume integral with sources, SSP combination.
+// ---------------------------------------------------------------------------
+// Tile stage kernel.  A block owns kStageBlock consecutive elements and runs
+// three phases separated by barriers:
+//   1. per element: modal state, bathymetry and geometry into shared memory;
+//      a block-wide prefix sum turns the edges this tile evaluates (boundary
+//      edges, edges to elements of other tiles, and shared interior edges
+//      once, from the reference's "in" element NEDEL(1)) into a dense task list;
+//   2. per (task, Lobatto point): one LLF evaluation in the reference's own
+//      in/ex orientation with its dry-side rules -> F, G_in, H_in, G_ex, H_ex;
+//   3. per element: edge contributions in the reference's order (boundary
+//      edges, then interior edges in edge-number order, the slot sum of
+//      add_internal_flux), rain, volume integral, SSP combination.
 // internal_edge_hydro.F, *_edge_hydro.F, rhs_dg_hydro.F, DG_hydro_timestep.F:238-290
+// ---------------------------------------------------------------------------
+
+// resident stage blocks per SM the register allocation targets
+#ifndef DGSWEM_STAGE_MIN_BLOCKS
+#define DGSWEM_STAGE_MIN_BLOCKS 4
+#endif
+
+// task word layout (int4 .x); .y in-side element, .z ex-side element or list
+struct TaskBits {
+  static constexpr int kKind = 0;      // 3 bits
+  static constexpr int kInLocal = 3;   // in-side element is in this tile
+  static constexpr int kExLocal = 4;   // ex-side element is in this tile
+  static constexpr int kLedIn = 5;     // 2 bits
+  static constexpr int kLedEx = 7;     // 2 bits
+  static constexpr int kFlip = 9;      // owner is the ex side: normal = -owner's normal
+  static constexpr int kOwner = 10;    // 8 bits, owner's local index
+  static constexpr int kOwnerLed = 18; // 2 bits
+};
+
+struct TileShared {
+  BasisP1 B;
+  double q[12][kStageBlock];    // ZE, QX, QY modes and HB modes
+  double geo[14][kStageBlock];  // AREAS; per local edge XLEN, nx, ny; y3-y1, y1-y2, x1-x3, x2-x1
+  int wd[kStageBlock];
+  int task_of[3][kStageBlock];
+  int warp_sum[kStageBlock / 32];
+  int ntask;
+};
+
+// dynamic shared memory: TileShared, then the task list (int4 each), then
+// 15 doubles of results per task
+constexpr size_t kTaskOffset = (sizeof(TileShared) + 15) / 16 * 16;
+__host__ __device__ constexpr size_t stage_shared_bytes(int max_tasks) {
+  return kTaskOffset + (size_t)(max_tasks + 1) * (sizeof(int4) + 15 * sizeof(double));
+}
+
+// One point of a tile task: (modal state of a side, its local edge, point)
+__device__ __forceinline__ void side_trace(const TileShared& S, const StageArgs& A, bool local, int el, int led,
+                                           int gp, double& z, double& u, double& v, double& h) {
+  const double p1 = S.B.phi_edge[led][gp][1], p2 = S.B.phi_edge[led][gp][2];
+  const int ne = A.m.ne;
+  if (local) {
+    z = S.q[0][el] + S.q[1][el] * p1 + S.q[2][el] * p2;
+    u = S.q[3][el] + S.q[4][el] * p1 + S.q[5][el] * p2;
+    v = S.q[6][el] + S.q[7][el] * p1 + S.q[8][el] * p2;
+    h = S.q[9][el] + S.q[10][el] * p1 + S.q[11][el] * p2;
+  } else {
+    const double* q = A.qin;
+    z = q[el] + q[(size_t)ne + el] * p1 + q[(size_t)2 * ne + el] * p2;
+    u = q[(size_t)3 * ne + el] + q[(size_t)4 * ne + el] * p1 + q[(size_t)5 * ne + el] * p2;
+    v = q[(size_t)6 * ne + el] + q[(size_t)7 * ne + el] * p1 + q[(size_t)8 * ne + el] * p2;
+    const double* hb = A.m.hb;
+    h = hb[el] + hb[(size_t)ne + el] * p1 + hb[(size_t)2 * ne + el] * p2;
+  }
+}
+
 template <bool kNonlin>
-__global__ void __launch_bounds__(kStageBlock) stage_p1(const __grid_constant__ StageArgs A) {
-  __shared__ BasisP1 B;
-  load_basis(B);
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kStageBlock, DGSWEM_STAGE_MIN_BLOCKS) stage_p1(const __grid_constant__ StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TileShared& S = *reinterpret_cast<TileShared*>(smem_raw);
+  int4* tasks = reinterpret_cast<int4*>(smem_raw + kTaskOffset);
   const MeshView& m = A.m;
   const Physics& P = A.ph;
   const int ne = m.ne;
-  if (e >= ne) return;
-
-  double q[9];
-#pragma unroll
-  for (int c = 0; c < 9; ++c) q[c] = A.qin[(size_t)c * ne + e];
-  double hbe[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) hbe[k] = m.hb[(size_t)k * ne + e];
-  int nd[3];
-  double xs[3], ys[3];
-#pragma unroll
-  for (int v = 0; v < 3; ++v) {
-    nd[v] = m.nm[(size_t)v * ne + e];
-    xs[v] = m.x[nd[v]];
-    ys[v] = m.y[nd[v]];
+  const int tid = threadIdx.x;
+  const int tile0 = blockIdx.x * kStageBlock;
+  const int e = tile0 + tid;
+  const bool valid = e < ne;
+  const int ntile = min(kStageBlock, ne - tile0);
+  {
+    const double* src = reinterpret_cast<const double*>(&cBasis);
+    double* dst = reinterpret_cast<double*>(&S.B);
+    for (int i = tid; i < (int)(sizeof(BasisP1) / sizeof(double)); i += blockDim.x) dst[i] = src[i];
   }
-  const int wde = A.wd[e];
-  const unsigned info = m.einfo[e];
-  // AREAS (read_input.F:1406) and the inverse Jacobian (prep_DG.F:970-981)
-  const double areas = (xs[0] - xs[2]) * (ys[1] - ys[2]) + (xs[2] - xs[1]) * (ys[0] - ys[2]);
 
+  // ---- phase 1: element data, ownership, dense task list ----
+  unsigned info = 0u;
+  int link[3] = {-1, -1, -1};
+  int own[3] = {0, 0, 0};
+  int nown = 0;
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) S.q[c][tid] = A.qin[(size_t)c * ne + e];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) S.q[9 + k][tid] = m.hb[(size_t)k * ne + e];
+    S.wd[tid] = A.wd[e];
+    double xs[3], ys[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const int nd = m.nm[(size_t)v * ne + e];
+      xs[v] = m.x[nd];
+      ys[v] = m.y[nd];
+    }
+    // AREAS (read_input.F:1406); XLEN and normals (calc_normal.F:41-48) on
+    // this element's counter-clockwise edges
+    S.geo[0][tid] = (xs[0] - xs[2]) * (ys[1] - ys[2]) + (xs[2] - xs[1]) * (ys[0] - ys[2]);
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      const int a = (l + 1) % 3, b = (l + 2) % 3;
+      const double dy = ys[b] - ys[a], dx = xs[b] - xs[a];
+      const double len = sqrt(dy * dy + dx * dx);
+      S.geo[1 + 3 * l][tid] = len;
+      S.geo[2 + 3 * l][tid] = (ys[b] - ys[a]) / len;
+      S.geo[3 + 3 * l][tid] = -(xs[b] - xs[a]) / len;
+    }
+    S.geo[10][tid] = ys[2] - ys[0];
+    S.geo[11][tid] = ys[0] - ys[1];
+    S.geo[12][tid] = xs[0] - xs[2];
+    S.geo[13][tid] = xs[1] - xs[0];
+    info = m.einfo[e];
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      link[l] = m.link[(size_t)l * ne + e];
+      const unsigned kind = ei_kind(info, l);
+      if (kind == kNone || kind == kIBarrier) continue;
+      if (kind == kInterior) {
+        const bool nbr_local = link[l] >= tile0 && link[l] < tile0 + ntile;
+        own[l] = (!nbr_local || ei_flag(info, l)) ? 1 : 0;
+      } else {
+        own[l] = 1;
+      }
+      nown += own[l];
+    }
+  }
+  // block exclusive scan of the owned-task counts
+  const int lane = tid & 31, warp = tid >> 5;
+  int incl = nown;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += t;
+  }
+  if (lane == 31) S.warp_sum[warp] = incl;
+  __syncthreads();
+  int base = incl - nown;
+  for (int w = 0; w < warp; ++w) base += S.warp_sum[w];
+  if (tid == blockDim.x - 1) S.ntask = base + nown;
+  if (valid) {
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      S.task_of[l][tid] = -1;
+      if (!own[l]) continue;
+      const unsigned kind = ei_kind(info, l);
+      int4 t;
+      unsigned fl = kind;
+      fl |= (unsigned)tid << TaskBits::kOwner;
+      fl |= (unsigned)l << TaskBits::kOwnerLed;
+      if (kind == kInterior) {
+        const int nb = link[l];
+        const bool nbr_local = nb >= tile0 && nb < tile0 + ntile;
+        const unsigned nled = ei_nled(info, l);
+        if (ei_flag(info, l)) {  // this element is NEDEL(1): the in side
+          fl |= 1u << TaskBits::kInLocal;
+          fl |= (unsigned)l << TaskBits::kLedIn;
+          fl |= nled << TaskBits::kLedEx;
+          if (nbr_local) fl |= 1u << TaskBits::kExLocal;
+          t.y = tid;
+          t.z = nbr_local ? nb - tile0 : nb;
+        } else {                 // the neighbour (another tile) is the in side
+          fl |= 1u << TaskBits::kExLocal;
+          fl |= nled << TaskBits::kLedIn;
+          fl |= (unsigned)l << TaskBits::kLedEx;
+          fl |= 1u << TaskBits::kFlip;
+          t.y = nb;
+          t.z = tid;
+        }
+      } else {
+        fl |= 1u << TaskBits::kInLocal;
+        fl |= (unsigned)l << TaskBits::kLedIn;
+        t.y = tid;
+        t.z = link[l];
+      }
+      t.x = (int)fl;
+      t.w = 0;
+      S.task_of[l][tid] = base;
+      tasks[base] = t;
+      ++base;
+    }
+  }
+  __syncthreads();
+  if (valid) {  // shared interior edges: read the owner's task
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+      if (ei_kind(info, l) == kInterior && !own[l])
+        S.task_of[l][tid] = S.task_of[ei_nled(info, l)][link[l] - tile0];
+  }
+
+  // ---- phase 2: one LLF per (task, point) ----
+  double* res = reinterpret_cast<double*>(tasks + S.ntask + (S.ntask & 1));  // [task][point][5]
+  const int nwork = 3 * S.ntask;
+  for (int w = tid; w < nwork; w += blockDim.x) {
+    const int ti = w / 3, I = w - 3 * ti;
+    const int4 t = tasks[ti];
+    const unsigned fl = (unsigned)t.x;
+    const unsigned kind = fl & 7u;
+    const bool in_local = (fl >> TaskBits::kInLocal) & 1u, ex_local = (fl >> TaskBits::kExLocal) & 1u;
+    const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
+    const int owner = (fl >> TaskBits::kOwner) & 255, oled = (fl >> TaskBits::kOwnerLed) & 3;
+    double nx = S.geo[2 + 3 * oled][owner], ny = S.geo[3 + 3 * oled][owner];
+    if ((fl >> TaskBits::kFlip) & 1u) { nx = -nx; ny = -ny; }
+    const int wd_in = in_local ? S.wd[t.y] : A.wd[t.y];
+    const int gin = in_local ? tile0 + t.y : t.y;  // global ids for the ics=2 tables
+    double* out = res + ((size_t)ti * 3 + I) * 5;
+    if (kind == kInterior) {
+      const int wd_ex = ex_local ? S.wd[t.z] : A.wd[t.z];
+      if (wd_in == 0 && wd_ex == 0) continue;
+      const int gp_in = I, gp_ex = 2 - I;
+      double zi, xi, yi, hi, zx, xx, yx, hx;
+      side_trace(S, A, in_local, t.y, led_in, gp_in, zi, xi, yi, hi);
+      side_trace(S, A, ex_local, t.z, led_ex, gp_ex, zx, xx, yx, hx);
+      const int gex = ex_local ? tile0 + t.z : t.z;
+      const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
+      const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
+      Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
+      double F = f.f, gi = f.g, hi2 = f.h, gx = f.g, hx2 = f.h;
+      // internal_edge_hydro.F:212-302: mass flux out of / into a dry element
+      if (fabs(f.f) > 1.0e-8 && (wd_in == 0 || wd_ex == 0)) {
+        const double tx = -ny, ty = nx;
+        if (wd_in == 0) {
+          if (f.f > 0.0) {
+            const double qne = xx * nx + yx * ny, qte = xx * tx + yx * ty;
+            const double qni = -qne, qti = qte, den = nx * ty - ny * tx;
+            const double qxi = (ty * qni - ny * qti) / den, qyi = (-tx * qni + nx * qti) / den;
+            Flux3 r = llf<kNonlin>(P, zx, zx, qxi, xx, qyi, yx, hx, hx, sfx, sfx, nx, ny, P.g);
+            F = r.f; gx = r.g; hx2 = r.h; gi = 0.0; hi2 = 0.0;
+          } else {
+            Flux3 r = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, 0.0);
+            gi = r.g; hi2 = r.h;
+          }
+        } else {
+          if (f.f < 0.0) {
+            const double qni = xi * nx + yi * ny, qti = xi * tx + yi * ty;
+            const double qne = -qni, qte = qti, den = nx * ty - ny * tx;
+            const double qxe = (ty * qne - ny * qte) / den, qye = (-tx * qne + nx * qte) / den;
+            Flux3 r = llf<kNonlin>(P, zi, zi, xi, qxe, yi, qye, hi, hi, sfi, sfi, nx, ny, P.g);
+            F = r.f; gi = r.g; hi2 = r.h; gx = 0.0; hx2 = 0.0;
+          } else {
+            Flux3 r = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, 0.0);
+            gx = r.g; hx2 = r.h;
+          }
+        }
+      }
+      out[0] = F; out[1] = gi; out[2] = hi2; out[3] = gx; out[4] = hx2;
+    } else {
+      if (wd_in == 0) continue;
+      double zi, xi, yi, hi, zx, xx, yx;
+      side_trace(S, A, true, t.y, led_in, I, zi, xi, yi, hi);
+      const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
+      ghost_state(A, S.B, kind, t.z, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
+      Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
+      out[0] = f.f; out[1] = f.g; out[2] = f.h;
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+
+  // ---- phase 3: accumulate in the reference's order, volume, SSP ----
+  const BasisP1& B = S.B;
+  const int wde = S.wd[tid];
+  const double areas = S.geo[0][tid];
   double rhs[9], isum[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) { rhs[c] = 0.0; isum[c] = 0.0; }
-
 #pragma unroll 1
   for (int s = 0; s < 3; ++s) {
     const int l = ei_order(info, s);
     const unsigned kind = ei_kind(info, l);
     if (kind == kNone) continue;
-    const int list = m.link[(size_t)l * ne + e];
     if (kind == kIBarrier) {
       double o[9];
-      ibarrier_side<kNonlin>(A, list, (int)ei_flag(info, l) ? 0 : 1, o);
+      ibarrier_side<kNonlin>(A, link[l], (int)ei_flag(info, l) ? 0 : 1, o);
 #pragma unroll
       for (int c = 0; c < 9; ++c) rhs[c] = rhs[c] + o[c];
       continue;
     }
-    const bool interior = kind == kInterior;
-    double qn[9], hbn[3];
-    int wdn = 1, nled = 0;
-    if (interior) {
-      wdn = A.wd[list];
+    const double xlen = S.geo[1 + 3 * l][tid];
+    const double* r = res + (size_t)S.task_of[l][tid] * 15;
+    if (kind == kInterior) {
+      const int nb = link[l];
+      const bool nbr_local = nb >= tile0 && nb < tile0 + ntile;
+      const int wdn = nbr_local ? S.wd[nb - tile0] : A.wd[nb];
       if (wde == 0 && wdn == 0) continue;
-      nled = (int)ei_nled(info, l);
+      const bool is_in = ei_flag(info, l) != 0;
+      const double edfac = xlen / areas;
+      double acc[9];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) qn[c] = A.qin[(size_t)c * ne + list];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) hbn[k] = m.hb[(size_t)k * ne + list];
-    } else {
-      if (wde == 0) continue;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) qn[c] = 0.0;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) hbn[k] = 0.0;
-    }
-    double xlen, nx, ny;
-    edge_geometry(xs, ys, l, xlen, nx, ny);
-    const double edfac = xlen / areas;
-    const bool own_first = interior ? ei_flag(info, l) != 0 : true;
-    double acc[9];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) acc[c] = interior ? 0.0 : rhs[c];
+      for (int c = 0; c < 9; ++c) acc[c] = 0.0;
 #pragma unroll 1
-    for (int I = 0; I < 3; ++I) {
-      const int j = own_first ? I : 2 - I;  // reference point order of this edge
-      const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(l * 3 + j) * ne + e] : 1.0;
-      const double sfx = (interior && m.sfac_edge) ? m.sfac_edge[(size_t)(nled * 3 + (2 - j)) * ne + list] : sfi;
-      double F, Gm, Hm;
-      edge_point<kNonlin>(A, B, kind, l, j, list, q, qn, nled, wde, wdn, hbe, hbn, sfi, sfx, nx, ny, F, Gm, Hm);
+      for (int I = 0; I < 3; ++I) {
+        const int j = is_in ? I : 2 - I;
+        const double* p = r + 5 * I;
+        const double F = p[0], Gm = is_in ? p[1] : p[3], Hm = is_in ? p[2] : p[4];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const double w = interior ? edfac * B.edgeq[l][j][k]
-                                  : 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][j][k] * B.wegp[j];
-        acc[k] = acc[k] - w * F;
-        acc[3 + k] = acc[3 + k] - w * Gm;
-        acc[6 + k] = acc[6 + k] - w * Hm;
+        for (int k = 0; k < 3; ++k) {
+          const double w = edfac * B.edgeq[l][j][k];
+          if (is_in) {  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
+            acc[k] = acc[k] - w * F;
+            acc[3 + k] = acc[3 + k] - w * Gm;
+            acc[6 + k] = acc[6 + k] - w * Hm;
+          } else {      // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
+            acc[k] = acc[k] + w * F;
+            acc[3 + k] = acc[3 + k] + w * Gm;
+            acc[6 + k] = acc[6 + k] + w * Hm;
+          }
+        }
       }
-    }
-    if (interior) {
 #pragma unroll
       for (int c = 0; c < 9; ++c) isum[c] = isum[c] + acc[c];
     } else {
+      if (wde == 0) continue;
+#pragma unroll 1
+      for (int I = 0; I < 3; ++I) {
+        const double* p = r + 5 * I;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) rhs[c] = acc[c];
+        for (int k = 0; k < 3; ++k) {
+          const double w = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
+          rhs[k] = rhs[k] - w * p[0];
+          rhs[3 + k] = rhs[3 + k] - w * p[1];
+          rhs[6 + k] = rhs[6 + k] - w * p[2];
+        }
+      }
     }
   }
 #pragma unroll
   for (int c = 0; c < 9; ++c) rhs[c] = rhs[c] + isum[c];  // add_internal_flux
 
+  double q[9], hbe[3];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) q[c] = S.q[c][tid];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) hbe[k] = S.q[9 + k][tid];
+
   // rhs_dg_hydro.F:58-470
   const double area = areas * 0.5;
-  const double drdx = 1.0 / area * (ys[2] - ys[0]);
-  const double dsdx = 1.0 / area * (ys[0] - ys[1]);
-  const double drdy = 1.0 / area * (xs[0] - xs[2]);
-  const double dsdy = 1.0 / area * (xs[1] - xs[0]);
+  const double drdx = 1.0 / area * S.geo[10][tid];
+  const double dsdx = 1.0 / area * S.geo[11][tid];
+  const double drdy = 1.0 / area * S.geo[12][tid];
+  const double dsdy = 1.0 / area * S.geo[13][tid];
+  int nd[3];
+#pragma unroll
+  for (int v = 0; v < 3; ++v) nd[v] = m.nm[(size_t)v * ne + e];
   double xfac[3][3], yfac[3][3];  // [mode][point]
 #pragma unroll
   for (int k = 0; k < 3; ++k)
