@@ -56,6 +56,7 @@ SIGNATURES = {
     "dgswem_cuda_download_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_set_met": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "dgswem_cuda_modal2nodal": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
+    "dgswem_cuda_modal2nodal_noalloc": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "dgswem_cuda_last_error": (C.c_int, [C.c_char_p, C.c_int]),
     "dgswem_cuda_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -6,6 +6,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -602,6 +603,32 @@ void run_steps(dgswem_cuda* h, int it0, int n) {
   }
 }
 
+// Nodal scratch of dgswem_cuda_modal2nodal_noalloc: ETA2, UU2, VV2 for up to
+// kScratchNodes nodes, each array starting at a multiple of kScratchNodes.
+// The CUDA loader reserves it with this module on each device; no call
+// allocates it.
+constexpr size_t kScratchNodes = DGSWEM_CUDA_NOALLOC_MAX_NODES;
+static __device__ __align__(256) double g_nodal_scratch[3 * kScratchNodes];
+
+// Device address of g_nodal_scratch on `device` (the current device), looked
+// up once per device ordinal under a lock; fixed-size table, no allocation.
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_lock;
+double* g_scratch_addr[kMaxScratchDevices] = {};
+
+double* nodal_scratch(int device) {
+  if (device < 0 || device >= kMaxScratchDevices)
+    throw Failure(DGSWEM_ERR_ARG, "modal2nodal_noalloc: device ordinal " + std::to_string(device) + " >= " +
+                                      std::to_string(kMaxScratchDevices));
+  std::lock_guard<std::mutex> guard(g_scratch_lock);
+  if (!g_scratch_addr[device]) {
+    void* p = nullptr;
+    DG_CUDA(cudaGetSymbolAddress(&p, g_nodal_scratch));
+    g_scratch_addr[device] = static_cast<double*>(p);
+  }
+  return g_scratch_addr[device];
+}
+
 }  // namespace
 
 extern "C" {
@@ -813,6 +840,30 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
     if (eta2) DG_CUDA(cudaMemcpyAsync(eta2, d, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (uu2) DG_CUDA(cudaMemcpyAsync(uu2, d + np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (vv2) DG_CUDA(cudaMemcpyAsync(vv2, d + 2 * (size_t)np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (nodecode)
+      DG_CUDA(cudaMemcpyAsync(nodecode, h->nodecode.p, np * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, double* vv2, int* nodecode) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    const int np = h->np;
+    if (np > DGSWEM_CUDA_NOALLOC_MAX_NODES)
+      throw Failure(DGSWEM_ERR_ARG, "modal2nodal_noalloc: NP = " + std::to_string(np) +
+                                        " exceeds the static scratch maximum DGSWEM_CUDA_NOALLOC_MAX_NODES = " +
+                                        std::to_string(DGSWEM_CUDA_NOALLOC_MAX_NODES));
+    DG_CUDA(cudaSetDevice(h->device));
+    double* eta = nodal_scratch(h->device);
+    double* uu = eta + kScratchNodes;
+    double* vv = uu + kScratchNodes;
+    h->v->modal2nodal(h->mesh, h->q[0].p, h->wd.p, h->ph.nleq, h->ph.leq, eta, uu, vv, h->nodecode.p,
+                      grid_for(np, kPointBlock), h->stream);
+    check_launch(h, "modal2nodal");
+    if (eta2) DG_CUDA(cudaMemcpyAsync(eta2, eta, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (uu2) DG_CUDA(cudaMemcpyAsync(uu2, uu, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (vv2) DG_CUDA(cudaMemcpyAsync(vv2, vv, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (nodecode)
       DG_CUDA(cudaMemcpyAsync(nodecode, h->nodecode.p, np * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     DG_CUDA(cudaStreamSynchronize(h->stream));

@@ -179,6 +179,17 @@ class HydroStep:
         _abi.check(self._lib.dgswem_cuda_modal2nodal(self._h, _dptr(eta), _dptr(uu), _dptr(vv), _iptr(nc)))
         return eta, uu, vv, nc
 
+    def modal2nodal_noalloc(self):
+        """modal2nodal through dgswem_cuda_modal2nodal_noalloc: the nodal
+        scratch is the library's static device array, no device allocation."""
+        eta = np.empty(self.np)
+        uu = np.empty(self.np)
+        vv = np.empty(self.np)
+        nc = np.empty(self.np, np.int32)
+        _abi.check(self._lib.dgswem_cuda_modal2nodal_noalloc(self._h, _dptr(eta), _dptr(uu), _dptr(vv),
+                                                             _iptr(nc)))
+        return eta, uu, vv, nc
+
 
 def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with

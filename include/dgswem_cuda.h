@@ -137,6 +137,31 @@ int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2,
 int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* vv2,
                             int* nodecode);
 
+/* Largest NP that dgswem_cuda_modal2nodal_noalloc accepts: its static device
+ * scratch holds ETA2, UU2 and VV2 for this many nodes (24 MiB). */
+#define DGSWEM_CUDA_NOALLOC_MAX_NODES (1 << 20)
+
+/* dgswem_cuda_modal2nodal that allocates nothing.  No counterpart in the
+ * reference (its modal2nodal fills the host arrays directly).  Same kernel and
+ * same results as dgswem_cuda_modal2nodal, but the nodal scratch is a static
+ * device array of DGSWEM_CUDA_NOALLOC_MAX_NODES nodes instead of the handle's
+ * staging buffer, which dgswem_cuda_modal2nodal grows (cudaFree + cudaMalloc)
+ * when 4 NP exceeds it.  For hosts that must not allocate or free device
+ * memory once the time loop runs: a host sharing the GPU with work on its own
+ * streams (cudaFree waits for the whole device) or one that has reserved the
+ * rest of HBM for its own pool (the allocation could fail mid-run).
+ * - NP > DGSWEM_CUDA_NOALLOC_MAX_NODES: DGSWEM_ERR_ARG, nothing launched.
+ * - The first call on each device looks up the scratch's device address
+ *   (cudaGetSymbolAddress, which may load the library's device module); make
+ *   that first call before any stream capture.
+ * - Nothing in the scratch has to start at zero: the kernel writes all NP
+ *   entries of each nodal array before they are copied out.
+ * - All handles on one device share the one scratch array: calls that overlap
+ *   in time on the same device (from several host threads) race on it and
+ *   must be serialised by the caller. */
+int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, double* vv2,
+                                    int* nodecode);
+
 /* Number of kernels the library launched since create (for accounting). */
 long long dgswem_cuda_kernel_launches(const dgswem_cuda* h);
 
