@@ -132,8 +132,8 @@ struct DevBuf {
 // Launchers of one compilation variant (kernels_fast.cu / kernels_strict.cu).
 struct Variant {
   void (*set_basis)(const BasisP1&);
-  size_t (*stage_smem)(int);
   void (*stage)(const StageArgs&, bool, unsigned, size_t, cudaStream_t);
+  void (*ibarrier)(const StageArgs&, bool, cudaStream_t);
   void (*node_minmax)(const LimitArgs&, unsigned, cudaStream_t);
   void (*limit_wetdry)(const LimitArgs&, unsigned, cudaStream_t);
   void (*modal2nodal)(const MeshView&, const double*, const int*, double, double, double*, double*,
@@ -142,10 +142,10 @@ struct Variant {
   void (*s2f)(const double*, double*, int, int, unsigned, cudaStream_t);
 };
 
-static const Variant kFast = {fast::set_basis, fast::stage_smem, fast::launch_stage, fast::launch_node_minmax,
+static const Variant kFast = {fast::set_basis, fast::launch_stage, fast::launch_ibarrier, fast::launch_node_minmax,
                               fast::launch_limit_wetdry, fast::launch_modal2nodal,
                               fast::launch_fortran_to_soa, fast::launch_soa_to_fortran};
-static const Variant kStrict = {strict::set_basis, strict::stage_smem, strict::launch_stage, strict::launch_node_minmax,
+static const Variant kStrict = {strict::set_basis, strict::launch_stage, strict::launch_ibarrier, strict::launch_node_minmax,
                                 strict::launch_limit_wetdry, strict::launch_modal2nodal,
                                 strict::launch_fortran_to_soa, strict::launch_soa_to_fortran};
 
@@ -165,7 +165,7 @@ struct dgswem_cuda {
   cudaEvent_t forcing_copied = nullptr;
   std::vector<double> emo_h, efa_h, qnam_h, qnph_h;
   int needs = 0, nfeds = 0;
-  int max_tasks = 0;  // largest edge-task list of a stage tile
+  size_t stage_smem = 0;  // dynamic shared memory of a stage tile
   cudaStream_t stream = nullptr;      // stream the launches go to
   cudaStream_t own_stream = nullptr;  // created with the context
   int ne = 0, np = 0, nrk = 0;
@@ -178,13 +178,15 @@ struct dgswem_cuda {
   Physics ph{};
   MeshView mesh{};
   // device arrays
-  DevBuf<double> x, y, dp, hb, cori, fric, manning, sfac_area, sfac_edge;
+  DevBuf<double> x, y, dp, hb, egeo, cori, fric, manning, sfac_area, sfac_edge;
   DevBuf<int> nm, link, star_ptr, star, ib_elem, ib_led;
-  DevBuf<unsigned> einfo;
+  DevBuf<unsigned> einfo, eslot, tile_tasks;
+  DevBuf<int> tile_task_ptr, tile_halo_ptr, tile_halo;
   DevBuf<double> emo_dg, efa_dg, qnam_dg, qnph_dg, ebht, ebcfsp, ibht, ibcfsb, ibcfsp;
   DevBuf<double> wsx, wsy, pr, minmax, staging;
   std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
   std::vector<DevBuf<double>> rhs;  // nrk RHS buffers (allocated when kept)
+  DevBuf<double> ib_rhs;  // internal-barrier terms of the current stage
   DevBuf<int> wd, nodecode;
   DevBuf<unsigned> err;
   long long launches = 0;
@@ -257,6 +259,106 @@ struct LaunchTimer {
 
 unsigned grid_for(int n, int block) { return (unsigned)((n + block - 1) / block); }
 
+// Stage tile plan: for each tile of kTile consecutive elements, the edge
+// tasks it evaluates and the out-of-tile neighbours (halo) they read.  Edge
+// ownership: a boundary edge of a listed kind and an internal-barrier side
+// belong to their element; an interior edge inside the tile is evaluated once,
+// by its in side NEDEL(1); an interior edge to another tile is evaluated by
+// both tiles, each for its own element, in the reference's in/ex orientation.
+// Tasks: interior edges in element order, then the boundary kinds grouped, so
+// that a warp's tasks mostly take one branch.
+void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const std::vector<unsigned>& einfo) {
+  const int ntile = (ne + kTile - 1) / kTile;
+  std::vector<int> task_ptr(ntile + 1, 0), halo_ptr(ntile + 1, 0), halo;
+  std::vector<unsigned> tasks;  // (word, list) pairs
+  std::vector<unsigned> eslot(ne, 0u);
+  std::vector<int> hl;
+  struct Task {
+    unsigned word, list;
+    int el, led;
+  };
+  std::vector<Task> tt;
+  int max_halo = 0, max_tasks = 0;
+  for (int t = 0; t < ntile; ++t) {
+    const int t0 = t * kTile, t1 = std::min(ne, t0 + kTile);
+    hl.clear();
+    for (int e = t0; e < t1; ++e)
+      for (int l = 0; l < 3; ++l)
+        if (ei_kind(einfo[e], l) == kInterior) {
+          const int nb = link[(size_t)l * ne + e];
+          if (nb < t0 || nb >= t1) hl.push_back(nb);
+        }
+    std::sort(hl.begin(), hl.end());
+    hl.erase(std::unique(hl.begin(), hl.end()), hl.end());
+    auto slot = [&](int g) -> unsigned {
+      if (g >= t0 && g < t1) return (unsigned)(g - t0);
+      return (unsigned)(kTile + (std::lower_bound(hl.begin(), hl.end(), g) - hl.begin()));
+    };
+    tt.clear();
+    for (int pass = 0; pass < 2; ++pass)  // interior edges, then boundary kinds
+      for (unsigned want = pass == 0 ? (unsigned)kInterior : 1u; want <= (pass == 0 ? 0u : 6u); ++want)
+        for (int e = t0; e < t1; ++e)
+          for (int l = 0; l < 3; ++l) {
+            const unsigned info = einfo[e], kind = ei_kind(info, l);
+            if (kind != want) continue;
+            const int lk = link[(size_t)l * ne + e];
+            unsigned w = kind << TaskBits::kKind, list = 0;
+            if (kind == kInterior) {
+              const bool local = lk >= t0 && lk < t1, in_side = ei_flag(info, l) != 0;
+              if (local && !in_side) continue;  // the in side's task
+              const unsigned nled = ei_nled(info, l);
+              if (in_side)
+                w |= (unsigned)l << TaskBits::kLedIn | nled << TaskBits::kLedEx | slot(e) << TaskBits::kInSlot |
+                     slot(lk) << TaskBits::kExSlot;
+              else
+                w |= nled << TaskBits::kLedIn | (unsigned)l << TaskBits::kLedEx | 1u << TaskBits::kFlip |
+                     slot(lk) << TaskBits::kInSlot | slot(e) << TaskBits::kExSlot;
+            } else {
+              w |= (unsigned)l << TaskBits::kLedIn | slot(e) << TaskBits::kInSlot;
+              list = kind == kIBarrier ? (unsigned)lk * 2u + (ei_flag(info, l) ? 0u : 1u) : (unsigned)lk;
+            }
+            tt.push_back({w, list, e, l});
+          }
+    for (int e = t0; e < t1; ++e) eslot[e] = kNoTask | kNoTask << 10 | kNoTask << 20;
+    auto set_slot = [&](int e, int l, unsigned ti) {
+      eslot[e] = (eslot[e] & ~(kNoTask << (10 * l))) | ti << (10 * l);
+    };
+    for (size_t i = 0; i < tt.size(); ++i) set_slot(tt[i].el, tt[i].led, (unsigned)i);
+    for (int e = t0; e < t1; ++e)  // shared edges inside the tile: the in side's task
+      for (int l = 0; l < 3; ++l) {
+        const unsigned info = einfo[e];
+        if (ei_kind(info, l) != kInterior || ei_flag(info, l)) continue;
+        const int nb = link[(size_t)l * ne + e];
+        if (nb < t0 || nb >= t1) continue;
+        set_slot(e, l, (eslot[nb] >> (10 * ei_nled(info, l))) & kNoTask);
+      }
+    for (const Task& k : tt) {
+      tasks.push_back(k.word);
+      tasks.push_back(k.list);
+    }
+    halo.insert(halo.end(), hl.begin(), hl.end());
+    task_ptr[t + 1] = task_ptr[t] + (int)tt.size();
+    halo_ptr[t + 1] = halo_ptr[t] + (int)hl.size();
+    max_halo = std::max(max_halo, (int)hl.size());
+    max_tasks = std::max(max_tasks, (int)tt.size());
+  }
+  if (max_halo + kTile > 512 || max_tasks >= (int)kNoTask)
+    throw Failure(DGSWEM_ERR_ARG, "stage tile plan exceeds the task word's slot range");
+  h->tile_task_ptr.upload(task_ptr);
+  h->tile_halo_ptr.upload(halo_ptr);
+  h->tile_tasks.upload(tasks.empty() ? std::vector<unsigned>(2, 0u) : tasks);
+  h->tile_halo.upload(halo.empty() ? std::vector<int>(1, 0) : halo);
+  h->eslot.upload(eslot);
+  h->mesh.max_halo = max_halo;
+  h->mesh.max_tasks = max_tasks;
+  h->stage_smem = stage_layout(max_halo, std::max(max_tasks, 1)).bytes;
+  int dev_smem = 0;
+  DG_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+  if (h->stage_smem > (size_t)dev_smem)
+    throw Failure(DGSWEM_ERR_ARG, "stage tile needs " + std::to_string(h->stage_smem) +
+                                      " bytes of shared memory, the device allows " + std::to_string(dev_smem));
+}
+
 void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   const int ne = s->ne, np = s->np, ned = s->nedges;
   auto need = [](bool ok, const char* what) {
@@ -289,7 +391,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   if (s->nfeds) mark(s->nfedn, s->nfeds, kFlow);
   if (s->nreds) mark(s->nredn, s->nreds, kRadiation);
   if (s->nebseg) mark(s->nebsegn, s->nebseg, kEBarrier);
-  std::vector<int> ib_elem(2 * (size_t)std::max(s->nibseg, 1), 0), ib_led(2 * (size_t)std::max(s->nibseg, 1), 0);
+  std::vector<int> ib_elem(2 * (size_t)std::max(s->nibseg, 1), -1), ib_led(2 * (size_t)std::max(s->nibseg, 1), 0);
   for (int L = 0; L < s->nibseg; ++L) {
     int gb = s->nibsegn[2 * L], gf = s->nibsegn[2 * L + 1];
     if (gf == 0) continue;  // no opposite edge: the reference skips the segment
@@ -343,23 +445,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     for (int slot = 0; slot < 3; ++slot) info |= (unsigned)key[slot].second << (18 + 2 * slot);
     einfo[e] = info;
   }
-  // tasks per stage tile (same ownership rule as stage_p1): boundary edges
-  // of the listed kinds, edges to another tile, shared edges once
-  for (int t0 = 0; t0 < ne; t0 += kStageBlock) {
-    const int t1 = std::min(ne, t0 + kStageBlock);
-    int n = 0;
-    for (int e = t0; e < t1; ++e)
-      for (int l = 0; l < 3; ++l) {
-        const unsigned kind = ei_kind(einfo[e], l);
-        if (kind == kNone || kind == kIBarrier) continue;
-        if (kind == kInterior) {
-          const int nb = link[(size_t)l * ne + e];
-          if (nb >= t0 && nb < t1 && !ei_flag(einfo[e], l)) continue;
-        }
-        ++n;
-      }
-    h->max_tasks = std::max(h->max_tasks, n);
-  }
+  build_tile_plan(h, ne, link, einfo);
   // node -> element star, element order
   std::vector<int> sp(np + 1, 0), st(3 * (size_t)ne);
   for (int e = 0; e < ne; ++e)
@@ -400,6 +486,37 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   if (s->load_manning) {
     need(s->manning != nullptr, "load_manning set without ManningsN");
     h->manning.upload(std::vector<double>(s->manning, s->manning + np));
+  }
+  // element geometry table (EGeo rows): the reference's formulas evaluated
+  // once, in the same order as the oracle, instead of every stage
+  {
+    std::vector<double> eg((size_t)EGeo::kRows * ne, 0.0);
+    auto at = [&](int r, int e) -> double& { return eg[(size_t)r * ne + e]; };
+    for (int e = 0; e < ne; ++e) {
+      double xs[3], ys[3];
+      for (int v = 0; v < 3; ++v) {
+        xs[v] = s->x[nm[(size_t)v * ne + e]];
+        ys[v] = s->y[nm[(size_t)v * ne + e]];
+      }
+      const double areas = (xs[0] - xs[2]) * (ys[1] - ys[2]) + (xs[2] - xs[1]) * (ys[0] - ys[2]);
+      at(EGeo::kAreas, e) = areas;
+      for (int l = 0; l < 3; ++l) {
+        const int a = (l + 1) % 3, b = (l + 2) % 3;
+        const double dy = ys[b] - ys[a], dx = xs[b] - xs[a];
+        const double len = std::sqrt(dy * dy + dx * dx);
+        at(EGeo::kXlen + l, e) = len;
+        at(EGeo::kNx + l, e) = (ys[b] - ys[a]) / len;
+        at(EGeo::kNy + l, e) = -(xs[b] - xs[a]) / len;
+      }
+      const double area = areas * 0.5;
+      at(EGeo::kDrdx, e) = 1.0 / area * (ys[2] - ys[0]);
+      at(EGeo::kDsdx, e) = 1.0 / area * (ys[0] - ys[1]);
+      at(EGeo::kDrdy, e) = 1.0 / area * (xs[0] - xs[2]);
+      at(EGeo::kDsdy, e) = 1.0 / area * (xs[1] - xs[0]);
+      if (s->load_manning)
+        at(EGeo::kNbar, e) = (s->manning[nm[e]] + s->manning[nm[(size_t)ne + e]] + s->manning[nm[(size_t)2 * ne + e]]) / 3.;
+    }
+    h->egeo.upload(eg);
   }
   if (s->ics == 2) {  // SFAC_ELEM / SFACED (prep_DG.F:1055-1100), host cos
     const BasisP1 B = make_basis_p1();
@@ -446,14 +563,20 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     h->ibht.upload(std::vector<double>(s->ibht, s->ibht + s->nibseg));
     h->ibcfsb.upload(std::vector<double>(s->ibcfsb, s->ibcfsb + s->nibseg));
     h->ibcfsp.upload(std::vector<double>(s->ibcfsp, s->ibcfsp + s->nibseg));
+    h->ib_rhs.alloc(18 * (size_t)s->nibseg);
   }
   MeshView& m = h->mesh;
   m.ne = ne;
   m.np = np;
   m.x = h->x.p; m.y = h->y.p; m.dp = h->dp.p; m.nm = h->nm.p; m.link = h->link.p; m.einfo = h->einfo.p;
-  m.hb = h->hb.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
+  m.hb = h->hb.p; m.egeo = h->egeo.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
   m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
   m.star_ptr = h->star_ptr.p; m.star = h->star.p;
+  m.tile_task_ptr = h->tile_task_ptr.p;
+  m.tile_tasks = reinterpret_cast<const uint2*>(h->tile_tasks.p);
+  m.tile_halo_ptr = h->tile_halo_ptr.p;
+  m.tile_halo = h->tile_halo.p;
+  m.eslot = h->eslot.p;
   m.needs = s->needs; m.nfeds = s->nfeds; m.nebseg = s->nebseg; m.nibseg = s->nibseg;
   m.nbfr = h->amig.empty() ? 0 : nbfr;
   m.nffr = h->famig.empty() ? 0 : nffr;
@@ -544,11 +667,17 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
   A.wsx = h->wsx.p;
   A.wsy = h->wsy.p;
   A.pr = h->pr.p;
+  A.ib_rhs = h->ib_rhs.p;
   A.err = h->err.p;
+  const bool nonlin = h->ph.nleq == 1.0 && h->ph.leq == 0.0;
+  if (h->mesh.nibseg > 0) {
+    LaunchTimer t(h, 3);
+    h->v->ibarrier(A, nonlin, h->stream);
+    t.done();
+  }
   {
     LaunchTimer t(h, 0);
-    h->v->stage(A, h->ph.nleq == 1.0 && h->ph.leq == 0.0, grid_for(ne, kStageBlock),
-                h->v->stage_smem(h->max_tasks), h->stream);
+    h->v->stage(A, nonlin, grid_for(ne, kTile), h->stage_smem, h->stream);
     t.done();
   }
   const bool wetdry = h->nolifa >= 2;
@@ -684,6 +813,7 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
     p.leq = s->leq;
     p.nleqg = s->nleq * s->g;
     p.fg_l = s->leq * s->g;
+    p.tau_cap = .9 * (1.0 / s->dtdp);
     p.cf = s->cf;
     p.hbreak = s->hbreak;
     p.ftheta = s->ftheta;

@@ -8,6 +8,10 @@
 //                      or index into the boundary list of that edge's kind
 //   einfo[e]           packed edge kinds, processing order, orientation bits
 //   hb[k*NE + e]       bathymetry modes HB(k,e)
+//   stage tile plan    per tile of kTile consecutive elements: its edge tasks
+//                      (uint2 each, interior edges first, then boundary kinds)
+//                      and its halo (out-of-tile neighbours, global ids);
+//                      eslot[e] names the task of each local edge
 // Geometry (areas, Jacobian, edge lengths and normals) is recomputed from the
 // nodal coordinates each stage, with the reference's formulas, instead of
 // streaming the reference's per-element tables (XFAC/YFAC/SRFAC/BATHED: ~100
@@ -60,6 +64,7 @@ struct MeshView {
   const int* __restrict__ link;
   const unsigned* __restrict__ einfo;
   const double* __restrict__ hb;
+  const double* __restrict__ egeo;      // [r*NE + e] element geometry rows (EGeo)
   const double* __restrict__ cori;      // per element, or null (uniform)
   const double* __restrict__ fric;      // per element, or null (uniform)
   const double* __restrict__ manning;   // nodal, or null
@@ -80,10 +85,72 @@ struct MeshView {
   const double* __restrict__ ibht;
   const double* __restrict__ ibcfsb;
   const double* __restrict__ ibcfsp;
+  // stage tile plan (built once at create from the edge graph)
+  int max_halo, max_tasks;                // largest halo / task list of a tile
+  const int* __restrict__ tile_task_ptr;  // [ntile+1] offsets into tile_tasks
+  const uint2* __restrict__ tile_tasks;   // TaskBits word, list index
+  const int* __restrict__ tile_halo_ptr;  // [ntile+1] offsets into tile_halo
+  const int* __restrict__ tile_halo;      // global element ids, ascending
+  const unsigned* __restrict__ eslot;     // task of local edge l: bits 10l..10l+9
 };
+
+// Stage tiles: kTile consecutive elements per block of kStageThreads.
+constexpr int kTile = 128;
+constexpr int kStageThreads = 256;
+constexpr unsigned kNoTask = 1023u;
+
+// Task word of the tile plan.  Slots index the tile's shared-memory element
+// rows: 0..kTile-1 the tile's own elements, kTile+j halo element j.
+struct TaskBits {
+  static constexpr int kKind = 0;     // 3 bits, EdgeKind
+  static constexpr int kLedIn = 3;    // 2 bits, local edge of the in side
+  static constexpr int kLedEx = 5;    // 2 bits, local edge of the ex side
+  static constexpr int kFlip = 7;     // the in side is a halo element: normal = -(ex side's normal)
+  static constexpr int kInSlot = 8;   // 9 bits
+  static constexpr int kExSlot = 17;  // 9 bits
+};
+
+// Rows of the element geometry table, computed once at create from the
+// nodal coordinates with the reference's formulas (read_input.F:1406 AREAS,
+// calc_normal.F:41-48 XLEN and normals on the counter-clockwise local edges,
+// rhs_dg_hydro.F's DRDX/DSDX/DRDY/DSDY from the area and the coordinate
+// differences) and the element mean of the nodal Manning n.
+struct EGeo {
+  static constexpr int kAreas = 0, kXlen = 1, kNx = 4, kNy = 7, kDrdx = 10, kDsdx = 11, kDrdy = 12, kDsdy = 13;
+  static constexpr int kNbar = 14, kRows = 15;
+};
+
+// Dynamic shared memory of the stage kernel (byte offsets).  Per-element
+// rows of geo: the EGeo rows copied from the table (same order), then the
+// hybrid friction factor and XLEN/AREAS per local edge.
+struct SGeo {
+  static constexpr int kHyb = EGeo::kRows, kEdfac = EGeo::kRows + 1;
+};
+constexpr int kGeoRows = EGeo::kRows + 4;
+constexpr int kVolRows = 8;  // per area point: fx fy gx gy hx hy sx sy
+struct StageLayout {
+  unsigned qs, geo, vol, res, wd, gid, tdry, info, bytes;
+};
+__host__ __device__ inline unsigned align16(unsigned x) { return (x + 15u) & ~15u; }
+__host__ __device__ inline StageLayout stage_layout(int max_halo, int max_tasks) {
+  StageLayout L;
+  const unsigned S = kTile + (unsigned)max_halo;
+  const unsigned T = (unsigned)max_tasks;
+  L.qs = align16((unsigned)sizeof(BasisP1));
+  L.geo = L.qs + 12u * S * 8u;                 // qs[12][S]: ZE, QX, QY, HB modes
+  L.vol = L.geo + kGeoRows * kTile * 8u;       // geo[kGeoRows][kTile]
+  L.res = L.vol + kVolRows * 3u * kTile * 8u;  // vol[kVolRows][3][kTile]
+  L.wd = L.res + 15u * T * 8u;                 // res[task][point][5]
+  L.gid = align16(L.wd + S * 4u);              // wd[S]
+  L.tdry = align16(L.gid + (unsigned)max_halo * 4u);
+  L.info = align16(L.tdry + T * 4u);          // einfo, eslot of the tile's elements
+  L.bytes = align16(L.info + 2u * kTile * 4u);
+  return L;
+}
 
 struct Physics {
   double g, h0, dtdp, nleq, leq, nleqg, fg_l;
+  double tau_cap;  // .9 * (1 / DTDP), the friction cap of rhs_dg_hydro.F
   double cori, fric, cf, hbreak, ftheta, fgamma;
   int iflinbf, ifhybf, ifnlfa, nws, rainfall, ics;
 };
@@ -105,6 +172,7 @@ struct StageArgs {
   const double* __restrict__ wsx;           // nodal met forcing (already ramped), or null
   const double* __restrict__ wsy;
   const double* __restrict__ pr;
+  double* ib_rhs;                           // [(2*seg + side)*9 + c] internal-barrier terms
   unsigned* err;                            // device error word
 };
 
@@ -124,8 +192,8 @@ struct LimitArgs {
 #define DGSWEM_DECLARE_LAUNCHERS(NS)                                                           \
   namespace NS {                                                                               \
   void set_basis(const BasisP1& b);                                                            \
-  size_t stage_smem(int max_tasks);                                                            \
   void launch_stage(const StageArgs& a, bool nonlin, unsigned grid, size_t smem, cudaStream_t s); \
+  void launch_ibarrier(const StageArgs& a, bool nonlin, cudaStream_t s);                       \
   void launch_node_minmax(const LimitArgs& a, unsigned grid, cudaStream_t s);                  \
   void launch_limit_wetdry(const LimitArgs& a, unsigned grid, cudaStream_t s);                 \
   void launch_modal2nodal(const MeshView& m, const double* q, const int* wd, double nleq,      \
@@ -140,7 +208,6 @@ struct LimitArgs {
 DGSWEM_DECLARE_LAUNCHERS(fast)
 DGSWEM_DECLARE_LAUNCHERS(strict)
 
-constexpr int kStageBlock = 128;
 constexpr int kPointBlock = 256;
 
 }  // namespace dgswem

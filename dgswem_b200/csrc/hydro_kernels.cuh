@@ -20,6 +20,30 @@ namespace DGSWEM_VARIANT {
 
 __constant__ BasisP1 cBasis;
 
+// Asynchronous global -> shared copies (cp.async, completion by
+// cp.async.wait_all): the data goes straight to shared memory.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// DEPTH**(1.D0/3.D0) of the Manning friction (rhs_dg_hydro.F).  The strict
+// variant calls pow with the reference's exponent; the fast variant takes
+// the cube root, which differs from it by less than an ulp's worth of the
+// exponent's rounding (1/3 is not a double) and costs a fraction of pow.
+__device__ __forceinline__ double cube_root(double x) {
+#ifdef DGSWEM_FAST_MATH
+  return cbrt(x);
+#else
+  return pow(x, 1.0 / 3.0);
+#endif
+}
+
 struct Flux3 {
   double f, g, h;
 };
@@ -268,474 +292,456 @@ __device__ __noinline__ void ibarrier_side(const StageArgs& A, int seg, int side
   }
 }
 
+// Internal-barrier sides of one stage, one thread per (segment, side), into
+// ib_rhs[(2*seg + side)*9 + c]; the stage kernel adds them at the edge's
+// place in each element's sum.  Runs before stage_p1 on the same stream
+// (both only read the stage's input state).  Segments without an opposite
+// edge (ib_elem < 0) are skipped, as in the reference.
+template <bool kNonlin>
+__global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ StageArgs A) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= 2 * A.m.nibseg) return;
+  const int seg = w >> 1, side = w & 1;
+  if (A.m.ib_elem[2 * seg] < 0) return;
+  ibarrier_side<kNonlin>(A, seg, side, A.ib_rhs + (size_t)w * 9);
+}
+
 // ---------------------------------------------------------------------------
-// Tile stage kernel.  A block owns kStageBlock consecutive elements and runs
-// three phases separated by barriers:
-//   1. per element: modal state, bathymetry and geometry into shared memory;
-//      a block-wide prefix sum turns the edges this tile evaluates (boundary
-//      edges, edges to elements of other tiles, and shared interior edges
-//      once, from the reference's "in" element NEDEL(1)) into a dense task list;
-//   2. per (task, Lobatto point): one LLF evaluation in the reference's own
-//      in/ex orientation with its dry-side rules -> F, G_in, H_in, G_ex, H_ex;
-//   3. per element: edge contributions in the reference's order (boundary
-//      edges, then interior edges in edge-number order, the slot sum of
-//      add_internal_flux), rain, volume integral, SSP combination.
+// Tile stage kernel.  Block b owns the kTile consecutive elements starting at
+// b*kTile and the part of the tile plan built for them at create: the edge
+// tasks the tile evaluates (boundary edges, edges to out-of-tile elements,
+// shared interior edges once) and the halo of out-of-tile neighbours those
+// tasks read.  Four phases separated by barriers, each spread over all
+// kStageThreads threads:
+//   1. tile and halo elements: modal state, bathymetry modes and wet/dry flag
+//      into shared memory; tile elements also their geometry;
+//   2. one thread per task: the three Lobatto points of an edge in the
+//      reference's own in/ex orientation with its dry-side rules ->
+//      F, G_in, H_in, G_ex, H_ex per point (internal-barrier sides come
+//      from ibarrier_sides);
+//   3. one thread per (element, area point): volume fluxes and sources;
+//   4. one thread per (element, variable): the three modes of that variable
+//      summed in the reference's order (boundary edges, interior edges in
+//      edge-number order as the slot sum of add_internal_flux, rain, area
+//      points), then the SSP combination.
 // internal_edge_hydro.F, *_edge_hydro.F, rhs_dg_hydro.F, DG_hydro_timestep.F:238-290
 // ---------------------------------------------------------------------------
 
 // resident stage blocks per SM the register allocation targets
 #ifndef DGSWEM_STAGE_MIN_BLOCKS
-#define DGSWEM_STAGE_MIN_BLOCKS 4
+#define DGSWEM_STAGE_MIN_BLOCKS 2
 #endif
 
-// task word layout (int4 .x); .y in-side element, .z ex-side element or list
-struct TaskBits {
-  static constexpr int kKind = 0;      // 3 bits
-  static constexpr int kInLocal = 3;   // in-side element is in this tile
-  static constexpr int kExLocal = 4;   // ex-side element is in this tile
-  static constexpr int kLedIn = 5;     // 2 bits
-  static constexpr int kLedEx = 7;     // 2 bits
-  static constexpr int kFlip = 9;      // owner is the ex side: normal = -owner's normal
-  static constexpr int kOwner = 10;    // 8 bits, owner's local index
-  static constexpr int kOwnerLed = 18; // 2 bits
-};
-
-struct TileShared {
-  BasisP1 B;
-  double q[12][kStageBlock];    // ZE, QX, QY modes and HB modes
-  double geo[14][kStageBlock];  // AREAS; per local edge XLEN, nx, ny; y3-y1, y1-y2, x1-x3, x2-x1
-  int wd[kStageBlock];
-  int task_of[3][kStageBlock];
-  int warp_sum[kStageBlock / 32];
-  int ntask;
-};
-
-// dynamic shared memory: TileShared, then the task list (int4 each), then
-// 15 doubles of results per task
-constexpr size_t kTaskOffset = (sizeof(TileShared) + 15) / 16 * 16;
-__host__ __device__ constexpr size_t stage_shared_bytes(int max_tasks) {
-  return kTaskOffset + (size_t)(max_tasks + 1) * (sizeof(int4) + 15 * sizeof(double));
-}
-
-// One point of a tile task: (modal state of a side, its local edge, point)
-__device__ __forceinline__ void side_trace(const TileShared& S, const StageArgs& A, bool local, int el, int led,
-                                           int gp, double& z, double& u, double& v, double& h) {
-  const double p1 = S.B.phi_edge[led][gp][1], p2 = S.B.phi_edge[led][gp][2];
-  const int ne = A.m.ne;
-  if (local) {
-    z = S.q[0][el] + S.q[1][el] * p1 + S.q[2][el] * p2;
-    u = S.q[3][el] + S.q[4][el] * p1 + S.q[5][el] * p2;
-    v = S.q[6][el] + S.q[7][el] * p1 + S.q[8][el] * p2;
-    h = S.q[9][el] + S.q[10][el] * p1 + S.q[11][el] * p2;
-  } else {
-    const double* q = A.qin;
-    z = q[el] + q[(size_t)ne + el] * p1 + q[(size_t)2 * ne + el] * p2;
-    u = q[(size_t)3 * ne + el] + q[(size_t)4 * ne + el] * p1 + q[(size_t)5 * ne + el] * p2;
-    v = q[(size_t)6 * ne + el] + q[(size_t)7 * ne + el] * p1 + q[(size_t)8 * ne + el] * p2;
-    const double* hb = A.m.hb;
-    h = hb[el] + hb[(size_t)ne + el] * p1 + hb[(size_t)2 * ne + el] * p2;
-  }
+// Trace at edge point (led, gp) of the 12 modal rows (ZE, QX, QY, HB) of
+// shared-memory slot `slot`; mode 0 of the basis is 1 on every edge point.
+__device__ __forceinline__ void slot_trace(const BasisP1& B, const double* qs, int S, int slot, int led, int gp,
+                                           double& z, double& u, double& v, double& h) {
+  const double p1 = B.phi_edge[led][gp][1], p2 = B.phi_edge[led][gp][2];
+  const double* q = qs + slot;
+  z = q[0] + q[S] * p1 + q[2 * S] * p2;
+  u = q[3 * S] + q[4 * S] * p1 + q[5 * S] * p2;
+  v = q[6 * S] + q[7 * S] * p1 + q[8 * S] * p2;
+  h = q[9 * S] + q[10 * S] * p1 + q[11 * S] * p2;
 }
 
 template <bool kNonlin>
-__global__ void __launch_bounds__(kStageBlock, DGSWEM_STAGE_MIN_BLOCKS) stage_p1(const __grid_constant__ StageArgs A) {
+__global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_p1(const __grid_constant__ StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TileShared& S = *reinterpret_cast<TileShared*>(smem_raw);
-  int4* tasks = reinterpret_cast<int4*>(smem_raw + kTaskOffset);
   const MeshView& m = A.m;
   const Physics& P = A.ph;
   const int ne = m.ne;
   const int tid = threadIdx.x;
-  const int tile0 = blockIdx.x * kStageBlock;
-  const int e = tile0 + tid;
-  const bool valid = e < ne;
-  const int ntile = min(kStageBlock, ne - tile0);
+  const int tile = blockIdx.x;
+  const int tile0 = tile * kTile;
+  const int n = min(kTile, ne - tile0);
+  const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
+  const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
+  const StageLayout L = stage_layout(m.max_halo, m.max_tasks);
+  const int S = kTile + m.max_halo;  // row stride of qs and wd
+  BasisP1& B = *reinterpret_cast<BasisP1*>(smem_raw);
+  double* qs = reinterpret_cast<double*>(smem_raw + L.qs);
+  double* geo = reinterpret_cast<double*>(smem_raw + L.geo);
+  double* vol = reinterpret_cast<double*>(smem_raw + L.vol);
+  double* res = reinterpret_cast<double*>(smem_raw + L.res);
+  int* wds = reinterpret_cast<int*>(smem_raw + L.wd);
+  int* gid = reinterpret_cast<int*>(smem_raw + L.gid);
+  int* tdry = reinterpret_cast<int*>(smem_raw + L.tdry);
+  unsigned* sinfo = reinterpret_cast<unsigned*>(smem_raw + L.info);  // [einfo | eslot][kTile]
   {
     const double* src = reinterpret_cast<const double*>(&cBasis);
-    double* dst = reinterpret_cast<double*>(&S.B);
-    for (int i = tid; i < (int)(sizeof(BasisP1) / sizeof(double)); i += blockDim.x) dst[i] = src[i];
+    double* dst = reinterpret_cast<double*>(&B);
+    for (int i = tid; i < (int)(sizeof(BasisP1) / sizeof(double)); i += kStageThreads) dst[i] = src[i];
   }
 
-  // ---- phase 1: element data, ownership, dense task list ----
-  unsigned info = 0u;
-  int link[3] = {-1, -1, -1};
-  int own[3] = {0, 0, 0};
-  int nown = 0;
-  if (valid) {
-#pragma unroll
-    for (int c = 0; c < 9; ++c) S.q[c][tid] = A.qin[(size_t)c * ne + e];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) S.q[9 + k][tid] = m.hb[(size_t)k * ne + e];
-    S.wd[tid] = A.wd[e];
-    double xs[3], ys[3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) {
-      const int nd = m.nm[(size_t)v * ne + e];
-      xs[v] = m.x[nd];
-      ys[v] = m.y[nd];
-    }
-    // AREAS (read_input.F:1406); XLEN and normals (calc_normal.F:41-48) on
-    // this element's counter-clockwise edges
-    S.geo[0][tid] = (xs[0] - xs[2]) * (ys[1] - ys[2]) + (xs[2] - xs[1]) * (ys[0] - ys[2]);
-#pragma unroll
-    for (int l = 0; l < 3; ++l) {
-      const int a = (l + 1) % 3, b = (l + 2) % 3;
-      const double dy = ys[b] - ys[a], dx = xs[b] - xs[a];
-      const double len = sqrt(dy * dy + dx * dx);
-      S.geo[1 + 3 * l][tid] = len;
-      S.geo[2 + 3 * l][tid] = (ys[b] - ys[a]) / len;
-      S.geo[3 + 3 * l][tid] = -(xs[b] - xs[a]) / len;
-    }
-    S.geo[10][tid] = ys[2] - ys[0];
-    S.geo[11][tid] = ys[0] - ys[1];
-    S.geo[12][tid] = xs[0] - xs[2];
-    S.geo[13][tid] = xs[1] - xs[0];
-    info = m.einfo[e];
-#pragma unroll
-    for (int l = 0; l < 3; ++l) {
-      link[l] = m.link[(size_t)l * ne + e];
-      const unsigned kind = ei_kind(info, l);
-      if (kind == kNone || kind == kIBarrier) continue;
-      if (kind == kInterior) {
-        const bool nbr_local = link[l] >= tile0 && link[l] < tile0 + ntile;
-        own[l] = (!nbr_local || ei_flag(info, l)) ? 1 : 0;
-      } else {
-        own[l] = 1;
-      }
-      nown += own[l];
-    }
+  // ---- phase 1: tile and halo elements into shared memory ----
+  // Asynchronous global->shared copies (cp.async), no register staging:
+  // halo element j by thread j (one index load, then its 13 values), the
+  // tile's rows (state, bathymetry, geometry table, flags) by all threads,
+  // consecutive threads on consecutive elements of a row.
+  int hg = -1;
+  if (tid < nh) {
+    hg = m.tile_halo[hbeg + tid];
+    gid[tid] = hg;
   }
-  // block exclusive scan of the owned-task counts
-  const int lane = tid & 31, warp = tid >> 5;
-  int incl = nown;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, incl, d);
-    if (lane >= d) incl += t;
-  }
-  if (lane == 31) S.warp_sum[warp] = incl;
-  __syncthreads();
-  int base = incl - nown;
-  for (int w = 0; w < warp; ++w) base += S.warp_sum[w];
-  if (tid == blockDim.x - 1) S.ntask = base + nown;
-  if (valid) {
-#pragma unroll
-    for (int l = 0; l < 3; ++l) {
-      S.task_of[l][tid] = -1;
-      if (!own[l]) continue;
-      const unsigned kind = ei_kind(info, l);
-      int4 t;
-      unsigned fl = kind;
-      fl |= (unsigned)tid << TaskBits::kOwner;
-      fl |= (unsigned)l << TaskBits::kOwnerLed;
-      if (kind == kInterior) {
-        const int nb = link[l];
-        const bool nbr_local = nb >= tile0 && nb < tile0 + ntile;
-        const unsigned nled = ei_nled(info, l);
-        if (ei_flag(info, l)) {  // this element is NEDEL(1): the in side
-          fl |= 1u << TaskBits::kInLocal;
-          fl |= (unsigned)l << TaskBits::kLedIn;
-          fl |= nled << TaskBits::kLedEx;
-          if (nbr_local) fl |= 1u << TaskBits::kExLocal;
-          t.y = tid;
-          t.z = nbr_local ? nb - tile0 : nb;
-        } else {                 // the neighbour (another tile) is the in side
-          fl |= 1u << TaskBits::kExLocal;
-          fl |= nled << TaskBits::kLedIn;
-          fl |= (unsigned)l << TaskBits::kLedEx;
-          fl |= 1u << TaskBits::kFlip;
-          t.y = nb;
-          t.z = tid;
-        }
+  {
+    const int ngeo = m.manning ? EGeo::kRows : EGeo::kNbar;
+    const int nrows = 12 + ngeo;
+    for (int it = tid; it < nrows * kTile; it += kStageThreads) {
+      const int r = it / kTile, w = it - r * kTile;
+      if (w >= n) continue;
+      const double* src;
+      double* dst;
+      if (r < 9) {
+        src = A.qin + (size_t)r * ne;
+        dst = qs + r * S;
+      } else if (r < 12) {
+        src = m.hb + (size_t)(r - 9) * ne;
+        dst = qs + r * S;
       } else {
-        fl |= 1u << TaskBits::kInLocal;
-        fl |= (unsigned)l << TaskBits::kLedIn;
-        t.y = tid;
-        t.z = link[l];
+        src = m.egeo + (size_t)(r - 12) * ne;
+        dst = geo + (r - 12) * kTile;
       }
-      t.x = (int)fl;
-      t.w = 0;
-      S.task_of[l][tid] = base;
-      tasks[base] = t;
-      ++base;
+      cp_async8(dst + w, src + tile0 + w);
     }
+    for (int it = tid; it < 3 * kTile; it += kStageThreads) {
+      const int r = it / kTile, w = it - r * kTile;
+      if (w >= n) continue;
+      if (r == 0)
+        cp_async4(wds + w, A.wd + tile0 + w);
+      else
+        cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
+    }
+    for (int j = tid; j < nh; j += kStageThreads) {
+      const int g = j == tid ? hg : m.tile_halo[hbeg + j];
+      if (j != tid) gid[j] = g;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) cp_async8(qs + c * S + kTile + j, A.qin + (size_t)c * ne + g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) cp_async8(qs + (9 + k) * S + kTile + j, m.hb + (size_t)k * ne + g);
+      cp_async4(wds + kTile + j, A.wd + g);
+    }
+    cp_async_wait_all();
   }
   __syncthreads();
-  if (valid) {  // shared interior edges: read the owner's task
+
+  // per-element factors used by phases 3 and 4 (visible after the next barrier)
+  if (tid < n) {
+    const double areas = geo[EGeo::kAreas * kTile + tid];
 #pragma unroll
     for (int l = 0; l < 3; ++l)
-      if (ei_kind(info, l) == kInterior && !own[l])
-        S.task_of[l][tid] = S.task_of[ei_nled(info, l)][link[l] - tile0];
+      geo[(SGeo::kEdfac + l) * kTile + tid] = geo[(EGeo::kXlen + l) * kTile + tid] / areas;
+    if (P.iflinbf == 0 && P.ifhybf == 1) {  // hybrid friction factor, from the element-mean depth
+      const double depth_c = qs[9 * S + tid] + qs[tid];
+      const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
+      geo[SGeo::kHyb * kTile + tid] = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
+    }
   }
 
-  // ---- phase 2: one LLF per (task, point) ----
-  double* res = reinterpret_cast<double*>(tasks + S.ntask + (S.ntask & 1));  // [task][point][5]
-  const int nwork = 3 * S.ntask;
-  for (int w = tid; w < nwork; w += blockDim.x) {
-    const int ti = w / 3, I = w - 3 * ti;
-    const int4 t = tasks[ti];
-    const unsigned fl = (unsigned)t.x;
+  // ---- phase 2: one thread per edge task, three Lobatto points ----
+  for (int w = tid; w < ntask; w += kStageThreads) {
+    const uint2 tk = m.tile_tasks[tbeg + w];
+    const unsigned fl = tk.x;
     const unsigned kind = fl & 7u;
-    const bool in_local = (fl >> TaskBits::kInLocal) & 1u, ex_local = (fl >> TaskBits::kExLocal) & 1u;
+    double* out = res + (size_t)w * 15;
+    if (kind == kIBarrier) continue;  // ibarrier_sides, launched before this kernel
+    const int sin = (fl >> TaskBits::kInSlot) & 511, sex = (fl >> TaskBits::kExSlot) & 511;
     const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
-    const int owner = (fl >> TaskBits::kOwner) & 255, oled = (fl >> TaskBits::kOwnerLed) & 3;
-    double nx = S.geo[2 + 3 * oled][owner], ny = S.geo[3 + 3 * oled][owner];
-    if ((fl >> TaskBits::kFlip) & 1u) { nx = -nx; ny = -ny; }
-    const int wd_in = in_local ? S.wd[t.y] : A.wd[t.y];
-    const int gin = in_local ? tile0 + t.y : t.y;  // global ids for the ics=2 tables
-    double* out = res + ((size_t)ti * 3 + I) * 5;
+    const bool flip = (fl >> TaskBits::kFlip) & 1u;
+    const int owner = flip ? sex : sin, oled = flip ? led_ex : led_in;
+    double nx = geo[(EGeo::kNx + oled) * kTile + owner], ny = geo[(EGeo::kNy + oled) * kTile + owner];
+    if (flip) { nx = -nx; ny = -ny; }
+    const int wd_in = wds[sin];
+    // global ids for the ics=2 tables
+    const int gin = sin < kTile ? tile0 + sin : gid[sin - kTile];
     if (kind == kInterior) {
-      const int wd_ex = ex_local ? S.wd[t.z] : A.wd[t.z];
-      if (wd_in == 0 && wd_ex == 0) continue;
-      const int gp_in = I, gp_ex = 2 - I;
-      double zi, xi, yi, hi, zx, xx, yx, hx;
-      side_trace(S, A, in_local, t.y, led_in, gp_in, zi, xi, yi, hi);
-      side_trace(S, A, ex_local, t.z, led_ex, gp_ex, zx, xx, yx, hx);
-      const int gex = ex_local ? tile0 + t.z : t.z;
-      const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
-      const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
-      Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
-      double F = f.f, gi = f.g, hi2 = f.h, gx = f.g, hx2 = f.h;
-      // internal_edge_hydro.F:212-302: mass flux out of / into a dry element
-      if (fabs(f.f) > 1.0e-8 && (wd_in == 0 || wd_ex == 0)) {
-        const double tx = -ny, ty = nx;
-        if (wd_in == 0) {
-          if (f.f > 0.0) {
-            const double qne = xx * nx + yx * ny, qte = xx * tx + yx * ty;
-            const double qni = -qne, qti = qte, den = nx * ty - ny * tx;
-            const double qxi = (ty * qni - ny * qti) / den, qyi = (-tx * qni + nx * qti) / den;
-            Flux3 r = llf<kNonlin>(P, zx, zx, qxi, xx, qyi, yx, hx, hx, sfx, sfx, nx, ny, P.g);
-            F = r.f; gx = r.g; hx2 = r.h; gi = 0.0; hi2 = 0.0;
-          } else {
-            Flux3 r = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, 0.0);
-            gi = r.g; hi2 = r.h;
+      const int wd_ex = wds[sex];
+      const int dry = wd_in == 0 && wd_ex == 0;
+      tdry[w] = dry;
+      if (dry) continue;
+      const int gex = sex < kTile ? tile0 + sex : gid[sex - kTile];
+#pragma unroll 1
+      for (int I = 0; I < 3; ++I) {
+        const int gp_in = I, gp_ex = 2 - I;
+        double zi, xi, yi, hi, zx, xx, yx, hx;
+        slot_trace(B, qs, S, sin, led_in, gp_in, zi, xi, yi, hi);
+        slot_trace(B, qs, S, sex, led_ex, gp_ex, zx, xx, yx, hx);
+        const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
+        const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
+        Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
+        double F = f.f, gi = f.g, hi2 = f.h, gx = f.g, hx2 = f.h;
+        // internal_edge_hydro.F:212-302: mass flux out of / into a dry
+        // element.  The four cases re-evaluate the flux once with changed
+        // arguments: the dry side's state replaced by the wet side's with
+        // reflected momentum (outflow from a dry element), or gravity off
+        // (G = 0) for the dry side's momentum flux.
+        if (fabs(f.f) > 1.0e-8 && (wd_in == 0 || wd_ex == 0)) {
+          const double tx = -ny, ty = nx, den = nx * ty - ny * tx;
+          const bool in_dry = wd_in == 0;
+          const bool reflect = in_dry ? f.f > 0.0 : f.f < 0.0;
+          // the wet side, whose momentum is reflected onto the dry side
+          const double qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
+          const double qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
+          const double qnr = -qnw, qtr = qtw;
+          const double qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
+          double a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
+          double a_hi = hi, a_hx = hx, a_si = sfi, a_sx = sfx, a_g = 0.0;
+          if (reflect) {
+            a_g = P.g;
+            if (in_dry) {
+              a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_si = sfx;
+            } else {
+              a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_sx = sfi;
+            }
           }
-        } else {
-          if (f.f < 0.0) {
-            const double qni = xi * nx + yi * ny, qti = xi * tx + yi * ty;
-            const double qne = -qni, qte = qti, den = nx * ty - ny * tx;
-            const double qxe = (ty * qne - ny * qte) / den, qye = (-tx * qne + nx * qte) / den;
-            Flux3 r = llf<kNonlin>(P, zi, zi, xi, qxe, yi, qye, hi, hi, sfi, sfi, nx, ny, P.g);
-            F = r.f; gi = r.g; hi2 = r.h; gx = 0.0; hx2 = 0.0;
+          const Flux3 r = llf<kNonlin>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_si, a_sx, nx, ny, a_g);
+          if (reflect) {
+            F = r.f;
+            if (in_dry) { gx = r.g; hx2 = r.h; gi = 0.0; hi2 = 0.0; }
+            else        { gi = r.g; hi2 = r.h; gx = 0.0; hx2 = 0.0; }
           } else {
-            Flux3 r = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, 0.0);
-            gx = r.g; hx2 = r.h;
+            if (in_dry) { gi = r.g; hi2 = r.h; }
+            else        { gx = r.g; hx2 = r.h; }
           }
         }
+        double* o = out + 5 * I;
+        o[0] = F; o[1] = gi; o[2] = hi2; o[3] = gx; o[4] = hx2;
       }
-      out[0] = F; out[1] = gi; out[2] = hi2; out[3] = gx; out[4] = hx2;
     } else {
       if (wd_in == 0) continue;
-      double zi, xi, yi, hi, zx, xx, yx;
-      side_trace(S, A, true, t.y, led_in, I, zi, xi, yi, hi);
-      const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
-      ghost_state(A, S.B, kind, t.z, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
-      Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
-      out[0] = f.f; out[1] = f.g; out[2] = f.h;
+#pragma unroll 1
+      for (int I = 0; I < 3; ++I) {
+        double zi, xi, yi, hi, zx, xx, yx;
+        slot_trace(B, qs, S, sin, led_in, I, zi, xi, yi, hi);
+        const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
+        ghost_state(A, B, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
+        Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
+        double* o = out + 5 * I;
+        o[0] = f.f; o[1] = f.g; o[2] = f.h;
+      }
     }
   }
   __syncthreads();
-  if (!valid) return;
 
-  // ---- phase 3: accumulate in the reference's order, volume, SSP ----
-  const BasisP1& B = S.B;
-  const int wde = S.wd[tid];
-  const double areas = S.geo[0][tid];
-  double rhs[9], isum[9];
-#pragma unroll
-  for (int c = 0; c < 9; ++c) { rhs[c] = 0.0; isum[c] = 0.0; }
-#pragma unroll 1
-  for (int s = 0; s < 3; ++s) {
-    const int l = ei_order(info, s);
-    const unsigned kind = ei_kind(info, l);
-    if (kind == kNone) continue;
-    if (kind == kIBarrier) {
-      double o[9];
-      ibarrier_side<kNonlin>(A, link[l], (int)ei_flag(info, l) ? 0 : 1, o);
-#pragma unroll
-      for (int c = 0; c < 9; ++c) rhs[c] = rhs[c] + o[c];
-      continue;
-    }
-    const double xlen = S.geo[1 + 3 * l][tid];
-    const double* r = res + (size_t)S.task_of[l][tid] * 15;
-    if (kind == kInterior) {
-      const int nb = link[l];
-      const bool nbr_local = nb >= tile0 && nb < tile0 + ntile;
-      const int wdn = nbr_local ? S.wd[nb - tile0] : A.wd[nb];
-      if (wde == 0 && wdn == 0) continue;
-      const bool is_in = ei_flag(info, l) != 0;
-      const double edfac = xlen / areas;
-      double acc[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) acc[c] = 0.0;
-#pragma unroll 1
-      for (int I = 0; I < 3; ++I) {
-        const int j = is_in ? I : 2 - I;
-        const double* p = r + 5 * I;
-        const double F = p[0], Gm = is_in ? p[1] : p[3], Hm = is_in ? p[2] : p[4];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const double w = edfac * B.edgeq[l][j][k];
-          if (is_in) {  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
-            acc[k] = acc[k] - w * F;
-            acc[3 + k] = acc[3 + k] - w * Gm;
-            acc[6 + k] = acc[6 + k] - w * Hm;
-          } else {      // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
-            acc[k] = acc[k] + w * F;
-            acc[3 + k] = acc[3 + k] + w * Gm;
-            acc[6 + k] = acc[6 + k] + w * Hm;
-          }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 9; ++c) isum[c] = isum[c] + acc[c];
-    } else {
-      if (wde == 0) continue;
-#pragma unroll 1
-      for (int I = 0; I < 3; ++I) {
-        const double* p = r + 5 * I;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const double w = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
-          rhs[k] = rhs[k] - w * p[0];
-          rhs[3 + k] = rhs[3 + k] - w * p[1];
-          rhs[6 + k] = rhs[6 + k] - w * p[2];
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < 9; ++c) rhs[c] = rhs[c] + isum[c];  // add_internal_flux
-
-  double q[9], hbe[3];
-#pragma unroll
-  for (int c = 0; c < 9; ++c) q[c] = S.q[c][tid];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) hbe[k] = S.q[9 + k][tid];
-
+  // ---- phase 3: volume fluxes and sources per (element, area point) ----
   // rhs_dg_hydro.F:58-470
-  const double area = areas * 0.5;
-  const double drdx = 1.0 / area * S.geo[10][tid];
-  const double dsdx = 1.0 / area * S.geo[11][tid];
-  const double drdy = 1.0 / area * S.geo[12][tid];
-  const double dsdy = 1.0 / area * S.geo[13][tid];
-  int nd[3];
+  for (int w = tid; w < 3 * kTile; w += kStageThreads) {
+    const int i = w / kTile, el = w - i * kTile;
+    if (el >= n) continue;
+    const int wde = wds[el];
+    if (wde == 0) continue;
+    const int e = tile0 + el;
+    double q[9], hbe[3];
 #pragma unroll
-  for (int v = 0; v < 3; ++v) nd[v] = m.nm[(size_t)v * ne + e];
-  double xfac[3][3], yfac[3][3];  // [mode][point]
+    for (int c = 0; c < 9; ++c) q[c] = qs[c * S + el];
 #pragma unroll
-  for (int k = 0; k < 3; ++k)
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const double dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
-      const double dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
-      xfac[k][i] = B.m_inv[k] * B.wagp[i] * dpx;
-      yfac[k][i] = B.m_inv[k] * B.wagp[i] * dpy;
-    }
-  if (P.rainfall == 1) {
-    const double src = 7.0556e-6;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + B.m_inv[k] * B.wagp[i] * B.phi_area[k][i] * src;
-  }
-  if (wde != 0) {
+    for (int k = 0; k < 3; ++k) hbe[k] = qs[(9 + k) * S + el];
+    const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+    const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
     const double NLEQ = kNonlin ? 1.0 : P.nleq, LEQ = kNonlin ? 0.0 : P.leq;
-    const double depth_c = hbe[0] + q[0];
-    const double fh_c = 1.0 / (kNonlin ? depth_c : NLEQ * depth_c + LEQ);
     const double cori = m.cori ? m.cori[e] : P.cori;
     double fric = m.fric ? m.fric[e] : P.fric;
-    double nbar = 0.0;
-    if (m.manning) nbar = (m.manning[nd[0]] + m.manning[nd[1]] + m.manning[nd[2]]) / 3.;
-    double dpsidx[3] = {0, 0, 0}, dpsidy[3] = {0, 0, 0};
+    double zq = q[0], uq = q[3], vq = q[6];
+    const double hq = hbe[0] * B.phi_area[0][i] + hbe[1] * B.phi_area[1][i] + hbe[2] * B.phi_area[2][i];
+    double dhx = 0.0, dhy = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      dhx = dhx + hbe[k] * (B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx);
+      dhy = dhy + hbe[k] * (B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy);
+    }
+    zq = zq + q[1] * B.phi_area[1][i] + q[2] * B.phi_area[2][i];
+    uq = uq + q[4] * B.phi_area[1][i] + q[5] * B.phi_area[2][i];
+    vq = vq + q[7] * B.phi_area[1][i] + q[8] * B.phi_area[2][i];
+    const double depth = zq + hq;
+    const double sfq = m.sfac_area ? m.sfac_area[(size_t)i * ne + e] : 1.0;
+    const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
+    const double fx = uq * f1 * sfq, fy = vq * f1;
+    const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
+    const double fg = P.nleqg * zq * wde;
+    const double fh = 1.0 / (kNonlin ? depth : NLEQ * depth + LEQ);
+    const double u = uq * fh, v = vq * fh;
+    const double huu = fu * u, hvv = fv * v, huv = fu * v;
+    const double gh2 = kNonlin ? fg * (0.5 * zq + hq) : fg * (0.5 * zq + hq) + P.fg_l * zq;
+    const double gx = (huu + gh2) * sfq, gy = huv;
+    const double hx = huv * sfq, hy = hvv + gh2;
+    if (m.manning) {
+      const double nbar = geo[EGeo::kNbar * kTile + el];
+      fric = P.g * (nbar * nbar) / cube_root(depth);
+      if (fric < P.cf) fric = P.cf;
+    }
+    double tau = fric;
+    if (P.iflinbf == 0) {
+      const double umag = sqrt(u * u + v * v);
+      tau = tau * umag * fh;
+      if (P.ifhybf == 1) tau = tau * geo[SGeo::kHyb * kTile + el];
+      tau = fmin(tau, P.tau_cap);
+    }
+    double sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
+    double sy = -(tau * vq) + fg * dhy - cori * uq;
     if (P.nws != 0) {
+      // met_forcing.F:49-66: the nodal fields are scaled by the ramp each stage
       const double drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
+      double dpsidx[3], dpsidy[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
         dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
       }
+      const double fw = 1.0 / f1, r = A.rampdg;
+      const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
+      const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
+      const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];
+      const double p0 = r * A.pr[n0], p1 = r * A.pr[n1], p2 = r * A.pr[n2];
+      sx = sx + fw * (wx0 * B.psi[0][i] + wx1 * B.psi[1][i] + wx2 * B.psi[2][i]) -
+           P.g * sfq * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
+      sy = sy + fw * (wy0 * B.psi[0][i] + wy1 * B.psi[1][i] + wy2 * B.psi[2][i]) -
+           P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
     }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      double zq = q[0], uq = q[3], vq = q[6];
-      const double hq = hbe[0] * B.phi_area[0][i] + hbe[1] * B.phi_area[1][i] + hbe[2] * B.phi_area[2][i];
-      double dhx = 0.0, dhy = 0.0;
+    double* vo = vol + i * kTile + el;
+    vo[0 * 3 * kTile] = fx;
+    vo[1 * 3 * kTile] = fy;
+    vo[2 * 3 * kTile] = gx;
+    vo[3 * 3 * kTile] = gy;
+    vo[4 * 3 * kTile] = hx;
+    vo[5 * 3 * kTile] = hy;
+    vo[6 * 3 * kTile] = sx;
+    vo[7 * 3 * kTile] = sy;
+  }
+  __syncthreads();
+
+  // ---- phase 4: per (element, variable) sums in the reference's order, SSP ----
+  for (int w = tid; w < 3 * kTile; w += kStageThreads) {
+    const int var = w / kTile, el = w - var * kTile;
+    if (el >= n) continue;
+    const int e = tile0 + el;
+    // SSP terms of stage 1 (DG_hydro_timestep.F:238-290) fetched first so
+    // that their latency overlaps the sums below; the combination itself
+    // keeps the reference's order
+    const bool hist0 = A.irk > 1;
+    double h0q[3] = {0.0, 0.0, 0.0}, h0r[3] = {0.0, 0.0, 0.0};
+    if (hist0) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        dhx = dhx + hbe[k] * (B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx);
-        dhy = dhy + hbe[k] * (B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy);
-      }
-      zq = zq + q[1] * B.phi_area[1][i] + q[2] * B.phi_area[2][i];
-      uq = uq + q[4] * B.phi_area[1][i] + q[5] * B.phi_area[2][i];
-      vq = vq + q[7] * B.phi_area[1][i] + q[8] * B.phi_area[2][i];
-      const double depth = zq + hq;
-      const double sfq = m.sfac_area ? m.sfac_area[(size_t)i * ne + e] : 1.0;
-      const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
-      const double fx = uq * f1 * sfq, fy = vq * f1;
-      const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
-      const double fg = P.nleqg * zq * wde;
-      const double fh = 1.0 / (kNonlin ? depth : NLEQ * depth + LEQ);
-      const double u = uq * fh, v = vq * fh;
-      const double huu = fu * u, hvv = fv * v, huv = fu * v;
-      const double gh2 = kNonlin ? fg * (0.5 * zq + hq) : fg * (0.5 * zq + hq) + P.fg_l * zq;
-      const double gx = (huu + gh2) * sfq, gy = huv;
-      const double hx = huv * sfq, hy = hvv + gh2;
-      if (m.manning) {
-        fric = P.g * (nbar * nbar) / pow(depth, 1.0 / 3.0);
-        if (fric < P.cf) fric = P.cf;
-      }
-      double tau = fric;
-      if (P.iflinbf == 0) {
-        const double umag = sqrt(u * u + v * v);
-        tau = tau * umag * fh;
-        if (P.ifhybf == 1) tau = tau * pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
-        tau = fmin(tau, .9 * (1.0 / P.dtdp));
-      }
-      double sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
-      double sy = -(tau * vq) + fg * dhy - cori * uq;
-      if (P.nws != 0) {
-        // met_forcing.F:49-66: the nodal fields are scaled by the ramp each stage
-        const double fw = 1.0 / f1, r = A.rampdg;
-        const int n0 = nd[0], n1 = nd[1], n2 = nd[2];
-        const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
-        const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];
-        const double p0 = r * A.pr[n0], p1 = r * A.pr[n1], p2 = r * A.pr[n2];
-        sx = sx + fw * (wx0 * B.psi[0][i] + wx1 * B.psi[1][i] + wx2 * B.psi[2][i]) -
-             P.g * sfq * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
-        sy = sy + fw * (wy0 * B.psi[0][i] + wy1 * B.psi[1][i] + wy2 * B.psi[2][i]) -
-             P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
-      }
-      const double sr0 = B.m_inv[0] * B.wagp[i] * B.phi_area[0][i];
-      rhs[3] = rhs[3] + sr0 * sx;
-      rhs[6] = rhs[6] + sr0 * sy;
-#pragma unroll
-      for (int k = 1; k < 3; ++k) {
-        const double sr = B.m_inv[k] * B.wagp[i] * B.phi_area[k][i];
-        rhs[k] = rhs[k] + xfac[k][i] * fx + yfac[k][i] * fy;
-        rhs[3 + k] = rhs[3 + k] + xfac[k][i] * gx + yfac[k][i] * gy + sr * sx;
-        rhs[6 + k] = rhs[6 + k] + xfac[k][i] * hx + yfac[k][i] * hy + sr * sy;
+        const size_t c = (size_t)(3 * var + k) * ne + e;
+        if (A.a[0] != 0.0) h0q[k] = A.qhist[0][c];
+        if (A.b[0] != 0.0) h0r[k] = A.rhist[0][c];
       }
     }
-  }
-  if (A.rout) {
+    const unsigned info = sinfo[el], slots = sinfo[kTile + el];
+    const int wde = wds[el];
+    double rhs[3] = {0.0, 0.0, 0.0}, isum[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-    for (int c = 0; c < 9; ++c) A.rout[(size_t)c * ne + e] = rhs[c];
-  }
-  // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
-  bool bad = false;
+    for (int s = 0; s < 3; ++s) {
+      const int l = ei_order(info, s);
+      const unsigned kind = ei_kind(info, l);
+      if (kind == kNone) continue;
+      const int ti = (slots >> (10 * l)) & kNoTask;
+      const double* r = res + (size_t)ti * 15;
+      if (kind == kIBarrier) {
+        const double* o = A.ib_rhs + (size_t)m.tile_tasks[tbeg + ti].y * 9;
 #pragma unroll
-  for (int c = 0; c < 9; ++c) {
-    double acc = 0.0;
-    for (int I = 0; I < A.irk; ++I) {
-      const bool cur = I == A.irk - 1;
-      if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? q[c] : A.qhist[I][(size_t)c * ne + e]);
-      if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rhs[c] : A.rhist[I][(size_t)c * ne + e]);
+        for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + o[3 * var + k];
+        continue;
+      }
+      if (kind == kInterior) {
+        if (tdry[ti]) continue;
+        const bool is_in = ei_flag(info, l) != 0;
+        const int comp = var == 0 ? 0 : (is_in ? var : var + 2);
+        const double edfac = geo[(SGeo::kEdfac + l) * kTile + el];
+        double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int I = 0; I < 3; ++I) {
+          const int j = is_in ? I : 2 - I;
+          const double val = r[5 * I + comp];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const double wk = edfac * B.edgeq[l][j][k];
+            if (is_in)  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
+              acc[k] = acc[k] - wk * val;
+            else        // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
+              acc[k] = acc[k] + wk * val;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) isum[k] = isum[k] + acc[k];
+      } else {
+        if (wde == 0) continue;
+        const double areas = geo[EGeo::kAreas * kTile + el];
+        const double xlen = geo[(EGeo::kXlen + l) * kTile + el];
+#pragma unroll
+        for (int I = 0; I < 3; ++I) {
+          const double val = r[5 * I + var];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const double wk = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
+            rhs[k] = rhs[k] - wk * val;
+          }
+        }
+      }
     }
-    bad = bad || isnan(acc);
-    A.qout[(size_t)c * ne + e] = acc;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + isum[k];  // add_internal_flux
+    if (var == 0 && P.rainfall == 1) {
+      const double src = 7.0556e-6;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + B.m_inv[k] * B.wagp[i] * B.phi_area[k][i] * src;
+    }
+    if (wde != 0) {
+      const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+      const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
+      // flux pair of this variable: (fx, fy), (gx, gy) or (hx, hy); source sx / sy
+      const double* vx = vol + (2 * var) * 3 * kTile + el;
+      const double* vy = vx + 3 * kTile;
+      const double* vs = vol + (var == 2 ? 7 : 6) * 3 * kTile + el;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double a = vx[i * kTile], b = vy[i * kTile];
+        if (var != 0) {
+          const double sr0 = B.m_inv[0] * B.wagp[i] * B.phi_area[0][i];
+          rhs[0] = rhs[0] + sr0 * vs[i * kTile];
+        }
+#pragma unroll
+        for (int k = 1; k < 3; ++k) {
+          const double dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
+          const double dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
+          const double xf = B.m_inv[k] * B.wagp[i] * dpx;
+          const double yf = B.m_inv[k] * B.wagp[i] * dpy;
+          if (var == 0) {
+            rhs[k] = rhs[k] + xf * a + yf * b;
+          } else {
+            const double sr = B.m_inv[k] * B.wagp[i] * B.phi_area[k][i];
+            rhs[k] = rhs[k] + xf * a + yf * b + sr * vs[i * kTile];
+          }
+        }
+      }
+    }
+    // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int c = 3 * var + k;
+      if (A.rout) A.rout[(size_t)c * ne + e] = rhs[k];
+      const double qc = qs[c * S + el];
+      double acc = 0.0;
+      if (hist0) {
+        if (A.a[0] != 0.0) acc = acc + A.a[0] * h0q[k];
+        if (A.b[0] != 0.0) acc = acc + A.b[0] * h0r[k];
+      }
+      for (int I = 1; I < A.irk; ++I) {
+        const bool cur = I == A.irk - 1;
+        if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc : A.qhist[I][(size_t)c * ne + e]);
+        if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rhs[k] : A.rhist[I][(size_t)c * ne + e]);
+      }
+      if (!hist0) {  // stage 1: the current stage is I = 0
+        if (A.a[0] != 0.0) acc = acc + A.a[0] * qc;
+        if (A.b[0] != 0.0) acc = acc + A.b[0] * rhs[k];
+      }
+      bad = bad || isnan(acc);
+      A.qout[(size_t)c * ne + e] = acc;
+    }
+    if (bad) atomicOr(A.err, 1u);
   }
-  if (bad) atomicOr(A.err, 1u);
 }
 
 // slopelimiter.F:3300-3404: min/max of element means over each node's star
