@@ -86,6 +86,12 @@ static BasisP1 make_basis_p1() {
     }
   const double vx[3] = {-1.0, 1.0, -1.0}, vy[3] = {-1.0, -1.0, 1.0};
   for (int v = 0; v < 3; ++v) p1_basis(vx[v], vy[v], B.phi_corner[v], nullptr, nullptr);
+  // products the kernels form left to right, M_INV * WAGP (* PHI_AREA)
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i) {
+      B.mw[k][i] = B.m_inv[k] * B.wagp[i];
+      B.srfac[k][i] = B.m_inv[k] * B.wagp[i] * B.phi_area[k][i];
+    }
   return B;
 }
 
@@ -181,7 +187,8 @@ struct dgswem_cuda {
   DevBuf<double> x, y, dp, hb, egeo, cori, fric, manning, sfac_area, sfac_edge;
   DevBuf<int> nm, link, star_ptr, star, ib_elem, ib_led;
   DevBuf<unsigned> einfo, eslot, tile_tasks;
-  DevBuf<int> tile_task_ptr, tile_halo_ptr, tile_halo;
+  DevBuf<int> tile_elem_ptr, tile_task_ptr, tile_halo_ptr, tile_halo;
+  int ntile = 0;
   DevBuf<double> emo_dg, efa_dg, qnam_dg, qnph_dg, ebht, ebcfsp, ibht, ibcfsb, ibcfsp;
   DevBuf<double> wsx, wsy, pr, minmax, staging;
   std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
@@ -268,7 +275,36 @@ unsigned grid_for(int n, int block) { return (unsigned)((n + block - 1) / block)
 // Tasks: interior edges in element order, then the boundary kinds grouped, so
 // that a warp's tasks mostly take one branch.
 void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const std::vector<unsigned>& einfo) {
-  const int ntile = (ne + kTile - 1) / kTile;
+  // Tiles: consecutive elements, at most kTile of them and at most
+  // kStageThreads edge tasks (one pass of the block over its tasks).  An
+  // element adds a task per listed boundary edge and per interior edge whose
+  // neighbour is not already in the tile.
+  std::vector<int> elem_ptr(1, 0);
+  {
+    int t0 = 0, count = 0;
+    for (int e = 0; e < ne; ++e) {
+      int add = 0;
+      for (int l = 0; l < 3; ++l) {
+        const unsigned kind = ei_kind(einfo[e], l);
+        if (kind == kNone) continue;
+        if (kind == kInterior) {
+          const int nb = link[(size_t)l * ne + e];
+          if (nb >= t0 && nb < e) continue;
+        }
+        ++add;
+      }
+      if (e - t0 == kTile || count + add > kStageThreads) {
+        elem_ptr.push_back(e);
+        t0 = e;
+        count = 0;
+        e -= 1;  // recount the element against the new tile
+        continue;
+      }
+      count += add;
+    }
+    elem_ptr.push_back(ne);
+  }
+  const int ntile = (int)elem_ptr.size() - 1;
   std::vector<int> task_ptr(ntile + 1, 0), halo_ptr(ntile + 1, 0), halo;
   std::vector<unsigned> tasks;  // (word, list) pairs
   std::vector<unsigned> eslot(ne, 0u);
@@ -280,7 +316,7 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
   std::vector<Task> tt;
   int max_halo = 0, max_tasks = 0;
   for (int t = 0; t < ntile; ++t) {
-    const int t0 = t * kTile, t1 = std::min(ne, t0 + kTile);
+    const int t0 = elem_ptr[t], t1 = elem_ptr[t + 1];
     hl.clear();
     for (int e = t0; e < t1; ++e)
       for (int l = 0; l < 3; ++l)
@@ -344,6 +380,8 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
   }
   if (max_halo + kTile > 512 || max_tasks >= (int)kNoTask)
     throw Failure(DGSWEM_ERR_ARG, "stage tile plan exceeds the task word's slot range");
+  h->ntile = ntile;
+  h->tile_elem_ptr.upload(elem_ptr);
   h->tile_task_ptr.upload(task_ptr);
   h->tile_halo_ptr.upload(halo_ptr);
   h->tile_tasks.upload(tasks.empty() ? std::vector<unsigned>(2, 0u) : tasks);
@@ -572,6 +610,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   m.hb = h->hb.p; m.egeo = h->egeo.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
   m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
   m.star_ptr = h->star_ptr.p; m.star = h->star.p;
+  m.tile_elem_ptr = h->tile_elem_ptr.p;
   m.tile_task_ptr = h->tile_task_ptr.p;
   m.tile_tasks = reinterpret_cast<const uint2*>(h->tile_tasks.p);
   m.tile_halo_ptr = h->tile_halo_ptr.p;
@@ -677,7 +716,7 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
   }
   {
     LaunchTimer t(h, 0);
-    h->v->stage(A, nonlin, grid_for(ne, kTile), h->stage_smem, h->stream);
+    h->v->stage(A, nonlin, (unsigned)h->ntile, h->stage_smem, h->stream);
     t.done();
   }
   const bool wetdry = h->nolifa >= 2;

@@ -8,7 +8,7 @@
 //                      or index into the boundary list of that edge's kind
 //   einfo[e]           packed edge kinds, processing order, orientation bits
 //   hb[k*NE + e]       bathymetry modes HB(k,e)
-//   stage tile plan    per tile of kTile consecutive elements: its edge tasks
+//   stage tile plan    per tile of up to kTile consecutive elements: its edge tasks
 //                      (uint2 each, interior edges first, then boundary kinds)
 //                      and its halo (out-of-tile neighbours, global ids);
 //                      eslot[e] names the task of each local edge
@@ -53,6 +53,8 @@ struct BasisP1 {
   double phi_corner[3][3];   // [vertex][mode]
   double psi[3][3];          // [vertex][area point] linear nodal basis
   double m_inv[3], wagp[3], wegp[3], xegp[3];
+  double mw[3][3];           // [mode][point] M_INV*WAGP
+  double srfac[3][3];        // [mode][point] M_INV*WAGP*PHI_AREA (SRFAC without the area)
 };
 
 struct MeshView {
@@ -87,6 +89,7 @@ struct MeshView {
   const double* __restrict__ ibcfsp;
   // stage tile plan (built once at create from the edge graph)
   int max_halo, max_tasks;                // largest halo / task list of a tile
+  const int* __restrict__ tile_elem_ptr;  // [ntile+1] first element of each tile
   const int* __restrict__ tile_task_ptr;  // [ntile+1] offsets into tile_tasks
   const uint2* __restrict__ tile_tasks;   // TaskBits word, list index
   const int* __restrict__ tile_halo_ptr;  // [ntile+1] offsets into tile_halo
@@ -94,9 +97,16 @@ struct MeshView {
   const unsigned* __restrict__ eslot;     // task of local edge l: bits 10l..10l+9
 };
 
-// Stage tiles: kTile consecutive elements per block of kStageThreads.
-constexpr int kTile = 128;
-constexpr int kStageThreads = 256;
+// Stage tiles: up to kTile consecutive elements and kStageThreads edge tasks
+// per block of kStageThreads.
+#ifndef DGSWEM_TILE
+#define DGSWEM_TILE 128
+#endif
+#ifndef DGSWEM_STAGE_THREADS
+#define DGSWEM_STAGE_THREADS 256
+#endif
+constexpr int kTile = DGSWEM_TILE;
+constexpr int kStageThreads = DGSWEM_STAGE_THREADS;
 constexpr unsigned kNoTask = 1023u;
 
 // Task word of the tile plan.  Slots index the tile's shared-memory element

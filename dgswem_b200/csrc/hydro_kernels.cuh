@@ -105,8 +105,12 @@ __device__ __forceinline__ Flux3 llf(const Physics& P, double ze_in, double ze_e
   const double ci = sqrt(G * ht_in * (ny * ny + nxsi * nxsi));
   const double une = kNonlin ? ue * nx + ve * ny : (ue * nx + ve * ny) * NLEQ;
   const double ce = sqrt(G * ht_ex * (ny * ny + nxse * nxse));
-  const double eig = fmax(fmax(fmax(fabs(uni + ci), fabs(uni)), fmax(fabs(uni - ci), fabs(une + ce))),
-                          fmax(fabs(une), fabs(une - ce)));
+  // max(|un+c|, |un|, |un-c|) over both sides.  For c >= 0 the rounded
+  // |un| + c equals the rounded larger of |un + c| and |un - c| exactly, so
+  // fmax(|un| + c, |un|) is the same value; with c = NaN (negative depth) both
+  // forms reduce to |un|, as fmax skips NaN operands.
+  const double ai = fabs(uni), ae = fabs(une);
+  const double eig = fmax(fmax(ai + ci, ai), fmax(ae + ce, ae));
   Flux3 r;
   r.f = f1a - 0.5 * eig * j1;
   if (kNonlin) {
@@ -307,8 +311,8 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 }
 
 // ---------------------------------------------------------------------------
-// Tile stage kernel.  Block b owns the kTile consecutive elements starting at
-// b*kTile and the part of the tile plan built for them at create: the edge
+// Tile stage kernel.  Block b owns tile b of the tile plan built at create:
+// up to kTile consecutive elements, and for them the edge
 // tasks the tile evaluates (boundary edges, edges to out-of-tile elements,
 // shared interior edges once) and the halo of out-of-tile neighbours those
 // tasks read.  Four phases separated by barriers, each spread over all
@@ -344,6 +348,240 @@ __device__ __forceinline__ void slot_trace(const BasisP1& B, const double* qs, i
   h = q[9 * S] + q[10 * S] * p1 + q[11 * S] * p2;
 }
 
+// Phase 3 of the stage kernel for area point I of tile element el (global
+// id e): volume fluxes and sources (rhs_dg_hydro.F:58-470) into
+// vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  C: the basis
+// tables in shared memory (I is a runtime index).
+template <bool kNonlin>
+__device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& C, const double* qs, int S,
+                                             const double* geo, double* vol, int I, int el, int e) {
+  const MeshView& m = A.m;
+  const Physics& P = A.ph;
+  const int ne = m.ne;
+  const int wde = 1;  // phase 3 runs for wet elements only
+  double q[9], hbe[3];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) q[c] = qs[c * S + el];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) hbe[k] = qs[(9 + k) * S + el];
+  const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+  const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
+  const double NLEQ = kNonlin ? 1.0 : P.nleq, LEQ = kNonlin ? 0.0 : P.leq;
+  const double cori = m.cori ? m.cori[e] : P.cori;
+  double fric = m.fric ? m.fric[e] : P.fric;
+  double zq = q[0], uq = q[3], vq = q[6];
+  const double hq = hbe[0] * C.phi_area[0][I] + hbe[1] * C.phi_area[1][I] + hbe[2] * C.phi_area[2][I];
+  double dhx = 0.0, dhy = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    dhx = dhx + hbe[k] * (C.drphi[k][I] * drdx + C.dsphi[k][I] * dsdx);
+    dhy = dhy + hbe[k] * (C.drphi[k][I] * drdy + C.dsphi[k][I] * dsdy);
+  }
+  zq = zq + q[1] * C.phi_area[1][I] + q[2] * C.phi_area[2][I];
+  uq = uq + q[4] * C.phi_area[1][I] + q[5] * C.phi_area[2][I];
+  vq = vq + q[7] * C.phi_area[1][I] + q[8] * C.phi_area[2][I];
+  const double depth = zq + hq;
+  const double sfq = m.sfac_area ? m.sfac_area[(size_t)I * ne + e] : 1.0;
+  const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
+  const double fx = uq * f1 * sfq, fy = vq * f1;
+  const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
+  const double fg = P.nleqg * zq * wde;
+  const double fh = 1.0 / (kNonlin ? depth : NLEQ * depth + LEQ);
+  const double u = uq * fh, v = vq * fh;
+  const double huu = fu * u, hvv = fv * v, huv = fu * v;
+  const double gh2 = kNonlin ? fg * (0.5 * zq + hq) : fg * (0.5 * zq + hq) + P.fg_l * zq;
+  const double gx = (huu + gh2) * sfq, gy = huv;
+  const double hx = huv * sfq, hy = hvv + gh2;
+  if (m.manning) {
+    const double nbar = geo[EGeo::kNbar * kTile + el];
+    fric = P.g * (nbar * nbar) / cube_root(depth);
+    if (fric < P.cf) fric = P.cf;
+  }
+  double tau = fric;
+  if (P.iflinbf == 0) {
+    const double umag = sqrt(u * u + v * v);
+    tau = tau * umag * fh;
+    if (P.ifhybf == 1) tau = tau * geo[SGeo::kHyb * kTile + el];
+    tau = fmin(tau, P.tau_cap);
+  }
+  double sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
+  double sy = -(tau * vq) + fg * dhy - cori * uq;
+  if (P.nws != 0) {
+    // met_forcing.F:49-66: the nodal fields are scaled by the ramp each stage
+    const double drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
+    double dpsidx[3], dpsidy[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
+      dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
+    }
+    const double fw = 1.0 / f1, r = A.rampdg;
+    const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
+    const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
+    const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];
+    const double p0 = r * A.pr[n0], p1 = r * A.pr[n1], p2 = r * A.pr[n2];
+    sx = sx + fw * (wx0 * C.psi[0][I] + wx1 * C.psi[1][I] + wx2 * C.psi[2][I]) -
+         P.g * sfq * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
+    sy = sy + fw * (wy0 * C.psi[0][I] + wy1 * C.psi[1][I] + wy2 * C.psi[2][I]) -
+         P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
+  }
+  double* vo = vol + I * kTile + el;
+  vo[0 * 3 * kTile] = fx;
+  vo[1 * 3 * kTile] = fy;
+  vo[2 * 3 * kTile] = gx;
+  vo[3 * 3 * kTile] = gy;
+  vo[4 * 3 * kTile] = hx;
+  vo[5 * 3 * kTile] = hy;
+  vo[6 * 3 * kTile] = sx;
+  vo[7 * 3 * kTile] = sy;
+}
+
+// Phase 4 of the stage kernel for variable V of tile element el (global id
+// e): the right-hand side of the variable's three modes summed in the
+// reference's order -- boundary edges, interior edges in edge-number order
+// (the slot sum of add_internal_flux), rain, area points -- then the SSP
+// combination (DG_hydro_timestep.F:238-290) written to qout.  B is the
+// shared-memory copy of the basis (runtime-indexed tables), cBasis the
+// constant-memory one (indices fixed by unrolled loops); V is the same for a
+// whole warp.
+template <bool kNonlin>
+__device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& B, const double* qs, int S,
+                                             const double* geo, const double* vol, const double* res,
+                                             const int* tdry, const unsigned* sinfo, const int* wds, int tbeg,
+                                             int V, int el, int e) {
+  const BasisP1& C = cBasis;
+  const MeshView& m = A.m;
+  const Physics& P = A.ph;
+  const int ne = m.ne;
+  // SSP terms of stage 1 fetched first so that their latency overlaps the
+  // sums below; the combination keeps the reference's order
+  const bool hist0 = A.irk > 1;
+  double h0q[3] = {0.0, 0.0, 0.0}, h0r[3] = {0.0, 0.0, 0.0};
+  if (hist0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const size_t c = (size_t)(3 * V + k) * ne + e;
+      if (A.a[0] != 0.0) h0q[k] = A.qhist[0][c];
+      if (A.b[0] != 0.0) h0r[k] = A.rhist[0][c];
+    }
+  }
+  const unsigned info = sinfo[el], slots = sinfo[kTile + el];
+  const int wde = wds[el];
+  double rhs[3] = {0.0, 0.0, 0.0}, isum[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int l = ei_order(info, s);
+    const unsigned kind = ei_kind(info, l);
+    if (kind == kNone) continue;
+    const int ti = (slots >> (10 * l)) & kNoTask;
+    const double* r = res + (size_t)ti * 15;
+    if (kind == kIBarrier) {
+      const double* o = A.ib_rhs + (size_t)m.tile_tasks[tbeg + ti].y * 9;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + o[3 * V + k];
+      continue;
+    }
+    if (kind == kInterior) {
+      if (tdry[ti]) continue;
+      const bool is_in = ei_flag(info, l) != 0;
+      const int comp = V == 0 ? 0 : (is_in ? V : V + 2);
+      const double edfac = geo[(SGeo::kEdfac + l) * kTile + el];
+      double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int I = 0; I < 3; ++I) {
+        const int j = is_in ? I : 2 - I;
+        const double val = r[5 * I + comp];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const double wk = edfac * B.edgeq[l][j][k];
+          if (is_in)  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
+            acc[k] = acc[k] - wk * val;
+          else        // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
+            acc[k] = acc[k] + wk * val;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) isum[k] = isum[k] + acc[k];
+    } else {
+      if (wde == 0) continue;
+      const double areas = geo[EGeo::kAreas * kTile + el];
+      const double xlen = geo[(EGeo::kXlen + l) * kTile + el];
+#pragma unroll
+      for (int I = 0; I < 3; ++I) {
+        const double val = r[5 * I + V];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const double wk = 2.0 * C.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * C.wegp[I];
+          rhs[k] = rhs[k] - wk * val;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + isum[k];  // add_internal_flux
+  if (V == 0 && P.rainfall == 1) {
+    const double src = 7.0556e-6;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + C.srfac[k][i] * src;
+  }
+  if (wde != 0) {
+    const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+    const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
+    // flux pair of this variable: (fx, fy), (gx, gy) or (hx, hy); source sx / sy
+    const double* vx = vol + (2 * V) * 3 * kTile + el;
+    const double* vy = vx + 3 * kTile;
+    const double* vs = vol + (V == 2 ? 7 : 6) * 3 * kTile + el;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double a = vx[i * kTile], b = vy[i * kTile];
+      if (V != 0) {
+        const double sr0 = C.srfac[0][i];
+        rhs[0] = rhs[0] + sr0 * vs[i * kTile];
+      }
+#pragma unroll
+      for (int k = 1; k < 3; ++k) {
+        const double dpx = C.drphi[k][i] * drdx + C.dsphi[k][i] * dsdx;
+        const double dpy = C.drphi[k][i] * drdy + C.dsphi[k][i] * dsdy;
+        const double xf = C.mw[k][i] * dpx;
+        const double yf = C.mw[k][i] * dpy;
+        if (V == 0) {
+          rhs[k] = rhs[k] + xf * a + yf * b;
+        } else {
+          const double sr = C.srfac[k][i];
+          rhs[k] = rhs[k] + xf * a + yf * b + sr * vs[i * kTile];
+        }
+      }
+    }
+  }
+  // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
+  bool bad = false;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int c = 3 * V + k;
+    if (A.rout) A.rout[(size_t)c * ne + e] = rhs[k];
+    const double qc = qs[c * S + el];
+    double acc = 0.0;
+    if (hist0) {
+      if (A.a[0] != 0.0) acc = acc + A.a[0] * h0q[k];
+      if (A.b[0] != 0.0) acc = acc + A.b[0] * h0r[k];
+    }
+    for (int I = 1; I < A.irk; ++I) {
+      const bool cur = I == A.irk - 1;
+      if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc : A.qhist[I][(size_t)c * ne + e]);
+      if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rhs[k] : A.rhist[I][(size_t)c * ne + e]);
+    }
+    if (!hist0) {  // stage 1: the current stage is I = 0
+      if (A.a[0] != 0.0) acc = acc + A.a[0] * qc;
+      if (A.b[0] != 0.0) acc = acc + A.b[0] * rhs[k];
+    }
+    bad = bad || isnan(acc);
+    A.qout[(size_t)c * ne + e] = acc;
+  }
+  if (bad) atomicOr(A.err, 1u);
+}
+
 template <bool kNonlin>
 __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_p1(const __grid_constant__ StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -352,8 +590,8 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   const int ne = m.ne;
   const int tid = threadIdx.x;
   const int tile = blockIdx.x;
-  const int tile0 = tile * kTile;
-  const int n = min(kTile, ne - tile0);
+  const int tile0 = m.tile_elem_ptr[tile];
+  const int n = m.tile_elem_ptr[tile + 1] - tile0;
   const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
   const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
   const StageLayout L = stage_layout(m.max_halo, m.max_tasks);
@@ -384,32 +622,25 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     gid[tid] = hg;
   }
   {
-    const int ngeo = m.manning ? EGeo::kRows : EGeo::kNbar;
-    const int nrows = 12 + ngeo;
-    for (int it = tid; it < nrows * kTile; it += kStageThreads) {
-      const int r = it / kTile, w = it - r * kTile;
-      if (w >= n) continue;
-      const double* src;
-      double* dst;
-      if (r < 9) {
-        src = A.qin + (size_t)r * ne;
-        dst = qs + r * S;
-      } else if (r < 12) {
-        src = m.hb + (size_t)(r - 9) * ne;
-        dst = qs + r * S;
-      } else {
-        src = m.egeo + (size_t)(r - 12) * ne;
-        dst = geo + (r - 12) * kTile;
+    // thread t: element t % kTile of every (kStageThreads / kTile)-th row
+    static_assert(kStageThreads % kTile == 0, "tile rows are copied by whole groups of kTile threads");
+    constexpr int kRowStep = kStageThreads / kTile;
+    const int w = tid % kTile, r0 = tid / kTile;
+    if (w < n) {
+      const int ngeo = m.manning ? EGeo::kRows : EGeo::kNbar;
+      const size_t step = (size_t)kRowStep * ne;
+      const double* src = A.qin + (size_t)r0 * ne + tile0 + w;
+      for (int r = r0; r < 9; r += kRowStep, src += step) cp_async8(qs + r * S + w, src);
+      src = m.hb + (size_t)r0 * ne + tile0 + w;
+      for (int r = r0; r < 3; r += kRowStep, src += step) cp_async8(qs + (9 + r) * S + w, src);
+      src = m.egeo + (size_t)r0 * ne + tile0 + w;
+      for (int r = r0; r < ngeo; r += kRowStep, src += step) cp_async8(geo + r * kTile + w, src);
+      for (int r = r0; r < 3; r += kRowStep) {
+        if (r == 0)
+          cp_async4(wds + w, A.wd + tile0 + w);
+        else
+          cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
       }
-      cp_async8(dst + w, src + tile0 + w);
-    }
-    for (int it = tid; it < 3 * kTile; it += kStageThreads) {
-      const int r = it / kTile, w = it - r * kTile;
-      if (w >= n) continue;
-      if (r == 0)
-        cp_async4(wds + w, A.wd + tile0 + w);
-      else
-        cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
     }
     for (int j = tid; j < nh; j += kStageThreads) {
       const int g = j == tid ? hg : m.tile_halo[hbeg + j];
@@ -425,15 +656,15 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   __syncthreads();
 
   // per-element factors used by phases 3 and 4 (visible after the next barrier)
-  if (tid < n) {
-    const double areas = geo[EGeo::kAreas * kTile + tid];
+  for (int el = tid; el < n; el += kStageThreads) {
+    const double areas = geo[EGeo::kAreas * kTile + el];
 #pragma unroll
     for (int l = 0; l < 3; ++l)
-      geo[(SGeo::kEdfac + l) * kTile + tid] = geo[(EGeo::kXlen + l) * kTile + tid] / areas;
+      geo[(SGeo::kEdfac + l) * kTile + el] = geo[(EGeo::kXlen + l) * kTile + el] / areas;
     if (P.iflinbf == 0 && P.ifhybf == 1) {  // hybrid friction factor, from the element-mean depth
-      const double depth_c = qs[9 * S + tid] + qs[tid];
+      const double depth_c = qs[9 * S + el] + qs[el];
       const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
-      geo[SGeo::kHyb * kTile + tid] = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
+      geo[SGeo::kHyb * kTile + el] = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
     }
   }
 
@@ -459,6 +690,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
       tdry[w] = dry;
       if (dry) continue;
       const int gex = sex < kTile ? tile0 + sex : gid[sex - kTile];
+      // the three points, then the dry-side rules (rare) as a second pass
 #pragma unroll 1
       for (int I = 0; I < 3; ++I) {
         const int gp_in = I, gp_ex = 2 - I;
@@ -467,17 +699,30 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
         slot_trace(B, qs, S, sex, led_ex, gp_ex, zx, xx, yx, hx);
         const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
         const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
-        Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
-        double F = f.f, gi = f.g, hi2 = f.h, gx = f.g, hx2 = f.h;
+        const Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
+        double* o = out + 5 * I;
+        o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
+      }
+      if (wd_in == 0 || wd_ex == 0) {
         // internal_edge_hydro.F:212-302: mass flux out of / into a dry
         // element.  The four cases re-evaluate the flux once with changed
         // arguments: the dry side's state replaced by the wet side's with
         // reflected momentum (outflow from a dry element), or gravity off
         // (G = 0) for the dry side's momentum flux.
-        if (fabs(f.f) > 1.0e-8 && (wd_in == 0 || wd_ex == 0)) {
+        const bool in_dry = wd_in == 0;
+#pragma unroll 1
+        for (int I = 0; I < 3; ++I) {
+          double* o = out + 5 * I;
+          const double F0 = o[0];
+          if (!(fabs(F0) > 1.0e-8)) continue;
+          const int gp_in = I, gp_ex = 2 - I;
+          double zi, xi, yi, hi, zx, xx, yx, hx;
+          slot_trace(B, qs, S, sin, led_in, gp_in, zi, xi, yi, hi);
+          slot_trace(B, qs, S, sex, led_ex, gp_ex, zx, xx, yx, hx);
+          const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
+          const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
           const double tx = -ny, ty = nx, den = nx * ty - ny * tx;
-          const bool in_dry = wd_in == 0;
-          const bool reflect = in_dry ? f.f > 0.0 : f.f < 0.0;
+          const bool reflect = in_dry ? F0 > 0.0 : F0 < 0.0;
           // the wet side, whose momentum is reflected onto the dry side
           const double qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
           const double qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
@@ -495,16 +740,14 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
           }
           const Flux3 r = llf<kNonlin>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_si, a_sx, nx, ny, a_g);
           if (reflect) {
-            F = r.f;
-            if (in_dry) { gx = r.g; hx2 = r.h; gi = 0.0; hi2 = 0.0; }
-            else        { gi = r.g; hi2 = r.h; gx = 0.0; hx2 = 0.0; }
+            o[0] = r.f;
+            if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0.0; o[2] = 0.0; }
+            else        { o[1] = r.g; o[2] = r.h; o[3] = 0.0; o[4] = 0.0; }
           } else {
-            if (in_dry) { gi = r.g; hi2 = r.h; }
-            else        { gx = r.g; hx2 = r.h; }
+            if (in_dry) { o[1] = r.g; o[2] = r.h; }
+            else        { o[3] = r.g; o[4] = r.h; }
           }
         }
-        double* o = out + 5 * I;
-        o[0] = F; o[1] = gi; o[2] = hi2; o[3] = gx; o[4] = hx2;
       }
     } else {
       if (wd_in == 0) continue;
@@ -523,88 +766,11 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   __syncthreads();
 
   // ---- phase 3: volume fluxes and sources per (element, area point) ----
-  // rhs_dg_hydro.F:58-470
+  // (the point is the same for a whole warp: kTile is a multiple of 32)
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int i = w / kTile, el = w - i * kTile;
-    if (el >= n) continue;
-    const int wde = wds[el];
-    if (wde == 0) continue;
-    const int e = tile0 + el;
-    double q[9], hbe[3];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) q[c] = qs[c * S + el];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) hbe[k] = qs[(9 + k) * S + el];
-    const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
-    const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
-    const double NLEQ = kNonlin ? 1.0 : P.nleq, LEQ = kNonlin ? 0.0 : P.leq;
-    const double cori = m.cori ? m.cori[e] : P.cori;
-    double fric = m.fric ? m.fric[e] : P.fric;
-    double zq = q[0], uq = q[3], vq = q[6];
-    const double hq = hbe[0] * B.phi_area[0][i] + hbe[1] * B.phi_area[1][i] + hbe[2] * B.phi_area[2][i];
-    double dhx = 0.0, dhy = 0.0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      dhx = dhx + hbe[k] * (B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx);
-      dhy = dhy + hbe[k] * (B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy);
-    }
-    zq = zq + q[1] * B.phi_area[1][i] + q[2] * B.phi_area[2][i];
-    uq = uq + q[4] * B.phi_area[1][i] + q[5] * B.phi_area[2][i];
-    vq = vq + q[7] * B.phi_area[1][i] + q[8] * B.phi_area[2][i];
-    const double depth = zq + hq;
-    const double sfq = m.sfac_area ? m.sfac_area[(size_t)i * ne + e] : 1.0;
-    const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
-    const double fx = uq * f1 * sfq, fy = vq * f1;
-    const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
-    const double fg = P.nleqg * zq * wde;
-    const double fh = 1.0 / (kNonlin ? depth : NLEQ * depth + LEQ);
-    const double u = uq * fh, v = vq * fh;
-    const double huu = fu * u, hvv = fv * v, huv = fu * v;
-    const double gh2 = kNonlin ? fg * (0.5 * zq + hq) : fg * (0.5 * zq + hq) + P.fg_l * zq;
-    const double gx = (huu + gh2) * sfq, gy = huv;
-    const double hx = huv * sfq, hy = hvv + gh2;
-    if (m.manning) {
-      const double nbar = geo[EGeo::kNbar * kTile + el];
-      fric = P.g * (nbar * nbar) / cube_root(depth);
-      if (fric < P.cf) fric = P.cf;
-    }
-    double tau = fric;
-    if (P.iflinbf == 0) {
-      const double umag = sqrt(u * u + v * v);
-      tau = tau * umag * fh;
-      if (P.ifhybf == 1) tau = tau * geo[SGeo::kHyb * kTile + el];
-      tau = fmin(tau, P.tau_cap);
-    }
-    double sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
-    double sy = -(tau * vq) + fg * dhy - cori * uq;
-    if (P.nws != 0) {
-      // met_forcing.F:49-66: the nodal fields are scaled by the ramp each stage
-      const double drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
-      double dpsidx[3], dpsidy[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
-        dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
-      }
-      const double fw = 1.0 / f1, r = A.rampdg;
-      const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
-      const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
-      const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];
-      const double p0 = r * A.pr[n0], p1 = r * A.pr[n1], p2 = r * A.pr[n2];
-      sx = sx + fw * (wx0 * B.psi[0][i] + wx1 * B.psi[1][i] + wx2 * B.psi[2][i]) -
-           P.g * sfq * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
-      sy = sy + fw * (wy0 * B.psi[0][i] + wy1 * B.psi[1][i] + wy2 * B.psi[2][i]) -
-           P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
-    }
-    double* vo = vol + i * kTile + el;
-    vo[0 * 3 * kTile] = fx;
-    vo[1 * 3 * kTile] = fy;
-    vo[2 * 3 * kTile] = gx;
-    vo[3 * 3 * kTile] = gy;
-    vo[4 * 3 * kTile] = hx;
-    vo[5 * 3 * kTile] = hy;
-    vo[6 * 3 * kTile] = sx;
-    vo[7 * 3 * kTile] = sy;
+    if (el >= n || wds[el] == 0) continue;
+    volume_point<kNonlin>(A, B, qs, S, geo, vol, i, el, tile0 + el);
   }
   __syncthreads();
 
@@ -612,135 +778,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int var = w / kTile, el = w - var * kTile;
     if (el >= n) continue;
-    const int e = tile0 + el;
-    // SSP terms of stage 1 (DG_hydro_timestep.F:238-290) fetched first so
-    // that their latency overlaps the sums below; the combination itself
-    // keeps the reference's order
-    const bool hist0 = A.irk > 1;
-    double h0q[3] = {0.0, 0.0, 0.0}, h0r[3] = {0.0, 0.0, 0.0};
-    if (hist0) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const size_t c = (size_t)(3 * var + k) * ne + e;
-        if (A.a[0] != 0.0) h0q[k] = A.qhist[0][c];
-        if (A.b[0] != 0.0) h0r[k] = A.rhist[0][c];
-      }
-    }
-    const unsigned info = sinfo[el], slots = sinfo[kTile + el];
-    const int wde = wds[el];
-    double rhs[3] = {0.0, 0.0, 0.0}, isum[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      const int l = ei_order(info, s);
-      const unsigned kind = ei_kind(info, l);
-      if (kind == kNone) continue;
-      const int ti = (slots >> (10 * l)) & kNoTask;
-      const double* r = res + (size_t)ti * 15;
-      if (kind == kIBarrier) {
-        const double* o = A.ib_rhs + (size_t)m.tile_tasks[tbeg + ti].y * 9;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + o[3 * var + k];
-        continue;
-      }
-      if (kind == kInterior) {
-        if (tdry[ti]) continue;
-        const bool is_in = ei_flag(info, l) != 0;
-        const int comp = var == 0 ? 0 : (is_in ? var : var + 2);
-        const double edfac = geo[(SGeo::kEdfac + l) * kTile + el];
-        double acc[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int I = 0; I < 3; ++I) {
-          const int j = is_in ? I : 2 - I;
-          const double val = r[5 * I + comp];
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const double wk = edfac * B.edgeq[l][j][k];
-            if (is_in)  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
-              acc[k] = acc[k] - wk * val;
-            else        // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
-              acc[k] = acc[k] + wk * val;
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) isum[k] = isum[k] + acc[k];
-      } else {
-        if (wde == 0) continue;
-        const double areas = geo[EGeo::kAreas * kTile + el];
-        const double xlen = geo[(EGeo::kXlen + l) * kTile + el];
-#pragma unroll
-        for (int I = 0; I < 3; ++I) {
-          const double val = r[5 * I + var];
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const double wk = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
-            rhs[k] = rhs[k] - wk * val;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + isum[k];  // add_internal_flux
-    if (var == 0 && P.rainfall == 1) {
-      const double src = 7.0556e-6;
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + B.m_inv[k] * B.wagp[i] * B.phi_area[k][i] * src;
-    }
-    if (wde != 0) {
-      const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
-      const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
-      // flux pair of this variable: (fx, fy), (gx, gy) or (hx, hy); source sx / sy
-      const double* vx = vol + (2 * var) * 3 * kTile + el;
-      const double* vy = vx + 3 * kTile;
-      const double* vs = vol + (var == 2 ? 7 : 6) * 3 * kTile + el;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const double a = vx[i * kTile], b = vy[i * kTile];
-        if (var != 0) {
-          const double sr0 = B.m_inv[0] * B.wagp[i] * B.phi_area[0][i];
-          rhs[0] = rhs[0] + sr0 * vs[i * kTile];
-        }
-#pragma unroll
-        for (int k = 1; k < 3; ++k) {
-          const double dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
-          const double dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
-          const double xf = B.m_inv[k] * B.wagp[i] * dpx;
-          const double yf = B.m_inv[k] * B.wagp[i] * dpy;
-          if (var == 0) {
-            rhs[k] = rhs[k] + xf * a + yf * b;
-          } else {
-            const double sr = B.m_inv[k] * B.wagp[i] * B.phi_area[k][i];
-            rhs[k] = rhs[k] + xf * a + yf * b + sr * vs[i * kTile];
-          }
-        }
-      }
-    }
-    // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
-    bool bad = false;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int c = 3 * var + k;
-      if (A.rout) A.rout[(size_t)c * ne + e] = rhs[k];
-      const double qc = qs[c * S + el];
-      double acc = 0.0;
-      if (hist0) {
-        if (A.a[0] != 0.0) acc = acc + A.a[0] * h0q[k];
-        if (A.b[0] != 0.0) acc = acc + A.b[0] * h0r[k];
-      }
-      for (int I = 1; I < A.irk; ++I) {
-        const bool cur = I == A.irk - 1;
-        if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc : A.qhist[I][(size_t)c * ne + e]);
-        if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rhs[k] : A.rhist[I][(size_t)c * ne + e]);
-      }
-      if (!hist0) {  // stage 1: the current stage is I = 0
-        if (A.a[0] != 0.0) acc = acc + A.a[0] * qc;
-        if (A.b[0] != 0.0) acc = acc + A.b[0] * rhs[k];
-      }
-      bad = bad || isnan(acc);
-      A.qout[(size_t)c * ne + e] = acc;
-    }
-    if (bad) atomicOr(A.err, 1u);
+    sum_variable<kNonlin>(A, B, qs, S, geo, vol, res, tdry, sinfo, wds, tbeg, var, el, tile0 + el);
   }
 }
 
@@ -763,6 +801,15 @@ __global__ void node_minmax(const __grid_constant__ LimitArgs L) {
   L.minmax[(size_t)3 * np + n] = xmax;
   L.minmax[(size_t)4 * np + n] = ymin;
   L.minmax[(size_t)5 * np + n] = ymax;
+}
+
+// x / d for the redistribution divisor d = max(1, kdp) in {1, 2, 3}: x / 1
+// and x / 2 are exact scalings (x * 0.5 is the same correctly rounded value
+// as x / 2), only d = 3 needs a division.
+__device__ __forceinline__ double div_count(double x, int kdp) {
+  if (kdp <= 1) return x;
+  if (kdp == 2) return x * 0.5;
+  return x / 3.0;
 }
 
 // slopelimiter.F:3434-3779 (vertex clamp + 3 redistribution sweeps) followed
@@ -801,10 +848,9 @@ __global__ void __launch_bounds__(256) limit_wetdry(const __grid_constant__ Limi
         int kdp = (dif[0] > 0) + (dif[1] > 0) + (dif[2] > 0);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const double div = fmax(1.0, (double)kdp);
           double redfac = 0.0;
-          if (dif[k] > 0) {
-            redfac = sumdif * signdif / div;
+          if (dif[k] > 0) {  // sumdif * signdif / max(1, kdp)
+            redfac = div_count(sumdif * signdif, kdp);
             kdp = kdp - 1;
           }
           const double redmax = signdif > 0 ? vx[k] - vmin[k] : vmax[k] - vx[k];
