@@ -138,6 +138,10 @@ struct SGeo {
 };
 constexpr int kGeoRows = EGeo::kRows + 4;
 constexpr int kVolRows = 8;  // per area point: fx fy gx gy hx hy sx sy
+// doubles per element slot of the shared state: 12 modal values and a pad,
+// a 112-byte stride that keeps 16-byte loads by 8 consecutive slots free of
+// bank conflicts
+constexpr unsigned kQStride = 14;
 struct StageLayout {
   unsigned qs, geo, vol, res, wd, gid, tdry, info, bytes;
 };
@@ -147,7 +151,7 @@ __host__ __device__ inline StageLayout stage_layout(int max_halo, int max_tasks)
   const unsigned S = kTile + (unsigned)max_halo;
   const unsigned T = (unsigned)max_tasks;
   L.qs = align16((unsigned)sizeof(BasisP1));
-  L.geo = L.qs + 12u * S * 8u;                 // qs[12][S]: ZE, QX, QY, HB modes
+  L.geo = L.qs + kQStride * S * 8u;            // qs[S][kQStride]: ZE, QX, QY, HB modes
   L.vol = L.geo + kGeoRows * kTile * 8u;       // geo[kGeoRows][kTile]
   L.res = L.vol + kVolRows * 3u * kTile * 8u;  // vol[kVolRows][3][kTile]
   L.wd = L.res + 15u * T * 8u;                 // res[task][point][5]

@@ -336,34 +336,43 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 #define DGSWEM_STAGE_MIN_BLOCKS 2
 #endif
 
-// Trace at edge point (led, gp) of the 12 modal rows (ZE, QX, QY, HB) of
-// shared-memory slot `slot`; mode 0 of the basis is 1 on every edge point.
-__device__ __forceinline__ void slot_trace(const BasisP1& B, const double* qs, int S, int slot, int led, int gp,
+// Trace at edge point (led, gp) of the 12 modal values (ZE, QX, QY, HB
+// modes, contiguous) of shared-memory slot `slot`; mode 0 of the basis is 1
+// on every edge point.
+__device__ __forceinline__ void slot_trace(const BasisP1& B, const double* qs, int slot, int led, int gp,
                                            double& z, double& u, double& v, double& h) {
   const double p1 = B.phi_edge[led][gp][1], p2 = B.phi_edge[led][gp][2];
-  const double* q = qs + slot;
-  z = q[0] + q[S] * p1 + q[2 * S] * p2;
-  u = q[3 * S] + q[4 * S] * p1 + q[5 * S] * p2;
-  v = q[6 * S] + q[7 * S] * p1 + q[8 * S] * p2;
-  h = q[9 * S] + q[10 * S] * p1 + q[11 * S] * p2;
+  const double2* q = reinterpret_cast<const double2*>(qs + slot * kQStride);
+  const double2 a = q[0], b = q[1], c = q[2], d = q[3], f = q[4], g = q[5];
+  z = a.x + a.y * p1 + b.x * p2;
+  u = b.y + c.x * p1 + c.y * p2;
+  v = d.x + d.y * p1 + f.x * p2;
+  h = f.y + g.x * p1 + g.y * p2;
 }
 
 // Phase 3 of the stage kernel for area point I of tile element el (global
 // id e): volume fluxes and sources (rhs_dg_hydro.F:58-470) into
 // vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  C: the basis
 // tables in shared memory (I is a runtime index).
-template <bool kNonlin>
-__device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& C, const double* qs, int S,
-                                             const double* geo, double* vol, int I, int el, int e) {
+template <bool kNonlin, bool kSph>
+__device__ __forceinline__ void volume_values(const StageArgs& A, const BasisP1& C, const double* qs, int S,
+                                              const double* geo, int I, int el, int e, double out[8]) {
   const MeshView& m = A.m;
   const Physics& P = A.ph;
   const int ne = m.ne;
   const int wde = 1;  // phase 3 runs for wet elements only
   double q[9], hbe[3];
+  {
+    const double2* s2 = reinterpret_cast<const double2*>(qs + el * kQStride);
 #pragma unroll
-  for (int c = 0; c < 9; ++c) q[c] = qs[c * S + el];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) hbe[k] = qs[(9 + k) * S + el];
+    for (int j = 0; j < 6; ++j) {
+      const double2 t = s2[j];
+      double* dst0 = 2 * j < 9 ? &q[2 * j] : &hbe[2 * j - 9];
+      double* dst1 = 2 * j + 1 < 9 ? &q[2 * j + 1] : &hbe[2 * j + 1 - 9];
+      *dst0 = t.x;
+      *dst1 = t.y;
+    }
+  }
   const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
   const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
   const double NLEQ = kNonlin ? 1.0 : P.nleq, LEQ = kNonlin ? 0.0 : P.leq;
@@ -381,7 +390,7 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& 
   uq = uq + q[4] * C.phi_area[1][I] + q[5] * C.phi_area[2][I];
   vq = vq + q[7] * C.phi_area[1][I] + q[8] * C.phi_area[2][I];
   const double depth = zq + hq;
-  const double sfq = m.sfac_area ? m.sfac_area[(size_t)I * ne + e] : 1.0;
+  const double sfq = kSph ? m.sfac_area[(size_t)I * ne + e] : 1.0;
   const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
   const double fx = uq * f1 * sfq, fy = vq * f1;
   const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
@@ -425,15 +434,17 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& 
     sy = sy + fw * (wy0 * C.psi[0][I] + wy1 * C.psi[1][I] + wy2 * C.psi[2][I]) -
          P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
   }
-  double* vo = vol + I * kTile + el;
-  vo[0 * 3 * kTile] = fx;
-  vo[1 * 3 * kTile] = fy;
-  vo[2 * 3 * kTile] = gx;
-  vo[3 * 3 * kTile] = gy;
-  vo[4 * 3 * kTile] = hx;
-  vo[5 * 3 * kTile] = hy;
-  vo[6 * 3 * kTile] = sx;
-  vo[7 * 3 * kTile] = sy;
+  out[0] = fx; out[1] = fy; out[2] = gx; out[3] = gy;
+  out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
+}
+
+template <bool kNonlin, bool kSph>
+__device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& C, const double* qs, int S,
+                                             const double* geo, double* vol, int I, int el, int e) {
+  double v[8];
+  volume_values<kNonlin, kSph>(A, C, qs, S, geo, I, el, e, v);
+#pragma unroll
+  for (int r = 0; r < 8; ++r) vol[(r * 3 + I) * kTile + el] = v[r];
 }
 
 // Phase 4 of the stage kernel for variable V of tile element el (global id
@@ -561,7 +572,7 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
   for (int k = 0; k < 3; ++k) {
     const int c = 3 * V + k;
     if (A.rout) A.rout[(size_t)c * ne + e] = rhs[k];
-    const double qc = qs[c * S + el];
+    const double qc = qs[el * kQStride + c];
     double acc = 0.0;
     if (hist0) {
       if (A.a[0] != 0.0) acc = acc + A.a[0] * h0q[k];
@@ -582,7 +593,7 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
   if (bad) atomicOr(A.err, 1u);
 }
 
-template <bool kNonlin>
+template <bool kNonlin, bool kSph>
 __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_p1(const __grid_constant__ StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const MeshView& m = A.m;
@@ -630,9 +641,9 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
       const int ngeo = m.manning ? EGeo::kRows : EGeo::kNbar;
       const size_t step = (size_t)kRowStep * ne;
       const double* src = A.qin + (size_t)r0 * ne + tile0 + w;
-      for (int r = r0; r < 9; r += kRowStep, src += step) cp_async8(qs + r * S + w, src);
+      for (int r = r0; r < 9; r += kRowStep, src += step) cp_async8(qs + w * kQStride + r, src);
       src = m.hb + (size_t)r0 * ne + tile0 + w;
-      for (int r = r0; r < 3; r += kRowStep, src += step) cp_async8(qs + (9 + r) * S + w, src);
+      for (int r = r0; r < 3; r += kRowStep, src += step) cp_async8(qs + w * kQStride + 9 + r, src);
       src = m.egeo + (size_t)r0 * ne + tile0 + w;
       for (int r = r0; r < ngeo; r += kRowStep, src += step) cp_async8(geo + r * kTile + w, src);
       for (int r = r0; r < 3; r += kRowStep) {
@@ -646,9 +657,9 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
       const int g = j == tid ? hg : m.tile_halo[hbeg + j];
       if (j != tid) gid[j] = g;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) cp_async8(qs + c * S + kTile + j, A.qin + (size_t)c * ne + g);
+      for (int c = 0; c < 9; ++c) cp_async8(qs + (kTile + j) * kQStride + c, A.qin + (size_t)c * ne + g);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) cp_async8(qs + (9 + k) * S + kTile + j, m.hb + (size_t)k * ne + g);
+      for (int k = 0; k < 3; ++k) cp_async8(qs + (kTile + j) * kQStride + 9 + k, m.hb + (size_t)k * ne + g);
       cp_async4(wds + kTile + j, A.wd + g);
     }
     cp_async_wait_all();
@@ -662,7 +673,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     for (int l = 0; l < 3; ++l)
       geo[(SGeo::kEdfac + l) * kTile + el] = geo[(EGeo::kXlen + l) * kTile + el] / areas;
     if (P.iflinbf == 0 && P.ifhybf == 1) {  // hybrid friction factor, from the element-mean depth
-      const double depth_c = qs[9 * S + el] + qs[el];
+      const double depth_c = qs[el * kQStride + 9] + qs[el * kQStride];
       const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
       geo[SGeo::kHyb * kTile + el] = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
     }
@@ -695,10 +706,10 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
       for (int I = 0; I < 3; ++I) {
         const int gp_in = I, gp_ex = 2 - I;
         double zi, xi, yi, hi, zx, xx, yx, hx;
-        slot_trace(B, qs, S, sin, led_in, gp_in, zi, xi, yi, hi);
-        slot_trace(B, qs, S, sex, led_ex, gp_ex, zx, xx, yx, hx);
-        const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
-        const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
+        slot_trace(B, qs, sin, led_in, gp_in, zi, xi, yi, hi);
+        slot_trace(B, qs, sex, led_ex, gp_ex, zx, xx, yx, hx);
+        const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
+        const double sfx = kSph ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
         const Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
         double* o = out + 5 * I;
         o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
@@ -717,10 +728,10 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
           if (!(fabs(F0) > 1.0e-8)) continue;
           const int gp_in = I, gp_ex = 2 - I;
           double zi, xi, yi, hi, zx, xx, yx, hx;
-          slot_trace(B, qs, S, sin, led_in, gp_in, zi, xi, yi, hi);
-          slot_trace(B, qs, S, sex, led_ex, gp_ex, zx, xx, yx, hx);
-          const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
-          const double sfx = m.sfac_edge ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
+          slot_trace(B, qs, sin, led_in, gp_in, zi, xi, yi, hi);
+          slot_trace(B, qs, sex, led_ex, gp_ex, zx, xx, yx, hx);
+          const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
+          const double sfx = kSph ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
           const double tx = -ny, ty = nx, den = nx * ty - ny * tx;
           const bool reflect = in_dry ? F0 > 0.0 : F0 < 0.0;
           // the wet side, whose momentum is reflected onto the dry side
@@ -754,8 +765,8 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
 #pragma unroll 1
       for (int I = 0; I < 3; ++I) {
         double zi, xi, yi, hi, zx, xx, yx;
-        slot_trace(B, qs, S, sin, led_in, I, zi, xi, yi, hi);
-        const double sfi = m.sfac_edge ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
+        slot_trace(B, qs, sin, led_in, I, zi, xi, yi, hi);
+        const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
         ghost_state(A, B, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
         Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
         double* o = out + 5 * I;
@@ -770,7 +781,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int i = w / kTile, el = w - i * kTile;
     if (el >= n || wds[el] == 0) continue;
-    volume_point<kNonlin>(A, B, qs, S, geo, vol, i, el, tile0 + el);
+    volume_point<kNonlin, kSph>(A, B, qs, S, geo, vol, i, el, tile0 + el);
   }
   __syncthreads();
 

@@ -134,12 +134,20 @@ def test_quarter_annulus_ssp52_no_limiter(built, scratch):
     check_state(g, o)
 
 
+# Fast variant on wet/dry decks: the wet/dry thresholds (H0 on vertex
+# depths, wetdry.F) make the step discontinuous, so FMA rounding near a front
+# is amplified over hundreds of steps beyond the 1e-10 bar that the strict
+# variant holds; the wet/dry flags must still agree exactly.
+RTOL_FAST_WETDRY = 1e-8
+
+
 @pytest.mark.parametrize("strict", [True, False])
 def test_sloping_beach_wetdry_manning(built, scratch, strict):
     """Config 2 physics on a small mesh: wet/dry, limiter, nodal Manning n."""
     path = decks.sloping_beach(scratch / "sb_par", nx=60, ny=12, lx=3000.0, ly=600.0, nsteps=400, dt=0.5)
     _, _, g, o = run_both(path, 400, strict=strict)
-    check_state(g, o)
+    print("sloping beach: relative differences", [rel_err(a, b) for a, b in zip(g[:3], o[:3])])
+    check_state(g, o, rtol=RTOL if strict else RTOL_FAST_WETDRY)
     assert 0 < g[3].sum() < len(g[3])  # both wet and dry elements present
 
 
