@@ -144,16 +144,18 @@ struct Variant {
   void (*limit_wetdry)(const LimitArgs&, unsigned, cudaStream_t);
   void (*modal2nodal)(const MeshView&, const double*, const int*, double, double, double*, double*,
                       double*, int*, unsigned, cudaStream_t);
-  void (*f2s)(const double*, double*, int, int, unsigned, cudaStream_t);
-  void (*s2f)(const double*, double*, int, int, unsigned, cudaStream_t);
+  void (*f2s)(const double*, double*, int, int, const int*, unsigned, cudaStream_t);
+  void (*s2f)(const double*, double*, int, int, const int*, unsigned, cudaStream_t);
+  void (*gather_int)(const int*, int*, const int*, int, unsigned, cudaStream_t);
 };
 
 static const Variant kFast = {fast::set_basis, fast::launch_stage, fast::launch_ibarrier, fast::launch_node_minmax,
                               fast::launch_limit_wetdry, fast::launch_modal2nodal,
-                              fast::launch_fortran_to_soa, fast::launch_soa_to_fortran};
+                              fast::launch_fortran_to_soa, fast::launch_soa_to_fortran, fast::launch_gather_int};
 static const Variant kStrict = {strict::set_basis, strict::launch_stage, strict::launch_ibarrier, strict::launch_node_minmax,
                                 strict::launch_limit_wetdry, strict::launch_modal2nodal,
-                                strict::launch_fortran_to_soa, strict::launch_soa_to_fortran};
+                                strict::launch_fortran_to_soa, strict::launch_soa_to_fortran,
+                                strict::launch_gather_int};
 
 }  // namespace dgswem
 
@@ -194,7 +196,8 @@ struct dgswem_cuda {
   std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
   std::vector<DevBuf<double>> rhs;  // nrk RHS buffers (allocated when kept)
   DevBuf<double> ib_rhs;  // internal-barrier terms of the current stage
-  DevBuf<int> wd, nodecode;
+  DevBuf<int> wd, nodecode, wd_staging;
+  DevBuf<int> perm, inv;  // device element order: perm[new] = input id, inv[input] = new
   DevBuf<unsigned> err;
   long long launches = 0;
   // per-kernel event timing (dgswem_cuda_profile)
@@ -397,6 +400,47 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
                                       " bytes of shared memory, the device allows " + std::to_string(dev_smem));
 }
 
+// Device element order: the elements sorted along a Morton (Z-order) curve
+// of their centroids (stable, so ties keep the input order), so that a stage
+// tile of consecutive elements is a compact patch of the mesh with a short
+// perimeter -- few edges to other tiles, a small halo.  perm[new] = old.
+// Nothing in the per-element arithmetic depends on the numbering: edge
+// orientation (NEDEL), the interior-edge order (edge numbers) and the node
+// stars (built in input order) are those of the input mesh.
+std::vector<int> morton_order(const dgswem_cuda_setup* s) {
+  const int ne = s->ne;
+  std::vector<double> cx(ne), cy(ne);
+  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+  for (int e = 0; e < ne; ++e) {
+    double sx = 0.0, sy = 0.0;
+    for (int v = 0; v < 3; ++v) {
+      const int n = s->nm[e + (size_t)ne * v] - 1;
+      sx += s->x[n];
+      sy += s->y[n];
+    }
+    cx[e] = sx / 3.0;
+    cy[e] = sy / 3.0;
+    x0 = std::min(x0, cx[e]); x1 = std::max(x1, cx[e]);
+    y0 = std::min(y0, cy[e]); y1 = std::max(y1, cy[e]);
+  }
+  const double span = std::max(std::max(x1 - x0, y1 - y0), 1e-300);
+  auto spread = [](uint64_t v) {  // bits of v at the even positions
+    uint64_t r = 0;
+    for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1u) << (2 * b);
+    return r;
+  };
+  std::vector<uint64_t> key(ne);
+  const double scale = (double)((1u << 21) - 1) / span;
+  for (int e = 0; e < ne; ++e) {
+    const uint64_t ix = (uint64_t)((cx[e] - x0) * scale), iy = (uint64_t)((cy[e] - y0) * scale);
+    key[e] = spread(ix) | spread(iy) << 1;
+  }
+  std::vector<int> perm(ne);
+  for (int e = 0; e < ne; ++e) perm[e] = e;
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+  return perm;
+}
+
 void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   const int ne = s->ne, np = s->np, ned = s->nedges;
   auto need = [](bool ok, const char* what) {
@@ -405,14 +449,18 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   need(s->nm && s->x && s->y && s->dp && s->neled && s->nedel && s->nedsd && s->hb, "setup lacks mesh arrays");
   need(s->ze && s->qx && s->qy && s->wdflg, "setup lacks the initial state");
   need(s->atvd && s->btvd && s->dtvd, "setup lacks RK tables");
-  // nodes, connectivity
-  std::vector<int> nm(3 * (size_t)ne);
+  // nodes, connectivity, in the device element order
   for (int e = 0; e < ne; ++e)
     for (int v = 0; v < 3; ++v) {
-      int n = s->nm[e + (size_t)ne * v];
+      const int n = s->nm[e + (size_t)ne * v];
       need(n >= 1 && n <= np, "NM refers to a node outside 1..NP");
-      nm[(size_t)v * ne + e] = n - 1;
     }
+  const std::vector<int> perm = morton_order(s);
+  std::vector<int> inv(ne);
+  for (int i = 0; i < ne; ++i) inv[perm[i]] = i;
+  std::vector<int> nm(3 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int v = 0; v < 3; ++v) nm[(size_t)v * ne + inv[e]] = s->nm[e + (size_t)ne * v] - 1;
   // boundary membership of each edge: kind, list index, side
   std::vector<int> bkind(ned + 1, -1), bidx(ned + 1, -1), bside(ned + 1, 0);
   auto mark = [&](const int* list, int n, unsigned kind) {
@@ -440,7 +488,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
       bkind[g] = kIBarrier;
       bidx[g] = L;
       bside[g] = side;
-      ib_elem[2 * L + side] = s->nedel[2 * (size_t)(g - 1)] - 1;
+      ib_elem[2 * L + side] = inv[s->nedel[2 * (size_t)(g - 1)] - 1];
       ib_led[2 * L + side] = s->nedsd[2 * (size_t)(g - 1)] - 1;
     }
   }
@@ -461,7 +509,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
         need(first || b == e + 1, "NEDEL does not contain the element of NELED");
         kind = kInterior;
         flag = first ? 1u : 0u;
-        lk = (first ? b : a) - 1;
+        lk = inv[(first ? b : a) - 1];
         nled = (unsigned)(s->nedsd[2 * (size_t)(g - 1) + (first ? 1 : 0)] - 1);
         key[l] = {(long long)8 << 40 | g, l};  // interior edges last, in edge-number order
       } else if (bkind[g] >= 0) {
@@ -474,17 +522,18 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
         lk = -1;
         key[l] = {(long long)9 << 40, l};
       }
-      link[(size_t)l * ne + e] = lk;
+      link[(size_t)l * ne + inv[e]] = lk;
       info |= kind << (3 * l);
       info |= flag << (9 + l);
       info |= (nled & 3u) << (12 + 2 * l);
     }
     std::sort(key.begin(), key.end());
     for (int slot = 0; slot < 3; ++slot) info |= (unsigned)key[slot].second << (18 + 2 * slot);
-    einfo[e] = info;
+    einfo[inv[e]] = info;
   }
   build_tile_plan(h, ne, link, einfo);
-  // node -> element star, element order
+  // node -> element star in the input element order (the order of the
+  // reference's loops over elements), holding device element ids
   std::vector<int> sp(np + 1, 0), st(3 * (size_t)ne);
   for (int e = 0; e < ne; ++e)
     for (int v = 0; v < 3; ++v) ++sp[nm[(size_t)v * ne + e] + 1];
@@ -492,8 +541,10 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   {
     std::vector<int> cur(sp.begin(), sp.end() - 1);
     for (int e = 0; e < ne; ++e)
-      for (int v = 0; v < 3; ++v) st[cur[nm[(size_t)v * ne + e]]++] = e;
+      for (int v = 0; v < 3; ++v) st[cur[nm[(size_t)v * ne + inv[e]]]++] = inv[e];
   }
+  h->perm.upload(perm);
+  h->inv.upload(inv);
   h->nm.upload(nm);
   h->link.upload(link);
   h->einfo.upload(einfo);
@@ -506,7 +557,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   h->dp.upload(std::vector<double>(s->dp, s->dp + np));
   std::vector<double> hb(3 * (size_t)ne);
   for (int e = 0; e < ne; ++e)
-    for (int k = 0; k < 3; ++k) hb[(size_t)k * ne + e] = s->hb[k + (size_t)s->dofh * e];
+    for (int k = 0; k < 3; ++k) hb[(size_t)k * ne + inv[e]] = s->hb[k + (size_t)s->dofh * e];
   h->hb.upload(hb);
   // per-element coefficients: a scalar when uniform
   auto uniform = [&](const double* a, double* val) {
@@ -517,8 +568,13 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     return true;
   };
   double c0 = 0.0, f0 = s->cf;
-  if (!uniform(s->cori_el, &c0)) h->cori.upload(std::vector<double>(s->cori_el, s->cori_el + ne));
-  if (!uniform(s->fric_el, &f0)) h->fric.upload(std::vector<double>(s->fric_el, s->fric_el + ne));
+  auto permuted = [&](const double* a) {
+    std::vector<double> out(ne);
+    for (int i = 0; i < ne; ++i) out[i] = a[perm[i]];
+    return out;
+  };
+  if (!uniform(s->cori_el, &c0)) h->cori.upload(permuted(s->cori_el));
+  if (!uniform(s->fric_el, &f0)) h->fric.upload(permuted(s->fric_el));
   h->ph.cori = c0;
   h->ph.fric = f0;
   if (s->load_manning) {
@@ -633,11 +689,14 @@ void upload_state(dgswem_cuda* h, const double* ze, const double* qx, const doub
     if (!src[var]) continue;
     DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], 3 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice,
                             h->stream));
-    h->v->f2s(h->staging.p, h->q[0].p, ne, var, grid_for(ne, kPointBlock), h->stream);
+    h->v->f2s(h->staging.p, h->q[0].p, ne, var, h->perm.p, grid_for(ne, kPointBlock), h->stream);
     check_launch(h, "fortran_to_soa");
   }
-  if (wdflg)
-    DG_CUDA(cudaMemcpyAsync(h->wd.p, wdflg, (size_t)ne * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if (wdflg) {
+    DG_CUDA(cudaMemcpyAsync(h->wd_staging.p, wdflg, (size_t)ne * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    h->v->gather_int(h->wd_staging.p, h->wd.p, h->perm.p, ne, grid_for(ne, kPointBlock), h->stream);
+    check_launch(h, "gather_int");
+  }
   DG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
@@ -881,6 +940,7 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
     for (int I = 0; I < s->nrk; ++I)
       if (h->keep_rhs[I]) h->rhs[I].alloc(9 * (size_t)s->ne);
     h->wd.alloc(s->ne);
+    h->wd_staging.alloc(s->ne);
     h->nodecode.alloc(s->np);
     h->minmax.alloc(6 * (size_t)s->np);
     h->err.alloc(1);
@@ -972,13 +1032,17 @@ int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* q
     double* dst[3] = {ze, qx, qy};
     for (int var = 0; var < 3; ++var) {
       if (!dst[var]) continue;
-      h->v->s2f(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var, grid_for(ne, kPointBlock), h->stream);
+      h->v->s2f(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var, h->inv.p, grid_for(ne, kPointBlock),
+                h->stream);
       check_launch(h, "soa_to_fortran");
       DG_CUDA(cudaMemcpyAsync(dst[var], h->staging.p + (size_t)3 * ne * var, 3 * (size_t)ne * sizeof(double),
                               cudaMemcpyDeviceToHost, h->stream));
     }
-    if (wdflg)
-      DG_CUDA(cudaMemcpyAsync(wdflg, h->wd.p, (size_t)ne * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (wdflg) {
+      h->v->gather_int(h->wd.p, h->wd_staging.p, h->inv.p, ne, grid_for(ne, kPointBlock), h->stream);
+      check_launch(h, "gather_int");
+      DG_CUDA(cudaMemcpyAsync(wdflg, h->wd_staging.p, (size_t)ne * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    }
     DG_CUDA(cudaStreamSynchronize(h->stream));
   });
 }

@@ -1,7 +1,9 @@
 // hydro_device.cuh -- device data layout and kernels of the p=1 DG hydro step.
 //
 // Layout in HBM (NE elements, NP nodes, all structure-of-arrays so a warp's
-// 32 consecutive elements make one coalesced transaction per field):
+// 32 consecutive elements make one coalesced transaction per field).
+// Elements are in the device order (a Morton curve of the centroids, built
+// at create; perm/inv map it to the input numbering):
 //   state   q[c*NE + e], c = 3*var + k  (var: 0 zeta, 1 qx, 2 qy; k: mode)
 //   nm[v*NE + e]       0-based vertex node ids
 //   link[l*NE + e]     across local edge l: neighbour element (interior edge)
@@ -213,10 +215,12 @@ struct LimitArgs {
   void launch_modal2nodal(const MeshView& m, const double* q, const int* wd, double nleq,      \
                           double leq, double* eta2, double* uu2, double* vv2, int* nodecode,   \
                           unsigned grid, cudaStream_t s);                                      \
-  void launch_fortran_to_soa(const double* f, double* q, int ne, int var, unsigned grid,       \
-                             cudaStream_t s);                                                  \
-  void launch_soa_to_fortran(const double* q, double* f, int ne, int var, unsigned grid,       \
-                             cudaStream_t s);                                                  \
+  void launch_fortran_to_soa(const double* f, double* q, int ne, int var, const int* perm,     \
+                             unsigned grid, cudaStream_t s);                                   \
+  void launch_soa_to_fortran(const double* q, double* f, int ne, int var, const int* inv,      \
+                             unsigned grid, cudaStream_t s);                                   \
+  void launch_gather_int(const int* src, int* dst, const int* idx, int n, unsigned grid,       \
+                         cudaStream_t s);                                                      \
   }
 
 DGSWEM_DECLARE_LAUNCHERS(fast)

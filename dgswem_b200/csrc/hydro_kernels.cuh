@@ -1019,18 +1019,30 @@ __global__ void modal2nodal_kernel(MeshView m, const double* __restrict__ q, con
 }
 
 // Fortran layout ZE(DOFH,NE) <-> state SoA q[c*NE+e] for one variable
-__global__ void fortran_to_soa(const double* __restrict__ f, double* __restrict__ q, int ne, int var) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= ne) return;
+// Host (Fortran) layout f[3*e + k] in input element order <-> device SoA
+// q[(3*var + k)*NE + i] in device element order: i = inv[e], e = perm[i].
+__global__ void fortran_to_soa(const double* __restrict__ f, double* __restrict__ q, int ne, int var,
+                               const int* __restrict__ perm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  const int e = perm[i];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) q[(size_t)(3 * var + k) * ne + e] = f[(size_t)3 * e + k];
+  for (int k = 0; k < 3; ++k) q[(size_t)(3 * var + k) * ne + i] = f[(size_t)3 * e + k];
 }
 
-__global__ void soa_to_fortran(const double* __restrict__ q, double* __restrict__ f, int ne, int var) {
+__global__ void soa_to_fortran(const double* __restrict__ q, double* __restrict__ f, int ne, int var,
+                               const int* __restrict__ inv) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= ne) return;
+  const int i = inv[e];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) f[(size_t)3 * e + k] = q[(size_t)(3 * var + k) * ne + e];
+  for (int k = 0; k < 3; ++k) f[(size_t)3 * e + k] = q[(size_t)(3 * var + k) * ne + i];
+}
+
+// dst[i] = src[idx[i]]: WDFLG between input and device element order
+__global__ void gather_int(const int* __restrict__ src, int* __restrict__ dst, const int* __restrict__ idx, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[idx[i]];
 }
 
 }  // namespace DGSWEM_VARIANT
