@@ -198,6 +198,8 @@ struct dgswem_cuda {
   DevBuf<double> ib_rhs;  // internal-barrier terms of the current stage
   DevBuf<int> wd, nodecode, wd_staging;
   DevBuf<int> perm, inv;  // device element order: perm[new] = input id, inv[input] = new
+  DevBuf<int> node_perm;  // device node order: node_perm[new] = input id
+  std::vector<int> node_perm_h;
   DevBuf<unsigned> err;
   long long launches = 0;
   // per-kernel event timing (dgswem_cuda_profile)
@@ -400,28 +402,21 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
                                       " bytes of shared memory, the device allows " + std::to_string(dev_smem));
 }
 
-// Device element order: the elements sorted along a Morton (Z-order) curve
-// of their centroids (stable, so ties keep the input order), so that a stage
-// tile of consecutive elements is a compact patch of the mesh with a short
-// perimeter -- few edges to other tiles, a small halo.  perm[new] = old.
-// Nothing in the per-element arithmetic depends on the numbering: edge
-// orientation (NEDEL), the interior-edge order (edge numbers) and the node
-// stars (built in input order) are those of the input mesh.
-std::vector<int> morton_order(const dgswem_cuda_setup* s) {
-  const int ne = s->ne;
-  std::vector<double> cx(ne), cy(ne);
+// Device element and node order: elements sorted along a Morton (Z-order)
+// curve of their centroids, nodes along the same curve of their coordinates
+// (stable sorts, ties keep the input order).  A stage tile of consecutive
+// elements is then a compact patch of the mesh with a short perimeter -- few
+// edges to other tiles, a small halo -- and the nodes an element touches lie
+// close together in memory.  perm[new] = input index.  Nothing in the
+// arithmetic depends on the numbering: edge orientation (NEDEL), the
+// interior-edge order (edge numbers) and the node stars (built in input
+// element order) are those of the input mesh.
+std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py) {
+  const int n = (int)px.size();
   double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
-  for (int e = 0; e < ne; ++e) {
-    double sx = 0.0, sy = 0.0;
-    for (int v = 0; v < 3; ++v) {
-      const int n = s->nm[e + (size_t)ne * v] - 1;
-      sx += s->x[n];
-      sy += s->y[n];
-    }
-    cx[e] = sx / 3.0;
-    cy[e] = sy / 3.0;
-    x0 = std::min(x0, cx[e]); x1 = std::max(x1, cx[e]);
-    y0 = std::min(y0, cy[e]); y1 = std::max(y1, cy[e]);
+  for (int i = 0; i < n; ++i) {
+    x0 = std::min(x0, px[i]); x1 = std::max(x1, px[i]);
+    y0 = std::min(y0, py[i]); y1 = std::max(y1, py[i]);
   }
   const double span = std::max(std::max(x1 - x0, y1 - y0), 1e-300);
   auto spread = [](uint64_t v) {  // bits of v at the even positions
@@ -429,14 +424,14 @@ std::vector<int> morton_order(const dgswem_cuda_setup* s) {
     for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1u) << (2 * b);
     return r;
   };
-  std::vector<uint64_t> key(ne);
+  std::vector<uint64_t> key(n);
   const double scale = (double)((1u << 21) - 1) / span;
-  for (int e = 0; e < ne; ++e) {
-    const uint64_t ix = (uint64_t)((cx[e] - x0) * scale), iy = (uint64_t)((cy[e] - y0) * scale);
-    key[e] = spread(ix) | spread(iy) << 1;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t ix = (uint64_t)((px[i] - x0) * scale), iy = (uint64_t)((py[i] - y0) * scale);
+    key[i] = spread(ix) | spread(iy) << 1;
   }
-  std::vector<int> perm(ne);
-  for (int e = 0; e < ne; ++e) perm[e] = e;
+  std::vector<int> perm(n);
+  for (int i = 0; i < n; ++i) perm[i] = i;
   std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
   return perm;
 }
@@ -455,12 +450,34 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
       const int n = s->nm[e + (size_t)ne * v];
       need(n >= 1 && n <= np, "NM refers to a node outside 1..NP");
     }
-  const std::vector<int> perm = morton_order(s);
-  std::vector<int> inv(ne);
+  std::vector<int> perm, inv(ne), node_perm, node_inv(np);
+  {
+    std::vector<double> cx(ne), cy(ne);
+    for (int e = 0; e < ne; ++e) {
+      double sx = 0.0, sy = 0.0;
+      for (int v = 0; v < 3; ++v) {
+        const int n = s->nm[e + (size_t)ne * v] - 1;
+        sx += s->x[n];
+        sy += s->y[n];
+      }
+      cx[e] = sx / 3.0;
+      cy[e] = sy / 3.0;
+    }
+    perm = morton_order(cx, cy);
+    node_perm = morton_order(std::vector<double>(s->x, s->x + np), std::vector<double>(s->y, s->y + np));
+  }
   for (int i = 0; i < ne; ++i) inv[perm[i]] = i;
+  for (int i = 0; i < np; ++i) node_inv[node_perm[i]] = i;
+  // nodal arrays in the device node order
+  auto node_permuted = [&](const double* a) {
+    std::vector<double> out(np);
+    for (int i = 0; i < np; ++i) out[i] = a[node_perm[i]];
+    return out;
+  };
+  const std::vector<double> xd = node_permuted(s->x), yd = node_permuted(s->y);
   std::vector<int> nm(3 * (size_t)ne);
   for (int e = 0; e < ne; ++e)
-    for (int v = 0; v < 3; ++v) nm[(size_t)v * ne + inv[e]] = s->nm[e + (size_t)ne * v] - 1;
+    for (int v = 0; v < 3; ++v) nm[(size_t)v * ne + inv[e]] = node_inv[s->nm[e + (size_t)ne * v] - 1];
   // boundary membership of each edge: kind, list index, side
   std::vector<int> bkind(ned + 1, -1), bidx(ned + 1, -1), bside(ned + 1, 0);
   auto mark = [&](const int* list, int n, unsigned kind) {
@@ -552,9 +569,11 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   h->star.upload(st);
   h->ib_elem.upload(ib_elem);
   h->ib_led.upload(ib_led);
-  h->x.upload(std::vector<double>(s->x, s->x + np));
-  h->y.upload(std::vector<double>(s->y, s->y + np));
-  h->dp.upload(std::vector<double>(s->dp, s->dp + np));
+  h->node_perm.upload(node_perm);
+  h->node_perm_h = node_perm;
+  h->x.upload(xd);
+  h->y.upload(yd);
+  h->dp.upload(node_permuted(s->dp));
   std::vector<double> hb(3 * (size_t)ne);
   for (int e = 0; e < ne; ++e)
     for (int k = 0; k < 3; ++k) hb[(size_t)k * ne + inv[e]] = s->hb[k + (size_t)s->dofh * e];
@@ -579,7 +598,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   h->ph.fric = f0;
   if (s->load_manning) {
     need(s->manning != nullptr, "load_manning set without ManningsN");
-    h->manning.upload(std::vector<double>(s->manning, s->manning + np));
+    h->manning.upload(node_permuted(s->manning));
   }
   // element geometry table (EGeo rows): the reference's formulas evaluated
   // once, in the same order as the oracle, instead of every stage
@@ -589,8 +608,8 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     for (int e = 0; e < ne; ++e) {
       double xs[3], ys[3];
       for (int v = 0; v < 3; ++v) {
-        xs[v] = s->x[nm[(size_t)v * ne + e]];
-        ys[v] = s->y[nm[(size_t)v * ne + e]];
+        xs[v] = xd[nm[(size_t)v * ne + e]];
+        ys[v] = yd[nm[(size_t)v * ne + e]];
       }
       const double areas = (xs[0] - xs[2]) * (ys[1] - ys[2]) + (xs[2] - xs[1]) * (ys[0] - ys[2]);
       at(EGeo::kAreas, e) = areas;
@@ -602,13 +621,15 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
         at(EGeo::kNx + l, e) = (ys[b] - ys[a]) / len;
         at(EGeo::kNy + l, e) = -(xs[b] - xs[a]) / len;
       }
+      for (int l = 0; l < 3; ++l) at(EGeo::kEdfac + l, e) = at(EGeo::kXlen + l, e) / areas;
       const double area = areas * 0.5;
       at(EGeo::kDrdx, e) = 1.0 / area * (ys[2] - ys[0]);
       at(EGeo::kDsdx, e) = 1.0 / area * (ys[0] - ys[1]);
       at(EGeo::kDrdy, e) = 1.0 / area * (xs[0] - xs[2]);
       at(EGeo::kDsdy, e) = 1.0 / area * (xs[1] - xs[0]);
       if (s->load_manning)
-        at(EGeo::kNbar, e) = (s->manning[nm[e]] + s->manning[nm[(size_t)ne + e]] + s->manning[nm[(size_t)2 * ne + e]]) / 3.;
+        at(EGeo::kNbar, e) = (s->manning[node_perm[nm[e]]] + s->manning[node_perm[nm[(size_t)ne + e]]] +
+                              s->manning[node_perm[nm[(size_t)2 * ne + e]]]) / 3.;
     }
     h->egeo.upload(eg);
   }
@@ -617,7 +638,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     const double R = 6378206.4;
     std::vector<double> sa(3 * (size_t)ne), se(9 * (size_t)ne);
     for (int e = 0; e < ne; ++e) {
-      const double y1 = s->y[nm[e]], y2 = s->y[nm[(size_t)ne + e]], y3 = s->y[nm[(size_t)2 * ne + e]];
+      const double y1 = yd[nm[e]], y2 = yd[nm[(size_t)ne + e]], y3 = yd[nm[(size_t)2 * ne + e]];
       const double yd[3] = {1.0 / 3.0 * (y1 + y2 + y3), -(1.0 / 6.0 * (y1 + y2)) + 1.0 / 3.0 * y3,
                             -(0.5 * y1) + 0.5 * y2};
       for (int i = 0; i < 3; ++i) {
@@ -665,7 +686,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   m.x = h->x.p; m.y = h->y.p; m.dp = h->dp.p; m.nm = h->nm.p; m.link = h->link.p; m.einfo = h->einfo.p;
   m.hb = h->hb.p; m.egeo = h->egeo.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
   m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
-  m.star_ptr = h->star_ptr.p; m.star = h->star.p;
+  m.star_ptr = h->star_ptr.p; m.star = h->star.p; m.node_perm = h->node_perm.p;
   m.tile_elem_ptr = h->tile_elem_ptr.p;
   m.tile_task_ptr = h->tile_task_ptr.p;
   m.tile_tasks = reinterpret_cast<const uint2*>(h->tile_tasks.p);
@@ -1052,10 +1073,19 @@ int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2, 
     if (!h || !wsx2 || !wsy2 || !pr2) throw Failure(DGSWEM_ERR_ARG, "null argument");
     if (h->nws != 1) throw Failure(DGSWEM_ERR_ARG, "met forcing needs NWS = 1");
     DG_CUDA(cudaSetDevice(h->device));
-    const size_t bytes = (size_t)h->np * sizeof(double);
-    DG_CUDA(cudaMemcpyAsync(h->wsx.p, wsx2, bytes, cudaMemcpyHostToDevice, h->stream));
-    DG_CUDA(cudaMemcpyAsync(h->wsy.p, wsy2, bytes, cudaMemcpyHostToDevice, h->stream));
-    DG_CUDA(cudaMemcpyAsync(h->pr.p, pr2, bytes, cudaMemcpyHostToDevice, h->stream));
+    // the fields in the device node order
+    const int np = h->np;
+    std::vector<double> buf(3 * (size_t)np);
+    for (int i = 0; i < np; ++i) {
+      const int n = h->node_perm_h[i];
+      buf[i] = wsx2[n];
+      buf[(size_t)np + i] = wsy2[n];
+      buf[(size_t)2 * np + i] = pr2[n];
+    }
+    const size_t bytes = (size_t)np * sizeof(double);
+    DG_CUDA(cudaMemcpyAsync(h->wsx.p, buf.data(), bytes, cudaMemcpyHostToDevice, h->stream));
+    DG_CUDA(cudaMemcpyAsync(h->wsy.p, buf.data() + np, bytes, cudaMemcpyHostToDevice, h->stream));
+    DG_CUDA(cudaMemcpyAsync(h->pr.p, buf.data() + 2 * (size_t)np, bytes, cudaMemcpyHostToDevice, h->stream));
     DG_CUDA(cudaStreamSynchronize(h->stream));
   });
 }

@@ -76,6 +76,7 @@ struct MeshView {
   const double* __restrict__ sfac_edge; // [(l*3+i)*NE+e] (ics=2) or null
   const int* __restrict__ star_ptr;     // node -> element star (CSR)
   const int* __restrict__ star;
+  const int* __restrict__ node_perm;    // device node -> input node
   // boundary lists
   int needs, nfeds, nebseg, nibseg, nbfr, nffr;
   const double* __restrict__ emo_dg;    // EMO_DG(NBFR,NEEDS,2)
@@ -105,7 +106,7 @@ struct MeshView {
 #define DGSWEM_TILE 128
 #endif
 #ifndef DGSWEM_STAGE_THREADS
-#define DGSWEM_STAGE_THREADS 256
+#define DGSWEM_STAGE_THREADS 384
 #endif
 constexpr int kTile = DGSWEM_TILE;
 constexpr int kStageThreads = DGSWEM_STAGE_THREADS;
@@ -126,19 +127,23 @@ struct TaskBits {
 // nodal coordinates with the reference's formulas (read_input.F:1406 AREAS,
 // calc_normal.F:41-48 XLEN and normals on the counter-clockwise local edges,
 // rhs_dg_hydro.F's DRDX/DSDX/DRDY/DSDY from the area and the coordinate
-// differences) and the element mean of the nodal Manning n.
+// differences, XLEN/AREAS of internal_edge_hydro.F) and the element mean of
+// the nodal Manning n.  The stage kernel copies the first kSmemRows (with
+// Manning n) into shared memory; AREAS and XLEN, used only by boundary
+// edges, are read from the table.
 struct EGeo {
-  static constexpr int kAreas = 0, kXlen = 1, kNx = 4, kNy = 7, kDrdx = 10, kDsdx = 11, kDrdy = 12, kDsdy = 13;
-  static constexpr int kNbar = 14, kRows = 15;
+  static constexpr int kNx = 0, kNy = 3, kDrdx = 6, kDsdx = 7, kDrdy = 8, kDsdy = 9, kEdfac = 10, kNbar = 13;
+  static constexpr int kAreas = 14, kXlen = 15, kRows = 18;
+  static constexpr int kSmemRows = 14;
 };
 
 // Dynamic shared memory of the stage kernel (byte offsets).  Per-element
-// rows of geo: the EGeo rows copied from the table (same order), then the
-// hybrid friction factor and XLEN/AREAS per local edge.
+// rows of geo: the first EGeo::kSmemRows rows of the table, then the hybrid
+// friction factor.
 struct SGeo {
-  static constexpr int kHyb = EGeo::kRows, kEdfac = EGeo::kRows + 1;
+  static constexpr int kHyb = EGeo::kSmemRows;
 };
-constexpr int kGeoRows = EGeo::kRows + 4;
+constexpr int kGeoRows = EGeo::kSmemRows + 1;
 constexpr int kVolRows = 8;  // per area point: fx fy gx gy hx hy sx sy
 // doubles per element slot of the shared state: 12 modal values and a pad,
 // a 112-byte stride that keeps 16-byte loads by 8 consecutive slots free of

@@ -496,7 +496,7 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
       if (tdry[ti]) continue;
       const bool is_in = ei_flag(info, l) != 0;
       const int comp = V == 0 ? 0 : (is_in ? V : V + 2);
-      const double edfac = geo[(SGeo::kEdfac + l) * kTile + el];
+      const double edfac = geo[(EGeo::kEdfac + l) * kTile + el];
       double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
@@ -515,8 +515,8 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
       for (int k = 0; k < 3; ++k) isum[k] = isum[k] + acc[k];
     } else {
       if (wde == 0) continue;
-      const double areas = geo[EGeo::kAreas * kTile + el];
-      const double xlen = geo[(EGeo::kXlen + l) * kTile + el];
+      const double areas = m.egeo[(size_t)EGeo::kAreas * ne + e];
+      const double xlen = m.egeo[(size_t)(EGeo::kXlen + l) * ne + e];
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
         const double val = r[5 * I + V];
@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     constexpr int kRowStep = kStageThreads / kTile;
     const int w = tid % kTile, r0 = tid / kTile;
     if (w < n) {
-      const int ngeo = m.manning ? EGeo::kRows : EGeo::kNbar;
+      const int ngeo = m.manning ? EGeo::kSmemRows : EGeo::kNbar;
       const size_t step = (size_t)kRowStep * ne;
       const double* src = A.qin + (size_t)r0 * ne + tile0 + w;
       for (int r = r0; r < 9; r += kRowStep, src += step) cp_async8(qs + w * kQStride + r, src);
@@ -666,13 +666,10 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   }
   __syncthreads();
 
-  // per-element factors used by phases 3 and 4 (visible after the next barrier)
-  for (int el = tid; el < n; el += kStageThreads) {
-    const double areas = geo[EGeo::kAreas * kTile + el];
-#pragma unroll
-    for (int l = 0; l < 3; ++l)
-      geo[(SGeo::kEdfac + l) * kTile + el] = geo[(EGeo::kXlen + l) * kTile + el] / areas;
-    if (P.iflinbf == 0 && P.ifhybf == 1) {  // hybrid friction factor, from the element-mean depth
+  // hybrid friction factor from the element-mean depth, used by phase 3
+  // (visible after the next barrier)
+  if (P.iflinbf == 0 && P.ifhybf == 1) {
+    for (int el = tid; el < n; el += kStageThreads) {
       const double depth_c = qs[el * kQStride + 9] + qs[el * kQStride];
       const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
       geo[SGeo::kHyb * kTile + el] = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
@@ -976,7 +973,8 @@ __global__ void __launch_bounds__(256) limit_wetdry(const __grid_constant__ Limi
   for (int c = 0; c < 9; ++c) L.q[(size_t)c * ne + e] = q[c];
 }
 
-// write_results.F:14-170 (modal2nodal) + NODECODE from the wet flags
+// write_results.F:14-170 (modal2nodal) + NODECODE from the wet flags; node n
+// of the device order writes its results at its input position
 __global__ void modal2nodal_kernel(MeshView m, const double* __restrict__ q, const int* __restrict__ wd,
                                    double nleq, double leq, double* eta2, double* uu2, double* vv2,
                                    int* nodecode) {
@@ -1012,10 +1010,11 @@ __global__ void modal2nodal_kernel(MeshView m, const double* __restrict__ q, con
     uu = uu + w * xd * fh;
     vv = vv + w * yd * fh;
   }
-  if (eta2) eta2[n] = et;
-  if (uu2) uu2[n] = uu;
-  if (vv2) vv2[n] = vv;
-  if (nodecode) nodecode[n] = wet;
+  const int out = m.node_perm[n];  // results in the input node order
+  if (eta2) eta2[out] = et;
+  if (uu2) uu2[out] = uu;
+  if (vv2) vv2[out] = vv;
+  if (nodecode) nodecode[out] = wet;
 }
 
 // Fortran layout ZE(DOFH,NE) <-> state SoA q[c*NE+e] for one variable
