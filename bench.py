@@ -30,14 +30,22 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 DOFS_PER_ELEMENT = 9  # 3 variables x 3 modes at p=1
-# Algorithmic bytes per element and stage for stage_p1 (FP64, SSP(2,2)
-# averaged over its two stages): stage state in 72 + step-base state 36 +
-# stage state out 72 + HB modes 24 + inverse Jacobian and area 40 + neighbour
-# ids 12 + WDFLG read 4 + Manning n 8.
-STAGE_KERNEL_BYTES = 72 + 36 + 72 + 24 + 40 + 12 + 4 + 8
-# whole-stage algorithmic bytes of the same workload (adds node ids 12,
-# node min/max write+read 24, WDFLG write 4)
-STAGE_TOTAL_BYTES = STAGE_KERNEL_BYTES + 12 + 24 + 4
+# Algorithmic bytes per element and stage for stage_p1 (FP64, SSP(2,2),
+# averaged over its two stages): stage state in 72 + step-start state 36
+# (stage 2 only) + stage state out 72 + HB modes 24 + geometry table rows
+# copied to shared memory 112 (normals, Jacobian terms, XLEN/AREAS, mean
+# Manning n) + WDFLG 4 + edge info 8 + tile plan 14 (1.63 edge tasks of 8
+# bytes and 0.25 halo ids per element on the Morton-ordered mesh).
+STAGE_KERNEL_BYTES = 72 + 36 + 72 + 24 + 112 + 4 + 8 + 14
+# whole-stage algorithmic bytes (adds node_minmax: element means 24 + node
+# min/max 24; limit_wetdry: state 72 + 72, node ids 12, node min/max 24,
+# HB modes 16, WDFLG 4 + 4, nodal depth 4)
+STAGE_TOTAL_BYTES = STAGE_KERNEL_BYTES + 48 + 72 + 72 + 12 + 24 + 16 + 8 + 4
+# DRAM bytes per element of one stage_p1 launch, dram__bytes_read.sum +
+# dram__bytes_write.sum from ncu on the same deck at 999,492 elements: the
+# mean of a stage-1 (291.6) and a stage-2 (364.0) launch; traffic grows with
+# the element count.
+STAGE_TRAFFIC_BYTES = 0.5 * (291.6 + 364.0)
 
 
 def rank_env():
@@ -299,7 +307,10 @@ def main(argv=None):
                 "d2h_bytes_per_step": state_bytes,
                 "how": "per step: upload ZE/QX/QY/WDFLG from pinned host memory, one hydro step, download"},
         "roofline": {"bound": "hbm", "kernel": "stage_p1", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": STAGE_TRAFFIC_BYTES * ne,
+                     "traffic_source": "ncu dram bytes per element of a stage-1 and a stage-2 launch (999,492 elements), "
+                                       "scaled by the element count",
                      "algorithmic_bytes_per_element_stage": STAGE_KERNEL_BYTES,
                      "avg_launch_ms": avg_stage_s * 1e3,
                      "stage_all_kernels_ms": stage_total_ms / max(stage_total_n, 1),
