@@ -319,10 +319,10 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 // kStageThreads threads:
 //   1. tile and halo elements: modal state, bathymetry modes and wet/dry flag
 //      into shared memory; tile elements also their geometry;
-//   2. one thread per task: the three Lobatto points of an edge in the
-//      reference's own in/ex orientation with its dry-side rules ->
-//      F, G_in, H_in, G_ex, H_ex per point (internal-barrier sides come
-//      from ibarrier_sides);
+//   2. one thread per (task, Lobatto point): the LLF flux of an edge point in
+//      the reference's own in/ex orientation with its dry-side rules ->
+//      F, G_in, H_in, G_ex, H_ex (internal-barrier sides come from
+//      ibarrier_sides);
 //   3. one thread per (element, area point): volume fluxes and sources;
 //   4. one thread per (element, variable): the three modes of that variable
 //      summed in the reference's order (boundary edges, interior edges in
@@ -676,13 +676,15 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     }
   }
 
-  // ---- phase 2: one thread per edge task, three Lobatto points ----
-  for (int w = tid; w < ntask; w += kStageThreads) {
-    const uint2 tk = m.tile_tasks[tbeg + w];
+  // ---- phase 2: one thread per (edge task, Lobatto point) ----
+  // (the three points of a task on adjacent lanes: same slots, broadcast loads)
+  for (int w = tid; w < 3 * ntask; w += kStageThreads) {
+    const int ti = w / 3, I = w - 3 * ti;
+    const uint2 tk = m.tile_tasks[tbeg + ti];
     const unsigned fl = tk.x;
     const unsigned kind = fl & 7u;
-    double* out = res + (size_t)w * 15;
     if (kind == kIBarrier) continue;  // ibarrier_sides, launched before this kernel
+    double* o = res + (size_t)ti * 15 + 5 * I;
     const int sin = (fl >> TaskBits::kInSlot) & 511, sex = (fl >> TaskBits::kExSlot) & 511;
     const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
     const bool flip = (fl >> TaskBits::kFlip) & 1u;
@@ -695,80 +697,60 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     if (kind == kInterior) {
       const int wd_ex = wds[sex];
       const int dry = wd_in == 0 && wd_ex == 0;
-      tdry[w] = dry;
+      if (I == 0) tdry[ti] = dry;
       if (dry) continue;
       const int gex = sex < kTile ? tile0 + sex : gid[sex - kTile];
-      // the three points, then the dry-side rules (rare) as a second pass
-#pragma unroll 1
-      for (int I = 0; I < 3; ++I) {
-        const int gp_in = I, gp_ex = 2 - I;
-        double zi, xi, yi, hi, zx, xx, yx, hx;
-        slot_trace(B, qs, sin, led_in, gp_in, zi, xi, yi, hi);
-        slot_trace(B, qs, sex, led_ex, gp_ex, zx, xx, yx, hx);
-        const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
-        const double sfx = kSph ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
-        const Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
-        double* o = out + 5 * I;
-        o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
-      }
-      if (wd_in == 0 || wd_ex == 0) {
+      const int gp_in = I, gp_ex = 2 - I;
+      double zi, xi, yi, hi, zx, xx, yx, hx;
+      slot_trace(B, qs, sin, led_in, gp_in, zi, xi, yi, hi);
+      slot_trace(B, qs, sex, led_ex, gp_ex, zx, xx, yx, hx);
+      const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
+      const double sfx = kSph ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
+      const Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
+      o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
+      if ((wd_in == 0 || wd_ex == 0) && fabs(f.f) > 1.0e-8) {
         // internal_edge_hydro.F:212-302: mass flux out of / into a dry
         // element.  The four cases re-evaluate the flux once with changed
         // arguments: the dry side's state replaced by the wet side's with
         // reflected momentum (outflow from a dry element), or gravity off
         // (G = 0) for the dry side's momentum flux.
         const bool in_dry = wd_in == 0;
-#pragma unroll 1
-        for (int I = 0; I < 3; ++I) {
-          double* o = out + 5 * I;
-          const double F0 = o[0];
-          if (!(fabs(F0) > 1.0e-8)) continue;
-          const int gp_in = I, gp_ex = 2 - I;
-          double zi, xi, yi, hi, zx, xx, yx, hx;
-          slot_trace(B, qs, sin, led_in, gp_in, zi, xi, yi, hi);
-          slot_trace(B, qs, sex, led_ex, gp_ex, zx, xx, yx, hx);
-          const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
-          const double sfx = kSph ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
-          const double tx = -ny, ty = nx, den = nx * ty - ny * tx;
-          const bool reflect = in_dry ? F0 > 0.0 : F0 < 0.0;
-          // the wet side, whose momentum is reflected onto the dry side
-          const double qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
-          const double qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
-          const double qnr = -qnw, qtr = qtw;
-          const double qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
-          double a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
-          double a_hi = hi, a_hx = hx, a_si = sfi, a_sx = sfx, a_g = 0.0;
-          if (reflect) {
-            a_g = P.g;
-            if (in_dry) {
-              a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_si = sfx;
-            } else {
-              a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_sx = sfi;
-            }
-          }
-          const Flux3 r = llf<kNonlin>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_si, a_sx, nx, ny, a_g);
-          if (reflect) {
-            o[0] = r.f;
-            if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0.0; o[2] = 0.0; }
-            else        { o[1] = r.g; o[2] = r.h; o[3] = 0.0; o[4] = 0.0; }
+        const double F0 = f.f;
+        const double tx = -ny, ty = nx, den = nx * ty - ny * tx;
+        const bool reflect = in_dry ? F0 > 0.0 : F0 < 0.0;
+        // the wet side, whose momentum is reflected onto the dry side
+        const double qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
+        const double qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
+        const double qnr = -qnw, qtr = qtw;
+        const double qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
+        double a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
+        double a_hi = hi, a_hx = hx, a_si = sfi, a_sx = sfx, a_g = 0.0;
+        if (reflect) {
+          a_g = P.g;
+          if (in_dry) {
+            a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_si = sfx;
           } else {
-            if (in_dry) { o[1] = r.g; o[2] = r.h; }
-            else        { o[3] = r.g; o[4] = r.h; }
+            a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_sx = sfi;
           }
+        }
+        const Flux3 r = llf<kNonlin>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_si, a_sx, nx, ny, a_g);
+        if (reflect) {
+          o[0] = r.f;
+          if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0.0; o[2] = 0.0; }
+          else        { o[1] = r.g; o[2] = r.h; o[3] = 0.0; o[4] = 0.0; }
+        } else {
+          if (in_dry) { o[1] = r.g; o[2] = r.h; }
+          else        { o[3] = r.g; o[4] = r.h; }
         }
       }
     } else {
       if (wd_in == 0) continue;
-#pragma unroll 1
-      for (int I = 0; I < 3; ++I) {
-        double zi, xi, yi, hi, zx, xx, yx;
-        slot_trace(B, qs, sin, led_in, I, zi, xi, yi, hi);
-        const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
-        ghost_state(A, B, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
-        Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
-        double* o = out + 5 * I;
-        o[0] = f.f; o[1] = f.g; o[2] = f.h;
-      }
+      double zi, xi, yi, hi, zx, xx, yx;
+      slot_trace(B, qs, sin, led_in, I, zi, xi, yi, hi);
+      const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
+      ghost_state(A, B, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
+      Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
+      o[0] = f.f; o[1] = f.g; o[2] = f.h;
     }
   }
   __syncthreads();
