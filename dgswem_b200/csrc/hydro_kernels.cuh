@@ -31,6 +31,10 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async8_s(unsigned dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+}
 
 // DEPTH**(1.D0/3.D0) of the Manning friction (rhs_dg_hydro.F).  The strict
 // variant calls pow with the reference's exponent; the fast variant takes
@@ -633,33 +637,48 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     gid[tid] = hg;
   }
   {
-    // thread t: element t % kTile of every (kStageThreads / kTile)-th row
+    // thread t: element t % kTile of every (kStageThreads / kTile)-th row;
+    // shared addresses as 32-bit offsets, rows unrolled
     static_assert(kStageThreads % kTile == 0, "tile rows are copied by whole groups of kTile threads");
     constexpr int kRowStep = kStageThreads / kTile;
     const int w = tid % kTile, r0 = tid / kTile;
+    const unsigned qs_s = smem_addr(qs), geo_s = smem_addr(geo);
     if (w < n) {
       const int ngeo = m.manning ? EGeo::kSmemRows : EGeo::kNbar;
       const size_t step = (size_t)kRowStep * ne;
+      const unsigned qdst = qs_s + (unsigned)(w * kQStride + r0) * 8u;
       const double* src = A.qin + (size_t)r0 * ne + tile0 + w;
-      for (int r = r0; r < 9; r += kRowStep, src += step) cp_async8(qs + w * kQStride + r, src);
+#pragma unroll
+      for (int j = 0; j < (9 + kRowStep - 1) / kRowStep; ++j)
+        if (r0 + j * kRowStep < 9) cp_async8_s(qdst + 8u * kRowStep * j, src + j * step);
       src = m.hb + (size_t)r0 * ne + tile0 + w;
-      for (int r = r0; r < 3; r += kRowStep, src += step) cp_async8(qs + w * kQStride + 9 + r, src);
+#pragma unroll
+      for (int j = 0; j < (3 + kRowStep - 1) / kRowStep; ++j)
+        if (r0 + j * kRowStep < 3) cp_async8_s(qdst + 72u + 8u * kRowStep * j, src + j * step);
+      const unsigned gdst = geo_s + (unsigned)(r0 * kTile + w) * 8u;
       src = m.egeo + (size_t)r0 * ne + tile0 + w;
-      for (int r = r0; r < ngeo; r += kRowStep, src += step) cp_async8(geo + r * kTile + w, src);
-      for (int r = r0; r < 3; r += kRowStep) {
+#pragma unroll
+      for (int j = 0; j < (EGeo::kSmemRows + kRowStep - 1) / kRowStep; ++j)
+        if (r0 + j * kRowStep < ngeo) cp_async8_s(gdst + 8u * kRowStep * kTile * j, src + j * step);
+#pragma unroll
+      for (int j = 0; j < (3 + kRowStep - 1) / kRowStep; ++j) {
+        const int r = r0 + j * kRowStep;
         if (r == 0)
           cp_async4(wds + w, A.wd + tile0 + w);
-        else
+        else if (r < 3)
           cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
       }
     }
     for (int j = tid; j < nh; j += kStageThreads) {
       const int g = j == tid ? hg : m.tile_halo[hbeg + j];
       if (j != tid) gid[j] = g;
+      const unsigned hdst = qs_s + (unsigned)((kTile + j) * kQStride) * 8u;
+      const double* q0 = A.qin + g;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) cp_async8(qs + (kTile + j) * kQStride + c, A.qin + (size_t)c * ne + g);
+      for (int c = 0; c < 9; ++c) cp_async8_s(hdst + 8u * c, q0 + (size_t)c * ne);
+      const double* h0 = m.hb + g;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) cp_async8(qs + (kTile + j) * kQStride + 9 + k, m.hb + (size_t)k * ne + g);
+      for (int k = 0; k < 3; ++k) cp_async8_s(hdst + 72u + 8u * k, h0 + (size_t)k * ne);
       cp_async4(wds + kTile + j, A.wd + g);
     }
     cp_async_wait_all();
