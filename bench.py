@@ -218,8 +218,14 @@ def main(argv=None):
     workdir = Path(args.workdir)
     workdir.mkdir(parents=True, exist_ok=True)
     path = ensure_deck(workdir, args.nx, args.ny, rank, world, dist if world > 1 else None)
+    # host setup: deck read + edge graph (READ_INPUT/PREP_DG), then device
+    # create (orders, tile plan, geometry table, uploads); wall clock
+    t_setup0 = time.perf_counter()
     deck = Deck(path)
+    t_setup1 = time.perf_counter()
     hs = HydroStep(deck, device=local)
+    torch.cuda.synchronize()
+    t_setup2 = time.perf_counter()
     ne, nrk = hs.ne, hs.nrk
     # all work on one dedicated stream; the events below are recorded on it
     stream = torch.cuda.Stream()
@@ -302,6 +308,7 @@ def main(argv=None):
         "data": "synthetic (seeded sloping-beach deck; no public dataset)",
         "config": workload_config(args, ne, nrk),
         "gpu_launches": int(launches),
+        "setup_s": {"deck_read": t_setup1 - t_setup0, "device_create": t_setup2 - t_setup1},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes,

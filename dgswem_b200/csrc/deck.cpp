@@ -19,11 +19,14 @@
 
 #include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <string_view>
+#include <system_error>
 #include <unordered_map>
 #include <vector>
 
@@ -33,68 +36,121 @@ constexpr double kPi = 3.141592653589793;
 constexpr double kDegToRad = kPi / 180.0;
 constexpr double kEarthRadius = 6378206.4;
 
-// A file read as Fortran list-directed records.
+// A file read as Fortran list-directed records: the whole file in one
+// buffer, records as (offset, length) pairs, fields as views into the buffer
+// (the node and element loops of a 2M-element fort.14 allocate nothing).
 class ListStream {
  public:
   bool load(const std::string& path) {
-    std::ifstream in(path);
+    std::ifstream in(path, std::ios::binary);
     if (!in) return false;
     path_ = path;
-    std::string s;
-    while (std::getline(in, s)) {
-      if (!s.empty() && s.back() == '\r') s.pop_back();
-      rec_.push_back(std::move(s));
+    in.seekg(0, std::ios::end);
+    const std::streamoff size = in.tellg();
+    in.seekg(0, std::ios::beg);
+    buf_.resize(size > 0 ? (size_t)size : 0);
+    if (size > 0) in.read(&buf_[0], size);
+    size_t i = 0, n = buf_.size();
+    while (i < n) {
+      size_t j = buf_.find('\n', i);
+      if (j == std::string::npos) j = n;
+      size_t len = j - i;
+      if (len > 0 && buf_[i + len - 1] == '\r') --len;
+      rec_.push_back({i, len});
+      i = j + 1;
     }
     return true;
   }
   const std::string& path() const { return path_; }
-  const std::vector<std::string>& records() const { return rec_; }
-  std::string record() {
-    if (next_ >= rec_.size()) throw dgswem::Failure(DGSWEM_ERR_IO, "premature end of " + path_);
-    return rec_[next_++];
+  std::vector<std::string> records() const {
+    std::vector<std::string> out;
+    out.reserve(rec_.size());
+    for (const auto& r : rec_) out.emplace_back(buf_, r.first, r.second);
+    return out;
   }
-  static void tokens(const std::string& s, std::vector<std::string>* out) {
+  std::string_view record_view() {
+    if (next_ >= rec_.size()) throw dgswem::Failure(DGSWEM_ERR_IO, "premature end of " + path_);
+    const auto& r = rec_[next_++];
+    return std::string_view(buf_.data() + r.first, r.second);
+  }
+  std::string record() { return std::string(record_view()); }
+  // fields of a record up to a '/' (end of the READ), blanks and commas separate
+  template <typename Out>
+  static void tokens(std::string_view s, Out* out) {
     size_t i = 0, n = s.size();
     while (i < n) {
       while (i < n && (std::isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
       if (i >= n || s[i] == '/') return;
       size_t j = i;
       while (j < n && !std::isspace((unsigned char)s[j]) && s[j] != ',' && s[j] != '/') ++j;
-      out->push_back(s.substr(i, j - i));
+      out->emplace_back(s.substr(i, j - i));
       i = j;
       if (i < n && s[i] == '/') return;
     }
   }
-  // one READ(u,*) of `n` items: starts a new record, spills onto following ones
-  std::vector<std::string> read(size_t n) {
-    std::vector<std::string> v;
-    while (v.size() < n) {
-      std::vector<std::string> t;
-      tokens(record(), &t);
-      for (size_t k = 0; k < t.size() && v.size() < n; ++k) v.push_back(t[k]);
+  // one READ(u,*) of `n` items into views: starts a new record, spills onto
+  // following ones
+  void read_fields(size_t n, std::string_view* out) {
+    size_t got = 0;
+    while (got < n) {
+      std::string_view s = record_view();
+      size_t i = 0, len = s.size();
+      while (i < len && got < n) {
+        while (i < len && (std::isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
+        if (i >= len || s[i] == '/') break;
+        size_t j = i;
+        while (j < len && !std::isspace((unsigned char)s[j]) && s[j] != ',' && s[j] != '/') ++j;
+        out[got++] = s.substr(i, j - i);
+        i = j;
+        if (i < len && s[i] == '/') break;
+      }
     }
-    return v;
   }
-  double real() { return as_real(read(1)[0]); }
-  int integer() { return as_int(read(1)[0]); }
-  static double as_real(std::string s) {
-    for (char& c : s)
+  std::vector<std::string> read(size_t n) {
+    std::vector<std::string_view> v(n);
+    read_fields(n, v.data());
+    return std::vector<std::string>(v.begin(), v.end());
+  }
+  double real() {
+    std::string_view v;
+    read_fields(1, &v);
+    return as_real(v);
+  }
+  int integer() {
+    std::string_view v;
+    read_fields(1, &v);
+    return as_int(v);
+  }
+  // Fortran reals, including D exponents
+  static double as_real(std::string_view s) {
+    double v = 0.0;
+    const char* b = s.data();
+    const char* e = b + s.size();
+    if (!s.empty() && *b == '+') ++b;
+    auto r = std::from_chars(b, e, v);
+    if (r.ec == std::errc() && r.ptr == e) return v;
+    std::string t(s);
+    for (char& c : t)
       if (c == 'd' || c == 'D') c = 'e';
     char* end = nullptr;
-    double v = std::strtod(s.c_str(), &end);
-    if (end == s.c_str()) throw dgswem::Failure(DGSWEM_ERR_IO, "expected a real, got '" + s + "'");
+    v = std::strtod(t.c_str(), &end);
+    if (end == t.c_str()) throw dgswem::Failure(DGSWEM_ERR_IO, "expected a real, got '" + t + "'");
     return v;
   }
-  static int as_int(const std::string& s) {
-    char* end = nullptr;
-    long v = std::strtol(s.c_str(), &end, 10);
-    if (end == s.c_str()) throw dgswem::Failure(DGSWEM_ERR_IO, "expected an integer, got '" + s + "'");
+  static int as_int(std::string_view s) {
+    long v = 0;
+    const char* b = s.data();
+    const char* e = b + s.size();
+    if (!s.empty() && *b == '+') ++b;
+    auto r = std::from_chars(b, e, v);
+    if (r.ec != std::errc() || r.ptr == b) throw dgswem::Failure(DGSWEM_ERR_IO, "expected an integer, got '" + std::string(s) + "'");
     return (int)v;
   }
 
  private:
   std::string path_;
-  std::vector<std::string> rec_;
+  std::string buf_;
+  std::vector<std::pair<size_t, size_t>> rec_;
   size_t next_ = 0;
 };
 
@@ -222,13 +278,15 @@ void read_fort13(const std::string& dir, dgswem_deck* d) {
       d->manning.assign(d->s.np, defaults[name]);
     }
     for (int i = 0; i < count; ++i) {
-      std::string r = f.record();
-      if (!take) continue;
-      std::vector<std::string> t;
-      ListStream::tokens(r, &t);
-      int node = ListStream::as_int(t.at(0));
+      if (!take) {
+        f.record_view();
+        continue;
+      }
+      std::string_view t[2];
+      f.read_fields(2, t);
+      int node = ListStream::as_int(t[0]);
       if (node < 1 || node > d->s.np) throw dgswem::Failure(DGSWEM_ERR_IO, "fort.13 node out of range");
-      d->manning[node - 1] = ListStream::as_real(t.at(1));
+      d->manning[node - 1] = ListStream::as_real(t[1]);
     }
   }
   if (!found) throw dgswem::Failure(DGSWEM_ERR_IO, "fort.13 has no mannings_n_at_sea_floor data");
@@ -293,7 +351,8 @@ void read_fort14_15(const std::string& dir, dgswem_deck* d, Fort15* p) {
   const int np = s.np, ne = s.ne;
   d->x.assign(np, 0.0); d->y.assign(np, 0.0); d->dp.assign(np, 0.0); d->sfea.assign(np, 0.0);
   for (int i = 0; i < np; ++i) {
-    auto t = f14.read(4);
+    std::string_view t[4];
+    f14.read_fields(4, t);
     int id = ListStream::as_int(t[0]);
     if (id < 1 || id > np) throw dgswem::Failure(DGSWEM_ERR_IO, "node number out of range in fort.14");
     double a = ListStream::as_real(t[1]), b = ListStream::as_real(t[2]);
@@ -313,7 +372,8 @@ void read_fort14_15(const std::string& dir, dgswem_deck* d, Fort15* p) {
     for (double& v : d->dp) v = std::max(v, s.h0);  // read_input.F:1356
   d->nm.assign(3 * (size_t)ne, 0);
   for (int i = 0; i < ne; ++i) {
-    auto t = f14.read(5);
+    std::string_view t[5];
+    f14.read_fields(5, t);
     int id = ListStream::as_int(t[0]);
     if (id < 1 || id > ne) throw dgswem::Failure(DGSWEM_ERR_IO, "element number out of range in fort.14");
     for (int v = 0; v < 3; ++v) {
