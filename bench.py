@@ -52,6 +52,23 @@ def rank_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(ms: float, world: int, dist=None, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank's device-timed milliseconds reduced
+    with MAX (NCCL on the GPUs; gloo with device="cpu")."""
+    if world <= 1 or dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, ne: int, nrk: int, steps: int, ms: float) -> float:
+    """DOF-stage updates/s of the whole job: every rank steps its own basin
+    of ne elements (weak scaling), timed by the slowest rank."""
+    return world * DOFS_PER_ELEMENT * ne * nrk * steps / (ms / 1e3)
+
+
 def ensure_deck(workdir: Path, nx: int, ny: int, rank: int, world: int, dist=None) -> Path:
     from dgswem_b200 import decks
     path = workdir / f"sloping_beach_{nx}x{ny}"
@@ -253,13 +270,10 @@ def main(argv=None):
     clocks = sampler.stop()
     launches = hs.kernel_launches - launches0
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, dist if world > 1 else None, "cuda")
     hs.synchronize()
     it0 += args.steps
-    value = world * DOFS_PER_ELEMENT * ne * nrk * args.steps / (ms_max / 1e3)
+    value = whole_job_rate(world, ne, nrk, args.steps, ms_max)
 
     # per-kernel event timing of the dominant kernel (same stream)
     prof_steps = 20
@@ -293,11 +307,8 @@ def main(argv=None):
         hs.download_into(nz, nqx, nqy, nwd)
     x1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = x0.elapsed_time(x1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * DOFS_PER_ELEMENT * ne * nrk * args.e2e_steps / (float(te.item()) / 1e3)
+    e2e_ms = max_over_ranks(x0.elapsed_time(x1), world, dist if world > 1 else None, "cuda")
+    e2e_value = whole_job_rate(world, ne, nrk, args.e2e_steps, e2e_ms)
     state_bytes = 9 * 8 * ne + 4 * ne
     hs.synchronize()
 
