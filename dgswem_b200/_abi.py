@@ -57,6 +57,17 @@ SIGNATURES = {
     "dgswem_cuda_set_met": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "dgswem_cuda_modal2nodal": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_modal2nodal_noalloc": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
+    "dgswem_cuda_create_part": (C.c_int, [C.POINTER(Setup), C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.POINTER(C.c_void_p)]),
+    "dgswem_cuda_part_info": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
+    "dgswem_cuda_stage_rhs": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dgswem_cuda_stage_limit": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_step_end": (C.c_int, [C.c_void_p]),
+    "dgswem_cuda_halo_count": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _ip, _ip]),
+    "dgswem_cuda_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "dgswem_cuda_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "dgswem_part_halo_ids": (C.c_int, [C.POINTER(Setup), C.c_int, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip,
+                                       _ip]),
     "dgswem_cuda_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "dgswem_cuda_last_error": (C.c_int, [C.c_char_p, C.c_int]),
     "dgswem_cuda_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

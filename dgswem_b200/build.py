@@ -23,8 +23,8 @@ LIBNAME = "libdgswem_cuda.so"
 # (source, extra nvcc flags): the strict kernel variant is compiled without
 # fused multiply-add contraction
 SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_strict.cu", ["-fmad=false"]),
-           ("deck.cpp", [])]
-HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h"]
+           ("deck.cpp", []), ("partition.cpp", [])]
+HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]

@@ -13,6 +13,7 @@
 #include "abi_util.h"
 #include "dgswem_cuda.h"
 #include "hydro_device.cuh"
+#include "partition.h"
 
 namespace dgswem {
 
@@ -147,15 +148,17 @@ struct Variant {
   void (*f2s)(const double*, double*, int, int, const int*, unsigned, cudaStream_t);
   void (*s2f)(const double*, double*, int, int, const int*, unsigned, cudaStream_t);
   void (*gather_int)(const int*, int*, const int*, int, unsigned, cudaStream_t);
+  void (*halo)(bool, double*, int*, int, const int*, int, int, double*, cudaStream_t);
 };
 
 static const Variant kFast = {fast::set_basis, fast::launch_stage, fast::launch_ibarrier, fast::launch_node_minmax,
                               fast::launch_limit_wetdry, fast::launch_modal2nodal,
-                              fast::launch_fortran_to_soa, fast::launch_soa_to_fortran, fast::launch_gather_int};
+                              fast::launch_fortran_to_soa, fast::launch_soa_to_fortran, fast::launch_gather_int,
+                              fast::launch_halo};
 static const Variant kStrict = {strict::set_basis, strict::launch_stage, strict::launch_ibarrier, strict::launch_node_minmax,
                                 strict::launch_limit_wetdry, strict::launch_modal2nodal,
                                 strict::launch_fortran_to_soa, strict::launch_soa_to_fortran,
-                                strict::launch_gather_int};
+                                strict::launch_gather_int, strict::launch_halo};
 
 }  // namespace dgswem
 
@@ -199,7 +202,12 @@ struct dgswem_cuda {
   DevBuf<int> wd, nodecode, wd_staging;
   DevBuf<int> perm, inv;  // device element order: perm[new] = input id, inv[input] = new
   DevBuf<int> node_perm;  // device node order: node_perm[new] = input id
-  std::vector<int> node_perm_h;
+  std::vector<int> node_perm_h, perm_h;
+  // partition (a single one for dgswem_cuda_create): local = owned + ghosts
+  int nparts = 1, part = 0, n_own = 0, ne_glob = 0, np_glob = 0;
+  // halo index lists (local element ids) per kind and peer: send then receive
+  DevBuf<int> halo_idx;
+  std::vector<size_t> halo_off[2][2];  // [kind][send 0 / recv 1][peer..peer+1]
   DevBuf<unsigned> err;
   long long launches = 0;
   // per-kernel event timing (dgswem_cuda_profile)
@@ -279,7 +287,10 @@ unsigned grid_for(int n, int block) { return (unsigned)((n + block - 1) / block)
 // both tiles, each for its own element, in the reference's in/ex orientation.
 // Tasks: interior edges in element order, then the boundary kinds grouped, so
 // that a warp's tasks mostly take one branch.
-void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const std::vector<unsigned>& einfo) {
+// Tiles cover the first n_tiled elements (the owned ones); `ne` is the row
+// stride of link (all local elements, ghosts included).
+void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>& link,
+                     const std::vector<unsigned>& einfo) {
   // Tiles: consecutive elements, at most kTile of them and at most
   // kStageThreads edge tasks (one pass of the block over its tasks).  An
   // element adds a task per listed boundary edge and per interior edge whose
@@ -287,7 +298,7 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
   std::vector<int> elem_ptr(1, 0);
   {
     int t0 = 0, count = 0;
-    for (int e = 0; e < ne; ++e) {
+    for (int e = 0; e < n_tiled; ++e) {
       int add = 0;
       for (int l = 0; l < 3; ++l) {
         const unsigned kind = ei_kind(einfo[e], l);
@@ -307,7 +318,7 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
       }
       count += add;
     }
-    elem_ptr.push_back(ne);
+    elem_ptr.push_back(n_tiled);
   }
   const int ntile = (int)elem_ptr.size() - 1;
   std::vector<int> task_ptr(ntile + 1, 0), halo_ptr(ntile + 1, 0), halo;
@@ -407,36 +418,13 @@ void build_tile_plan(dgswem_cuda* h, int ne, const std::vector<int>& link, const
 // (stable sorts, ties keep the input order).  A stage tile of consecutive
 // elements is then a compact patch of the mesh with a short perimeter -- few
 // edges to other tiles, a small halo -- and the nodes an element touches lie
-// close together in memory.  perm[new] = input index.  Nothing in the
+// close together in memory.  perm[local] = input index.  Nothing in the
 // arithmetic depends on the numbering: edge orientation (NEDEL), the
 // interior-edge order (edge numbers) and the node stars (built in input
-// element order) are those of the input mesh.
-std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py) {
-  const int n = (int)px.size();
-  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
-  for (int i = 0; i < n; ++i) {
-    x0 = std::min(x0, px[i]); x1 = std::max(x1, px[i]);
-    y0 = std::min(y0, py[i]); y1 = std::max(y1, py[i]);
-  }
-  const double span = std::max(std::max(x1 - x0, y1 - y0), 1e-300);
-  auto spread = [](uint64_t v) {  // bits of v at the even positions
-    uint64_t r = 0;
-    for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1u) << (2 * b);
-    return r;
-  };
-  std::vector<uint64_t> key(n);
-  const double scale = (double)((1u << 21) - 1) / span;
-  for (int i = 0; i < n; ++i) {
-    const uint64_t ix = (uint64_t)((px[i] - x0) * scale), iy = (uint64_t)((py[i] - y0) * scale);
-    key[i] = spread(ix) | spread(iy) << 1;
-  }
-  std::vector<int> perm(n);
-  for (int i = 0; i < n; ++i) perm[i] = i;
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
-  return perm;
-}
-
-void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
+// element order) are those of the input mesh.  A partitioned handle keeps
+// its owned elements (a contiguous range of the global Morton order) first,
+// then its ghost elements (partition.h).
+void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& plan) {
   const int ne = s->ne, np = s->np, ned = s->nedges;
   auto need = [](bool ok, const char* what) {
     if (!ok) throw Failure(DGSWEM_ERR_ARG, what);
@@ -444,40 +432,33 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   need(s->nm && s->x && s->y && s->dp && s->neled && s->nedel && s->nedsd && s->hb, "setup lacks mesh arrays");
   need(s->ze && s->qx && s->qy && s->wdflg, "setup lacks the initial state");
   need(s->atvd && s->btvd && s->dtvd, "setup lacks RK tables");
-  // nodes, connectivity, in the device element order
-  for (int e = 0; e < ne; ++e)
-    for (int v = 0; v < 3; ++v) {
-      const int n = s->nm[e + (size_t)ne * v];
-      need(n >= 1 && n <= np, "NM refers to a node outside 1..NP");
-    }
-  std::vector<int> perm, inv(ne), node_perm, node_inv(np);
+  // local elements (owned, then ghosts) and the nodes they touch
+  const std::vector<int>& perm = plan.local;
+  const int nl = (int)perm.size(), n_own = plan.n_own;
+  std::vector<int> inv(ne, -1);
+  for (int i = 0; i < nl; ++i) inv[perm[i]] = i;
+  std::vector<int> node_perm, node_inv(np, -1);
   {
-    std::vector<double> cx(ne), cy(ne);
-    for (int e = 0; e < ne; ++e) {
-      double sx = 0.0, sy = 0.0;
-      for (int v = 0; v < 3; ++v) {
-        const int n = s->nm[e + (size_t)ne * v] - 1;
-        sx += s->x[n];
-        sy += s->y[n];
-      }
-      cx[e] = sx / 3.0;
-      cy[e] = sy / 3.0;
-    }
-    perm = morton_order(cx, cy);
-    node_perm = morton_order(std::vector<double>(s->x, s->x + np), std::vector<double>(s->y, s->y + np));
+    std::vector<char> used(np, 0);
+    for (int i = 0; i < nl; ++i)
+      for (int v = 0; v < 3; ++v) used[s->nm[perm[i] + (size_t)ne * v] - 1] = 1;
+    const std::vector<int> norder =
+        morton_order(std::vector<double>(s->x, s->x + np), std::vector<double>(s->y, s->y + np));
+    for (int n : norder)
+      if (used[n]) node_perm.push_back(n);
   }
-  for (int i = 0; i < ne; ++i) inv[perm[i]] = i;
-  for (int i = 0; i < np; ++i) node_inv[node_perm[i]] = i;
+  const int npl = (int)node_perm.size();
+  for (int i = 0; i < npl; ++i) node_inv[node_perm[i]] = i;
   // nodal arrays in the device node order
   auto node_permuted = [&](const double* a) {
-    std::vector<double> out(np);
-    for (int i = 0; i < np; ++i) out[i] = a[node_perm[i]];
+    std::vector<double> out(npl);
+    for (int i = 0; i < npl; ++i) out[i] = a[node_perm[i]];
     return out;
   };
   const std::vector<double> xd = node_permuted(s->x), yd = node_permuted(s->y);
-  std::vector<int> nm(3 * (size_t)ne);
-  for (int e = 0; e < ne; ++e)
-    for (int v = 0; v < 3; ++v) nm[(size_t)v * ne + inv[e]] = node_inv[s->nm[e + (size_t)ne * v] - 1];
+  std::vector<int> nm(3 * (size_t)nl);
+  for (int i = 0; i < nl; ++i)
+    for (int v = 0; v < 3; ++v) nm[(size_t)v * nl + i] = node_inv[s->nm[perm[i] + (size_t)ne * v] - 1];
   // boundary membership of each edge: kind, list index, side
   std::vector<int> bkind(ned + 1, -1), bidx(ned + 1, -1), bside(ned + 1, 0);
   auto mark = [&](const int* list, int n, unsigned kind) {
@@ -508,10 +489,12 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
       ib_elem[2 * L + side] = inv[s->nedel[2 * (size_t)(g - 1)] - 1];
       ib_led[2 * L + side] = s->nedsd[2 * (size_t)(g - 1)] - 1;
     }
+    if (ib_elem[2 * L] < 0 || ib_elem[2 * L + 1] < 0) ib_elem[2 * L] = ib_elem[2 * L + 1] = -1;  // not local
   }
-  std::vector<int> link(3 * (size_t)ne, -1);
-  std::vector<unsigned> einfo(ne, 0u);
-  for (int e = 0; e < ne; ++e) {
+  std::vector<int> link(3 * (size_t)nl, -1);
+  std::vector<unsigned> einfo(nl, 0u);
+  for (int i = 0; i < nl; ++i) {
+    const int e = perm[i];
     unsigned info = 0u;
     std::array<std::pair<long long, int>, 3> key;
     for (int l = 0; l < 3; ++l) {
@@ -529,6 +512,12 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
         lk = inv[(first ? b : a) - 1];
         nled = (unsigned)(s->nedsd[2 * (size_t)(g - 1) + (first ? 1 : 0)] - 1);
         key[l] = {(long long)8 << 40 | g, l};  // interior edges last, in edge-number order
+        if (lk < 0) {  // a ghost's neighbour outside the partition: never evaluated
+          need(i >= n_own, "partition halo lacks an edge neighbour of an owned element");
+          kind = kNone;
+          flag = 0;
+          nled = 0;
+        }
       } else if (bkind[g] >= 0) {
         kind = (unsigned)bkind[g];
         lk = bidx[g];
@@ -539,29 +528,34 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
         lk = -1;
         key[l] = {(long long)9 << 40, l};
       }
-      link[(size_t)l * ne + inv[e]] = lk;
+      link[(size_t)l * nl + i] = lk;
       info |= kind << (3 * l);
       info |= flag << (9 + l);
       info |= (nled & 3u) << (12 + 2 * l);
     }
     std::sort(key.begin(), key.end());
     for (int slot = 0; slot < 3; ++slot) info |= (unsigned)key[slot].second << (18 + 2 * slot);
-    einfo[inv[e]] = info;
+    einfo[i] = info;
   }
-  build_tile_plan(h, ne, link, einfo);
+  build_tile_plan(h, n_own, nl, link, einfo);
   // node -> element star in the input element order (the order of the
-  // reference's loops over elements), holding device element ids
-  std::vector<int> sp(np + 1, 0), st(3 * (size_t)ne);
-  for (int e = 0; e < ne; ++e)
-    for (int v = 0; v < 3; ++v) ++sp[nm[(size_t)v * ne + e] + 1];
-  for (int n = 0; n < np; ++n) sp[n + 1] += sp[n];
+  // reference's loops over elements), holding device element ids; complete
+  // for every node of an owned element
+  std::vector<int> sp(npl + 1, 0), st(3 * (size_t)nl);
+  for (int i = 0; i < nl; ++i)
+    for (int v = 0; v < 3; ++v) ++sp[nm[(size_t)v * nl + i] + 1];
+  for (int n = 0; n < npl; ++n) sp[n + 1] += sp[n];
   {
     std::vector<int> cur(sp.begin(), sp.end() - 1);
-    for (int e = 0; e < ne; ++e)
-      for (int v = 0; v < 3; ++v) st[cur[nm[(size_t)v * ne + inv[e]]]++] = inv[e];
+    for (int e = 0; e < ne; ++e) {
+      const int i = inv[e];
+      if (i < 0) continue;
+      for (int v = 0; v < 3; ++v) st[cur[nm[(size_t)v * nl + i]]++] = i;
+    }
   }
   h->perm.upload(perm);
   h->inv.upload(inv);
+  h->perm_h = perm;
   h->nm.upload(nm);
   h->link.upload(link);
   h->einfo.upload(einfo);
@@ -574,9 +568,9 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   h->x.upload(xd);
   h->y.upload(yd);
   h->dp.upload(node_permuted(s->dp));
-  std::vector<double> hb(3 * (size_t)ne);
-  for (int e = 0; e < ne; ++e)
-    for (int k = 0; k < 3; ++k) hb[(size_t)k * ne + inv[e]] = s->hb[k + (size_t)s->dofh * e];
+  std::vector<double> hb(3 * (size_t)nl);
+  for (int i = 0; i < nl; ++i)
+    for (int k = 0; k < 3; ++k) hb[(size_t)k * nl + i] = s->hb[k + (size_t)s->dofh * perm[i]];
   h->hb.upload(hb);
   // per-element coefficients: a scalar when uniform
   auto uniform = [&](const double* a, double* val) {
@@ -588,8 +582,8 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   };
   double c0 = 0.0, f0 = s->cf;
   auto permuted = [&](const double* a) {
-    std::vector<double> out(ne);
-    for (int i = 0; i < ne; ++i) out[i] = a[perm[i]];
+    std::vector<double> out(nl);
+    for (int i = 0; i < nl; ++i) out[i] = a[perm[i]];
     return out;
   };
   if (!uniform(s->cori_el, &c0)) h->cori.upload(permuted(s->cori_el));
@@ -603,13 +597,13 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   // element geometry table (EGeo rows): the reference's formulas evaluated
   // once, in the same order as the oracle, instead of every stage
   {
-    std::vector<double> eg((size_t)EGeo::kRows * ne, 0.0);
-    auto at = [&](int r, int e) -> double& { return eg[(size_t)r * ne + e]; };
-    for (int e = 0; e < ne; ++e) {
+    std::vector<double> eg((size_t)EGeo::kRows * nl, 0.0);
+    auto at = [&](int r, int e) -> double& { return eg[(size_t)r * nl + e]; };
+    for (int e = 0; e < nl; ++e) {
       double xs[3], ys[3];
       for (int v = 0; v < 3; ++v) {
-        xs[v] = xd[nm[(size_t)v * ne + e]];
-        ys[v] = yd[nm[(size_t)v * ne + e]];
+        xs[v] = xd[nm[(size_t)v * nl + e]];
+        ys[v] = yd[nm[(size_t)v * nl + e]];
       }
       const double areas = (xs[0] - xs[2]) * (ys[1] - ys[2]) + (xs[2] - xs[1]) * (ys[0] - ys[2]);
       at(EGeo::kAreas, e) = areas;
@@ -628,29 +622,29 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
       at(EGeo::kDrdy, e) = 1.0 / area * (xs[0] - xs[2]);
       at(EGeo::kDsdy, e) = 1.0 / area * (xs[1] - xs[0]);
       if (s->load_manning)
-        at(EGeo::kNbar, e) = (s->manning[node_perm[nm[e]]] + s->manning[node_perm[nm[(size_t)ne + e]]] +
-                              s->manning[node_perm[nm[(size_t)2 * ne + e]]]) / 3.;
+        at(EGeo::kNbar, e) = (s->manning[node_perm[nm[e]]] + s->manning[node_perm[nm[(size_t)nl + e]]] +
+                              s->manning[node_perm[nm[(size_t)2 * nl + e]]]) / 3.;
     }
     h->egeo.upload(eg);
   }
   if (s->ics == 2) {  // SFAC_ELEM / SFACED (prep_DG.F:1055-1100), host cos
     const BasisP1 B = make_basis_p1();
     const double R = 6378206.4;
-    std::vector<double> sa(3 * (size_t)ne), se(9 * (size_t)ne);
-    for (int e = 0; e < ne; ++e) {
-      const double y1 = yd[nm[e]], y2 = yd[nm[(size_t)ne + e]], y3 = yd[nm[(size_t)2 * ne + e]];
+    std::vector<double> sa(3 * (size_t)nl), se(9 * (size_t)nl);
+    for (int e = 0; e < nl; ++e) {
+      const double y1 = yd[nm[e]], y2 = yd[nm[(size_t)nl + e]], y3 = yd[nm[(size_t)2 * nl + e]];
       const double yd[3] = {1.0 / 3.0 * (y1 + y2 + y3), -(1.0 / 6.0 * (y1 + y2)) + 1.0 / 3.0 * y3,
                             -(0.5 * y1) + 0.5 * y2};
       for (int i = 0; i < 3; ++i) {
         double yel = 0.0;
         for (int k = 0; k < 3; ++k) yel = yel + yd[k] * B.phi_area[k][i];
-        sa[(size_t)i * ne + e] = std::cos(s->sfea0) / std::cos(yel / R);
+        sa[(size_t)i * nl + e] = std::cos(s->sfea0) / std::cos(yel / R);
       }
       for (int l = 0; l < 3; ++l)
         for (int i = 0; i < 3; ++i) {
           double yed = 0.0;
           for (int k = 0; k < 3; ++k) yed = yed + yd[k] * B.phi_edge[l][i][k];
-          se[(size_t)(l * 3 + i) * ne + e] = std::cos(s->sfea0) / std::cos(yed / R);
+          se[(size_t)(l * 3 + i) * nl + e] = std::cos(s->sfea0) / std::cos(yed / R);
         }
     }
     h->sfac_area.upload(sa);
@@ -681,8 +675,15 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
     h->ib_rhs.alloc(18 * (size_t)s->nibseg);
   }
   MeshView& m = h->mesh;
-  m.ne = ne;
-  m.np = np;
+  m.ne = nl;
+  m.np = npl;
+  h->ne = nl;
+  h->np = npl;
+  h->n_own = n_own;
+  h->ne_glob = ne;
+  h->np_glob = np;
+  h->nparts = plan.nparts;
+  h->part = plan.part;
   m.x = h->x.p; m.y = h->y.p; m.dp = h->dp.p; m.nm = h->nm.p; m.link = h->link.p; m.einfo = h->einfo.p;
   m.hb = h->hb.p; m.egeo = h->egeo.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
   m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
@@ -702,20 +703,46 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s) {
   m.ibht = h->ibht.p; m.ibcfsb = h->ibcfsb.p; m.ibcfsp = h->ibcfsp.p;
 }
 
+// Halo index lists of a partitioned handle (local element ids), per kind,
+// send lists then receive lists, peer by peer (partition.h).
+void build_halo(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& plan) {
+  std::vector<int> inv(s->ne, -1);
+  for (size_t i = 0; i < plan.local.size(); ++i) inv[plan.local[i]] = (int)i;
+  std::vector<int> idx;
+  for (int k = 0; k < 2; ++k)
+    for (int dir = 0; dir < 2; ++dir) {
+      auto& off = h->halo_off[k][dir];
+      off.assign(1, idx.size());
+      const auto& lists = dir == 0 ? plan.send[k] : plan.recv[k];
+      for (int q = 0; q < plan.nparts; ++q) {
+        for (int e : lists[q]) {
+          const int i = inv[e];
+          if (i < 0 || (dir == 0) != (i < plan.n_own))
+            throw Failure(DGSWEM_ERR_ARG, "partition halo list refers to an element of the wrong kind");
+          idx.push_back(i);
+        }
+        off.push_back(idx.size());
+      }
+    }
+  h->halo_idx.upload(idx.empty() ? std::vector<int>(1, 0) : idx);
+}
+
+// Host state (Fortran layout, input element order, all NE elements) -> the
+// local elements' device state (stage buffer 1) and WDFLG.
 void upload_state(dgswem_cuda* h, const double* ze, const double* qx, const double* qy, const int* wdflg) {
-  const int ne = h->ne;
-  h->staging.ensure(3 * (size_t)ne);
+  const int nl = h->ne, ng = h->ne_glob;
+  h->staging.ensure(3 * (size_t)ng);
   const double* src[3] = {ze, qx, qy};
   for (int var = 0; var < 3; ++var) {
     if (!src[var]) continue;
-    DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], 3 * (size_t)ne * sizeof(double), cudaMemcpyHostToDevice,
+    DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], 3 * (size_t)ng * sizeof(double), cudaMemcpyHostToDevice,
                             h->stream));
-    h->v->f2s(h->staging.p, h->q[0].p, ne, var, h->perm.p, grid_for(ne, kPointBlock), h->stream);
+    h->v->f2s(h->staging.p, h->q[0].p, nl, var, h->perm.p, grid_for(nl, kPointBlock), h->stream);
     check_launch(h, "fortran_to_soa");
   }
   if (wdflg) {
-    DG_CUDA(cudaMemcpyAsync(h->wd_staging.p, wdflg, (size_t)ne * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    h->v->gather_int(h->wd_staging.p, h->wd.p, h->perm.p, ne, grid_for(ne, kPointBlock), h->stream);
+    DG_CUDA(cudaMemcpyAsync(h->wd_staging.p, wdflg, (size_t)ng * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    h->v->gather_int(h->wd_staging.p, h->wd.p, h->perm.p, nl, grid_for(nl, kPointBlock), h->stream);
     check_launch(h, "gather_int");
   }
   DG_CUDA(cudaStreamSynchronize(h->stream));
@@ -764,8 +791,10 @@ void stage_forcing(const dgswem_cuda* h, double timedg, double rampdg, double* o
   }
 }
 
-void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
-  const int nrk = h->nrk, ne = h->ne;
+// One RK stage: the stage kernel writes stage buffer irk for the owned
+// elements (launch_stage_rhs), then the limiter and WETDRY (launch_limit).
+void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing) {
+  const int nrk = h->nrk;
   StageArgs A{};
   A.m = h->mesh;
   A.ph = h->ph;
@@ -799,6 +828,10 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
     h->v->stage(A, nonlin, (unsigned)h->ntile, h->stage_smem, h->stream);
     t.done();
   }
+}
+
+// SLOPELIMITER5 and WETDRY on stage buffer irk (owned elements)
+void launch_limit(dgswem_cuda* h, int irk) {
   const bool wetdry = h->nolifa >= 2;
   if (h->slopeflag != 0 || wetdry) {
     LimitArgs L{};
@@ -809,6 +842,7 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
     L.wd = h->wd.p;
     L.slopeflag = h->slopeflag;
     L.wetdry = wetdry ? 1 : 0;
+    L.ne_act = h->n_own;
     L.err = h->err.p;
     if (h->slopeflag != 0) {
       LaunchTimer t(h, 1);
@@ -816,13 +850,18 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
       t.done();
     }
     LaunchTimer t(h, 2);
-    h->v->limit_wetdry(L, grid_for(ne, kPointBlock), h->stream);
+    h->v->limit_wetdry(L, grid_for(h->n_own, kPointBlock), h->stream);
     t.done();
   }
 }
 
 // Steps it0 .. it0+n-1: the host forcing of each chunk of steps is computed
 // into pinned memory and copied with one transfer ahead of its kernels.
+void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
+  launch_stage_rhs(h, it, irk, forcing);
+  launch_limit(h, irk);
+}
+
 void run_steps(dgswem_cuda* h, int it0, int n) {
   const int nrk = h->nrk;
   for (int done = 0; done < n;) {
@@ -888,10 +927,8 @@ int dgswem_cuda_last_error(char* buf, int buflen) {
   return DGSWEM_OK;
 }
 
-int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem_cuda** out) {
-  return guarded([&]() {
-    if (!s || !out) throw Failure(DGSWEM_ERR_ARG, "null argument");
-    *out = nullptr;
+static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int nparts, int device, int flags) {
+  {
     if (flags & ~DGSWEM_CUDA_STRICT) throw Failure(DGSWEM_ERR_ARG, "unknown flags");
     if (s->dofh != 3) throw Failure(DGSWEM_ERR_ARG, "only p=1 (DOFH=3) is implemented on the device");
     if (s->ne <= 0 || s->np <= 0 || s->nedges <= 0) throw Failure(DGSWEM_ERR_ARG, "empty mesh");
@@ -951,26 +988,29 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
       kStrict.set_basis(B);
       DG_CUDA(cudaGetLastError());
     }
-    build_layout(h.get(), s);
+    const PartPlan plan = make_part_plan(s, part, nparts);
+    build_layout(h.get(), s, plan);
+    build_halo(h.get(), s, plan);
+    const size_t nl = (size_t)h->ne, npl = (size_t)h->np;
     h->q.resize(s->nrk + 1);
     for (auto& b : h->q) {
-      b.alloc(9 * (size_t)s->ne);
+      b.alloc(9 * nl);
       DG_CUDA(cudaMemset(b.p, 0, b.n * sizeof(double)));
     }
     h->rhs.resize(s->nrk);
     for (int I = 0; I < s->nrk; ++I)
-      if (h->keep_rhs[I]) h->rhs[I].alloc(9 * (size_t)s->ne);
-    h->wd.alloc(s->ne);
+      if (h->keep_rhs[I]) h->rhs[I].alloc(9 * nl);
+    h->wd.alloc(nl);
     h->wd_staging.alloc(s->ne);
     h->nodecode.alloc(s->np);
-    h->minmax.alloc(6 * (size_t)s->np);
+    h->minmax.alloc(6 * npl);
     h->err.alloc(1);
     DG_CUDA(cudaMemset(h->err.p, 0, sizeof(unsigned)));
     if (s->nws == 1) {
-      h->wsx.alloc(s->np); h->wsy.alloc(s->np); h->pr.alloc(s->np);
-      DG_CUDA(cudaMemset(h->wsx.p, 0, s->np * sizeof(double)));
-      DG_CUDA(cudaMemset(h->wsy.p, 0, s->np * sizeof(double)));
-      DG_CUDA(cudaMemset(h->pr.p, 0, s->np * sizeof(double)));
+      h->wsx.alloc(npl); h->wsy.alloc(npl); h->pr.alloc(npl);
+      DG_CUDA(cudaMemset(h->wsx.p, 0, npl * sizeof(double)));
+      DG_CUDA(cudaMemset(h->wsy.p, 0, npl * sizeof(double)));
+      DG_CUDA(cudaMemset(h->pr.p, 0, npl * sizeof(double)));
     }
     // host-side boundary forcing (ocean and flow harmonics)
     h->needs = s->needs;
@@ -992,7 +1032,25 @@ int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem
       DG_CUDA(cudaEventCreateWithFlags(&h->forcing_copied, cudaEventDisableTiming));
     }
     upload_state(h.get(), s->ze, s->qx, s->qy, s->wdflg);
-    *out = h.release();
+    return h.release();
+  }
+}
+
+int dgswem_cuda_create(const dgswem_cuda_setup* s, int device, int flags, dgswem_cuda** out) {
+  return guarded([&]() {
+    if (!s || !out) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    *out = nullptr;
+    *out = create_handle(s, 0, 1, device, flags);
+  });
+}
+
+int dgswem_cuda_create_part(const dgswem_cuda_setup* s, int part, int nparts, int device, int flags,
+                            dgswem_cuda** out) {
+  return guarded([&]() {
+    if (!s || !out) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (nparts < 1 || part < 0 || part >= nparts) throw Failure(DGSWEM_ERR_ARG, "partition index out of range");
+    *out = create_handle(s, part, nparts, device, flags);
   });
 }
 
@@ -1011,6 +1069,9 @@ void dgswem_cuda_destroy(dgswem_cuda* h) {
 int dgswem_cuda_hydro_timestep(dgswem_cuda* h, int it) {
   return guarded([&]() {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nparts != 1)
+      throw Failure(DGSWEM_ERR_ARG, "a partitioned handle steps through dgswem_cuda_stage_rhs / _stage_limit / "
+                                    "_step_end with halo exchanges in between");
     DG_CUDA(cudaSetDevice(h->device));
     run_steps(h, it, 1);
   });
@@ -1019,6 +1080,9 @@ int dgswem_cuda_hydro_timestep(dgswem_cuda* h, int it) {
 int dgswem_cuda_run(dgswem_cuda* h, int it0, int nsteps) {
   return guarded([&]() {
     if (!h || nsteps < 0) throw Failure(DGSWEM_ERR_ARG, "bad arguments");
+    if (h->nparts != 1)
+      throw Failure(DGSWEM_ERR_ARG, "a partitioned handle steps through dgswem_cuda_stage_rhs / _stage_limit / "
+                                    "_step_end with halo exchanges in between");
     DG_CUDA(cudaSetDevice(h->device));
     run_steps(h, it0, nsteps);
   });
@@ -1048,23 +1112,45 @@ int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* q
   return guarded([&]() {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     DG_CUDA(cudaSetDevice(h->device));
-    const int ne = h->ne;
-    h->staging.ensure(9 * (size_t)ne);
     double* dst[3] = {ze, qx, qy};
+    if (h->nparts == 1) {  // every element is owned: scatter to input order on the device
+      const int ne = h->ne;
+      h->staging.ensure(9 * (size_t)ne);
+      for (int var = 0; var < 3; ++var) {
+        if (!dst[var]) continue;
+        h->v->s2f(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var, h->inv.p, grid_for(ne, kPointBlock),
+                  h->stream);
+        check_launch(h, "soa_to_fortran");
+        DG_CUDA(cudaMemcpyAsync(dst[var], h->staging.p + (size_t)3 * ne * var, 3 * (size_t)ne * sizeof(double),
+                                cudaMemcpyDeviceToHost, h->stream));
+      }
+      if (wdflg) {
+        h->v->gather_int(h->wd.p, h->wd_staging.p, h->inv.p, ne, grid_for(ne, kPointBlock), h->stream);
+        check_launch(h, "gather_int");
+        DG_CUDA(cudaMemcpyAsync(wdflg, h->wd_staging.p, (size_t)ne * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      }
+      DG_CUDA(cudaStreamSynchronize(h->stream));
+      return;
+    }
+    // a partition: the owned elements' entries of the input-order arrays;
+    // the others are left as they are
+    const int no = h->n_own, nl = h->ne;
+    std::vector<double> buf(3 * (size_t)no);
+    std::vector<int> wbuf(no);
     for (int var = 0; var < 3; ++var) {
       if (!dst[var]) continue;
-      h->v->s2f(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var, h->inv.p, grid_for(ne, kPointBlock),
-                h->stream);
-      check_launch(h, "soa_to_fortran");
-      DG_CUDA(cudaMemcpyAsync(dst[var], h->staging.p + (size_t)3 * ne * var, 3 * (size_t)ne * sizeof(double),
-                              cudaMemcpyDeviceToHost, h->stream));
+      for (int k = 0; k < 3; ++k)
+        DG_CUDA(cudaMemcpyAsync(buf.data() + (size_t)k * no, h->q[0].p + (size_t)(3 * var + k) * nl,
+                                (size_t)no * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      DG_CUDA(cudaStreamSynchronize(h->stream));
+      for (int i = 0; i < no; ++i)
+        for (int k = 0; k < 3; ++k) dst[var][(size_t)3 * h->perm_h[i] + k] = buf[(size_t)k * no + i];
     }
     if (wdflg) {
-      h->v->gather_int(h->wd.p, h->wd_staging.p, h->inv.p, ne, grid_for(ne, kPointBlock), h->stream);
-      check_launch(h, "gather_int");
-      DG_CUDA(cudaMemcpyAsync(wdflg, h->wd_staging.p, (size_t)ne * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      DG_CUDA(cudaMemcpyAsync(wbuf.data(), h->wd.p, (size_t)no * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      DG_CUDA(cudaStreamSynchronize(h->stream));
+      for (int i = 0; i < no; ++i) wdflg[h->perm_h[i]] = wbuf[i];
     }
-    DG_CUDA(cudaStreamSynchronize(h->stream));
   });
 }
 
@@ -1093,6 +1179,7 @@ int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2, 
 int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* vv2, int* nodecode) {
   return guarded([&]() {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "modal2nodal needs the whole mesh (a handle of dgswem_cuda_create)");
     DG_CUDA(cudaSetDevice(h->device));
     const int np = h->np;
     h->staging.ensure(4 * (size_t)np);
@@ -1112,6 +1199,7 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
 int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, double* vv2, int* nodecode) {
   return guarded([&]() {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "modal2nodal needs the whole mesh (a handle of dgswem_cuda_create)");
     const int np = h->np;
     if (np > DGSWEM_CUDA_NOALLOC_MAX_NODES)
       throw Failure(DGSWEM_ERR_ARG, "modal2nodal_noalloc: NP = " + std::to_string(np) +
@@ -1131,6 +1219,84 @@ int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, d
       DG_CUDA(cudaMemcpyAsync(nodecode, h->nodecode.p, np * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     DG_CUDA(cudaStreamSynchronize(h->stream));
   });
+}
+
+int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (irk < 1 || irk > h->nrk) throw Failure(DGSWEM_ERR_ARG, "stage out of range");
+    DG_CUDA(cudaSetDevice(h->device));
+    const double* dev = nullptr;
+    if (h->forcing_per_stage) {  // this stage's boundary forcing, host cos, one small copy
+      if (h->forcing_copied) DG_CUDA(cudaEventSynchronize(h->forcing_copied));
+      double timedg, rampdg;
+      stage_clock(h, it, irk, &timedg, &rampdg);
+      stage_forcing(h, timedg, rampdg, h->forcing_host);
+      DG_CUDA(cudaMemcpyAsync(h->forcing_dev.p, h->forcing_host, h->forcing_per_stage * sizeof(double),
+                              cudaMemcpyHostToDevice, h->stream));
+      DG_CUDA(cudaEventRecord(h->forcing_copied, h->stream));
+      dev = h->forcing_dev.p;
+    }
+    launch_stage_rhs(h, it, irk, dev);
+  });
+}
+
+int dgswem_cuda_stage_limit(dgswem_cuda* h, int irk) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (irk < 1 || irk > h->nrk) throw Failure(DGSWEM_ERR_ARG, "stage out of range");
+    DG_CUDA(cudaSetDevice(h->device));
+    launch_limit(h, irk);
+  });
+}
+
+int dgswem_cuda_step_end(dgswem_cuda* h) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    std::swap(h->q[0], h->q[h->nrk]);  // stage NRK+1 becomes stage 1
+  });
+}
+
+int dgswem_cuda_part_info(const dgswem_cuda* h, int* part, int* nparts, int* n_owned, int* n_local) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (part) *part = h->part;
+    if (nparts) *nparts = h->nparts;
+    if (n_owned) *n_owned = h->n_own;
+    if (n_local) *n_local = h->ne;
+  });
+}
+
+int dgswem_cuda_halo_count(const dgswem_cuda* h, int kind, int peer, int* nsend, int* nrecv) {
+  return guarded([&]() {
+    if (!h || !nsend || !nrecv) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    if (kind != kHaloMeans && kind != kHaloFull) throw Failure(DGSWEM_ERR_ARG, "unknown halo kind");
+    if (peer < 0 || peer >= h->nparts) throw Failure(DGSWEM_ERR_ARG, "peer out of range");
+    *nsend = (int)(h->halo_off[kind][0][peer + 1] - h->halo_off[kind][0][peer]);
+    *nrecv = (int)(h->halo_off[kind][1][peer + 1] - h->halo_off[kind][1][peer]);
+  });
+}
+
+static int halo_copy(dgswem_cuda* h, int kind, int peer, int irk, double* buf, bool pack) {
+  return guarded([&]() {
+    if (!h || !buf) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    if (kind != kHaloMeans && kind != kHaloFull) throw Failure(DGSWEM_ERR_ARG, "unknown halo kind");
+    if (peer < 0 || peer >= h->nparts) throw Failure(DGSWEM_ERR_ARG, "peer out of range");
+    if (irk < 0 || irk > h->nrk) throw Failure(DGSWEM_ERR_ARG, "stage buffer out of range");
+    DG_CUDA(cudaSetDevice(h->device));
+    const auto& off = h->halo_off[kind][pack ? 0 : 1];
+    const int n = (int)(off[peer + 1] - off[peer]);
+    h->v->halo(pack, h->q[irk].p, h->wd.p, h->ne, h->halo_idx.p + off[peer], n, kind, buf, h->stream);
+    if (n > 0) check_launch(h, pack ? "halo_pack" : "halo_unpack");
+  });
+}
+
+int dgswem_cuda_halo_pack(dgswem_cuda* h, int kind, int peer, int irk, double* buf) {
+  return halo_copy(h, kind, peer, irk, buf, true);
+}
+
+int dgswem_cuda_halo_unpack(dgswem_cuda* h, int kind, int peer, int irk, const double* buf) {
+  return halo_copy(h, kind, peer, irk, const_cast<double*>(buf), false);
 }
 
 long long dgswem_cuda_kernel_launches(const dgswem_cuda* h) { return h ? h->launches : -1; }

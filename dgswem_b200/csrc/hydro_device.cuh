@@ -204,6 +204,7 @@ struct LimitArgs {
   double* minmax;            // [6*NP]: zmin zmax qxmin qxmax qymin qymax
   int* wd;                   // WDFLG (read + write)
   int slopeflag, wetdry;
+  int ne_act;                // elements limited / wet-dried: the owned ones (the first ne_act)
   unsigned* err;
 };
 
@@ -226,6 +227,8 @@ struct LimitArgs {
                              unsigned grid, cudaStream_t s);                                   \
   void launch_gather_int(const int* src, int* dst, const int* idx, int n, unsigned grid,       \
                          cudaStream_t s);                                                      \
+  void launch_halo(bool pack, double* q, int* wd, int ne, const int* idx, int n, int kind,     \
+                   double* buf, cudaStream_t s);                                               \
   }
 
 DGSWEM_DECLARE_LAUNCHERS(fast)

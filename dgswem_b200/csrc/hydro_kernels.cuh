@@ -826,7 +826,7 @@ __device__ __forceinline__ double div_count(double x, int kdp) {
 __global__ void __launch_bounds__(256) limit_wetdry(const __grid_constant__ LimitArgs L) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const int ne = L.m.ne, np = L.m.np;
-  if (e >= ne) return;
+  if (e >= L.ne_act) return;
   const BasisP1& B = cBasis;
   int nd[3];
 #pragma unroll
@@ -1037,6 +1037,40 @@ __global__ void soa_to_fortran(const double* __restrict__ q, double* __restrict_
   const int i = inv[e];
 #pragma unroll
   for (int k = 0; k < 3; ++k) f[(size_t)3 * e + k] = q[(size_t)(3 * var + k) * ne + i];
+}
+
+// Halo of a partitioned handle: the states of stage buffer q (row stride ne)
+// at local element ids idx[0..n) to / from a contiguous buffer.  kind 0: the
+// element means of ZE, QX, QY (3 doubles); kind 1: the nine modal values and
+// WDFLG (10 doubles, WDFLG as 0.0 / 1.0).
+__global__ void halo_pack(const double* __restrict__ q, const int* __restrict__ wd, int ne,
+                          const int* __restrict__ idx, int n, int kind, double* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int i = idx[j];
+  if (kind == 0) {
+#pragma unroll
+    for (int v = 0; v < 3; ++v) out[(size_t)3 * j + v] = q[(size_t)(3 * v) * ne + i];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) out[(size_t)10 * j + c] = q[(size_t)c * ne + i];
+    out[(size_t)10 * j + 9] = (double)wd[i];
+  }
+}
+
+__global__ void halo_unpack(double* __restrict__ q, int* __restrict__ wd, int ne, const int* __restrict__ idx,
+                            int n, int kind, const double* __restrict__ in) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int i = idx[j];
+  if (kind == 0) {
+#pragma unroll
+    for (int v = 0; v < 3; ++v) q[(size_t)(3 * v) * ne + i] = in[(size_t)3 * j + v];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) q[(size_t)c * ne + i] = in[(size_t)10 * j + c];
+    wd[i] = (int)in[(size_t)10 * j + 9];
+  }
 }
 
 // dst[i] = src[idx[i]]: WDFLG between input and device element order

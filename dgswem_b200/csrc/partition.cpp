@@ -1,0 +1,154 @@
+// partition.cpp -- element partition and halo lists (see partition.h).  The
+// reference decomposes with METIS through adcprep and exchanges ghost
+// elements with MPI (messenger_elem.F); here a partition is a contiguous
+// range of the Morton order, and the halo is derived from the edge graph.
+#include "partition.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+
+#include "abi_util.h"
+
+namespace dgswem {
+
+std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py) {
+  const int n = (int)px.size();
+  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+  for (int i = 0; i < n; ++i) {
+    x0 = std::min(x0, px[i]); x1 = std::max(x1, px[i]);
+    y0 = std::min(y0, py[i]); y1 = std::max(y1, py[i]);
+  }
+  const double span = std::max(std::max(x1 - x0, y1 - y0), 1e-300);
+  auto spread = [](uint64_t v) {  // bits of v at the even positions
+    uint64_t r = 0;
+    for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1u) << (2 * b);
+    return r;
+  };
+  std::vector<uint64_t> key(n);
+  const double scale = (double)((1u << 21) - 1) / span;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t ix = (uint64_t)((px[i] - x0) * scale), iy = (uint64_t)((py[i] - y0) * scale);
+    key[i] = spread(ix) | spread(iy) << 1;
+  }
+  std::vector<int> perm(n);
+  for (int i = 0; i < n; ++i) perm[i] = i;
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+  return perm;
+}
+
+PartPlan make_part_plan(const dgswem_cuda_setup* s, int part, int nparts) {
+  const int ne = s->ne, np = s->np;
+  if (nparts < 1 || part < 0 || part >= nparts) throw Failure(DGSWEM_ERR_ARG, "partition index out of range");
+  if (nparts > ne) throw Failure(DGSWEM_ERR_ARG, "more partitions than elements");
+  PartPlan P;
+  P.part = part;
+  P.nparts = nparts;
+  {
+    std::vector<double> cx(ne), cy(ne);
+    for (int e = 0; e < ne; ++e) {
+      double sx = 0.0, sy = 0.0;
+      for (int v = 0; v < 3; ++v) {
+        const int n = s->nm[e + (size_t)ne * v] - 1;
+        if (n < 0 || n >= np) throw Failure(DGSWEM_ERR_ARG, "NM refers to a node outside 1..NP");
+        sx += s->x[n];
+        sy += s->y[n];
+      }
+      cx[e] = sx / 3.0;
+      cy[e] = sy / 3.0;
+    }
+    P.order = morton_order(cx, cy);
+  }
+  std::vector<int> pos(ne);
+  for (int i = 0; i < ne; ++i) pos[P.order[i]] = i;
+  P.owner.assign(ne, 0);
+  for (int q = 0; q < nparts; ++q) {
+    const long lo = (long)q * ne / nparts, hi = (long)(q + 1) * ne / nparts;
+    for (long i = lo; i < hi; ++i) P.owner[P.order[i]] = q;
+  }
+  P.send[0].assign(nparts, {});
+  P.send[1].assign(nparts, {});
+  P.recv[0].assign(nparts, {});
+  P.recv[1].assign(nparts, {});
+  const long lo = (long)part * ne / nparts, hi = (long)(part + 1) * ne / nparts;
+  P.n_own = (int)(hi - lo);
+  P.local.assign(P.order.begin() + lo, P.order.begin() + hi);
+  if (nparts == 1) return P;
+  // adjacency: edges (NEDEL of the interior edges), barrier partners, node stars
+  std::vector<std::vector<int>> full_nb(ne);
+  for (int g = 0; g < s->nedges; ++g) {
+    const int a = s->nedel[2 * (size_t)g], b = s->nedel[2 * (size_t)g + 1];
+    if (a != 0 && b != 0) {
+      full_nb[a - 1].push_back(b - 1);
+      full_nb[b - 1].push_back(a - 1);
+    }
+  }
+  for (int L = 0; L < s->nibseg; ++L) {
+    const int gb = s->nibsegn[2 * L], gf = s->nibsegn[2 * L + 1];
+    if (gb == 0 || gf == 0) continue;
+    const int eb = s->nedel[2 * (size_t)(gb - 1)] - 1, ef = s->nedel[2 * (size_t)(gf - 1)] - 1;
+    if (eb < 0 || ef < 0) continue;
+    full_nb[eb].push_back(ef);
+    full_nb[ef].push_back(eb);
+  }
+  std::vector<int> sp(np + 1, 0), st(3 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int v = 0; v < 3; ++v) ++sp[s->nm[e + (size_t)ne * v]];
+  for (int n = 0; n < np; ++n) sp[n + 1] += sp[n];
+  {
+    std::vector<int> cur(sp.begin(), sp.end() - 1);
+    for (int e = 0; e < ne; ++e)
+      for (int v = 0; v < 3; ++v) st[cur[s->nm[e + (size_t)ne * v] - 1]++] = e;
+  }
+  std::vector<char> ghost_kind(ne, 0);  // bit k: a halo of kind k
+  for (long i = lo; i < hi; ++i) {
+    const int e = P.order[i];
+    std::vector<char> sent_to(2 * (size_t)nparts, 0);
+    for (int nb : full_nb[e]) {
+      const int q = P.owner[nb];
+      if (q == part) continue;
+      ghost_kind[nb] |= 2;
+      if (!sent_to[2 * q + 1]) { P.send[kHaloFull][q].push_back(e); sent_to[2 * q + 1] = 1; }
+    }
+    for (int v = 0; v < 3; ++v) {
+      const int n = s->nm[e + (size_t)ne * v] - 1;
+      for (int k = sp[n]; k < sp[n + 1]; ++k) {
+        const int nb = st[k];
+        const int q = P.owner[nb];
+        if (q == part) continue;
+        ghost_kind[nb] |= 1;
+        if (!sent_to[2 * q]) { P.send[kHaloMeans][q].push_back(e); sent_to[2 * q] = 1; }
+      }
+    }
+  }
+  std::vector<int> ghosts;
+  for (int e = 0; e < ne; ++e)
+    if (ghost_kind[e]) {
+      ghosts.push_back(e);
+      if (ghost_kind[e] & 1) P.recv[kHaloMeans][P.owner[e]].push_back(e);
+      if (ghost_kind[e] & 2) P.recv[kHaloFull][P.owner[e]].push_back(e);
+    }
+  std::sort(ghosts.begin(), ghosts.end(), [&](int a, int b) { return pos[a] < pos[b]; });
+  P.local.insert(P.local.end(), ghosts.begin(), ghosts.end());
+  for (int k = 0; k < 2; ++k)
+    for (auto& v : P.send[k]) std::sort(v.begin(), v.end());
+  return P;
+}
+
+}  // namespace dgswem
+
+extern "C" int dgswem_part_halo_ids(const dgswem_cuda_setup* s, int part, int nparts, int peer, int kind,
+                                    int* send_ids, int* nsend, int* recv_ids, int* nrecv) {
+  return dgswem::guarded([&]() {
+    if (!s || !nsend || !nrecv) throw dgswem::Failure(DGSWEM_ERR_ARG, "null argument");
+    if (kind != dgswem::kHaloMeans && kind != dgswem::kHaloFull) throw dgswem::Failure(DGSWEM_ERR_ARG, "unknown halo kind");
+    if (peer < 0 || peer >= nparts) throw dgswem::Failure(DGSWEM_ERR_ARG, "peer out of range");
+    const dgswem::PartPlan P = dgswem::make_part_plan(s, part, nparts);
+    const auto& snd = P.send[kind][peer];
+    const auto& rcv = P.recv[kind][peer];
+    *nsend = (int)snd.size();
+    *nrecv = (int)rcv.size();
+    if (send_ids) std::copy(snd.begin(), snd.end(), send_ids);
+    if (recv_ids) std::copy(rcv.begin(), rcv.end(), recv_ids);
+  });
+}

@@ -78,20 +78,28 @@ class HydroStep:
 
     STRICT = 1  # DGSWEM_CUDA_STRICT
 
-    def __init__(self, setup, device: int = 0, strict: bool = False):
+    def __init__(self, setup, device: int = 0, strict: bool = False, part: int = 0, nparts: int = 1):
         """strict=True selects the kernels compiled without FMA contraction
         (bitwise reproducible against the non-contracting FP64 oracle);
-        the default is the FMA-contracted fast form."""
+        the default is the FMA-contracted fast form.  nparts > 1 makes a
+        partition handle (dgswem_cuda_create_part), stepped by
+        ``PartitionedRun``."""
         self._lib = _abi.load()
         self.strict = bool(strict)
         self._deck = setup if isinstance(setup, Deck) else None
         sp = setup.setup if isinstance(setup, Deck) else setup
         s = sp.contents
         self.ne, self.np, self.dofh, self.nrk = s.ne, s.np, s.dofh, s.nrk
+        self.slopeflag = s.slopeflag
+        self.part, self.nparts = int(part), int(nparts)
         h = C.c_void_p()
         flags = self.STRICT if strict else 0
-        _abi.check(self._lib.dgswem_cuda_create(sp, int(device), flags, C.byref(h)))
+        if self.nparts == 1:
+            _abi.check(self._lib.dgswem_cuda_create(sp, int(device), flags, C.byref(h)))
+        else:
+            _abi.check(self._lib.dgswem_cuda_create_part(sp, self.part, self.nparts, int(device), flags, C.byref(h)))
         self._h = h
+        self.device = int(device)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -145,11 +153,12 @@ class HydroStep:
 
     # -- state ----------------------------------------------------------------
     def state(self):
-        """(ze, qx, qy, wdflg) of stage 1; ze has shape (ne, dofh)."""
-        ze = np.empty((self.ne, self.dofh))
-        qx = np.empty_like(ze)
-        qy = np.empty_like(ze)
-        wd = np.empty(self.ne, np.int32)
+        """(ze, qx, qy, wdflg) of stage 1; ze has shape (ne, dofh).  A
+        partition fills its owned elements' rows (the others are NaN / -1)."""
+        ze = np.full((self.ne, self.dofh), np.nan)
+        qx = np.full_like(ze, np.nan)
+        qy = np.full_like(ze, np.nan)
+        wd = np.full(self.ne, -1, np.int32)
         _abi.check(self._lib.dgswem_cuda_download_state(self._h, _dptr(ze), _dptr(qx), _dptr(qy), _iptr(wd)))
         return ze, qx, qy, wd
 
@@ -165,6 +174,32 @@ class HydroStep:
         wd = None if wdflg is None else np.ascontiguousarray(wdflg, dtype=np.int32)
         _abi.check(self._lib.dgswem_cuda_upload_state(self._h, _dptr(ze), _dptr(qx), _dptr(qy),
                                                       _iptr(wd) if wd is not None else None))
+
+    # -- partition handles (dgswem_cuda_create_part) ----------------------------
+    def part_info(self) -> dict:
+        v = [C.c_int() for _ in range(4)]
+        _abi.check(self._lib.dgswem_cuda_part_info(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("part", "nparts", "owned", "local"), (x.value for x in v)))
+
+    def stage_rhs(self, it: int, irk: int) -> None:
+        _abi.check(self._lib.dgswem_cuda_stage_rhs(self._h, int(it), int(irk)))
+
+    def stage_limit(self, irk: int) -> None:
+        _abi.check(self._lib.dgswem_cuda_stage_limit(self._h, int(irk)))
+
+    def step_end(self) -> None:
+        _abi.check(self._lib.dgswem_cuda_step_end(self._h))
+
+    def halo_count(self, kind: int, peer: int):
+        ns, nr = C.c_int(), C.c_int()
+        _abi.check(self._lib.dgswem_cuda_halo_count(self._h, int(kind), int(peer), C.byref(ns), C.byref(nr)))
+        return ns.value, nr.value
+
+    def halo_pack(self, kind: int, peer: int, irk: int, dev_ptr: int) -> None:
+        _abi.check(self._lib.dgswem_cuda_halo_pack(self._h, int(kind), int(peer), int(irk), C.c_void_p(dev_ptr)))
+
+    def halo_unpack(self, kind: int, peer: int, irk: int, dev_ptr: int) -> None:
+        _abi.check(self._lib.dgswem_cuda_halo_unpack(self._h, int(kind), int(peer), int(irk), C.c_void_p(dev_ptr)))
 
     def set_met(self, wsx2, wsy2, pr2) -> None:
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (wsx2, wsy2, pr2)]
@@ -189,6 +224,110 @@ class HydroStep:
         _abi.check(self._lib.dgswem_cuda_modal2nodal_noalloc(self._h, _dptr(eta), _dptr(uu), _dptr(vv),
                                                              _iptr(nc)))
         return eta, uu, vv, nc
+
+
+class PartitionedRun:
+    """A mesh split into ``nparts`` partition handles stepped in lock-step by
+    one process, the halos moved between the handles through device buffers
+    (the stage sequence of DG_hydro_timestep.F with the ghost updates of
+    :493-514 and :555-579).  ``devices`` places the partitions (default: all
+    on GPU 0); partitions on one device share one stream, so every pack,
+    unpack and kernel of a stage is ordered without host synchronisation.
+    Across devices the halo moves by peer copies with a device
+    synchronisation per exchange.  A multi-process run replaces the buffer
+    moves by NCCL send/receive of the same packed buffers."""
+
+    HALO_WIDTH = (3, 10)  # doubles per element of halo kinds 0 and 1
+
+    def __init__(self, setup, nparts: int, devices=None, strict: bool = False):
+        import torch
+        self._torch = torch
+        self.nparts = int(nparts)
+        self.devices = list(devices) if devices is not None else [0] * self.nparts
+        if len(self.devices) != self.nparts:
+            raise ValueError("one device per partition")
+        self.parts = [HydroStep(setup, device=d, strict=strict, part=p, nparts=self.nparts)
+                      for p, d in enumerate(self.devices)]
+        self.ne, self.nrk, self.dofh = self.parts[0].ne, self.parts[0].nrk, self.parts[0].dofh
+        self.slopeflag = self.parts[0].slopeflag
+        self.streams = {d: torch.cuda.Stream(device=d) for d in sorted(set(self.devices))}
+        for hs, d in zip(self.parts, self.devices):
+            hs.set_stream(self.streams[d].cuda_stream)
+        self.single_device = len(self.streams) == 1
+        # per (kind, sender p, receiver q): a buffer on p's device, and on q's
+        # device when they differ
+        self.buf = {}
+        for kind in (0, 1):
+            w = self.HALO_WIDTH[kind]
+            for p in range(self.nparts):
+                for q in range(self.nparts):
+                    if p == q:
+                        continue
+                    ns, _ = self.parts[p].halo_count(kind, q)
+                    _, nr = self.parts[q].halo_count(kind, p)
+                    if ns != nr:
+                        raise RuntimeError(f"halo lists disagree: {p}->{q} sends {ns}, {q} expects {nr}")
+                    if ns == 0:
+                        continue
+                    src = torch.empty(ns * w, dtype=torch.float64, device=f"cuda:{self.devices[p]}")
+                    dst = src if self.devices[p] == self.devices[q] else \
+                        torch.empty(ns * w, dtype=torch.float64, device=f"cuda:{self.devices[q]}")
+                    self.buf[(kind, p, q)] = (src, dst)
+
+    def close(self):
+        for hs in self.parts:
+            hs.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _exchange(self, kind: int, irk: int) -> None:
+        for (k, p, q), (src, _) in self.buf.items():
+            if k == kind:
+                self.parts[p].halo_pack(kind, q, irk, src.data_ptr())
+        if not self.single_device:
+            for d in self.streams:
+                self._torch.cuda.synchronize(d)
+            for (k, p, q), (src, dst) in self.buf.items():
+                if k == kind and dst is not src:
+                    dst.copy_(src)
+            for d in self.streams:
+                self._torch.cuda.synchronize(d)
+        for (k, p, q), (_, dst) in self.buf.items():
+            if k == kind:
+                self.parts[q].halo_unpack(kind, p, irk, dst.data_ptr())
+
+    def timestep(self, it: int) -> None:
+        for irk in range(1, self.nrk + 1):
+            for hs in self.parts:
+                hs.stage_rhs(it, irk)
+            if self.slopeflag != 0:
+                self._exchange(0, irk)
+            for hs in self.parts:
+                hs.stage_limit(irk)
+            self._exchange(1, irk)
+        for hs in self.parts:
+            hs.step_end()
+
+    def run(self, it0: int, nsteps: int) -> None:
+        for it in range(it0, it0 + nsteps):
+            self.timestep(it)
+
+    def synchronize(self) -> None:
+        for hs in self.parts:
+            hs.synchronize()
+
+    def state(self):
+        """(ze, qx, qy, wdflg) of the whole mesh, each partition's owned rows."""
+        ze = np.full((self.ne, self.dofh), np.nan)
+        qx, qy = np.full_like(ze, np.nan), np.full_like(ze, np.nan)
+        wd = np.full(self.ne, -1, np.int32)
+        for hs in self.parts:
+            hs.download_into(ze, qx, qy, wd)
+        return ze, qx, qy, wd
 
 
 def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False):

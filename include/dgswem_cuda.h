@@ -109,6 +109,53 @@ typedef struct dgswem_cuda dgswem_cuda;
  * (src/dgswem.F:196). */
 int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
                        dgswem_cuda** out);
+
+/* ---- partitioned mesh (one handle per GPU) --------------------------------
+ * The reference runs one MPI rank per METIS subdomain and exchanges ghost
+ * elements after the SSP update and after the limiter/WETDRY
+ * (DG_hydro_timestep.F:493-514, 555-579; messenger_elem.F).  Here partition
+ * `part` of `nparts` owns a contiguous range of the elements' Morton order
+ * and keeps ghost copies of its neighbours; the caller moves the halo
+ * between handles (NCCL, peer copies, or device copies on one GPU) between
+ * the stage calls:
+ *
+ *   for each RK stage irk:  stage_rhs(it, irk) on every partition
+ *                           halo kind 0 (pack -> move -> unpack), if SLOPEFLAG
+ *                           stage_limit(irk) on every partition
+ *                           halo kind 1
+ *   step_end() on every partition
+ *
+ * Halo kind 0: element means of ZE, QX, QY (3 doubles per element) of the
+ * elements sharing a node with another partition's elements, read by that
+ * partition's limiter node pass.  Kind 1: the nine modal values and WDFLG (10
+ * doubles) of the elements sharing an edge (or an internal barrier) with
+ * another partition's elements.  Buffers are device memory of the handle's
+ * device; pack/unpack run on the handle's stream (dgswem_cuda_set_stream).
+ * The state upload takes the whole input-order arrays (NE elements); the
+ * download writes the owned elements' entries only.  dgswem_cuda_hydro_timestep,
+ * dgswem_cuda_run and modal2nodal need a whole-mesh handle (nparts = 1).
+ * No counterpart in the reference's C interface. */
+int dgswem_cuda_create_part(const dgswem_cuda_setup* setup, int part, int nparts, int device,
+                            int flags, dgswem_cuda** out);
+int dgswem_cuda_part_info(const dgswem_cuda* h, int* part, int* nparts, int* n_owned,
+                          int* n_local);
+/* One RK stage's right-hand side and SSP update of the owned elements
+ * (stage buffer irk, 1..NRK), then the limiter and WETDRY of the same stage,
+ * then the end of the step (the stage-NRK+1 state becomes the step state). */
+int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk);
+int dgswem_cuda_stage_limit(dgswem_cuda* h, int irk);
+int dgswem_cuda_step_end(dgswem_cuda* h);
+/* Elements this partition sends to / receives from `peer` for halo `kind`;
+ * a buffer holds 3 (kind 0) or 10 (kind 1) doubles per element, in the order
+ * of the peer's matching list (ascending input element ids). */
+int dgswem_cuda_halo_count(const dgswem_cuda* h, int kind, int peer, int* nsend, int* nrecv);
+int dgswem_cuda_halo_pack(dgswem_cuda* h, int kind, int peer, int irk, double* buf);
+int dgswem_cuda_halo_unpack(dgswem_cuda* h, int kind, int peer, int irk, const double* buf);
+/* Host-only: the input element ids (0-based, ascending) partition `part`
+ * sends to / receives from `peer` for halo `kind` (NULL id arrays: counts
+ * only).  Needs no GPU. */
+int dgswem_part_halo_ids(const dgswem_cuda_setup* setup, int part, int nparts, int peer, int kind,
+                         int* send_ids, int* nsend, int* recv_ids, int* nrecv);
 void dgswem_cuda_destroy(dgswem_cuda* h);
 
 /* One DG_HYDRO_TIMESTEP(IT) (src/DG_hydro_timestep.F:24-744): all RK stages,
