@@ -330,6 +330,67 @@ class PartitionedRun:
         return ze, qx, qy, wd
 
 
+class DistributedPartition:
+    """One partition per process and GPU (torch.distributed with NCCL): rank
+    r steps partition r of the group and moves its halos with NCCL
+    send/receive of the packed buffers that ``PartitionedRun`` moves by
+    device copies -- the reference's MPI ghost updates (messenger_elem.F)
+    over NVLink.  The handle launches on torch's current stream, so each
+    pack, transfer and unpack is stream-ordered after the kernels that
+    produce its data; every rank issues the same sequence of exchanges (one
+    batched send/receive per halo kind and stage)."""
+
+    def __init__(self, setup, strict: bool = False, group=None):
+        import torch
+        import torch.distributed as dist
+        self._torch, self._dist, self._group = torch, dist, group
+        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        dev = torch.cuda.current_device()
+        self.hs = HydroStep(setup, device=dev, strict=strict, part=self.rank, nparts=self.world)
+        self.hs.set_stream(torch.cuda.current_stream().cuda_stream)
+        self.nrk, self.slopeflag = self.hs.nrk, self.hs.slopeflag
+        self.buf = {}  # (kind, peer) -> (send buffer, receive buffer, nsend, nrecv)
+        for kind in (0, 1):
+            w = PartitionedRun.HALO_WIDTH[kind]
+            for q in range(self.world):
+                if q == self.rank:
+                    continue
+                ns, nr = self.hs.halo_count(kind, q)
+                if ns or nr:
+                    self.buf[(kind, q)] = (torch.empty(max(ns, 1) * w, dtype=torch.float64, device=dev),
+                                           torch.empty(max(nr, 1) * w, dtype=torch.float64, device=dev), ns, nr)
+
+    def close(self):
+        self.hs.close()
+
+    def _exchange(self, kind: int, irk: int) -> None:
+        dist = self._dist
+        ops = []
+        for (k, q), (snd, rcv, ns, nr) in self.buf.items():
+            if k != kind:
+                continue
+            if ns:
+                self.hs.halo_pack(kind, q, irk, snd.data_ptr())
+                ops.append(dist.P2POp(dist.isend, snd, q, self._group))
+            if nr:
+                ops.append(dist.P2POp(dist.irecv, rcv, q, self._group))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for (k, q), (_, rcv, _, nr) in self.buf.items():
+            if k == kind and nr:
+                self.hs.halo_unpack(kind, q, irk, rcv.data_ptr())
+
+    def timestep(self, it: int) -> None:
+        for irk in range(1, self.nrk + 1):
+            self.hs.stage_rhs(it, irk)
+            if self.slopeflag != 0:
+                self._exchange(0, irk)
+            self.hs.stage_limit(irk)
+            self._exchange(1, irk)
+        self.hs.step_end()
+
+
 def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with
     DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  Returns the
