@@ -823,7 +823,10 @@ __device__ __forceinline__ double div_count(double x, int kdp) {
 
 // slopelimiter.F:3434-3779 (vertex clamp + 3 redistribution sweeps) followed
 // by wetdry.F:61-548 for the same element.
-__global__ void __launch_bounds__(256) limit_wetdry(const __grid_constant__ LimitArgs L) {
+// 4 resident blocks of 256 per SM (64 registers, no spills): more warps to
+// cover the limiter's dependent FP64 chains than the 3 blocks an unbounded
+// allocation allows
+__global__ void __launch_bounds__(256, 4) limit_wetdry(const __grid_constant__ LimitArgs L) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const int ne = L.m.ne, np = L.m.np;
   if (e >= L.ne_act) return;
