@@ -66,11 +66,14 @@ def _fmt(v: float) -> str:
 
 
 def write_deck(path, x, y, dp, elems, open_segs, land_segs, ctl: Controls, emo=None, efa=None,
-               manning=None):
+               manning=None, flow=None):
     """Write fort.14, fort.15, fort.dg (and fort.13 when ``manning`` is given).
 
     elems: (ne, 3) 1-based counter-clockwise connectivity.  open_segs: list of
-    1-based node arrays.  land_segs: list of (node array, ibtype)."""
+    1-based node arrays.  land_segs: list of (node array, ibtype).  flow: for
+    periodic flux boundaries (ibtype 2/12/22), (frequency, nodal factor,
+    equilibrium argument in degrees, amplitudes, phases in degrees) with one
+    amplitude and phase per flux-boundary node, in boundary order."""
     path = Path(path)
     path.mkdir(parents=True, exist_ok=True)
     npn, ne = len(x), len(elems)
@@ -124,7 +127,12 @@ def write_deck(path, x, y, dp, elems, open_segs, land_segs, ctl: Controls, emo=N
     if nbfr:
         lines += ["M2", f"{_fmt(ctl.amig)} 1.0 0.0", "M2"]
         lines += [f"{_fmt(a)} {_fmt(p)}" for a, p in zip(emo, efa)]
-    lines += ["110.0 ! ANGINN", "0 0.0 1.0 1 ! NOUTE", "0 ! NSTAE", "0 0.0 1.0 1 ! NOUTV", "0 ! NSTAV"]
+    lines += ["110.0 ! ANGINN"]
+    if flow is not None:  # periodic flux boundary forcing (read_input.F:2971-3045)
+        w, ffac, face, famp, fph = flow
+        lines += ["1 ! NFFR", "FLOW", f"{_fmt(w)} {_fmt(ffac)} {_fmt(face)}", "FLOW"]
+        lines += [f"{_fmt(a)} {_fmt(ph)}" for a, ph in zip(famp, fph)]
+    lines += ["0 0.0 1.0 1 ! NOUTE", "0 ! NSTAE", "0 0.0 1.0 1 ! NOUTV", "0 ! NSTAV"]
     if ctl.nws != 0:
         lines += ["0 0.0 1.0 1 ! NOUTM", "0 ! NSTAM"]
     lines += [f"1 0.0 {_fmt(rnday + 1.0)} {nspool} ! NOUTGE", "0 0.0 1.0 1 ! NOUTGV", "0 ! NFREQ",
@@ -159,8 +167,14 @@ def _grid_triangles(ni: int, nj: int) -> np.ndarray:
     return np.stack([t1, t2], 1).reshape(-1, 3)
 
 
-def quarter_annulus(path, nr: int = 16, nth: int = 32, amp: float = 0.3048, **kw) -> Path:
-    """Tidal quarter annulus (the reference's quarter_annular geometry)."""
+def quarter_annulus(path, nr: int = 16, nth: int = 32, amp: float = 0.3048, flow_amp: float | None = None,
+                    radiation: bool = False, **kw) -> Path:
+    """Tidal quarter annulus (the reference's quarter_annular geometry).
+
+    flow_amp: make the radial side at 90 degrees a periodic flux boundary
+    (ibtype 2) with normal flux amplitude flow_amp (m^2/s) at the tide's
+    frequency; radiation: make the inner arc a radiation boundary (ibtype 30).
+    Otherwise both are land (ibtype 0)."""
     ctl = Controls(title="quarter annulus", nolibf=0, nolifa=1, tau=1e-4, dt=10.0, nsteps=4460,
                    rk_stage=2, rk_order=2, slopeflag=0, h0=1.0, nramp=1, dramp=2.0)
     for k, v in kw.items():
@@ -176,10 +190,20 @@ def quarter_annulus(path, nr: int = 16, nth: int = 32, amp: float = 0.3048, **kw
     elems = _grid_triangles(nr, nth)
     nid = lambda i, j: i * (nth + 1) + j + 1  # noqa: E731
     ocean = [nid(nr, j) for j in range(nth + 1)]
-    land = [nid(i, nth) for i in range(nr, -1, -1)] + [nid(0, j) for j in range(nth - 1, -1, -1)] + \
-           [nid(i, 0) for i in range(1, nr + 1)]
-    return write_deck(path, x, y, dp, elems, [ocean], [(land, 0)], ctl,
-                      emo=np.full(len(ocean), amp), efa=np.zeros(len(ocean)))
+    if flow_amp is None and not radiation:
+        land = [nid(i, nth) for i in range(nr, -1, -1)] + [nid(0, j) for j in range(nth - 1, -1, -1)] + \
+               [nid(i, 0) for i in range(1, nr + 1)]
+        return write_deck(path, x, y, dp, elems, [ocean], [(land, 0)], ctl,
+                          emo=np.full(len(ocean), amp), efa=np.zeros(len(ocean)))
+    top = [nid(i, nth) for i in range(nr, -1, -1)]
+    inner = [nid(0, j) for j in range(nth, -1, -1)]
+    bottom = [nid(i, 0) for i in range(0, nr + 1)]
+    segs = [(top, 2 if flow_amp is not None else 0), (inner, 30 if radiation else 0), (bottom, 0)]
+    flow = None
+    if flow_amp is not None:
+        flow = (ctl.amig, 1.0, 0.0, np.full(len(top), flow_amp), np.zeros(len(top)))
+    return write_deck(path, x, y, dp, elems, [ocean], segs, ctl,
+                      emo=np.full(len(ocean), amp), efa=np.zeros(len(ocean)), flow=flow)
 
 
 def sloping_beach(path, nx: int = 2236, ny: int = 447, lx: float = 100e3, ly: float = 20e3,

@@ -13,6 +13,9 @@ def _decks(scratch):
     out = [golden_dir(c) for c in GOLDEN_CASES]
     out.append(decks.quarter_annulus(scratch / "qa_small", nr=8, nth=16, nsteps=20))
     out.append(decks.sloping_beach(scratch / "sb_small", nx=40, ny=8, nsteps=20))
+    # periodic flux (ibtype 2) and radiation (ibtype 30) boundaries
+    out.append(decks.quarter_annulus(scratch / "qa_flowrad", nr=8, nth=16, nsteps=20, flow_amp=0.05,
+                                     radiation=True))
     return out
 
 

@@ -118,6 +118,24 @@ def test_fast_limiter_ties(built, scratch, nramp, rk):
     np.testing.assert_array_equal(g[3], o[3])
 
 
+@pytest.mark.parametrize("strict", [True, False])
+def test_flow_and_radiation_boundaries(built, scratch, strict):
+    """Periodic flux boundary (flow_edge_hydro.F: prescribed normal flux from
+    QNAM/QNPH) on one side and a radiation boundary (radiation_edge_hydro.F)
+    on another, with ocean forcing and land: strict bit for bit, fast at the
+    FP64 bar."""
+    path = decks.quarter_annulus(scratch / f"qa_flowrad_{strict}", nr=8, nth=16, nsteps=120, flow_amp=0.05,
+                                 radiation=True, nolibf=1, cf=0.0025)
+    deck = Deck(path)
+    assert deck.s.nfeds > 0 and deck.s.nreds > 0
+    deck.close()
+    _, _, g, o = run_both(path, 120, strict=strict)
+    if strict:
+        check_bitwise(g, o)
+    else:
+        check_state(g, o)
+
+
 def test_quarter_annulus_config1_linear_friction(built, scratch):
     """Config 1 geometry (1024 elements, SSP(2,2), linear friction), 300
     steps, fast variant."""
