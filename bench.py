@@ -12,6 +12,10 @@ DG_HYDRO_TIMESTEP over the whole mesh.  The deck is generated (seeded) into
 
 Multi-GPU (torchrun): each rank steps its own replica of the basin; the path
 has no data exchange between independent meshes (weak scaling, replicas only).
+
+The line's "mixed" object is the mixed-precision form (FP32 edge, volume and
+limiter terms; FP64 state, SSP combination and wet/dry) on the same deck: its
+rate, its speed-up over the FP64 line and its error against the FP64 form.
 """
 from __future__ import annotations
 
@@ -134,6 +138,68 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def mass(deck, ze) -> float:
+    """Total water volume: sum over elements of (ZE mode 1 + HB mode 1) * area."""
+    s = deck.s
+    ne = s.ne
+    nm = deck.int_array("nm", 3 * ne).reshape(3, ne) - 1
+    x, y = deck.real_array("x", s.np), deck.real_array("y", s.np)
+    a, b, c = nm
+    areas = (x[a] - x[c]) * (y[b] - y[c]) + (x[c] - x[b]) * (y[a] - y[c])
+    hb = deck.real_array("hb", 3 * ne).reshape(ne, 3)
+    return float(np.sum((ze[:, 0] + hb[:, 0]) * areas * 0.5))
+
+
+def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
+    """The mixed-precision form (DGSWEM_CUDA_MIXED) on the same deck: its rate
+    (same timing rules as the FP64 line), per-kernel times, and its error
+    against the FP64 form after ``--mixed-err-steps`` steps from the initial
+    state (nodal elevation and velocity, element-mean elevation, total water
+    volume, wet/dry flags)."""
+    import torch
+    from dgswem_b200 import HydroStep
+    hm = HydroStep(deck, device=device, mixed=True)
+    hm.set_stream(stream.cuda_stream)
+    hm.run(1, args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    hm.run(args.warmup + 1, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+    hm.profile(True)
+    hm.run(args.warmup + 1 + args.steps, 20)
+    prof = hm.profile_read()
+    hm.profile(False)
+    hm.close()
+    value = whole_job_rate(world, deck.s.ne, deck.s.nrk, args.steps, ms)
+    # error against the FP64 form, both from the deck's initial state
+    n = args.mixed_err_steps
+    outs = []
+    for kw in ({}, {"mixed": True}):
+        with HydroStep(deck, device=device, **kw) as h:
+            h.set_stream(stream.cuda_stream)
+            h.run(1, n)
+            h.synchronize()
+            outs.append((h.state(), h.modal2nodal()))
+    (sf, nf), (sm, nmx) = outs
+    wet = (nf[3] == 1) & (nmx[3] == 1)
+    mf, mm = mass(deck, sf[0]), mass(deck, sm[0])
+    err = {"steps": n,
+           "eta_nodal_linf_m": float(np.abs(nmx[0] - nf[0])[wet].max()),
+           "ze_mean_linf_m": float(np.abs(sm[0][:, 0] - sf[0][:, 0]).max()),
+           "vel_nodal_linf_ms": float(max(np.abs(nmx[1] - nf[1])[wet].max(), np.abs(nmx[2] - nf[2])[wet].max())),
+           "mass_rel": (mm - mf) / mf,
+           "wdflg_differ": int((sm[3] != sf[3]).sum())}
+    return {"value": value, "unit": "DOF-stage/s", "ms_per_step": ms / args.steps,
+            "dtype": "f32 edge/volume/limiter terms, f64 state, SSP, wet/dry",
+            "per_kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items() if v[1]},
+            "err_vs_fp64": err}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -217,6 +283,9 @@ def main(argv=None):
     ap.add_argument("--cpu-steps", type=int, default=12, help="oracle steps in the cpu_baseline sample")
     ap.add_argument("--ref-max-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
+    ap.add_argument("--mixed-err-steps", type=int, default=200,
+                    help="steps of the mixed-vs-FP64 error comparison")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -335,6 +404,10 @@ def main(argv=None):
                      "stage_all_kernels_frac": STAGE_TOTAL_BYTES * ne / (stage_total_ms / 1e3 / max(stage_total_n, 1)) / 1e9 / peak,
                      "per_kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items() if v[1]}},
     }
+    if not args.no_mixed:
+        mixed = mixed_arm(deck, stream, args, world, dist if world > 1 else None, local)
+        mixed["speedup_vs_fp64"] = mixed["value"] / value
+        line["mixed"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, secs = cpu_baseline(path, args.cpu_steps, threads)

@@ -21,9 +21,11 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIBNAME = "libdgswem_cuda.so"
 # (source, extra nvcc flags): the strict kernel variant is compiled without
-# fused multiply-add contraction
+# fused multiply-add contraction; the mixed one is the fast one with FP32
+# edge and volume arithmetic, whose FP32 divisions and square roots are the
+# approximate ones (the flags do not change FP64 operations)
 SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_strict.cu", ["-fmad=false"]),
-           ("deck.cpp", []), ("partition.cpp", [])]
+           ("kernels_mixed.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]), ("deck.cpp", []), ("partition.cpp", [])]
 HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

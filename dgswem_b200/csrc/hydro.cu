@@ -136,8 +136,10 @@ struct DevBuf {
   ~DevBuf() { release(); }
 };
 
-// Launchers of one compilation variant (kernels_fast.cu / kernels_strict.cu).
+// Launchers of one compilation variant (kernels_fast.cu / kernels_strict.cu /
+// kernels_mixed.cu) and the byte size of its stage kernel's arithmetic type.
 struct Variant {
+  unsigned real_bytes;
   void (*set_basis)(const BasisP1&);
   void (*stage)(const StageArgs&, bool, unsigned, size_t, cudaStream_t);
   void (*ibarrier)(const StageArgs&, bool, cudaStream_t);
@@ -151,14 +153,18 @@ struct Variant {
   void (*halo)(bool, double*, int*, int, const int*, int, int, double*, cudaStream_t);
 };
 
-static const Variant kFast = {fast::set_basis, fast::launch_stage, fast::launch_ibarrier, fast::launch_node_minmax,
+static const Variant kFast = {8, fast::set_basis, fast::launch_stage, fast::launch_ibarrier, fast::launch_node_minmax,
                               fast::launch_limit_wetdry, fast::launch_modal2nodal,
                               fast::launch_fortran_to_soa, fast::launch_soa_to_fortran, fast::launch_gather_int,
                               fast::launch_halo};
-static const Variant kStrict = {strict::set_basis, strict::launch_stage, strict::launch_ibarrier, strict::launch_node_minmax,
+static const Variant kStrict = {8, strict::set_basis, strict::launch_stage, strict::launch_ibarrier, strict::launch_node_minmax,
                                 strict::launch_limit_wetdry, strict::launch_modal2nodal,
                                 strict::launch_fortran_to_soa, strict::launch_soa_to_fortran,
                                 strict::launch_gather_int, strict::launch_halo};
+static const Variant kMixed = {4, mixed::set_basis, mixed::launch_stage, mixed::launch_ibarrier, mixed::launch_node_minmax,
+                               mixed::launch_limit_wetdry, mixed::launch_modal2nodal,
+                               mixed::launch_fortran_to_soa, mixed::launch_soa_to_fortran,
+                               mixed::launch_gather_int, mixed::launch_halo};
 
 }  // namespace dgswem
 
@@ -190,6 +196,7 @@ struct dgswem_cuda {
   MeshView mesh{};
   // device arrays
   DevBuf<double> x, y, dp, hb, egeo, cori, fric, manning, sfac_area, sfac_edge;
+  DevBuf<float> egeof;  // FP32 geometry rows of a mixed-precision handle
   DevBuf<int> nm, link, star_ptr, star, ib_elem, ib_led;
   DevBuf<unsigned> einfo, eslot, tile_tasks;
   DevBuf<int> tile_elem_ptr, tile_task_ptr, tile_halo_ptr, tile_halo;
@@ -405,7 +412,7 @@ void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>
   h->eslot.upload(eslot);
   h->mesh.max_halo = max_halo;
   h->mesh.max_tasks = max_tasks;
-  h->stage_smem = stage_layout(max_halo, std::max(max_tasks, 1)).bytes;
+  h->stage_smem = stage_layout(max_halo, std::max(max_tasks, 1), h->v->real_bytes).bytes;
   int dev_smem = 0;
   DG_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
   if (h->stage_smem > (size_t)dev_smem)
@@ -626,6 +633,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& pl
                               s->manning[node_perm[nm[(size_t)2 * nl + e]]]) / 3.;
     }
     h->egeo.upload(eg);
+    if (h->v->real_bytes == 4) h->egeof.upload(std::vector<float>(eg.begin(), eg.end()));
   }
   if (s->ics == 2) {  // SFAC_ELEM / SFACED (prep_DG.F:1055-1100), host cos
     const BasisP1 B = make_basis_p1();
@@ -685,7 +693,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& pl
   h->nparts = plan.nparts;
   h->part = plan.part;
   m.x = h->x.p; m.y = h->y.p; m.dp = h->dp.p; m.nm = h->nm.p; m.link = h->link.p; m.einfo = h->einfo.p;
-  m.hb = h->hb.p; m.egeo = h->egeo.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
+  m.hb = h->hb.p; m.egeo = h->egeo.p; m.egeof = h->egeof.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
   m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
   m.star_ptr = h->star_ptr.p; m.star = h->star.p; m.node_perm = h->node_perm.p;
   m.tile_elem_ptr = h->tile_elem_ptr.p;
@@ -798,6 +806,11 @@ void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing) {
   StageArgs A{};
   A.m = h->mesh;
   A.ph = h->ph;
+  {
+    const Physics& p = h->ph;
+    A.pf = PhysF{(float)p.g, (float)p.nleq, (float)p.leq, (float)p.nleqg, (float)p.fg_l, (float)p.tau_cap,
+                 (float)p.cori, (float)p.fric, (float)p.cf};
+  }
   A.irk = irk;
   A.qin = h->q[irk - 1].p;
   A.qout = h->q[irk].p;
@@ -929,7 +942,9 @@ int dgswem_cuda_last_error(char* buf, int buflen) {
 
 static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int nparts, int device, int flags) {
   {
-    if (flags & ~DGSWEM_CUDA_STRICT) throw Failure(DGSWEM_ERR_ARG, "unknown flags");
+    if (flags & ~(DGSWEM_CUDA_STRICT | DGSWEM_CUDA_MIXED)) throw Failure(DGSWEM_ERR_ARG, "unknown flags");
+    if ((flags & DGSWEM_CUDA_STRICT) && (flags & DGSWEM_CUDA_MIXED))
+      throw Failure(DGSWEM_ERR_ARG, "DGSWEM_CUDA_STRICT and DGSWEM_CUDA_MIXED exclude each other");
     if (s->dofh != 3) throw Failure(DGSWEM_ERR_ARG, "only p=1 (DOFH=3) is implemented on the device");
     if (s->ne <= 0 || s->np <= 0 || s->nedges <= 0) throw Failure(DGSWEM_ERR_ARG, "empty mesh");
     if (s->nrk < 1 || s->nrk > kMaxStages) throw Failure(DGSWEM_ERR_ARG, "nrk out of range");
@@ -943,7 +958,7 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     DG_CUDA(cudaSetDevice(device));
     std::unique_ptr<dgswem_cuda> h(new dgswem_cuda());
     h->device = device;
-    h->v = (flags & DGSWEM_CUDA_STRICT) ? &kStrict : &kFast;
+    h->v = (flags & DGSWEM_CUDA_STRICT) ? &kStrict : (flags & DGSWEM_CUDA_MIXED) ? &kMixed : &kFast;
     h->ne = s->ne;
     h->np = s->np;
     h->nrk = s->nrk;
@@ -986,6 +1001,7 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
       const BasisP1 B = make_basis_p1();
       kFast.set_basis(B);
       kStrict.set_basis(B);
+      kMixed.set_basis(B);
       DG_CUDA(cudaGetLastError());
     }
     const PartPlan plan = make_part_plan(s, part, nparts);

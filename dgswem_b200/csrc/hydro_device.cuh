@@ -46,18 +46,23 @@ __host__ __device__ inline unsigned ei_nled(unsigned info, int l) { return (info
 __host__ __device__ inline unsigned ei_order(unsigned info, int s) { return (info >> (18 + 2 * s)) & 3u; }
 
 // p=1 basis tables (orthogonal_basis_v1.F, prep_DG.F:648-870), Lobatto edge
-// rule (quad_rules_general.F) and 3-point area rule (quadrature_v1.F:255-260)
-struct BasisP1 {
-  double phi_edge[3][3][3];  // [led][point][mode]
-  double edgeq[3][3][3];     // 2*M_INV*PHI_EDGE*WEGP
-  double phi_area[3][3];     // [mode][point]
-  double drphi[3][3], dsphi[3][3];
-  double phi_corner[3][3];   // [vertex][mode]
-  double psi[3][3];          // [vertex][area point] linear nodal basis
-  double m_inv[3], wagp[3], wegp[3], xegp[3];
-  double mw[3][3];           // [mode][point] M_INV*WAGP
-  double srfac[3][3];        // [mode][point] M_INV*WAGP*PHI_AREA (SRFAC without the area)
+// rule (quad_rules_general.F) and 3-point area rule (quadrature_v1.F:255-260).
+// Built in FP64 on the host; the mixed-precision kernels also keep an FP32
+// copy for their FP32 arithmetic.
+template <class T>
+struct BasisT {
+  T phi_edge[3][3][3];  // [led][point][mode]
+  T edgeq[3][3][3];     // 2*M_INV*PHI_EDGE*WEGP
+  T phi_area[3][3];     // [mode][point]
+  T drphi[3][3], dsphi[3][3];
+  T phi_corner[3][3];   // [vertex][mode]
+  T psi[3][3];          // [vertex][area point] linear nodal basis
+  T m_inv[3], wagp[3], wegp[3], xegp[3];
+  T mw[3][3];           // [mode][point] M_INV*WAGP
+  T srfac[3][3];        // [mode][point] M_INV*WAGP*PHI_AREA (SRFAC without the area)
 };
+using BasisP1 = BasisT<double>;
+static_assert(sizeof(BasisT<float>) * 2 == sizeof(BasisT<double>), "basis tables are plain arrays");
 
 struct MeshView {
   int ne, np;
@@ -69,6 +74,7 @@ struct MeshView {
   const unsigned* __restrict__ einfo;
   const double* __restrict__ hb;
   const double* __restrict__ egeo;      // [r*NE + e] element geometry rows (EGeo)
+  const float* __restrict__ egeof;      // the same rows in FP32 (mixed-precision handles), or null
   const double* __restrict__ cori;      // per element, or null (uniform)
   const double* __restrict__ fric;      // per element, or null (uniform)
   const double* __restrict__ manning;   // nodal, or null
@@ -149,19 +155,28 @@ constexpr int kVolRows = 8;  // per area point: fx fy gx gy hx hy sx sy
 // a 112-byte stride that keeps 16-byte loads by 8 consecutive slots free of
 // bank conflicts
 constexpr unsigned kQStride = 14;
+// floats per element slot of the FP32 copy of the shared state (mixed
+// precision): the 12 modal values, three 16-byte loads, a 48-byte stride
+// that is conflict-free for 8 consecutive slots
+constexpr unsigned kQfStride = 12;
 struct StageLayout {
-  unsigned qs, geo, vol, res, wd, gid, tdry, info, bytes;
+  unsigned qs, geo, qf, vol, res, wd, gid, tdry, info, bytes;
 };
 __host__ __device__ inline unsigned align16(unsigned x) { return (x + 15u) & ~15u; }
-__host__ __device__ inline StageLayout stage_layout(int max_halo, int max_tasks) {
+// rb: bytes of the arithmetic type of the edge and volume terms (8: FP64
+// kernels; 4: mixed precision, which adds the FP32 slot copy qf)
+__host__ __device__ inline StageLayout stage_layout(int max_halo, int max_tasks, unsigned rb) {
   StageLayout L;
   const unsigned S = kTile + (unsigned)max_halo;
   const unsigned T = (unsigned)max_tasks;
-  L.qs = align16((unsigned)sizeof(BasisP1));
-  L.geo = L.qs + kQStride * S * 8u;            // qs[S][kQStride]: ZE, QX, QY, HB modes
-  L.vol = L.geo + kGeoRows * kTile * 8u;       // geo[kGeoRows][kTile]
-  L.res = L.vol + kVolRows * 3u * kTile * 8u;  // vol[kVolRows][3][kTile]
-  L.wd = L.res + 15u * T * 8u;                 // res[task][point][5]
+  L.qs = align16(rb == 8u ? (unsigned)sizeof(BasisT<double>) : (unsigned)sizeof(BasisT<float>));
+  // qs[S][kQStride]: ZE, QX, QY, HB modes (mixed: the tile's own slots only,
+  // for the FP64 SSP combination; the edge and volume terms read qf)
+  L.geo = L.qs + kQStride * (rb == 8u ? S : (unsigned)kTile) * 8u;
+  L.qf = L.geo + kGeoRows * kTile * rb;        // geo[kGeoRows][kTile] in the arithmetic type
+  L.vol = L.qf + (rb == 8u ? 0u : kQfStride * S * 4u);  // qf[S][kQfStride] (mixed only)
+  L.res = L.vol + kVolRows * 3u * kTile * rb;  // vol[kVolRows][3][kTile]
+  L.wd = L.res + 15u * T * rb;                 // res[task][point][5]
   L.gid = align16(L.wd + S * 4u);              // wd[S]
   L.tdry = align16(L.gid + (unsigned)max_halo * 4u);
   L.info = align16(L.tdry + T * 4u);          // einfo, eslot of the tile's elements
@@ -176,9 +191,15 @@ struct Physics {
   int iflinbf, ifhybf, ifnlfa, nws, rainfall, ics;
 };
 
+// Physics constants of the stage kernel's FP32 terms (mixed precision)
+struct PhysF {
+  float g, nleq, leq, nleqg, fg_l, tau_cap, cori, fric, cf;
+};
+
 struct StageArgs {
   MeshView m;
   Physics ph;
+  PhysF pf;  // ph rounded to FP32
   int irk;                                  // 1-based stage
   const double* __restrict__ qin;           // state of stage irk (edges read it)
   double* qout;                             // state of stage irk+1
@@ -210,7 +231,9 @@ struct LimitArgs {
 
 // Kernel launchers, one set per compilation variant: `fast` lets the
 // compiler contract a*b+c into FMA; `strict` (-fmad=false) keeps every
-// product and sum separately rounded, the evaluation the FP64 oracle uses.
+// product and sum separately rounded, the evaluation the FP64 oracle uses;
+// `mixed` is `fast` with the stage kernel's edge and volume arithmetic in
+// FP32 (state, SSP combination, limiter and wet/dry stay FP64).
 #define DGSWEM_DECLARE_LAUNCHERS(NS)                                                           \
   namespace NS {                                                                               \
   void set_basis(const BasisP1& b);                                                            \
@@ -233,6 +256,7 @@ struct LimitArgs {
 
 DGSWEM_DECLARE_LAUNCHERS(fast)
 DGSWEM_DECLARE_LAUNCHERS(strict)
+DGSWEM_DECLARE_LAUNCHERS(mixed)
 
 constexpr int kPointBlock = 256;
 

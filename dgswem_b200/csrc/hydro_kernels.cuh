@@ -20,6 +20,38 @@ namespace DGSWEM_VARIANT {
 
 __constant__ BasisP1 cBasis;
 
+// Arithmetic type of the stage kernel's edge and volume terms: FP64, or
+// FP32 in the mixed-precision variant (kernels_mixed.cu), whose state,
+// SSP combination, ocean depth-positivity fix, limiter and wet/dry stay FP64.
+#ifdef DGSWEM_MIXED
+typedef float real;
+#else
+typedef double real;
+#endif
+__constant__ BasisT<real> cBasisR;  // cBasis in that type
+
+// Element geometry rows in the arithmetic type
+__device__ __forceinline__ const real* egeo_r(const MeshView& m) {
+#ifdef DGSWEM_MIXED
+  return m.egeof;
+#else
+  return m.egeo;
+#endif
+}
+
+// Physics constants of the stage kernel's terms in the arithmetic type
+struct PhysR {
+  real g, nleq, leq, nleqg, fg_l, tau_cap, cori, fric, cf;
+};
+__device__ __forceinline__ PhysR phys_r(const StageArgs& A) {
+#ifdef DGSWEM_MIXED
+  const PhysF& p = A.pf;
+#else
+  const Physics& p = A.ph;
+#endif
+  return PhysR{p.g, p.nleq, p.leq, p.nleqg, p.fg_l, p.tau_cap, p.cori, p.fric, p.cf};
+}
+
 // Asynchronous global -> shared copies (cp.async, completion by
 // cp.async.wait_all): the data goes straight to shared memory.
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
@@ -35,6 +67,9 @@ __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)
 __device__ __forceinline__ void cp_async8_s(unsigned dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async4_s(unsigned dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
 
 // DEPTH**(1.D0/3.D0) of the Manning friction (rhs_dg_hydro.F).  The strict
 // variant calls pow with the reference's exponent; the fast variant takes
@@ -47,83 +82,92 @@ __device__ __forceinline__ double cube_root(double x) {
   return pow(x, 1.0 / 3.0);
 #endif
 }
+__device__ __forceinline__ float cube_root(float x) { return cbrtf(x); }
 
-struct Flux3 {
-  double f, g, h;
+template <class T>
+struct Flux3T {
+  T f, g, h;
 };
+using Flux3 = Flux3T<double>;
 
-// numerical_flux.F:750-914, Local Lax-Friedrichs.  kNonlin specialises
-// NLEQ=1, LEQ=0 (the products with 1 and sums with 0 it removes are exact).
-template <bool kNonlin>
-__device__ __forceinline__ Flux3 llf(const Physics& P, double ze_in, double ze_ex, double qx_in,
-                                     double qx_ex, double qy_in, double qy_ex, double hb_in,
-                                     double hb_ex, double sf_in, double sf_ex, double nx, double ny,
-                                     double G) {
-  const double NLEQ = kNonlin ? 1.0 : P.nleq;
-  const double LEQ = kNonlin ? 0.0 : P.leq;
-  const double nleqg = G * NLEQ;
-  const double j1 = ze_ex - ze_in, j2 = qx_ex - qx_in, j3 = qy_ex - qy_in;
-  double ht_in, f1, fx1i, fy1i, fh, ui, vi, fx2i, fy2i, fx3i, fy3i;
+// Total depth HT = ZE*NLEQ + HB of numerical_flux.F's flux evaluation.
+template <bool kNonlin, class T>
+__device__ __forceinline__ T depth(const Physics& P, T ze, T hb) {
+  return kNonlin ? ze + hb : ze * T(P.nleq) + hb;
+}
+
+// numerical_flux.F:750-914, Local Lax-Friedrichs, in arithmetic type T.
+// kNonlin specialises NLEQ=1, LEQ=0 (the products with 1 and sums with 0 it
+// removes are exact).  ht_in / ht_ex: the total depths, depth(ze, hb) --
+// passed in so that the mixed-precision kernels can supply them from FP32
+// depth traces rather than from an FP32 sum of elevation and bathymetry.
+template <bool kNonlin, class T>
+__device__ __forceinline__ Flux3T<T> llf(const Physics& P, T ze_in, T ze_ex, T qx_in, T qx_ex, T qy_in,
+                                         T qy_ex, T hb_in, T hb_ex, T ht_in, T ht_ex, T sf_in, T sf_ex, T nx,
+                                         T ny, T G) {
+  const T NLEQ = kNonlin ? T(1) : T(P.nleq);
+  const T LEQ = kNonlin ? T(0) : T(P.leq);
+  const T nleqg = G * NLEQ;
+  const T j1 = ze_ex - ze_in, j2 = qx_ex - qx_in, j3 = qy_ex - qy_in;
+  T f1, fx1i, fy1i, fh, ui, vi, fx2i, fy2i, fx3i, fy3i;
   {
-    ht_in = kNonlin ? ze_in + hb_in : ze_in * NLEQ + hb_in;
-    f1 = kNonlin ? 1.0 : NLEQ + LEQ * hb_in;
+    f1 = kNonlin ? T(1) : NLEQ + LEQ * hb_in;
     fx1i = qx_in * f1 * sf_in;
     fy1i = qy_in * f1;
-    const double fu = kNonlin ? qx_in : NLEQ * qx_in;
-    const double fv = kNonlin ? qy_in : NLEQ * qy_in;
-    const double fg = nleqg * ze_in;
-    fh = 1.0 / (kNonlin ? ht_in : NLEQ * ht_in + LEQ);
+    const T fu = kNonlin ? qx_in : NLEQ * qx_in;
+    const T fv = kNonlin ? qy_in : NLEQ * qy_in;
+    const T fg = nleqg * ze_in;
+    fh = T(1) / (kNonlin ? ht_in : NLEQ * ht_in + LEQ);
     ui = qx_in * fh;
     vi = qy_in * fh;
-    const double huu = fu * ui, hvv = fv * vi, huv = fu * vi;
-    const double gh2 = kNonlin ? fg * (0.5 * ze_in + hb_in) : fg * (0.5 * ze_in + hb_in) + P.fg_l * ze_in;
+    const T huu = fu * ui, hvv = fv * vi, huv = fu * vi;
+    const T gh2 = kNonlin ? fg * (T(0.5) * ze_in + hb_in) : fg * (T(0.5) * ze_in + hb_in) + T(P.fg_l) * ze_in;
     fx2i = (huu + gh2) * sf_in;
     fy2i = huv;
     fx3i = huv * sf_in;
     fy3i = hvv + gh2;
   }
-  double ht_ex, fx1e, fy1e, ue, ve, fx2e, fy2e, fx3e, fy3e;
+  T fx1e, fy1e, ue, ve, fx2e, fy2e, fx3e, fy3e;
   {
-    ht_ex = kNonlin ? ze_ex + hb_ex : ze_ex * NLEQ + hb_ex;
-    const double f1e = kNonlin ? 1.0 : NLEQ + LEQ * hb_ex;
+    const T f1e = kNonlin ? T(1) : NLEQ + LEQ * hb_ex;
     fx1e = qx_ex * f1e * sf_ex;
     fy1e = qy_ex * f1e;
-    const double fu = kNonlin ? qx_ex : NLEQ * qx_ex;
-    const double fv = kNonlin ? qy_ex : NLEQ * qy_ex;
-    const double fg = nleqg * ze_ex;
-    const double fhe = 1.0 / (kNonlin ? ht_ex : NLEQ * ht_ex + LEQ);
+    const T fu = kNonlin ? qx_ex : NLEQ * qx_ex;
+    const T fv = kNonlin ? qy_ex : NLEQ * qy_ex;
+    const T fg = nleqg * ze_ex;
+    const T fhe = T(1) / (kNonlin ? ht_ex : NLEQ * ht_ex + LEQ);
     ue = qx_ex * fhe;
     ve = qy_ex * fhe;
-    const double huu = fu * ue, hvv = fv * ve, huv = fu * ve;
-    const double gh2 = kNonlin ? fg * (0.5 * ze_ex + hb_ex) : fg * (0.5 * ze_ex + hb_ex) + P.fg_l * ze_ex;
+    const T huu = fu * ue, hvv = fv * ve, huv = fu * ve;
+    const T gh2 = kNonlin ? fg * (T(0.5) * ze_ex + hb_ex) : fg * (T(0.5) * ze_ex + hb_ex) + T(P.fg_l) * ze_ex;
     fx2e = (huu + gh2) * sf_ex;
     fy2e = huv;
     fx3e = huv * sf_ex;
     fy3e = hvv + gh2;
   }
-  const double f1a = 0.5 * ((fx1i + fx1e) * nx + (fy1i + fy1e) * ny);
-  const double f2a = 0.5 * ((fx2i + fx2e) * nx + (fy2i + fy2e) * ny);
-  const double f3a = 0.5 * ((fx3i + fx3e) * nx + (fy3i + fy3e) * ny);
-  const double uni = kNonlin ? ui * nx + vi * ny : (ui * nx + vi * ny) * NLEQ;
-  const double nxsi = nx * sf_in, nxse = nx * sf_ex;
-  const double ci = sqrt(G * ht_in * (ny * ny + nxsi * nxsi));
-  const double une = kNonlin ? ue * nx + ve * ny : (ue * nx + ve * ny) * NLEQ;
-  const double ce = sqrt(G * ht_ex * (ny * ny + nxse * nxse));
+  const T f1a = T(0.5) * ((fx1i + fx1e) * nx + (fy1i + fy1e) * ny);
+  const T f2a = T(0.5) * ((fx2i + fx2e) * nx + (fy2i + fy2e) * ny);
+  const T f3a = T(0.5) * ((fx3i + fx3e) * nx + (fy3i + fy3e) * ny);
+  const T uni = kNonlin ? ui * nx + vi * ny : (ui * nx + vi * ny) * NLEQ;
+  const T nxsi = nx * sf_in, nxse = nx * sf_ex;
+  const T ci = sqrt(G * ht_in * (ny * ny + nxsi * nxsi));
+  const T une = kNonlin ? ue * nx + ve * ny : (ue * nx + ve * ny) * NLEQ;
+  const T ce = sqrt(G * ht_ex * (ny * ny + nxse * nxse));
   // max(|un+c|, |un|, |un-c|) over both sides.  For c >= 0 the rounded
   // |un| + c equals the rounded larger of |un + c| and |un - c| exactly, so
   // fmax(|un| + c, |un|) is the same value; with c = NaN (negative depth) both
   // forms reduce to |un|, as fmax skips NaN operands.
-  const double ai = fabs(uni), ae = fabs(une);
-  const double eig = fmax(fmax(ai + ci, ai), fmax(ae + ce, ae));
-  Flux3 r;
-  r.f = f1a - 0.5 * eig * j1;
+  const T ai = fabs(uni), ae = fabs(une);
+  const T eig = fmax(fmax(ai + ci, ai), fmax(ae + ce, ae));
+  Flux3T<T> r;
+  r.f = f1a - T(0.5) * eig * j1;
   if (kNonlin) {
-    r.g = f2a - 0.5 * eig * j2;
-    r.h = f3a - 0.5 * eig * j3;
+    r.g = f2a - T(0.5) * eig * j2;
+    r.h = f3a - T(0.5) * eig * j3;
   } else {
-    const double nx2 = NLEQ + LEQ * nx * nx, ny2 = NLEQ + LEQ * ny * ny, nxy = nx * ny;
-    r.g = f2a - 0.5 * eig * (j2 * nx2 + LEQ * j3 * nxy);
-    r.h = f3a - 0.5 * eig * (j3 * ny2 + LEQ * j2 * nxy);
+    const T nx2 = NLEQ + LEQ * nx * nx, ny2 = NLEQ + LEQ * ny * ny, nxy = nx * ny;
+    r.g = f2a - T(0.5) * eig * (j2 * nx2 + LEQ * j3 * nxy);
+    r.h = f3a - T(0.5) * eig * (j3 * ny2 + LEQ * j2 * nxy);
   }
   return r;
 }
@@ -148,11 +192,12 @@ __device__ __forceinline__ void edge_trace(const BasisP1& B, const double* q, in
 // (land_edge_hydro.F:201-218, ocean_edge_hydro.F:148-177 and 255-259,
 // flow_edge_hydro.F:126-150, radiation_edge_hydro.F:173-193,
 // ebarrier_edge_hydro.F:120-160).  Point j of the edge, normal (nx, ny).
-__device__ __forceinline__ void ghost_state(const StageArgs& A, const BasisP1& B, unsigned kind, int list, int j,
-                                            double zi, double xi, double yi, double hbi, double nx, double ny,
-                                            double& zx, double& xx, double& yx) {
+// The ocean elevation sum and its depth-positivity fix are FP64 in every
+// variant.
+__device__ __forceinline__ void ghost_state(const StageArgs& A, unsigned kind, int list, int j, real zi, real xi,
+                                            real yi, real hbi, real nx, real ny, real& zx, real& xx, real& yx) {
   const Physics& P = A.ph;
-  const double tx = -ny, ty = nx;
+  const real tx = -ny, ty = nx;
   zx = zi;
   xx = xi;
   yx = yi;
@@ -161,40 +206,42 @@ __device__ __forceinline__ void ghost_state(const StageArgs& A, const BasisP1& B
     double zsum = 0.0;
     for (int f = 0; f < A.m.nbfr; ++f) {
       const double* zg = A.ocean_zg + ((size_t)f * A.m.needs + list) * 2;
-      zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * B.xegp[j]);
+      zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * cBasis.xegp[j]);
     }
-    zx = zsum;
-    if (zx * P.ifnlfa + hbi <= 0) zx = fabs(hbi) + P.h0;
+    const double hbd = hbi;
+    if (zsum * P.ifnlfa + hbd <= 0) zsum = fabs(hbd) + P.h0;
+    zx = (real)zsum;
   } else if (kind == kLand) {
-    const double qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
-    const double qne = -qn, qte = qt, den = 1.0 / (nx * ty - ny * tx);
+    const real qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
+    const real qne = -qn, qte = qt, den = real(1) / (nx * ty - ny * tx);
     xx = (ty * qne - ny * qte) * den;
     yx = (-tx * qne + nx * qte) * den;
   } else if (kind == kFlow) {
     // per-point terms QNAM_GP*RFF*COS(ARG) come from the host for this stage
-    double qne = 0.0;
-    xx = 0.0;
-    yx = 0.0;
+    real qne = 0;
+    xx = 0;
+    yx = 0;
     for (int f = 0; f < A.m.nffr; ++f) {
-      qne = qne + A.flow_qn[((size_t)f * A.m.nfeds + list) * 3 + j];
-      xx = -(ty * qne - ny * 0.0) / (nx * ty - ny * tx);
-      yx = -(-tx * qne + nx * 0.0) / (nx * ty - ny * tx);
+      qne = qne + (real)A.flow_qn[((size_t)f * A.m.nfeds + list) * 3 + j];
+      xx = -(ty * qne - ny * real(0)) / (nx * ty - ny * tx);
+      yx = -(-tx * qne + nx * real(0)) / (nx * ty - ny * tx);
     }
   } else if (kind == kRadiation) {
-    const double qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
-    const double qne = -qn + 2 * sqrt(P.g / (hbi + zi)) * zi, qte = qt, den = 1.0 / (nx * ty - ny * tx);
+    const real qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
+    const real qne = -qn + real(2) * sqrt(real(P.g) / (hbi + zi)) * zi, qte = qt,
+               den = real(1) / (nx * ty - ny * tx);
     xx = (ty * qne - ny * qte) * den;
     yx = (-tx * qne + nx * qte) * den;
   } else if (kind == kEBarrier) {
-    const double above = zi - A.m.ebht[list];
-    const double subsup = 2.0 * above / 3.0;
-    double qne, qte;
-    if (above < 0.01) {
+    const real above = zi - (real)A.m.ebht[list];
+    const real subsup = real(2) * above / real(3);
+    real qne, qte;
+    if (above < real(0.01)) {
       qne = -(xi * nx + yi * ny);
       qte = xi * tx + yi * ty;
     } else {
-      qne = A.rampdg * A.m.ebcfsp[list] * subsup * sqrt(subsup * P.g);
-      qte = 0.0;
+      qne = (real)A.rampdg * (real)A.m.ebcfsp[list] * subsup * sqrt(subsup * real(P.g));
+      qte = 0;
     }
     xx = (ty * qne - ny * qte) / (nx * ty - ny * tx);
     yx = (-tx * qne + nx * qte) / (nx * ty - ny * tx);
@@ -245,6 +292,7 @@ __device__ __noinline__ void ibarrier_side(const StageArgs& A, int seg, int side
     edge_trace(B, qf, ledf, gpf, zef, qxf, qyf);
     const double hbbp = hbb[0] + hbb[1] * B.phi_edge[ledb][gpb][1] + hbb[2] * B.phi_edge[ledb][gpb][2];
     const double hbfp = hbf[0] + hbf[1] * B.phi_edge[ledf][gpf][1] + hbf[2] * B.phi_edge[ledf][gpf][2];
+    const double htb = depth<kNonlin>(P, zeb, hbbp), htf = depth<kNonlin>(P, zef, hbfp);
     const double sfb = m.sfac_edge ? m.sfac_edge[(size_t)(ledb * 3 + gpb) * ne + elb] : 1.0;
     const double sff = m.sfac_edge ? m.sfac_edge[(size_t)(ledf * 3 + gpf) * ne + elf] : 1.0;
     double aboveb = 0.0, abovef = 0.0;
@@ -275,18 +323,20 @@ __device__ __noinline__ void ibarrier_side(const StageArgs& A, int seg, int side
     if (weir <= 0) {
       qxe = (tyb * qbn - nyb * qbt) / (nxb * tyb - nyb * txb);
       qye = (-txb * qbn + nxb * qbt) / (nxb * tyb - nyb * txb);
-      fb = llf<kNonlin>(P, zeb, zeb, qxb, qxe, qyb, qye, hbbp, hbbp, sfb, sfb, nxb, nyb, P.g);
+      fb = llf<kNonlin>(P, zeb, zeb, qxb, qxe, qyb, qye, hbbp, hbbp, htb, htb, sfb, sfb, nxb, nyb, P.g);
       if (weir < 0) {  // the front side keeps the back side's exterior momentum
-        ff = llf<kNonlin>(P, zef, zef, qxf, qxe, qyf, qye, hbfp, hbfp, sff, sff, nxf, nyf, wdf == 0 ? 0.0 : P.g);
+        ff = llf<kNonlin>(P, zef, zef, qxf, qxe, qyf, qye, hbfp, hbfp, htf, htf, sff, sff, nxf, nyf,
+                          wdf == 0 ? 0.0 : P.g);
         done = true;
       }
     }
     if (!done && weir >= 0) {
       qxe = (tyf * qfn - nyf * qft) / (nxf * tyf - nyf * txf);
       qye = (-txf * qfn + nxf * qft) / (nxf * tyf - nyf * txf);
-      ff = llf<kNonlin>(P, zef, zef, qxf, qxe, qyf, qye, hbfp, hbfp, sff, sff, nxf, nyf, P.g);
+      ff = llf<kNonlin>(P, zef, zef, qxf, qxe, qyf, qye, hbfp, hbfp, htf, htf, sff, sff, nxf, nyf, P.g);
       if (weir > 0)
-        fb = llf<kNonlin>(P, zeb, zeb, qxb, qxe, qyb, qye, hbbp, hbbp, sfb, sfb, nxb, nyb, wdb == 0 ? 0.0 : P.g);
+        fb = llf<kNonlin>(P, zeb, zeb, qxb, qxe, qyb, qye, hbbp, hbbp, htb, htb, sfb, sfb, nxb, nyb,
+                          wdb == 0 ? 0.0 : P.g);
     }
     const Flux3 fo = side == 0 ? fb : ff;
     const int led = side == 0 ? ledb : ledf, gp = side == 0 ? gpb : gpf;
@@ -340,51 +390,85 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 #define DGSWEM_STAGE_MIN_BLOCKS 2
 #endif
 
-// Trace at edge point (led, gp) of the 12 modal values (ZE, QX, QY, HB
-// modes, contiguous) of shared-memory slot `slot`; mode 0 of the basis is 1
-// on every edge point.
-__device__ __forceinline__ void slot_trace(const BasisP1& B, const double* qs, int slot, int led, int gp,
-                                           double& z, double& u, double& v, double& h) {
-  const double p1 = B.phi_edge[led][gp][1], p2 = B.phi_edge[led][gp][2];
-  const double2* q = reinterpret_cast<const double2*>(qs + slot * kQStride);
-  const double2 a = q[0], b = q[1], c = q[2], d = q[3], f = q[4], g = q[5];
-  z = a.x + a.y * p1 + b.x * p2;
-  u = b.y + c.x * p1 + c.y * p2;
-  v = d.x + d.y * p1 + f.x * p2;
-  h = f.y + g.x * p1 + g.y * p2;
+// The 12 modal values (ZE, QX, QY, HB modes, contiguous) of shared-memory
+// slot `slot` in the arithmetic type: the FP64 slots qs (stride kQStride),
+// or their FP32 copy (stride kQfStride) in the mixed variant.
+__device__ __forceinline__ void slot_values(const real* qt, int slot, real v[12]) {
+#ifdef DGSWEM_MIXED
+  const float4* q = reinterpret_cast<const float4*>(qt + slot * kQfStride);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const float4 t = q[j];
+    v[4 * j] = t.x; v[4 * j + 1] = t.y; v[4 * j + 2] = t.z; v[4 * j + 3] = t.w;
+  }
+#else
+  const double2* q = reinterpret_cast<const double2*>(qt + slot * kQStride);
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const double2 t = q[j];
+    v[2 * j] = t.x; v[2 * j + 1] = t.y;
+  }
+#endif
+}
+
+// Trace at edge point (led, gp) of slot `slot`'s ZE, QX, QY and HB; mode 0
+// of the basis is 1 on every edge point.
+__device__ __forceinline__ void slot_trace(const BasisT<real>& B, const real* qt, int slot, int led, int gp,
+                                           real& z, real& u, real& v, real& h) {
+  const real p1 = B.phi_edge[led][gp][1], p2 = B.phi_edge[led][gp][2];
+  real q[12];
+  slot_values(qt, slot, q);
+  z = q[0] + q[1] * p1 + q[2] * p2;
+  u = q[3] + q[4] * p1 + q[5] * p2;
+  v = q[6] + q[7] * p1 + q[8] * p2;
+  h = q[9] + q[10] * p1 + q[11] * p2;
+}
+
+// Bathymetry hb and total depth ht at a trace point from elevation z and the
+// slot's fourth trace w: w is HB in the FP64 kernels; the mixed kernels'
+// FP32 slots hold the depth modes ZE + HB (summed in FP64, then rounded), so
+// that a thin water column keeps FP32 relative accuracy instead of being the
+// difference of two rounded values of metres.
+template <bool kNonlin>
+__device__ __forceinline__ void trace_depth(const Physics& P, real z, real w, real& hb, real& ht) {
+#ifdef DGSWEM_MIXED
+  hb = w - z;
+  ht = kNonlin ? w : depth<kNonlin>(P, z, hb);
+#else
+  hb = w;
+  ht = depth<kNonlin>(P, z, hb);
+#endif
 }
 
 // Phase 3 of the stage kernel for area point I of tile element el (global
 // id e): volume fluxes and sources (rhs_dg_hydro.F:58-470) into
 // vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  C: the basis
-// tables in shared memory (I is a runtime index).
+// tables in shared memory (I is a runtime index); qt: the slots in the
+// arithmetic type.
 template <bool kNonlin, bool kSph>
-__device__ __forceinline__ void volume_values(const StageArgs& A, const BasisP1& C, const double* qs, int S,
-                                              const double* geo, int I, int el, int e, double out[8]) {
+__device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<real>& C, const real* qt,
+                                              const real* geo, int I, int el, int e, real out[8]) {
   const MeshView& m = A.m;
   const Physics& P = A.ph;
+  const PhysR R = phys_r(A);
   const int ne = m.ne;
   const int wde = 1;  // phase 3 runs for wet elements only
-  double q[9], hbe[3];
-  {
-    const double2* s2 = reinterpret_cast<const double2*>(qs + el * kQStride);
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      const double2 t = s2[j];
-      double* dst0 = 2 * j < 9 ? &q[2 * j] : &hbe[2 * j - 9];
-      double* dst1 = 2 * j + 1 < 9 ? &q[2 * j + 1] : &hbe[2 * j + 1 - 9];
-      *dst0 = t.x;
-      *dst1 = t.y;
-    }
-  }
-  const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
-  const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
-  const double NLEQ = kNonlin ? 1.0 : P.nleq, LEQ = kNonlin ? 0.0 : P.leq;
-  const double cori = m.cori ? m.cori[e] : P.cori;
-  double fric = m.fric ? m.fric[e] : P.fric;
-  double zq = q[0], uq = q[3], vq = q[6];
-  const double hq = hbe[0] * C.phi_area[0][I] + hbe[1] * C.phi_area[1][I] + hbe[2] * C.phi_area[2][I];
-  double dhx = 0.0, dhy = 0.0;
+  real q[12];
+  slot_values(qt, el, q);
+#ifdef DGSWEM_MIXED
+  // the slot holds the depth modes ZE + HB (see trace_depth)
+  const real hbe[3] = {q[9] - q[0], q[10] - q[1], q[11] - q[2]};
+#else
+  const real* hbe = q + 9;
+#endif
+  const real drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+  const real drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
+  const real NLEQ = kNonlin ? real(1) : R.nleq, LEQ = kNonlin ? real(0) : R.leq;
+  const real cori = m.cori ? (real)m.cori[e] : R.cori;
+  real fric = m.fric ? (real)m.fric[e] : R.fric;
+  real zq = q[0], uq = q[3], vq = q[6];
+  const real hq = hbe[0] * C.phi_area[0][I] + hbe[1] * C.phi_area[1][I] + hbe[2] * C.phi_area[2][I];
+  real dhx = 0, dhy = 0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     dhx = dhx + hbe[k] * (C.drphi[k][I] * drdx + C.dsphi[k][I] * dsdx);
@@ -393,60 +477,65 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisP1&
   zq = zq + q[1] * C.phi_area[1][I] + q[2] * C.phi_area[2][I];
   uq = uq + q[4] * C.phi_area[1][I] + q[5] * C.phi_area[2][I];
   vq = vq + q[7] * C.phi_area[1][I] + q[8] * C.phi_area[2][I];
-  const double depth = zq + hq;
-  const double sfq = kSph ? m.sfac_area[(size_t)I * ne + e] : 1.0;
-  const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
-  const double fx = uq * f1 * sfq, fy = vq * f1;
-  const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
-  const double fg = P.nleqg * zq * wde;
-  const double fh = 1.0 / (kNonlin ? depth : NLEQ * depth + LEQ);
-  const double u = uq * fh, v = vq * fh;
-  const double huu = fu * u, hvv = fv * v, huv = fu * v;
-  const double gh2 = kNonlin ? fg * (0.5 * zq + hq) : fg * (0.5 * zq + hq) + P.fg_l * zq;
-  const double gx = (huu + gh2) * sfq, gy = huv;
-  const double hx = huv * sfq, hy = hvv + gh2;
+#ifdef DGSWEM_MIXED
+  const real depth =
+      kNonlin ? q[9] + q[10] * C.phi_area[1][I] + q[11] * C.phi_area[2][I] : zq + hq;
+#else
+  const real depth = zq + hq;
+#endif
+  const real sfq = kSph ? (real)m.sfac_area[(size_t)I * ne + e] : real(1);
+  const real f1 = kNonlin ? real(1) : NLEQ + LEQ * hq;
+  const real fx = uq * f1 * sfq, fy = vq * f1;
+  const real fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
+  const real fg = R.nleqg * zq * wde;
+  const real fh = real(1) / (kNonlin ? depth : NLEQ * depth + LEQ);
+  const real u = uq * fh, v = vq * fh;
+  const real huu = fu * u, hvv = fv * v, huv = fu * v;
+  const real gh2 = kNonlin ? fg * (real(0.5) * zq + hq) : fg * (real(0.5) * zq + hq) + R.fg_l * zq;
+  const real gx = (huu + gh2) * sfq, gy = huv;
+  const real hx = huv * sfq, hy = hvv + gh2;
   if (m.manning) {
-    const double nbar = geo[EGeo::kNbar * kTile + el];
-    fric = P.g * (nbar * nbar) / cube_root(depth);
-    if (fric < P.cf) fric = P.cf;
+    const real nbar = geo[EGeo::kNbar * kTile + el];
+    fric = R.g * (nbar * nbar) / cube_root(depth);
+    if (fric < R.cf) fric = R.cf;
   }
-  double tau = fric;
+  real tau = fric;
   if (P.iflinbf == 0) {
-    const double umag = sqrt(u * u + v * v);
+    const real umag = sqrt(u * u + v * v);
     tau = tau * umag * fh;
     if (P.ifhybf == 1) tau = tau * geo[SGeo::kHyb * kTile + el];
-    tau = fmin(tau, P.tau_cap);
+    tau = fmin(tau, R.tau_cap);
   }
-  double sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
-  double sy = -(tau * vq) + fg * dhy - cori * uq;
+  real sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
+  real sy = -(tau * vq) + fg * dhy - cori * uq;
   if (P.nws != 0) {
     // met_forcing.F:49-66: the nodal fields are scaled by the ramp each stage
-    const double drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
-    double dpsidx[3], dpsidy[3];
+    const real drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
+    real dpsidx[3], dpsidy[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
       dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
     }
-    const double fw = 1.0 / f1, r = A.rampdg;
+    const real fw = real(1) / f1, r = (real)A.rampdg;
     const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
-    const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
-    const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];
-    const double p0 = r * A.pr[n0], p1 = r * A.pr[n1], p2 = r * A.pr[n2];
+    const real wx0 = r * (real)A.wsx[n0], wx1 = r * (real)A.wsx[n1], wx2 = r * (real)A.wsx[n2];
+    const real wy0 = r * (real)A.wsy[n0], wy1 = r * (real)A.wsy[n1], wy2 = r * (real)A.wsy[n2];
+    const real p0 = r * (real)A.pr[n0], p1 = r * (real)A.pr[n1], p2 = r * (real)A.pr[n2];
     sx = sx + fw * (wx0 * C.psi[0][I] + wx1 * C.psi[1][I] + wx2 * C.psi[2][I]) -
-         P.g * sfq * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
+         R.g * sfq * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
     sy = sy + fw * (wy0 * C.psi[0][I] + wy1 * C.psi[1][I] + wy2 * C.psi[2][I]) -
-         P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
+         R.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
   }
   out[0] = fx; out[1] = fy; out[2] = gx; out[3] = gy;
   out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
 }
 
 template <bool kNonlin, bool kSph>
-__device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& C, const double* qs, int S,
-                                             const double* geo, double* vol, int I, int el, int e) {
-  double v[8];
-  volume_values<kNonlin, kSph>(A, C, qs, S, geo, I, el, e, v);
+__device__ __forceinline__ void volume_point(const StageArgs& A, const BasisT<real>& C, const real* qt,
+                                             const real* geo, real* vol, int I, int el, int e) {
+  real v[8];
+  volume_values<kNonlin, kSph>(A, C, qt, geo, I, el, e, v);
 #pragma unroll
   for (int r = 0; r < 8; ++r) vol[(r * 3 + I) * kTile + el] = v[r];
 }
@@ -456,15 +545,17 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisP1& 
 // reference's order -- boundary edges, interior edges in edge-number order
 // (the slot sum of add_internal_flux), rain, area points -- then the SSP
 // combination (DG_hydro_timestep.F:238-290) written to qout.  B is the
-// shared-memory copy of the basis (runtime-indexed tables), cBasis the
+// shared-memory copy of the basis (runtime-indexed tables), cBasisR the
 // constant-memory one (indices fixed by unrolled loops); V is the same for a
-// whole warp.
+// whole warp.  The sums are in the arithmetic type, the SSP combination in
+// FP64 (in the mixed variant: the RHS rounded to FP32, the stage states and
+// their combination FP64).
 template <bool kNonlin>
-__device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& B, const double* qs, int S,
-                                             const double* geo, const double* vol, const double* res,
+__device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisT<real>& B, const double* qs,
+                                             const real* geo, const real* vol, const real* res,
                                              const int* tdry, const unsigned* sinfo, const int* wds, int tbeg,
                                              int V, int el, int e) {
-  const BasisP1& C = cBasis;
+  const BasisT<real>& C = cBasisR;
   const MeshView& m = A.m;
   const Physics& P = A.ph;
   const int ne = m.ne;
@@ -482,33 +573,33 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
   }
   const unsigned info = sinfo[el], slots = sinfo[kTile + el];
   const int wde = wds[el];
-  double rhs[3] = {0.0, 0.0, 0.0}, isum[3] = {0.0, 0.0, 0.0};
+  real rhs[3] = {0, 0, 0}, isum[3] = {0, 0, 0};
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
     const int l = ei_order(info, s);
     const unsigned kind = ei_kind(info, l);
     if (kind == kNone) continue;
     const int ti = (slots >> (10 * l)) & kNoTask;
-    const double* r = res + (size_t)ti * 15;
+    const real* r = res + (size_t)ti * 15;
     if (kind == kIBarrier) {
       const double* o = A.ib_rhs + (size_t)m.tile_tasks[tbeg + ti].y * 9;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + o[3 * V + k];
+      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + (real)o[3 * V + k];
       continue;
     }
     if (kind == kInterior) {
       if (tdry[ti]) continue;
       const bool is_in = ei_flag(info, l) != 0;
       const int comp = V == 0 ? 0 : (is_in ? V : V + 2);
-      const double edfac = geo[(EGeo::kEdfac + l) * kTile + el];
-      double acc[3] = {0.0, 0.0, 0.0};
+      const real edfac = geo[(EGeo::kEdfac + l) * kTile + el];
+      real acc[3] = {0, 0, 0};
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
         const int j = is_in ? I : 2 - I;
-        const double val = r[5 * I + comp];
+        const real val = r[5 * I + comp];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const double wk = edfac * B.edgeq[l][j][k];
+          const real wk = edfac * B.edgeq[l][j][k];
           if (is_in)  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
             acc[k] = acc[k] - wk * val;
           else        // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
@@ -519,14 +610,14 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
       for (int k = 0; k < 3; ++k) isum[k] = isum[k] + acc[k];
     } else {
       if (wde == 0) continue;
-      const double areas = m.egeo[(size_t)EGeo::kAreas * ne + e];
-      const double xlen = m.egeo[(size_t)(EGeo::kXlen + l) * ne + e];
+      const real areas = egeo_r(m)[(size_t)EGeo::kAreas * ne + e];
+      const real xlen = egeo_r(m)[(size_t)(EGeo::kXlen + l) * ne + e];
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
-        const double val = r[5 * I + V];
+        const real val = r[5 * I + V];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const double wk = 2.0 * C.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * C.wegp[I];
+          const real wk = real(2) * C.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * C.wegp[I];
           rhs[k] = rhs[k] - wk * val;
         }
       }
@@ -535,36 +626,36 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
 #pragma unroll
   for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + isum[k];  // add_internal_flux
   if (V == 0 && P.rainfall == 1) {
-    const double src = 7.0556e-6;
+    const real src = real(7.0556e-6);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + C.srfac[k][i] * src;
   }
   if (wde != 0) {
-    const double drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
-    const double drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
+    const real drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+    const real drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
     // flux pair of this variable: (fx, fy), (gx, gy) or (hx, hy); source sx / sy
-    const double* vx = vol + (2 * V) * 3 * kTile + el;
-    const double* vy = vx + 3 * kTile;
-    const double* vs = vol + (V == 2 ? 7 : 6) * 3 * kTile + el;
+    const real* vx = vol + (2 * V) * 3 * kTile + el;
+    const real* vy = vx + 3 * kTile;
+    const real* vs = vol + (V == 2 ? 7 : 6) * 3 * kTile + el;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const double a = vx[i * kTile], b = vy[i * kTile];
+      const real a = vx[i * kTile], b = vy[i * kTile];
       if (V != 0) {
-        const double sr0 = C.srfac[0][i];
+        const real sr0 = C.srfac[0][i];
         rhs[0] = rhs[0] + sr0 * vs[i * kTile];
       }
 #pragma unroll
       for (int k = 1; k < 3; ++k) {
-        const double dpx = C.drphi[k][i] * drdx + C.dsphi[k][i] * dsdx;
-        const double dpy = C.drphi[k][i] * drdy + C.dsphi[k][i] * dsdy;
-        const double xf = C.mw[k][i] * dpx;
-        const double yf = C.mw[k][i] * dpy;
+        const real dpx = C.drphi[k][i] * drdx + C.dsphi[k][i] * dsdx;
+        const real dpy = C.drphi[k][i] * drdy + C.dsphi[k][i] * dsdy;
+        const real xf = C.mw[k][i] * dpx;
+        const real yf = C.mw[k][i] * dpy;
         if (V == 0) {
           rhs[k] = rhs[k] + xf * a + yf * b;
         } else {
-          const double sr = C.srfac[k][i];
+          const real sr = C.srfac[k][i];
           rhs[k] = rhs[k] + xf * a + yf * b + sr * vs[i * kTile];
         }
       }
@@ -575,7 +666,8 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const int c = 3 * V + k;
-    if (A.rout) A.rout[(size_t)c * ne + e] = rhs[k];
+    const double rk = (double)rhs[k];
+    if (A.rout) A.rout[(size_t)c * ne + e] = rk;
     const double qc = qs[el * kQStride + c];
     double acc = 0.0;
     if (hist0) {
@@ -585,11 +677,11 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisP1& 
     for (int I = 1; I < A.irk; ++I) {
       const bool cur = I == A.irk - 1;
       if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc : A.qhist[I][(size_t)c * ne + e]);
-      if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rhs[k] : A.rhist[I][(size_t)c * ne + e]);
+      if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rk : A.rhist[I][(size_t)c * ne + e]);
     }
     if (!hist0) {  // stage 1: the current stage is I = 0
       if (A.a[0] != 0.0) acc = acc + A.a[0] * qc;
-      if (A.b[0] != 0.0) acc = acc + A.b[0] * rhs[k];
+      if (A.b[0] != 0.0) acc = acc + A.b[0] * rk;
     }
     bad = bad || isnan(acc);
     A.qout[(size_t)c * ne + e] = acc;
@@ -609,24 +701,98 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   const int n = m.tile_elem_ptr[tile + 1] - tile0;
   const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
   const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
-  const StageLayout L = stage_layout(m.max_halo, m.max_tasks);
-  const int S = kTile + m.max_halo;  // row stride of qs and wd
-  BasisP1& B = *reinterpret_cast<BasisP1*>(smem_raw);
+  const StageLayout L = stage_layout(m.max_halo, m.max_tasks, (unsigned)sizeof(real));
+  BasisT<real>& B = *reinterpret_cast<BasisT<real>*>(smem_raw);
   double* qs = reinterpret_cast<double*>(smem_raw + L.qs);
-  double* geo = reinterpret_cast<double*>(smem_raw + L.geo);
-  double* vol = reinterpret_cast<double*>(smem_raw + L.vol);
-  double* res = reinterpret_cast<double*>(smem_raw + L.res);
+  real* geo = reinterpret_cast<real*>(smem_raw + L.geo);
+#ifdef DGSWEM_MIXED
+  real* qt = reinterpret_cast<real*>(smem_raw + L.qf);  // FP32 copy of the slots
+#else
+  const real* qt = qs;
+#endif
+  real* vol = reinterpret_cast<real*>(smem_raw + L.vol);
+  real* res = reinterpret_cast<real*>(smem_raw + L.res);
   int* wds = reinterpret_cast<int*>(smem_raw + L.wd);
   int* gid = reinterpret_cast<int*>(smem_raw + L.gid);
   int* tdry = reinterpret_cast<int*>(smem_raw + L.tdry);
   unsigned* sinfo = reinterpret_cast<unsigned*>(smem_raw + L.info);  // [einfo | eslot][kTile]
   {
-    const double* src = reinterpret_cast<const double*>(&cBasis);
-    double* dst = reinterpret_cast<double*>(&B);
-    for (int i = tid; i < (int)(sizeof(BasisP1) / sizeof(double)); i += kStageThreads) dst[i] = src[i];
+    const real* src = reinterpret_cast<const real*>(&cBasisR);
+    real* dst = reinterpret_cast<real*>(&B);
+    for (int i = tid; i < (int)(sizeof(BasisT<real>) / sizeof(real)); i += kStageThreads) dst[i] = src[i];
   }
 
   // ---- phase 1: tile and halo elements into shared memory ----
+#ifdef DGSWEM_MIXED
+  // Thread w < kTile: tile element w's 12 modal values (state rows and
+  // bathymetry rows; consecutive threads on consecutive elements of a row)
+  // into registers, then its FP32 slot and the FP64 state the SSP
+  // combination reads.  The other threads: the geometry rows and flags
+  // (cp.async) and the halo elements' FP32 slots, one thread per element.
+  {
+    static_assert(kStageThreads > kTile && (kStageThreads - kTile) % kTile == 0,
+                  "geometry rows are copied by whole groups of kTile threads");
+    if (tid < kTile) {
+      if (tid < n) {
+        double v[12];
+        const double* src = A.qin + tile0 + tid;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) v[r] = src[(size_t)r * ne];
+        src = m.hb + tile0 + tid;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[9 + k] = src[(size_t)k * ne];
+        double2* d = reinterpret_cast<double2*>(qs + tid * kQStride);
+#pragma unroll
+        for (int j = 0; j < 5; ++j) d[j] = make_double2(v[2 * j], v[2 * j + 1]);
+        // FP32 slot: ZE, QX, QY modes and the depth modes ZE + HB (FP64 sums)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) v[9 + k] = v[k] + v[9 + k];
+        float4* f = reinterpret_cast<float4*>(qt + tid * kQfStride);
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          f[j] = make_float4((float)v[4 * j], (float)v[4 * j + 1], (float)v[4 * j + 2], (float)v[4 * j + 3]);
+      }
+    } else {
+      constexpr int kU = kStageThreads - kTile, kStep = kU / kTile;
+      const int u = tid - kTile, w = u % kTile, r0 = u / kTile;
+      if (w < n) {
+        const int ngeo = m.manning ? EGeo::kSmemRows : EGeo::kNbar;
+        const size_t step = (size_t)kStep * ne;
+        const unsigned gdst = smem_addr(geo) + (unsigned)(r0 * kTile + w) * 4u;
+        const real* gsrc = egeo_r(m) + (size_t)r0 * ne + tile0 + w;
+#pragma unroll
+        for (int j = 0; j < (EGeo::kSmemRows + kStep - 1) / kStep; ++j)
+          if (r0 + j * kStep < ngeo) cp_async4_s(gdst + 4u * kStep * kTile * j, gsrc + j * step);
+#pragma unroll
+        for (int j = 0; j < (3 + kStep - 1) / kStep; ++j) {
+          const int r = r0 + j * kStep;
+          if (r == 0)
+            cp_async4(wds + w, A.wd + tile0 + w);
+          else if (r < 3)
+            cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
+        }
+      }
+      for (int j = u; j < nh; j += kU) {
+        const int g = m.tile_halo[hbeg + j];
+        gid[j] = g;
+        cp_async4(wds + kTile + j, A.wd + g);
+        double d[12];
+#pragma unroll
+        for (int r = 0; r < 9; ++r) d[r] = A.qin[(size_t)r * ne + g];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) d[9 + k] = d[k] + m.hb[(size_t)k * ne + g];
+        float v[12];
+#pragma unroll
+        for (int r = 0; r < 12; ++r) v[r] = (float)d[r];
+        float4* f = reinterpret_cast<float4*>(qt + (kTile + j) * kQfStride);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) f[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
+    }
+    cp_async_wait_all();
+  }
+  __syncthreads();
+#else
   // Asynchronous global->shared copies (cp.async), no register staging:
   // halo element j by thread j (one index load, then its 13 values), the
   // tile's rows (state, bathymetry, geometry table, flags) by all threads,
@@ -655,11 +821,17 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
 #pragma unroll
       for (int j = 0; j < (3 + kRowStep - 1) / kRowStep; ++j)
         if (r0 + j * kRowStep < 3) cp_async8_s(qdst + 72u + 8u * kRowStep * j, src + j * step);
-      const unsigned gdst = geo_s + (unsigned)(r0 * kTile + w) * 8u;
-      src = m.egeo + (size_t)r0 * ne + tile0 + w;
+      constexpr unsigned rb = sizeof(real);
+      const unsigned gdst = geo_s + (unsigned)(r0 * kTile + w) * rb;
+      const real* gsrc = egeo_r(m) + (size_t)r0 * ne + tile0 + w;
 #pragma unroll
-      for (int j = 0; j < (EGeo::kSmemRows + kRowStep - 1) / kRowStep; ++j)
-        if (r0 + j * kRowStep < ngeo) cp_async8_s(gdst + 8u * kRowStep * kTile * j, src + j * step);
+      for (int j = 0; j < (EGeo::kSmemRows + kRowStep - 1) / kRowStep; ++j) {
+        if (r0 + j * kRowStep >= ngeo) continue;
+        if (rb == 8)
+          cp_async8_s(gdst + rb * kRowStep * kTile * j, gsrc + j * step);
+        else
+          cp_async4_s(gdst + rb * kRowStep * kTile * j, gsrc + j * step);
+      }
 #pragma unroll
       for (int j = 0; j < (3 + kRowStep - 1) / kRowStep; ++j) {
         const int r = r0 + j * kRowStep;
@@ -684,14 +856,20 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     cp_async_wait_all();
   }
   __syncthreads();
+#endif
 
   // hybrid friction factor from the element-mean depth, used by phase 3
   // (visible after the next barrier)
   if (P.iflinbf == 0 && P.ifhybf == 1) {
     for (int el = tid; el < n; el += kStageThreads) {
-      const double depth_c = qs[el * kQStride + 9] + qs[el * kQStride];
-      const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
-      geo[SGeo::kHyb * kTile + el] = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
+#ifdef DGSWEM_MIXED
+      const real depth_c = qt[el * kQfStride + 9];  // depth mode 1
+#else
+      const real depth_c = (real)(qs[el * kQStride + 9] + qs[el * kQStride]);
+#endif
+      const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
+      geo[SGeo::kHyb * kTile + el] =
+          pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
     }
   }
 
@@ -703,12 +881,12 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
     const unsigned fl = tk.x;
     const unsigned kind = fl & 7u;
     if (kind == kIBarrier) continue;  // ibarrier_sides, launched before this kernel
-    double* o = res + (size_t)ti * 15 + 5 * I;
+    real* o = res + (size_t)ti * 15 + 5 * I;
     const int sin = (fl >> TaskBits::kInSlot) & 511, sex = (fl >> TaskBits::kExSlot) & 511;
     const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
     const bool flip = (fl >> TaskBits::kFlip) & 1u;
     const int owner = flip ? sex : sin, oled = flip ? led_ex : led_in;
-    double nx = geo[(EGeo::kNx + oled) * kTile + owner], ny = geo[(EGeo::kNy + oled) * kTile + owner];
+    real nx = geo[(EGeo::kNx + oled) * kTile + owner], ny = geo[(EGeo::kNy + oled) * kTile + owner];
     if (flip) { nx = -nx; ny = -ny; }
     const int wd_in = wds[sin];
     // global ids for the ics=2 tables
@@ -720,43 +898,47 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
       if (dry) continue;
       const int gex = sex < kTile ? tile0 + sex : gid[sex - kTile];
       const int gp_in = I, gp_ex = 2 - I;
-      double zi, xi, yi, hi, zx, xx, yx, hx;
-      slot_trace(B, qs, sin, led_in, gp_in, zi, xi, yi, hi);
-      slot_trace(B, qs, sex, led_ex, gp_ex, zx, xx, yx, hx);
-      const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : 1.0;
-      const double sfx = kSph ? m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : 1.0;
-      const Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, sfi, sfx, nx, ny, P.g);
+      real zi, xi, yi, wi, zx, xx, yx, wx, hi, hti, hx, htx;
+      slot_trace(B, qt, sin, led_in, gp_in, zi, xi, yi, wi);
+      slot_trace(B, qt, sex, led_ex, gp_ex, zx, xx, yx, wx);
+      trace_depth<kNonlin>(P, zi, wi, hi, hti);
+      trace_depth<kNonlin>(P, zx, wx, hx, htx);
+      const real sfi = kSph ? (real)m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : real(1);
+      const real sfx = kSph ? (real)m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : real(1);
+      const Flux3T<real> f =
+          llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, sfi, sfx, nx, ny, real(P.g));
       o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
-      if ((wd_in == 0 || wd_ex == 0) && fabs(f.f) > 1.0e-8) {
+      if ((wd_in == 0 || wd_ex == 0) && fabs(f.f) > real(1.0e-8)) {
         // internal_edge_hydro.F:212-302: mass flux out of / into a dry
         // element.  The four cases re-evaluate the flux once with changed
         // arguments: the dry side's state replaced by the wet side's with
         // reflected momentum (outflow from a dry element), or gravity off
         // (G = 0) for the dry side's momentum flux.
         const bool in_dry = wd_in == 0;
-        const double F0 = f.f;
-        const double tx = -ny, ty = nx, den = nx * ty - ny * tx;
-        const bool reflect = in_dry ? F0 > 0.0 : F0 < 0.0;
+        const real F0 = f.f;
+        const real tx = -ny, ty = nx, den = nx * ty - ny * tx;
+        const bool reflect = in_dry ? F0 > real(0) : F0 < real(0);
         // the wet side, whose momentum is reflected onto the dry side
-        const double qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
-        const double qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
-        const double qnr = -qnw, qtr = qtw;
-        const double qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
-        double a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
-        double a_hi = hi, a_hx = hx, a_si = sfi, a_sx = sfx, a_g = 0.0;
+        const real qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
+        const real qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
+        const real qnr = -qnw, qtr = qtw;
+        const real qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
+        real a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
+        real a_hi = hi, a_hx = hx, a_ti = hti, a_tx = htx, a_si = sfi, a_sx = sfx, a_g = 0;
         if (reflect) {
-          a_g = P.g;
+          a_g = real(P.g);
           if (in_dry) {
-            a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_si = sfx;
+            a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_ti = htx; a_si = sfx;
           } else {
-            a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_sx = sfi;
+            a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_tx = hti; a_sx = sfi;
           }
         }
-        const Flux3 r = llf<kNonlin>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_si, a_sx, nx, ny, a_g);
+        const Flux3T<real> r = llf<kNonlin, real>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_ti, a_tx,
+                                                  a_si, a_sx, nx, ny, a_g);
         if (reflect) {
           o[0] = r.f;
-          if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0.0; o[2] = 0.0; }
-          else        { o[1] = r.g; o[2] = r.h; o[3] = 0.0; o[4] = 0.0; }
+          if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0; o[2] = 0; }
+          else        { o[1] = r.g; o[2] = r.h; o[3] = 0; o[4] = 0; }
         } else {
           if (in_dry) { o[1] = r.g; o[2] = r.h; }
           else        { o[3] = r.g; o[4] = r.h; }
@@ -764,11 +946,15 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
       }
     } else {
       if (wd_in == 0) continue;
-      double zi, xi, yi, hi, zx, xx, yx;
-      slot_trace(B, qs, sin, led_in, I, zi, xi, yi, hi);
-      const double sfi = kSph ? m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : 1.0;
-      ghost_state(A, B, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
-      Flux3 f = llf<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hi, sfi, sfi, nx, ny, P.g);
+      real zi, xi, yi, wi, zx, xx, yx, hi, hti;
+      slot_trace(B, qt, sin, led_in, I, zi, xi, yi, wi);
+      trace_depth<kNonlin>(P, zi, wi, hi, hti);
+      const real sfi = kSph ? (real)m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : real(1);
+      ghost_state(A, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);
+      // only the ocean ghost has its own elevation (the others copy zi)
+      const real htx = kind == kOcean ? depth<kNonlin>(P, zx, hi) : hti;
+      const Flux3T<real> f =
+          llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hi, hti, htx, sfi, sfi, nx, ny, real(P.g));
       o[0] = f.f; o[1] = f.g; o[2] = f.h;
     }
   }
@@ -779,7 +965,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int i = w / kTile, el = w - i * kTile;
     if (el >= n || wds[el] == 0) continue;
-    volume_point<kNonlin, kSph>(A, B, qs, S, geo, vol, i, el, tile0 + el);
+    volume_point<kNonlin, kSph>(A, B, qt, geo, vol, i, el, tile0 + el);
   }
   __syncthreads();
 
@@ -787,7 +973,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int var = w / kTile, el = w - var * kTile;
     if (el >= n) continue;
-    sum_variable<kNonlin>(A, B, qs, S, geo, vol, res, tdry, sinfo, wds, tbeg, var, el, tile0 + el);
+    sum_variable<kNonlin>(A, B, qs, geo, vol, res, tdry, sinfo, wds, tbeg, var, el, tile0 + el);
   }
 }
 
@@ -815,14 +1001,16 @@ __global__ void node_minmax(const __grid_constant__ LimitArgs L) {
 // x / d for the redistribution divisor d = max(1, kdp) in {1, 2, 3}: x / 1
 // and x / 2 are exact scalings (x * 0.5 is the same correctly rounded value
 // as x / 2), only d = 3 needs a division.
-__device__ __forceinline__ double div_count(double x, int kdp) {
+__device__ __forceinline__ real div_count(real x, int kdp) {
   if (kdp <= 1) return x;
-  if (kdp == 2) return x * 0.5;
-  return x / 3.0;
+  if (kdp == 2) return x * real(0.5);
+  return x / real(3);
 }
 
 // slopelimiter.F:3434-3779 (vertex clamp + 3 redistribution sweeps) followed
-// by wetdry.F:61-548 for the same element.
+// by wetdry.F:61-548 for the same element.  The limiter arithmetic is in the
+// arithmetic type (FP32 in the mixed variant, on deviations from the element
+// mean, which it does not change), WETDRY in FP64.
 // 4 resident blocks of 256 per SM (64 registers, no spills): more warps to
 // cover the limiter's dependent FP64 chains than the 3 blocks an unbounded
 // allocation allows
@@ -841,7 +1029,24 @@ __global__ void __launch_bounds__(256, 4) limit_wetdry(const __grid_constant__ L
 #pragma unroll
     for (int var = 0; var < 3; ++var) {
       double* zc = &q[3 * var];
-      double vmin[3], vmax[3], vx[3];
+#ifdef DGSWEM_MIXED
+      // FP32 on deviations from the element mean (mode 1): vertex value -
+      // mode 1 and bound - mode 1 (differences in FP64).  The sweeps and
+      // the rebuild of modes 2-3 are the reference's with mode 1 = 0 (the
+      // mean cancels exactly in both), so FP32 rounds only the small
+      // deviations, not the full vertex values.
+      const real z0 = 0;
+      real vmin[3], vmax[3], vx[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        vmin[a] = (real)(L.minmax[(size_t)(2 * var) * np + nd[a]] - zc[0]);
+        vmax[a] = (real)(L.minmax[(size_t)(2 * var + 1) * np + nd[a]] - zc[0]);
+        vx[a] = (real)(B.phi_corner[a][1] * zc[1] + B.phi_corner[a][2] * zc[2]);
+        vx[a] = fmax(fmin(vx[a], vmax[a]), vmin[a]);
+      }
+#else
+      const real z0 = zc[0];
+      real vmin[3], vmax[3], vx[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         vmin[a] = L.minmax[(size_t)(2 * var) * np + nd[a]];
@@ -849,30 +1054,31 @@ __global__ void __launch_bounds__(256, 4) limit_wetdry(const __grid_constant__ L
         vx[a] = zc[0] + B.phi_corner[a][1] * zc[1] + B.phi_corner[a][2] * zc[2];
         vx[a] = fmax(fmin(vx[a], vmax[a]), vmin[a]);
       }
+#endif
 #pragma unroll
       for (int sweep = 0; sweep < 3; ++sweep) {
-        const double sumloc = (vx[0] + vx[1] + vx[2]) / 3.0;
-        double sumdif = (sumloc - zc[0]) * 3.0;
-        const double signdif = copysign(1.0, sumdif);
-        double dif[3];
+        const real sumloc = (vx[0] + vx[1] + vx[2]) / real(3);
+        real sumdif = (sumloc - z0) * real(3);
+        const real signdif = copysign(real(1), sumdif);
+        real dif[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) dif[a] = (vx[a] - zc[0]) * signdif;
+        for (int a = 0; a < 3; ++a) dif[a] = (vx[a] - z0) * signdif;
         int kdp = (dif[0] > 0) + (dif[1] > 0) + (dif[2] > 0);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          double redfac = 0.0;
+          real redfac = 0;
           if (dif[k] > 0) {  // sumdif * signdif / max(1, kdp)
             redfac = div_count(sumdif * signdif, kdp);
             kdp = kdp - 1;
           }
-          const double redmax = signdif > 0 ? vx[k] - vmin[k] : vmax[k] - vx[k];
+          const real redmax = signdif > 0 ? vx[k] - vmin[k] : vmax[k] - vx[k];
           redfac = fmin(redfac, redmax);
           sumdif = sumdif - redfac * signdif;
           vx[k] = vx[k] - redfac * signdif;
         }
       }
-      zc[1] = -(1.0 / 6.0 * (vx[0] + vx[1])) + 1.0 / 3.0 * vx[2];
-      zc[2] = -(.5 * vx[0]) + .5 * vx[1];
+      zc[1] = -(real(1.0 / 6.0) * (vx[0] + vx[1])) + real(1.0 / 3.0) * vx[2];
+      zc[2] = -(real(.5) * vx[0]) + real(.5) * vx[1];
     }
   }
   if (L.wetdry) {

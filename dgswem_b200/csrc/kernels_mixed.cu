@@ -1,0 +1,14 @@
+// kernels_mixed.cu -- the mixed-precision variant: the fast variant with the
+// stage kernel's edge traces, numerical fluxes, boundary ghost states,
+// volume fluxes and sources and the per-mode right-hand-side sums in FP32.
+// The state, the SSP-RK combination (so the element-mean elevation
+// accumulates across stages in FP64), the ocean depth-positivity fix, the
+// slope limiter and WETDRY stay FP64.
+#define DGSWEM_VARIANT mixed
+#define DGSWEM_FAST_MATH 1
+#define DGSWEM_MIXED 1
+// FP32 terms need fewer registers and a smaller tile in shared memory:
+// three resident stage blocks per SM (56 registers)
+#define DGSWEM_STAGE_MIN_BLOCKS 3
+#include "hydro_kernels.cuh"
+#include "kernel_launch.inc"

@@ -77,15 +77,22 @@ class HydroStep:
     ``dgswem_cuda_setup``."""
 
     STRICT = 1  # DGSWEM_CUDA_STRICT
+    MIXED = 2   # DGSWEM_CUDA_MIXED
 
-    def __init__(self, setup, device: int = 0, strict: bool = False, part: int = 0, nparts: int = 1):
+    def __init__(self, setup, device: int = 0, strict: bool = False, part: int = 0, nparts: int = 1,
+                 mixed: bool = False):
         """strict=True selects the kernels compiled without FMA contraction
         (bitwise reproducible against the non-contracting FP64 oracle);
-        the default is the FMA-contracted fast form.  nparts > 1 makes a
+        mixed=True the mixed-precision kernels (FP32 edge and volume
+        arithmetic, FP64 state, SSP combination, limiter and wet/dry); the
+        default is the FMA-contracted FP64 fast form.  nparts > 1 makes a
         partition handle (dgswem_cuda_create_part), stepped by
         ``PartitionedRun``."""
         self._lib = _abi.load()
+        if strict and mixed:
+            raise ValueError("strict and mixed exclude each other")
         self.strict = bool(strict)
+        self.mixed = bool(mixed)
         self._deck = setup if isinstance(setup, Deck) else None
         sp = setup.setup if isinstance(setup, Deck) else setup
         s = sp.contents
@@ -93,7 +100,7 @@ class HydroStep:
         self.slopeflag = s.slopeflag
         self.part, self.nparts = int(part), int(nparts)
         h = C.c_void_p()
-        flags = self.STRICT if strict else 0
+        flags = self.STRICT if strict else (self.MIXED if mixed else 0)
         if self.nparts == 1:
             _abi.check(self._lib.dgswem_cuda_create(sp, int(device), flags, C.byref(h)))
         else:
@@ -239,14 +246,14 @@ class PartitionedRun:
 
     HALO_WIDTH = (3, 10)  # doubles per element of halo kinds 0 and 1
 
-    def __init__(self, setup, nparts: int, devices=None, strict: bool = False):
+    def __init__(self, setup, nparts: int, devices=None, strict: bool = False, mixed: bool = False):
         import torch
         self._torch = torch
         self.nparts = int(nparts)
         self.devices = list(devices) if devices is not None else [0] * self.nparts
         if len(self.devices) != self.nparts:
             raise ValueError("one device per partition")
-        self.parts = [HydroStep(setup, device=d, strict=strict, part=p, nparts=self.nparts)
+        self.parts = [HydroStep(setup, device=d, strict=strict, part=p, nparts=self.nparts, mixed=mixed)
                       for p, d in enumerate(self.devices)]
         self.ne, self.nrk, self.dofh = self.parts[0].ne, self.parts[0].nrk, self.parts[0].dofh
         self.slopeflag = self.parts[0].slopeflag
@@ -340,13 +347,13 @@ class DistributedPartition:
     produce its data; every rank issues the same sequence of exchanges (one
     batched send/receive per halo kind and stage)."""
 
-    def __init__(self, setup, strict: bool = False, group=None):
+    def __init__(self, setup, strict: bool = False, group=None, mixed: bool = False):
         import torch
         import torch.distributed as dist
         self._torch, self._dist, self._group = torch, dist, group
         self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
         dev = torch.cuda.current_device()
-        self.hs = HydroStep(setup, device=dev, strict=strict, part=self.rank, nparts=self.world)
+        self.hs = HydroStep(setup, device=dev, strict=strict, part=self.rank, nparts=self.world, mixed=mixed)
         self.hs.set_stream(torch.cuda.current_stream().cuda_stream)
         self.nrk, self.slopeflag = self.hs.nrk, self.hs.slopeflag
         self.buf = {}  # (kind, peer) -> (send buffer, receive buffer, nsend, nrecv)
@@ -391,7 +398,8 @@ class DistributedPartition:
         self.hs.step_end()
 
 
-def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False):
+def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False,
+             mixed: bool = False):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with
     DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  Returns the
     list of (it, eta2) snapshots; writes them to ``out`` when given."""
@@ -401,7 +409,7 @@ def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict:
     noutge = deck.control("noutge")
     nolifa = deck.s.nolifa
     snaps = []
-    with HydroStep(deck, device, strict=strict) as hs:
+    with HydroStep(deck, device, strict=strict, mixed=mixed) as hs:
         count = 0
         for it in range(1, nt + 1):
             hs.timestep(it)

@@ -103,6 +103,14 @@ typedef struct dgswem_cuda dgswem_cuda;
  * separately in the reference's evaluation order (bitwise reproducible
  * against a non-contracting FP64 CPU build except through pow()). */
 #define DGSWEM_CUDA_STRICT 1
+/* DGSWEM_CUDA_MIXED: mixed precision.  The stage kernel's edge traces,
+ * numerical fluxes, boundary ghost states, volume fluxes and sources and the
+ * right-hand-side sums run in FP32; the state (ZE/QX/QY modes), the SSP-RK
+ * combination (so the element-mean elevation accumulates across stages in
+ * FP64), the ocean depth-positivity fix, the slope limiter and WETDRY stay
+ * FP64.  Results differ from the FP64 forms by the FP32 rounding of the
+ * right-hand side.  Excludes DGSWEM_CUDA_STRICT. */
+#define DGSWEM_CUDA_MIXED 2
 
 /* Copies the setup to GPU `device` and builds the device layout.
  * Replaces the state the reference keeps in module arrays after PREP_DG
