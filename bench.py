@@ -16,6 +16,9 @@ has no data exchange between independent meshes (weak scaling, replicas only).
 The line's "mixed" object is the mixed-precision form (FP32 edge, volume and
 limiter terms; FP64 state, SSP combination and wet/dry) on the same deck: its
 rate, its speed-up over the FP64 line and its error against the FP64 form.
+The "ensemble" object is the batched configuration: 256 seeded members of
+5k-200k elements (about 13.5M in all) advanced by one handle in mixed
+precision, with the batched-vs-one-at-a-time rate of its first 16 members.
 """
 from __future__ import annotations
 
@@ -200,6 +203,62 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
             "err_vs_fp64": err}
 
 
+def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
+    """The batched configuration: ``--ensemble-members`` seeded members
+    (rectangles and quarter annuli, element counts log-uniform in [5k, 200k],
+    tidal amplitude, Manning n and wind drawn per member), mixed precision,
+    advanced by one handle on the merged meshes.  Also times the first 16
+    members as a 16-member ensemble and one member at a time (a handle per
+    member, the same steps), for the batching gain on meshes of this size."""
+    import torch
+    from dgswem_b200 import HydroStep, decks
+    from dgswem_b200.ensemble import Ensemble, make_members
+    specs = decks.ensemble_specs(args.ensemble_members)
+    t0 = time.perf_counter()
+    ds, met = make_members(Path(args.workdir) / "ensemble", specs, workers=min(16, os.cpu_count() or 1))
+    t_decks = time.perf_counter() - t0
+    k, w = args.ensemble_steps, args.warmup
+
+    def timed(run, first_it):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(first_it, k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def batched(members, wsx, wsy, pr):
+        with Ensemble(members, device=device, mixed=True) as ens:
+            ens.hs.set_stream(stream.cuda_stream)
+            ens.set_met(wsx, wsy, pr)
+            ens.run(1, w)
+            l0 = ens.hs.kernel_launches
+            ms = timed(ens.run, w + 1)
+            return ms, ens.hs.kernel_launches - l0, ens.total_elements, ens.nrk
+
+    ms, launches, ne_tot, nrk = batched(ds, *met)
+    ms = max_over_ranks(ms, world, dist, "cuda")
+    sub = min(16, len(ds))
+    ms_sub, _, ne_sub, _ = batched(ds[:sub], *(f[:sub] for f in met))
+    ms_one = 0.0
+    for i in range(sub):
+        with HydroStep(ds[i], device=device, mixed=True) as hs:
+            hs.set_stream(stream.cuda_stream)
+            hs.set_met(met[0][i], met[1][i], met[2][i])
+            hs.run(1, w)
+            ms_one += timed(hs.run, w + 1)
+    rate = lambda ne, t: DOFS_PER_ELEMENT * ne * nrk * k / (t / 1e3)  # noqa: E731
+    for d in ds:
+        d.close()
+    return {"members": len(specs), "elements": int(ne_tot), "steps": k, "warmup": w,
+            "value": whole_job_rate(world, ne_tot, nrk, k, ms), "unit": "DOF-stage/s",
+            "ms_per_step": ms / k, "dtype": "mixed (f32 edge/volume/limiter, f64 state/SSP/wet-dry)",
+            "gpu_launches": int(launches), "deck_write_read_s": t_decks,
+            "subset16": {"elements": int(ne_sub), "batched_rate": rate(ne_sub, ms_sub),
+                         "one_at_a_time_rate": rate(ne_sub, ms_one), "batching_speedup": ms_one / ms_sub}}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -284,6 +343,8 @@ def main(argv=None):
     ap.add_argument("--ref-max-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
+    ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=40)
     ap.add_argument("--mixed-err-steps", type=int, default=200,
                     help="steps of the mixed-vs-FP64 error comparison")
     args = ap.parse_args(argv)
@@ -408,6 +469,8 @@ def main(argv=None):
         mixed = mixed_arm(deck, stream, args, world, dist if world > 1 else None, local)
         mixed["speedup_vs_fp64"] = mixed["value"] / value
         line["mixed"] = mixed
+    if args.ensemble_members > 0:
+        line["ensemble"] = ensemble_arm(args, stream, local, world, dist if world > 1 else None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, secs = cpu_baseline(path, args.cpu_steps, threads)

@@ -10,5 +10,6 @@ include/dgswem_cuda.h.
         eta, uu, vv, nodecode = hs.modal2nodal()
 """
 from .hydro import Deck, DistributedPartition, HydroStep, PartitionedRun, run_case, write_fort63  # noqa: F401
+from .ensemble import Ensemble  # noqa: F401
 
-__all__ = ["Deck", "DistributedPartition", "HydroStep", "PartitionedRun", "run_case", "write_fort63"]
+__all__ = ["Deck", "DistributedPartition", "Ensemble", "HydroStep", "PartitionedRun", "run_case", "write_fort63"]

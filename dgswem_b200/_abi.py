@@ -78,6 +78,7 @@ SIGNATURES = {
     "dgswem_deck_setup": (C.POINTER(Setup), [C.c_void_p]),
     "dgswem_deck_int": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]),
     "dgswem_deck_close": (None, [C.c_void_p]),
+    "dgswem_deck_merge": (C.c_int, [C.POINTER(C.POINTER(Setup)), C.c_int, C.POINTER(C.c_void_p)]),
 }
 
 _lib = None

@@ -21,9 +21,11 @@
 #include <cctype>
 #include <charconv>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <string>
 #include <string_view>
 #include <system_error>
@@ -933,3 +935,170 @@ extern "C" int dgswem_deck_int(const dgswem_deck* d, const char* key, int* value
 }
 
 extern "C" void dgswem_deck_close(dgswem_deck* d) { delete d; }
+
+// ---- ensembles -------------------------------------------------------------
+// One setup holding n independent meshes side by side (no shared nodes, so no
+// edge joins two instances): every per-node, per-element, per-edge and
+// per-boundary-edge array is concatenated and its ids offset by the preceding
+// instances' counts.  A handle created from it advances all instances in
+// each kernel launch.  What the kernels read as one value for the whole mesh
+// (time step, RK tables, physics switches and constants, tidal and flow
+// constituents) must be the same in every instance; per-instance forcing
+// lives in the per-edge amplitudes (EMO_DG/EFA_DG, QNAM_DG/QNPH_DG), the
+// nodal Manning n and the nodal met fields.  No counterpart in the reference
+// (one mesh per run there).
+namespace {
+
+template <class T>
+void append_offset(std::vector<T>& dst, const T* src, size_t n, T off, bool keep_zero) {
+  for (size_t i = 0; i < n; ++i) dst.push_back(keep_zero && src[i] == 0 ? 0 : src[i] + off);
+}
+
+template <class T>
+void append(std::vector<T>& dst, const T* src, size_t n) {
+  if (n) dst.insert(dst.end(), src, src + n);
+}
+
+bool same(const double* a, const double* b, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!(a[i] == b[i])) return false;
+  return true;
+}
+
+void check_compatible(const dgswem_cuda_setup& a, const dgswem_cuda_setup& b, int i) {
+  auto fail = [&](const char* what) {
+    throw dgswem::Failure(DGSWEM_ERR_ARG, "ensemble member " + std::to_string(i) + ": " + what +
+                                              " differs from member 0 (it is one value for the whole ensemble)");
+  };
+  if (a.dofh != b.dofh || a.nrk != b.nrk) fail("DOFH / RK stages");
+  if (a.ics != b.ics || a.nolifa != b.nolifa || a.iflinbf != b.iflinbf || a.ifhybf != b.ifhybf ||
+      a.ifnlfa != b.ifnlfa || a.nramp != b.nramp || a.nws != b.nws || a.rainfall != b.rainfall ||
+      a.slopeflag != b.slopeflag || a.load_manning != b.load_manning)
+    fail("a physics switch");
+  const double sa[] = {a.nleq, a.leq, a.g, a.h0, a.dtdp, a.statim, a.dramp, a.cf, a.hbreak, a.ftheta, a.fgamma, a.sfea0};
+  const double sb[] = {b.nleq, b.leq, b.g, b.h0, b.dtdp, b.statim, b.dramp, b.cf, b.hbreak, b.ftheta, b.fgamma, b.sfea0};
+  if (!same(sa, sb, sizeof(sa) / sizeof(sa[0]))) fail("a physics constant or the time step");
+  const size_t nn = (size_t)a.nrk * a.nrk;
+  if (!same(a.atvd, b.atvd, nn) || !same(a.btvd, b.btvd, nn) || !same(a.dtvd, b.dtvd, a.nrk)) fail("the RK tables");
+  if (a.nbfr != b.nbfr || !same(a.amig, b.amig, a.nbfr) || !same(a.ff, b.ff, a.nbfr) ||
+      !same(a.face, b.face, a.nbfr) || !same(a.per, b.per, a.nbfr))
+    fail("the tidal constituents");
+  if (a.nffr != b.nffr || !same(a.famig, b.famig, a.nffr) || !same(a.fff, b.fff, a.nffr) ||
+      !same(a.fface, b.fface, a.nffr) || !same(a.fper, b.fper, a.nffr))
+    fail("the flow constituents");
+}
+
+// per-boundary-edge harmonic table X(NF, NEDGE, 2) of every member into the
+// merged X(NF, sum NEDGE, 2)
+void merge_harmonic(std::vector<double>& dst, const std::vector<const dgswem_cuda_setup*>& p, int nf,
+                    int dgswem_cuda_setup::*count, const double* dgswem_cuda_setup::*arr) {
+  const int nb = std::max(nf, 1);
+  size_t total = 0;
+  for (auto* s : p) total += (size_t)(s->*count);
+  dst.assign((size_t)nb * total * 2, 0.0);
+  size_t off = 0;
+  for (auto* s : p) {
+    const int ned = s->*count;
+    const double* src = s->*arr;
+    if (src && nf > 0)
+      for (int f = 0; f < nf; ++f)
+        for (int e = 0; e < ned; ++e)
+          for (int ipt = 0; ipt < 2; ++ipt)
+            dst[f + (size_t)nb * ((off + e) + total * ipt)] = src[f + (size_t)nb * (e + (size_t)ned * ipt)];
+    off += ned;
+  }
+}
+
+}  // namespace
+
+extern "C" int dgswem_deck_merge(const dgswem_cuda_setup* const* parts, int n, dgswem_deck** out) {
+  return dgswem::guarded([&]() {
+    if (!parts || !out || n < 1) throw dgswem::Failure(DGSWEM_ERR_ARG, "null argument or empty ensemble");
+    *out = nullptr;
+    std::vector<const dgswem_cuda_setup*> p(parts, parts + n);
+    for (int i = 0; i < n; ++i) {
+      if (!p[i]) throw dgswem::Failure(DGSWEM_ERR_ARG, "null ensemble member");
+      if (i) check_compatible(*p[0], *p[i], i);
+    }
+    std::unique_ptr<dgswem_deck> d(new dgswem_deck());
+    const dgswem_cuda_setup& s0 = *p[0];
+    dgswem_cuda_setup& s = d->s;
+    s = s0;  // switches, constants, counts of constituents
+    long long ne = 0, np = 0, ned = 0;
+    s.nieds = s.nleds = s.needs = s.nfeds = s.nreds = s.nebseg = s.nibseg = 0;
+    for (auto* m : p) {
+      ne += m->ne; np += m->np; ned += m->nedges;
+      s.nieds += m->nieds; s.nleds += m->nleds; s.needs += m->needs; s.nfeds += m->nfeds;
+      s.nreds += m->nreds; s.nebseg += m->nebseg; s.nibseg += m->nibseg;
+    }
+    if (ne > INT32_MAX / 3 || np > INT32_MAX || ned > INT32_MAX / 2)
+      throw dgswem::Failure(DGSWEM_ERR_ARG, "ensemble exceeds 32-bit element / node / edge ids");
+    s.ne = (int)ne; s.np = (int)np; s.nedges = (int)ned;
+    d->nm.assign(3 * (size_t)ne, 0);
+    d->neled.assign(3 * (size_t)ne, 0);
+    int eoff = 0, noff = 0, edoff = 0;
+    for (auto* m : p) {
+      for (int v = 0; v < 3; ++v)
+        for (int e = 0; e < m->ne; ++e) d->nm[(size_t)(eoff + e) + (size_t)ne * v] = m->nm[e + (size_t)m->ne * v] + noff;
+      for (size_t i = 0; i < 3 * (size_t)m->ne; ++i)
+        d->neled[3 * (size_t)eoff + i] = m->neled[i] == 0 ? 0 : m->neled[i] + edoff;
+      append(d->x, m->x, m->np);
+      append(d->y, m->y, m->np);
+      append(d->dp, m->dp, m->np);
+      if (s.load_manning) append(d->manning, m->manning, m->np);
+      append_offset(d->nedno, m->nedno, 2 * (size_t)m->nedges, noff, true);
+      append_offset(d->nedel, m->nedel, 2 * (size_t)m->nedges, eoff, true);
+      append(d->nedsd, m->nedsd, 2 * (size_t)m->nedges);
+      append_offset(d->niedn, m->niedn, m->nieds, edoff, false);
+      append_offset(d->nledn, m->nledn, m->nleds, edoff, false);
+      append_offset(d->needn, m->needn, m->needs, edoff, false);
+      append_offset(d->nfedn, m->nfedn, m->nfeds, edoff, false);
+      append_offset(d->nredn, m->nredn, m->nreds, edoff, false);
+      append_offset(d->nebsegn, m->nebsegn, m->nebseg, edoff, false);
+      append_offset(d->nibsegn, m->nibsegn, 2 * (size_t)m->nibseg, edoff, true);
+      append(d->hb, m->hb, 3 * (size_t)m->ne);
+      append(d->cori_el, m->cori_el, m->ne);
+      append(d->fric_el, m->fric_el, m->ne);
+      append(d->ze, m->ze, 3 * (size_t)m->ne);
+      append(d->qx, m->qx, 3 * (size_t)m->ne);
+      append(d->qy, m->qy, 3 * (size_t)m->ne);
+      append(d->wdflg, m->wdflg, m->ne);
+      append(d->ebht, m->ebht, m->nebseg);
+      append(d->ebcfsp, m->ebcfsp, m->nebseg);
+      append(d->ibht, m->ibht, m->nibseg);
+      append(d->ibcfsb, m->ibcfsb, m->nibseg);
+      append(d->ibcfsp, m->ibcfsp, m->nibseg);
+      eoff += m->ne; noff += m->np; edoff += m->nedges;
+    }
+    merge_harmonic(d->emo_dg, p, s0.nbfr, &dgswem_cuda_setup::needs, &dgswem_cuda_setup::emo_dg);
+    merge_harmonic(d->efa_dg, p, s0.nbfr, &dgswem_cuda_setup::needs, &dgswem_cuda_setup::efa_dg);
+    merge_harmonic(d->qnam_dg, p, s0.nffr, &dgswem_cuda_setup::nfeds, &dgswem_cuda_setup::qnam_dg);
+    merge_harmonic(d->qnph_dg, p, s0.nffr, &dgswem_cuda_setup::nfeds, &dgswem_cuda_setup::qnph_dg);
+    d->atvd.assign(s0.atvd, s0.atvd + (size_t)s0.nrk * s0.nrk);
+    d->btvd.assign(s0.btvd, s0.btvd + (size_t)s0.nrk * s0.nrk);
+    d->dtvd.assign(s0.dtvd, s0.dtvd + s0.nrk);
+    d->amig.assign(s0.amig, s0.amig + s0.nbfr);
+    d->ff.assign(s0.ff, s0.ff + s0.nbfr);
+    d->face.assign(s0.face, s0.face + s0.nbfr);
+    d->per.assign(s0.per, s0.per + s0.nbfr);
+    d->famig.assign(s0.famig, s0.famig + s0.nffr);
+    d->fff.assign(s0.fff, s0.fff + s0.nffr);
+    d->fface.assign(s0.fface, s0.fface + s0.nffr);
+    d->fper.assign(s0.fper, s0.fper + s0.nffr);
+    s.atvd = d->atvd.data(); s.btvd = d->btvd.data(); s.dtvd = d->dtvd.data();
+    s.nm = d->nm.data(); s.x = d->x.data(); s.y = d->y.data(); s.dp = d->dp.data();
+    s.nedno = d->nedno.data(); s.nedel = d->nedel.data(); s.nedsd = d->nedsd.data(); s.neled = d->neled.data();
+    s.niedn = d->niedn.data(); s.nledn = d->nledn.data(); s.needn = d->needn.data(); s.nfedn = d->nfedn.data();
+    s.nredn = d->nredn.data(); s.nebsegn = d->nebsegn.data(); s.nibsegn = d->nibsegn.data();
+    s.hb = d->hb.data(); s.cori_el = d->cori_el.data(); s.fric_el = d->fric_el.data();
+    s.manning = d->manning.empty() ? nullptr : d->manning.data();
+    s.ze = d->ze.data(); s.qx = d->qx.data(); s.qy = d->qy.data(); s.wdflg = d->wdflg.data();
+    s.amig = d->amig.data(); s.ff = d->ff.data(); s.face = d->face.data(); s.per = d->per.data();
+    s.emo_dg = d->emo_dg.data(); s.efa_dg = d->efa_dg.data();
+    s.famig = d->famig.data(); s.fff = d->fff.data(); s.fface = d->fface.data(); s.fper = d->fper.data();
+    s.qnam_dg = d->qnam_dg.data(); s.qnph_dg = d->qnph_dg.data();
+    s.ebht = d->ebht.data(); s.ebcfsp = d->ebcfsp.data();
+    s.ibht = d->ibht.data(); s.ibcfsb = d->ibcfsb.data(); s.ibcfsp = d->ibcfsp.data();
+    *out = d.release();
+  });
+}

@@ -449,8 +449,10 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& pl
     std::vector<char> used(np, 0);
     for (int i = 0; i < nl; ++i)
       for (int v = 0; v < 3; ++v) used[s->nm[perm[i] + (size_t)ne * v] - 1] = 1;
+    std::vector<int> ncomp;
+    mesh_components(s, &ncomp);
     const std::vector<int> norder =
-        morton_order(std::vector<double>(s->x, s->x + np), std::vector<double>(s->y, s->y + np));
+        morton_order(std::vector<double>(s->x, s->x + np), std::vector<double>(s->y, s->y + np), ncomp);
     for (int n : norder)
       if (used[n]) node_perm.push_back(n);
   }

@@ -12,29 +12,73 @@
 
 namespace dgswem {
 
-std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py) {
+std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py,
+                              const std::vector<int>& group) {
   const int n = (int)px.size();
-  double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+  const bool grouped = !group.empty();
+  int ng = 1;
+  if (grouped)
+    for (int i = 0; i < n; ++i) ng = std::max(ng, group[i] + 1);
+  // bounding box of each group
+  std::vector<double> x0(ng, 1e300), x1(ng, -1e300), y0(ng, 1e300), y1(ng, -1e300);
   for (int i = 0; i < n; ++i) {
-    x0 = std::min(x0, px[i]); x1 = std::max(x1, px[i]);
-    y0 = std::min(y0, py[i]); y1 = std::max(y1, py[i]);
+    const int g = grouped ? group[i] : 0;
+    x0[g] = std::min(x0[g], px[i]); x1[g] = std::max(x1[g], px[i]);
+    y0[g] = std::min(y0[g], py[i]); y1[g] = std::max(y1[g], py[i]);
   }
-  const double span = std::max(std::max(x1 - x0, y1 - y0), 1e-300);
   auto spread = [](uint64_t v) {  // bits of v at the even positions
     uint64_t r = 0;
     for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1u) << (2 * b);
     return r;
   };
   std::vector<uint64_t> key(n);
-  const double scale = (double)((1u << 21) - 1) / span;
   for (int i = 0; i < n; ++i) {
-    const uint64_t ix = (uint64_t)((px[i] - x0) * scale), iy = (uint64_t)((py[i] - y0) * scale);
+    const int g = grouped ? group[i] : 0;
+    const double span = std::max(std::max(x1[g] - x0[g], y1[g] - y0[g]), 1e-300);
+    const double scale = (double)((1u << 21) - 1) / span;
+    const uint64_t ix = (uint64_t)((px[i] - x0[g]) * scale), iy = (uint64_t)((py[i] - y0[g]) * scale);
     key[i] = spread(ix) | spread(iy) << 1;
   }
   std::vector<int> perm(n);
   for (int i = 0; i < n; ++i) perm[i] = i;
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+    const int ga = grouped ? group[a] : 0, gb = grouped ? group[b] : 0;
+    return ga != gb ? ga < gb : key[a] < key[b];
+  });
   return perm;
+}
+
+std::vector<int> mesh_components(const dgswem_cuda_setup* s, std::vector<int>* node_comp) {
+  const int ne = s->ne, np = s->np;
+  std::vector<int> parent(np);
+  for (int i = 0; i < np; ++i) parent[i] = i;
+  auto find = [&](int a) {
+    while (parent[a] != a) a = parent[a] = parent[parent[a]];
+    return a;
+  };
+  for (int e = 0; e < ne; ++e) {
+    const int a = find(s->nm[e] - 1);
+    for (int v = 1; v < 3; ++v) {
+      const int b = find(s->nm[e + (size_t)ne * v] - 1);
+      if (a != b) parent[b] = a;
+    }
+  }
+  // components numbered by their first element in input order
+  std::vector<int> label(np, -1), elem(ne);
+  int nc = 0;
+  for (int e = 0; e < ne; ++e) {
+    const int r = find(s->nm[e] - 1);
+    if (label[r] < 0) label[r] = nc++;
+    elem[e] = label[r];
+  }
+  if (node_comp) {
+    node_comp->assign(np, 0);
+    for (int i = 0; i < np; ++i) {
+      const int r = find(i);
+      (*node_comp)[i] = label[r] < 0 ? 0 : label[r];  // a node in no element: any group
+    }
+  }
+  return elem;
 }
 
 PartPlan make_part_plan(const dgswem_cuda_setup* s, int part, int nparts) {
@@ -57,7 +101,7 @@ PartPlan make_part_plan(const dgswem_cuda_setup* s, int part, int nparts) {
       cx[e] = sx / 3.0;
       cy[e] = sy / 3.0;
     }
-    P.order = morton_order(cx, cy);
+    P.order = morton_order(cx, cy, mesh_components(s, nullptr));
   }
   std::vector<int> pos(ne);
   for (int i = 0; i < ne; ++i) pos[P.order[i]] = i;

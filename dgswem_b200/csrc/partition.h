@@ -9,12 +9,21 @@
 namespace dgswem {
 
 // Indices sorting points along a Morton (Z-order) curve (stable: ties keep
-// the input order).
-std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py);
+// the input order).  With `group` (one id per point, 0..G-1), points are
+// sorted by group first and along the curve of their group's own bounding
+// box within it, so that disjoint meshes sharing the same coordinates (the
+// members of a merged ensemble) stay contiguous.
+std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py,
+                              const std::vector<int>& group = {});
+
+// Connected components of the mesh (elements joined by shared nodes),
+// numbered by their first element in input order: one id per element, and
+// per node in *node_comp when given.  A connected mesh is one component.
+std::vector<int> mesh_components(const dgswem_cuda_setup* s, std::vector<int>* node_comp);
 
 // Partition `part` of `nparts`: the elements at positions
-// [part*NE/nparts, (part+1)*NE/nparts) of the global Morton order of the
-// element centroids, plus the ghost elements its stage needs from other
+// [part*NE/nparts, (part+1)*NE/nparts) of the global order of the element
+// centroids (by component, then Morton), plus the ghost elements its stage needs from other
 // partitions.  Halo kinds:
 //   kHaloMeans (0): elements sharing a node with an owned element -- the
 //     limiter's node min/max reads their element means after the stage RHS;

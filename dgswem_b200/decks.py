@@ -226,3 +226,69 @@ def sloping_beach(path, nx: int = 2236, ny: int = 447, lx: float = 100e3, ly: fl
     manning = 0.025 * rng.uniform(0.8, 1.2, X.size)
     return write_deck(path, X.ravel(), Y.ravel(), dp.ravel(), elems, [ocean], [(land, 0)], ctl,
                       emo=np.full(len(ocean), amp), efa=np.zeros(len(ocean)), manning=manning)
+
+
+# ---- batched ensembles -------------------------------------------------------
+ENSEMBLE_KINDS = ("rectangle", "annulus")
+
+
+def ensemble_member(path, kind: str, ne: int, amp: float, n_manning: float, seed: int, dt: float = 0.5,
+                    nsteps: int = 2000) -> Path:
+    """One member of a batched ensemble, about ``ne`` elements: a 20 x 4 km
+    rectangular basin sloping from 20 m to -2 m (wet/dry shore, seeded
+    0.05 m bed noise; kind "rectangle") or the quarter annulus of the
+    reference's tidal test (kind "annulus").  Tidal amplitude ``amp`` (m) on
+    the open boundary, uniform nodal Manning n.  All members share what a
+    merged ensemble requires to be common: Manning friction, WETDRY, slope
+    limiter 5, NWS=1 (nodal met fields set per member at run time),
+    SSP(2,2), H0 = 0.01 m and the time step (0.5 s is stable for the finest
+    200k-element members of either kind)."""
+    ctl = Controls(title=f"ensemble {kind}", nolibf=1, nolifa=2, cf=0.0025, dt=dt, nsteps=nsteps, rk_stage=2,
+                   rk_order=2, slopeflag=5, h0=0.01, nramp=1, dramp=1.0, manning=True, nws=1)
+    rng = np.random.default_rng(seed)
+    if kind == "rectangle":
+        nx = max(5, int(round(math.sqrt(ne * 5 / 2))))
+        ny = max(1, int(round(ne / (2 * nx))))
+        lx, ly = 20e3, 4e3
+        xs, ys = np.linspace(0.0, lx, nx + 1), np.linspace(0.0, ly, ny + 1)
+        X, Y = np.meshgrid(xs, ys, indexing="ij")
+        dp = 20.0 + (-2.0 - 20.0) * X / lx + rng.normal(0.0, 0.05, X.shape)
+        elems = _grid_triangles(nx, ny)
+        nid = lambda i, j: i * (ny + 1) + j + 1  # noqa: E731
+        ocean = [nid(0, j) for j in range(ny, -1, -1)]
+        land = [nid(i, 0) for i in range(0, nx + 1)] + [nid(nx, j) for j in range(1, ny + 1)] + \
+               [nid(i, ny) for i in range(nx - 1, -1, -1)]
+        x, y, dp = X.ravel(), Y.ravel(), dp.ravel()
+    elif kind == "annulus":
+        nr = max(2, int(round(math.sqrt(ne / 4))))
+        nth = max(2, int(round(ne / (2 * nr))))
+        r0, r1 = 60960.0, 152400.0
+        R, T = np.meshgrid(np.linspace(r0, r1, nr + 1), np.linspace(0.0, 0.5 * math.pi, nth + 1), indexing="ij")
+        x, y = (R * np.cos(T)).ravel(), (R * np.sin(T)).ravel()
+        x[np.abs(x) < 1e-6] = 0.0
+        dp = (3.048 * (R / r0) ** 2).ravel()
+        elems = _grid_triangles(nr, nth)
+        nid = lambda i, j: i * (nth + 1) + j + 1  # noqa: E731
+        ocean = [nid(nr, j) for j in range(nth + 1)]
+        land = [nid(i, nth) for i in range(nr, -1, -1)] + [nid(0, j) for j in range(nth - 1, -1, -1)] + \
+               [nid(i, 0) for i in range(1, nr + 1)]
+    else:
+        raise ValueError(f"unknown ensemble member kind {kind!r}")
+    return write_deck(path, x, y, dp, elems, [ocean], [(land, 0)], ctl, emo=np.full(len(ocean), amp),
+                      efa=np.zeros(len(ocean)), manning=np.full(len(x), n_manning))
+
+
+def ensemble_specs(n: int, seed: int = 20261203, ne_min: int = 5000, ne_max: int = 200000) -> list:
+    """Seeded member parameters of the batched configuration: element counts
+    log-uniform in [ne_min, ne_max], rectangle or quarter annulus, tidal
+    amplitude U[0.2, 2] m, Manning n U[0.015, 0.04], wind stress U[0, 0.3] Pa
+    (direction U[0, 360) degrees)."""
+    rng = np.random.default_rng(seed)
+    ne = np.exp(rng.uniform(math.log(ne_min), math.log(ne_max), n)).astype(int)
+    kinds = rng.integers(0, 2, n)
+    amp = rng.uniform(0.2, 2.0, n)
+    nman = rng.uniform(0.015, 0.04, n)
+    wind = rng.uniform(0.0, 0.3, n)
+    wdir = rng.uniform(0.0, 360.0, n)
+    return [dict(kind=ENSEMBLE_KINDS[int(kinds[i])], ne=int(ne[i]), amp=float(amp[i]), n_manning=float(nman[i]),
+                 wind_pa=float(wind[i]), wind_deg=float(wdir[i]), seed=seed + 1 + i) for i in range(n)]

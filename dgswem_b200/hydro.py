@@ -39,6 +39,23 @@ class Deck:
         self._h = h
         self.setup = self._lib.dgswem_deck_setup(h)
 
+    @classmethod
+    def merge(cls, decks) -> "Deck":
+        """dgswem_deck_merge: one deck holding the given decks' meshes side by
+        side (ensemble members in order; ids offset by the preceding
+        members' counts).  The members may be closed afterwards."""
+        decks = list(decks)
+        lib = _abi.load()
+        arr = (C.POINTER(_abi.Setup) * len(decks))(*[d.setup for d in decks])
+        h = C.c_void_p()
+        _abi.check(lib.dgswem_deck_merge(arr, len(decks), C.byref(h)))
+        self = cls.__new__(cls)
+        self.path = None
+        self._lib = lib
+        self._h = h
+        self.setup = lib.dgswem_deck_setup(h)
+        return self
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.dgswem_deck_close(self._h)

@@ -250,6 +250,19 @@ const dgswem_cuda_setup* dgswem_deck_setup(const dgswem_deck* d);
 int dgswem_deck_int(const dgswem_deck* d, const char* key, int* value);
 void dgswem_deck_close(dgswem_deck* d);
 
+/* ---- ensembles (no counterpart in the reference: one mesh per run there) ---
+ * Merges n setups into one deck whose setup holds the n meshes side by side:
+ * element, node and edge arrays concatenated in member order, ids offset by
+ * the preceding members' counts (member i's elements are ids
+ * sum(ne[0..i-1]) + 1 ..).  A handle created from it advances every member
+ * in each kernel launch.  Time step, RK tables, physics switches and
+ * constants and the tidal / flow constituents must be equal across members
+ * (DGSWEM_ERR_ARG otherwise); amplitudes per boundary edge, Manning n per
+ * node and met fields per node may differ.  The merged deck owns copies;
+ * the members may be closed afterwards.  Run controls (dgswem_deck_int) of
+ * the merged deck are 0. */
+int dgswem_deck_merge(const dgswem_cuda_setup* const* parts, int n, dgswem_deck** out);
+
 #ifdef __cplusplus
 }
 #endif
