@@ -79,6 +79,17 @@ SIGNATURES = {
     "dgswem_deck_int": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]),
     "dgswem_deck_close": (None, [C.c_void_p]),
     "dgswem_deck_merge": (C.c_int, [C.POINTER(C.POINTER(Setup)), C.c_int, C.POINTER(C.c_void_p)]),
+    "dgswem_cuda_set_params": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "dgswem_cuda_state_save": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_state_load": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_gauges": (C.c_int, [C.c_void_p, C.c_int, _ip, _dp]),
+    "dgswem_cuda_gauge_eta": (C.c_int, [C.c_void_p, _dp]),
+    "dgswem_cuda_adjoint_begin": (C.c_int, [C.c_void_p]),
+    "dgswem_cuda_adjoint_seed": (C.c_int, [C.c_void_p, _dp]),
+    "dgswem_cuda_adjoint_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_adjoint_read": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
+    "dgswem_cuda_misfit_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp]),
+    "dgswem_cuda_adjoint_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp]),
 }
 
 _lib = None

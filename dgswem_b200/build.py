@@ -25,7 +25,8 @@ LIBNAME = "libdgswem_cuda.so"
 # edge and volume arithmetic, whose FP32 divisions and square roots are the
 # approximate ones (the flags do not change FP64 operations)
 SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_strict.cu", ["-fmad=false"]),
-           ("kernels_mixed.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]), ("deck.cpp", []), ("partition.cpp", [])]
+           ("kernels_mixed.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
+           ("adjoint.cu", ["-fmad=true"]), ("deck.cpp", []), ("partition.cpp", [])]
 HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

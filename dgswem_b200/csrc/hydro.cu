@@ -224,6 +224,27 @@ struct dgswem_cuda {
   std::vector<Pending> pending;
   double prof_ms[4] = {0, 0, 0, 0};
   long long prof_n[4] = {0, 0, 0, 0};
+  // discrete adjoint (dgswem_cuda_adjoint_*): lam[I-1] / nu[I-1] the
+  // cotangents of stage state I and of its right-hand side; lam[nrk] the
+  // current one (of the state the last adjoint step started from)
+  int nreds = 0;
+  std::vector<DevBuf<double>> adj_lam, adj_nu;
+  DevBuf<double> adj_gn, adj_ghb, adj_eb;
+  DevBuf<int> adj_edges;  // (element, local edge): interior edges from the in side, land / ocean edges
+  int adj_nedge = 0;
+  bool adj_on = false;
+  // stage states and stage forcing of the steps of one checkpoint segment
+  // (dgswem_cuda_adjoint_sweep)
+  std::vector<DevBuf<double>> adj_stage;
+  DevBuf<double> adj_forc;
+  // gauges: device element, ZE basis values, values / weights; grouped by
+  // element (CSR over distinct elements, gauges in input order) for the seed
+  int ngauge = 0, ngroup = 0;
+  DevBuf<int> gauge_elem, group_elem, group_ptr, group_gauge;
+  DevBuf<double> gauge_phi, gauge_val, eta_rec, w_rec;
+  // state slots of dgswem_cuda_state_save / _load (checkpoints)
+  std::vector<DevBuf<double>> slot_q;
+  std::vector<DevBuf<int>> slot_wd;
 };
 
 namespace {
@@ -933,6 +954,142 @@ double* nodal_scratch(int device) {
 
 }  // namespace
 
+namespace {
+
+// The scope of the discrete adjoint (adjoint.cu); DGSWEM_ERR_ARG otherwise.
+// Allocates its buffers and zeroes the state cotangent and the gradients.
+void adjoint_prepare(dgswem_cuda* h) {
+  auto no = [](const char* what) {
+    throw Failure(DGSWEM_ERR_ARG, std::string("the discrete adjoint does not cover ") + what);
+  };
+  if (h->nparts != 1) no("partitioned handles");
+  if (h->v == &kMixed) no("the mixed-precision form (FP64 handles only)");
+  if (!(h->ph.nleq == 1.0 && h->ph.leq == 0.0)) no("NLEQ=0 (linearised) runs");
+  if (h->ph.ics != 1) no("ICS=2");
+  if (h->slopeflag != 0) no("the slope limiter (its frozen-branch adjoint is not built)");
+  if (h->nolifa >= 2) no("WETDRY (its frozen-branch adjoint is not built)");
+  if (h->nfeds > 0 || h->nreds > 0 || h->mesh.nebseg > 0 || h->mesh.nibseg > 0)
+    no("flow, radiation or barrier boundaries");
+  if (h->ph.iflinbf == 0 && h->ph.ifhybf == 1) no("hybrid friction");
+  const size_t n9 = 9 * (size_t)h->ne;
+  if (h->adj_lam.size() != (size_t)h->nrk + 1) {
+    h->adj_lam.clear();
+    h->adj_nu.clear();
+    h->adj_lam.resize(h->nrk + 1);
+    h->adj_nu.resize(h->nrk);
+    for (auto& b : h->adj_lam) b.alloc(n9);
+    for (auto& b : h->adj_nu) b.alloc(n9);
+    h->adj_gn.alloc((size_t)h->ne);
+    h->adj_ghb.alloc(3 * (size_t)h->ne);
+    h->adj_eb.alloc(36 * (size_t)h->ne);
+    // slots of edges in no list are never written: zero once
+    DG_CUDA(cudaMemset(h->adj_eb.p, 0, 36 * (size_t)h->ne * sizeof(double)));
+    std::vector<unsigned> info(h->ne);
+    DG_CUDA(cudaMemcpy(info.data(), h->einfo.p, h->ne * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    std::vector<int> edges;
+    for (int e = 0; e < h->ne; ++e)
+      for (int l = 0; l < 3; ++l) {
+        const unsigned k = ei_kind(info[e], l);
+        if ((k == kInterior && ei_flag(info[e], l)) || k == kLand || k == kOcean) {
+          edges.push_back(e);
+          edges.push_back(l);
+        }
+      }
+    h->adj_nedge = (int)(edges.size() / 2);
+    h->adj_edges.upload(edges.empty() ? std::vector<int>(2, 0) : edges);
+  }
+  DG_CUDA(cudaMemsetAsync(h->adj_lam[h->nrk].p, 0, n9 * sizeof(double), h->stream));
+  DG_CUDA(cudaMemsetAsync(h->adj_gn.p, 0, (size_t)h->ne * sizeof(double), h->stream));
+  DG_CUDA(cudaMemsetAsync(h->adj_ghb.p, 0, 3 * (size_t)h->ne * sizeof(double), h->stream));
+  h->adj_on = true;
+}
+
+// Carry the state cotangent adj_lam[nrk] back through step `it`, whose stage
+// I state is stage[I-1] and stage forcing `forcing` (nrk blocks of
+// forcing_per_stage, or null); adds the step's parameter gradient.
+void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const double* forcing) {
+  const int nrk = h->nrk;
+  const size_t n9 = 9 * (size_t)h->ne;
+  for (int I = 0; I < nrk; ++I) {
+    DG_CUDA(cudaMemsetAsync(h->adj_lam[I].p, 0, n9 * sizeof(double), h->stream));
+    DG_CUDA(cudaMemsetAsync(h->adj_nu[I].p, 0, n9 * sizeof(double), h->stream));
+  }
+  for (int j = nrk + 1; j >= 1; --j) {
+    if (j <= nrk) {
+      AdjArgs a{};
+      a.m = h->mesh;
+      a.ph = h->ph;
+      a.q = stage[j - 1];
+      a.nu = h->adj_nu[j - 1].p;
+      a.lam = h->adj_lam[j - 1].p;
+      a.g_n = h->mesh.manning ? h->adj_gn.p : nullptr;
+      a.g_hb = h->adj_ghb.p;
+      a.ocean_zg = forcing ? forcing + (size_t)(j - 1) * h->forcing_per_stage : nullptr;
+      a.pr = h->nws ? h->pr.p : nullptr;
+      a.eb = h->adj_eb.p;
+      a.edges = h->adj_edges.p;
+      a.nedge = h->adj_nedge;
+      double timedg;
+      stage_clock(h, it, j, &timedg, &a.rampdg);
+      adj::launch_rhs_vjp(a, h->stream);
+      check_launch(h, "edge_vjp");
+      check_launch(h, "elem_vjp");
+    }
+    if (j >= 2) {
+      const int irk = j - 1;
+      SspAdjArgs b{};
+      b.lam_j = h->adj_lam[j - 1].p;
+      b.n = irk;
+      b.len = (long long)n9;
+      for (int I = 1; I <= irk; ++I) {
+        b.lam[I - 1] = h->adj_lam[I - 1].p;
+        b.nu[I - 1] = h->adj_nu[I - 1].p;
+        b.a[I - 1] = h->atvd[(size_t)(irk - 1) * nrk + (I - 1)];
+        b.b[I - 1] = h->btvd[(size_t)(irk - 1) * nrk + (I - 1)] * h->dtdp;
+      }
+      adj::launch_ssp_adj(b, h->stream);
+      check_launch(h, "ssp_adj");
+    }
+  }
+  std::swap(h->adj_lam[0].p, h->adj_lam[nrk].p);  // the cotangent of stage 1 = of the step's start
+}
+
+void ensure_slot(dgswem_cuda* h, int slot) {
+  if ((size_t)slot >= h->slot_q.size()) {
+    h->slot_q.resize(slot + 1);
+    h->slot_wd.resize(slot + 1);
+  }
+  if (!h->slot_q[slot].p) {
+    h->slot_q[slot].alloc(9 * (size_t)h->ne);
+    h->slot_wd[slot].alloc((size_t)h->ne);
+  }
+}
+
+void save_slot(dgswem_cuda* h, int slot) {
+  ensure_slot(h, slot);
+  DG_CUDA(cudaMemcpyAsync(h->slot_q[slot].p, h->q[0].p, 9 * (size_t)h->ne * sizeof(double),
+                          cudaMemcpyDeviceToDevice, h->stream));
+  DG_CUDA(cudaMemcpyAsync(h->slot_wd[slot].p, h->wd.p, (size_t)h->ne * sizeof(int), cudaMemcpyDeviceToDevice,
+                          h->stream));
+}
+
+void load_slot(dgswem_cuda* h, int slot) {
+  if (slot < 0 || (size_t)slot >= h->slot_q.size() || !h->slot_q[slot].p)
+    throw Failure(DGSWEM_ERR_ARG, "state slot " + std::to_string(slot) + " was never saved");
+  DG_CUDA(cudaMemcpyAsync(h->q[0].p, h->slot_q[slot].p, 9 * (size_t)h->ne * sizeof(double),
+                          cudaMemcpyDeviceToDevice, h->stream));
+  DG_CUDA(cudaMemcpyAsync(h->wd.p, h->slot_wd[slot].p, (size_t)h->ne * sizeof(int), cudaMemcpyDeviceToDevice,
+                          h->stream));
+}
+
+void seed_gauges(dgswem_cuda* h, const double* w_dev) {
+  adj::launch_gauge_seed(h->adj_lam[h->nrk].p, h->ne, h->group_elem.p, h->group_ptr.p, h->group_gauge.p,
+                         h->gauge_phi.p, w_dev, h->ngroup, h->stream);
+  if (h->ngroup > 0) check_launch(h, "gauge_seed");
+}
+
+}  // namespace
+
 extern "C" {
 
 int dgswem_cuda_last_error(char* buf, int buflen) {
@@ -966,6 +1123,7 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     h->nrk = s->nrk;
     h->nramp = s->nramp;
     h->slopeflag = s->slopeflag;
+    h->nreds = s->nreds;
     h->nolifa = s->nolifa;
     h->nws = s->nws;
     h->dtdp = s->dtdp;
@@ -1004,6 +1162,7 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
       kFast.set_basis(B);
       kStrict.set_basis(B);
       kMixed.set_basis(B);
+      adj::set_basis(B);
       DG_CUDA(cudaGetLastError());
     }
     const PartPlan plan = make_part_plan(s, part, nparts);
@@ -1349,6 +1508,245 @@ int dgswem_cuda_profile_read(dgswem_cuda* h, double* ms, long long* launches) {
     for (int k = 0; k < 4; ++k) {
       if (ms) ms[k] = h->prof_ms[k];
       if (launches) launches[k] = h->prof_n[k];
+    }
+  });
+}
+
+
+// ---- parameters, state slots, gauges and the discrete adjoint ---------------
+// (no counterparts in the reference)
+
+int dgswem_cuda_set_params(dgswem_cuda* h, const double* nbar, const double* hb) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "set_params needs the whole mesh (a handle of dgswem_cuda_create)");
+    DG_CUDA(cudaSetDevice(h->device));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    const int ne = h->ne;
+    if (nbar) {
+      if (!h->mesh.manning) throw Failure(DGSWEM_ERR_ARG, "set_params: the deck has no Manning n (NWP / fort.13)");
+      std::vector<double> row(ne);
+      for (int i = 0; i < ne; ++i) row[i] = nbar[h->perm_h[i]];
+      DG_CUDA(cudaMemcpy(h->egeo.p + (size_t)EGeo::kNbar * ne, row.data(), ne * sizeof(double),
+                         cudaMemcpyHostToDevice));
+      if (h->egeof.p) {
+        std::vector<float> rf(row.begin(), row.end());
+        DG_CUDA(cudaMemcpy(h->egeof.p + (size_t)EGeo::kNbar * ne, rf.data(), ne * sizeof(float),
+                           cudaMemcpyHostToDevice));
+      }
+    }
+    if (hb) {
+      std::vector<double> d(3 * (size_t)ne);
+      for (int k = 0; k < 3; ++k)
+        for (int i = 0; i < ne; ++i) d[(size_t)k * ne + i] = hb[3 * (size_t)h->perm_h[i] + k];
+      DG_CUDA(cudaMemcpy(h->hb.p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  });
+}
+
+int dgswem_cuda_state_save(dgswem_cuda* h, int slot) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (slot < 0) throw Failure(DGSWEM_ERR_ARG, "negative state slot");
+    DG_CUDA(cudaSetDevice(h->device));
+    save_slot(h, slot);
+  });
+}
+
+int dgswem_cuda_state_load(dgswem_cuda* h, int slot) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    load_slot(h, slot);
+  });
+}
+
+int dgswem_cuda_gauges(dgswem_cuda* h, int ng, const int* elem, const double* phi) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "gauges need the whole mesh (a handle of dgswem_cuda_create)");
+    if (ng < 0 || (ng > 0 && (!elem || !phi))) throw Failure(DGSWEM_ERR_ARG, "gauges: bad arguments");
+    DG_CUDA(cudaSetDevice(h->device));
+    std::vector<int> inv(h->ne);
+    for (int i = 0; i < h->ne; ++i) inv[h->perm_h[i]] = i;
+    std::vector<int> ed(std::max(ng, 1), 0);
+    for (int g = 0; g < ng; ++g) {
+      if (elem[g] < 1 || elem[g] > h->ne) throw Failure(DGSWEM_ERR_ARG, "gauge element outside 1..NE");
+      ed[g] = inv[elem[g] - 1];
+    }
+    h->ngauge = ng;
+    h->gauge_elem.upload(ed);
+    h->gauge_phi.upload(ng > 0 ? std::vector<double>(phi, phi + 3 * (size_t)ng) : std::vector<double>(3, 0.0));
+    h->gauge_val.alloc(std::max(ng, 1));
+    // distinct elements, each with its gauges in input order
+    std::vector<int> order(ng);
+    for (int g = 0; g < ng; ++g) order[g] = g;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ed[a] < ed[b]; });
+    std::vector<int> gel, gptr(1, 0), ggauge;
+    for (int i = 0; i < ng; ++i) {
+      if (i == 0 || ed[order[i]] != ed[order[i - 1]]) {
+        if (i) gptr.push_back(i);
+        gel.push_back(ed[order[i]]);
+      }
+      ggauge.push_back(order[i]);
+    }
+    gptr.push_back(ng);
+    h->ngroup = (int)gel.size();
+    h->group_elem.upload(gel.empty() ? std::vector<int>(1, 0) : gel);
+    h->group_ptr.upload(gptr);
+    h->group_gauge.upload(ggauge.empty() ? std::vector<int>(1, 0) : ggauge);
+  });
+}
+
+int dgswem_cuda_gauge_eta(dgswem_cuda* h, double* eta) {
+  return guarded([&]() {
+    if (!h || !eta) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    DG_CUDA(cudaSetDevice(h->device));
+    if (h->ngauge == 0) return;
+    adj::launch_gauge_eval(h->q[0].p, h->ne, h->gauge_elem.p, h->gauge_phi.p, h->ngauge, h->gauge_val.p,
+                           h->stream);
+    check_launch(h, "gauge_eval");
+    DG_CUDA(cudaMemcpyAsync(eta, h->gauge_val.p, h->ngauge * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int dgswem_cuda_adjoint_begin(dgswem_cuda* h) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    DG_CUDA(cudaSetDevice(h->device));
+    adjoint_prepare(h);
+  });
+}
+
+int dgswem_cuda_adjoint_seed(dgswem_cuda* h, const double* w) {
+  return guarded([&]() {
+    if (!h || !w) throw Failure(DGSWEM_ERR_ARG, "null argument");
+    if (!h->adj_on) throw Failure(DGSWEM_ERR_ARG, "call dgswem_cuda_adjoint_begin first");
+    DG_CUDA(cudaSetDevice(h->device));
+    if (h->ngauge == 0) return;
+    // from pageable memory the copy has read w when it returns
+    DG_CUDA(cudaMemcpyAsync(h->gauge_val.p, w, h->ngauge * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    seed_gauges(h, h->gauge_val.p);
+  });
+}
+
+int dgswem_cuda_adjoint_step(dgswem_cuda* h, int it) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (!h->adj_on) throw Failure(DGSWEM_ERR_ARG, "call dgswem_cuda_adjoint_begin first");
+    DG_CUDA(cudaSetDevice(h->device));
+    // recompute step `it` from the loaded state: stage I's state is q[I-1]
+    // (I >= 2) and q[nrk] (I = 1, swapped there at the end of the step)
+    run_steps(h, it, 1);
+    const int nrk = h->nrk;
+    std::vector<const double*> st(nrk);
+    for (int I = 1; I <= nrk; ++I) st[I - 1] = I == 1 ? h->q[nrk].p : h->q[I - 1].p;
+    adjoint_stages(h, it, st.data(), h->forcing_per_stage ? h->forcing_dev.p : nullptr);
+  });
+}
+
+int dgswem_cuda_misfit_forward(dgswem_cuda* h, int it0, int nsteps, int every, double* eta) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (nsteps < 0 || every < 1) throw Failure(DGSWEM_ERR_ARG, "misfit_forward: bad step counts");
+    DG_CUDA(cudaSetDevice(h->device));
+    const int ng = h->ngauge;
+    h->eta_rec.ensure(std::max<size_t>((size_t)nsteps * ng, 1));
+    for (int k = 0; k < nsteps; ++k) {
+      if (k % every == 0) save_slot(h, k / every);
+      run_steps(h, it0 + k, 1);
+      if (ng > 0) {
+        adj::launch_gauge_eval(h->q[0].p, h->ne, h->gauge_elem.p, h->gauge_phi.p, ng, h->eta_rec.p + (size_t)k * ng,
+                               h->stream);
+        check_launch(h, "gauge_eval");
+      }
+    }
+    if (eta && ng > 0 && nsteps > 0)
+      DG_CUDA(cudaMemcpyAsync(eta, h->eta_rec.p, (size_t)nsteps * ng * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    unsigned err = 0;
+    DG_CUDA(cudaMemcpy(&err, h->err.p, sizeof(err), cudaMemcpyDeviceToHost));
+    if (err) throw Failure(DGSWEM_ERR_NUMERIC, "NaN in the state during misfit_forward");
+  });
+}
+
+int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, const double* w) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (nsteps < 1 || every < 1) throw Failure(DGSWEM_ERR_ARG, "adjoint_sweep: bad step counts");
+    DG_CUDA(cudaSetDevice(h->device));
+    adjoint_prepare(h);
+    const int nrk = h->nrk, ng = h->ngauge;
+    const int nseg = (nsteps + every - 1) / every;
+    for (int s = 0; s < nseg; ++s)
+      if ((size_t)s >= h->slot_q.size() || !h->slot_q[s].p)
+        throw Failure(DGSWEM_ERR_ARG, "adjoint_sweep: run dgswem_cuda_misfit_forward with the same steps first");
+    if (ng > 0) {
+      h->w_rec.ensure((size_t)nsteps * ng);
+      DG_CUDA(cudaMemcpyAsync(h->w_rec.p, w, (size_t)nsteps * ng * sizeof(double), cudaMemcpyHostToDevice,
+                              h->stream));
+    }
+    const size_t n9 = 9 * (size_t)h->ne, fstep = (size_t)nrk * h->forcing_per_stage;
+    const int seg_steps = std::min(every, nsteps);
+    if (h->adj_stage.size() < (size_t)seg_steps * (nrk - 1)) {
+      h->adj_stage.resize((size_t)seg_steps * (nrk - 1));
+      for (auto& b : h->adj_stage)
+        if (!b.p) b.alloc(n9);
+    }
+    if (fstep) h->adj_forc.ensure(fstep * seg_steps);
+    std::vector<const double*> st(nrk);
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+      const int k0 = seg * every, k1 = std::min(k0 + every, nsteps);
+      // forward over the segment, keeping each step's start state, stage
+      // states and stage forcing
+      load_slot(h, seg);
+      for (int k = k0; k < k1; ++k) {
+        const int j = k - k0;
+        save_slot(h, nseg + j);
+        run_steps(h, it0 + k, 1);
+        for (int I = 2; I <= nrk; ++I)
+          DG_CUDA(cudaMemcpyAsync(h->adj_stage[(size_t)j * (nrk - 1) + (I - 2)].p, h->q[I - 1].p,
+                                  n9 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        if (fstep)
+          DG_CUDA(cudaMemcpyAsync(h->adj_forc.p + (size_t)j * fstep, h->forcing_dev.p, fstep * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+      }
+      // backward: step k maps state k-1 to state k
+      for (int k = k1; k > k0; --k) {
+        const int j = k - 1 - k0;
+        if (ng > 0) seed_gauges(h, h->w_rec.p + (size_t)(k - 1) * ng);
+        st[0] = h->slot_q[nseg + j].p;
+        for (int I = 2; I <= nrk; ++I) st[I - 1] = h->adj_stage[(size_t)j * (nrk - 1) + (I - 2)].p;
+        adjoint_stages(h, it0 + k - 1, st.data(), fstep ? h->adj_forc.p + (size_t)j * fstep : nullptr);
+      }
+    }
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int dgswem_cuda_adjoint_read(dgswem_cuda* h, double* g_nbar, double* g_hb, double* lam_ze, double* lam_qx,
+                             double* lam_qy) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (!h->adj_on) throw Failure(DGSWEM_ERR_ARG, "call dgswem_cuda_adjoint_begin first");
+    DG_CUDA(cudaSetDevice(h->device));
+    const int ne = h->ne;
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<double> gn(ne), gh(3 * (size_t)ne), lam(9 * (size_t)ne);
+    DG_CUDA(cudaMemcpy(gn.data(), h->adj_gn.p, ne * sizeof(double), cudaMemcpyDeviceToHost));
+    DG_CUDA(cudaMemcpy(gh.data(), h->adj_ghb.p, gh.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    DG_CUDA(cudaMemcpy(lam.data(), h->adj_lam[h->nrk].p, lam.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ne; ++i) {
+      const size_t e = (size_t)h->perm_h[i];
+      if (g_nbar) g_nbar[e] = h->mesh.manning ? gn[i] : 0.0;
+      for (int k = 0; k < 3; ++k) {
+        if (g_hb) g_hb[3 * e + k] = gh[(size_t)k * ne + i];
+        if (lam_ze) lam_ze[3 * e + k] = lam[(size_t)k * ne + i];
+        if (lam_qx) lam_qx[3 * e + k] = lam[(size_t)(3 + k) * ne + i];
+        if (lam_qy) lam_qy[3 * e + k] = lam[(size_t)(6 + k) * ne + i];
+      }
     }
   });
 }

@@ -258,6 +258,50 @@ DGSWEM_DECLARE_LAUNCHERS(fast)
 DGSWEM_DECLARE_LAUNCHERS(strict)
 DGSWEM_DECLARE_LAUNCHERS(mixed)
 
+// ---- discrete adjoint (adjoint.cu) ----------------------------------------
+// Vector-Jacobian product of one RK stage's right-hand side L(q; n, HB) at
+// stage state q: lam += (dL/dq)^T nu, g_n += (dL/dnbar)^T nu (element-mean
+// Manning n), g_hb += (dL/dHB)^T nu.  Two kernels: per (edge, point) into
+// the per-element scratch eb (each slot written by one thread), then per
+// element (volume terms and the gather of eb).
+struct AdjArgs {
+  MeshView m;
+  Physics ph;
+  const double* __restrict__ q;         // stage state at which L was evaluated
+  const double* __restrict__ nu;        // cotangent of L, 9*NE
+  double* lam;                          // += (dL/dq)^T nu, 9*NE
+  double* g_n;                          // += per element, or null (no Manning n)
+  double* g_hb;                         // += [k*NE + e]
+  const double* __restrict__ ocean_zg;  // this stage's ocean forcing (as StageArgs)
+  const double* __restrict__ pr;        // nodal pressure (NWS=1), or null
+  double rampdg;
+  double* eb;                           // 36*NE scratch: edge-point trace cotangents
+  const int* __restrict__ edges;        // (element, local edge) pairs: interior edges from the in side, boundary edges
+  int nedge;
+};
+// One stage of the reverse SSP-RK accumulation: lam_I += a_I lam_j and
+// nu_I += b_I lam_j for I < n (b_I already times DT).
+struct SspAdjArgs {
+  const double* lam_j;
+  double* lam[kMaxStages];
+  double* nu[kMaxStages];
+  double a[kMaxStages], b[kMaxStages];
+  int n;
+  long long len;
+};
+namespace adj {
+void set_basis(const BasisP1& b);
+void launch_rhs_vjp(const AdjArgs& a, cudaStream_t s);
+void launch_ssp_adj(const SspAdjArgs& a, cudaStream_t s);
+// eta[slot*ng + g] = sum_k phi[g*3+k] * q[k*NE + elem[g]] (ZE at gauge points)
+void launch_gauge_eval(const double* q, int ne, const int* elem, const double* phi, int ng, double* eta,
+                       cudaStream_t s);
+// lam[k*NE + elem[g]] += phi[g*3+k] * w[g] (misfit seed of the ZE modes),
+// over the gauge groups (distinct elements gel, CSR gptr / ggauge)
+void launch_gauge_seed(double* lam, int ne, const int* gel, const int* gptr, const int* ggauge, const double* phi,
+                       const double* w, int ngroup, cudaStream_t s);
+}  // namespace adj
+
 constexpr int kPointBlock = 256;
 
 }  // namespace dgswem

@@ -292,3 +292,28 @@ def ensemble_specs(n: int, seed: int = 20261203, ne_min: int = 5000, ne_max: int
     wdir = rng.uniform(0.0, 360.0, n)
     return [dict(kind=ENSEMBLE_KINDS[int(kinds[i])], ne=int(ne[i]), amp=float(amp[i]), n_manning=float(nman[i]),
                  wind_pa=float(wind[i]), wind_deg=float(wdir[i]), seed=seed + 1 + i) for i in range(n)]
+
+
+def smooth_basin(path, nx: int = 158, ny: int = 32, lx: float = 20e3, ly: float = 4e3, amp: float = 0.5,
+                 n0: float = 0.025, dt: float = 1.0, nsteps: int = 100, **kw) -> Path:
+    """Always-wet rectangular basin with smooth fields, for gradient checks:
+    depth 20 m at the open (x = 0) edge to 5 m at the far wall plus a smooth
+    Gaussian shoal, nodal Manning n = n0 (1 + 0.2 sin) varying smoothly,
+    quadratic friction with the Manning floor CF = 1e-4 (below every
+    element's Manning coefficient, so no element sits on it), no WETDRY, no slope limiter, SSP(2,2), tide of
+    amplitude ``amp`` on the open edge, land elsewhere."""
+    ctl = Controls(title="smooth basin", nolibf=1, nolifa=1, cf=1e-4, dt=dt, nsteps=nsteps, rk_stage=2, rk_order=2,
+                   slopeflag=0, h0=0.01, nramp=1, dramp=0.05, manning=True)
+    for k, v in kw.items():
+        setattr(ctl, k, v)
+    xs, ys = np.linspace(0.0, lx, nx + 1), np.linspace(0.0, ly, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    dp = 20.0 - 15.0 * X / lx - 3.0 * np.exp(-(((X - 0.6 * lx) / (0.1 * lx)) ** 2 + ((Y - 0.5 * ly) / (0.2 * ly)) ** 2))
+    elems = _grid_triangles(nx, ny)
+    nid = lambda i, j: i * (ny + 1) + j + 1  # noqa: E731
+    ocean = [nid(0, j) for j in range(ny, -1, -1)]
+    land = [nid(i, 0) for i in range(0, nx + 1)] + [nid(nx, j) for j in range(1, ny + 1)] + \
+           [nid(i, ny) for i in range(nx - 1, -1, -1)]
+    manning = n0 * (1.0 + 0.2 * np.sin(2 * math.pi * X / lx) * np.cos(math.pi * Y / ly))
+    return write_deck(path, X.ravel(), Y.ravel(), dp.ravel(), elems, [ocean], [(land, 0)], ctl,
+                      emo=np.full(len(ocean), amp), efa=np.zeros(len(ocean)), manning=manning.ravel())

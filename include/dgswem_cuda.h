@@ -239,6 +239,60 @@ int dgswem_cuda_profile_read(dgswem_cuda* h, double* ms, long long* launches);
 /* Last error message of the calling thread (NUL-terminated, truncated). */
 int dgswem_cuda_last_error(char* buf, int buflen);
 
+/* ---- parameters, state slots, gauges, discrete adjoint ---------------------
+ * No counterparts in the reference.  All need a whole-mesh handle
+ * (dgswem_cuda_create).
+ *
+ * dgswem_cuda_set_params: replace the element-mean Manning n (nbar[NE], input
+ * element order; the deck must have nodal Manning n) and/or the bathymetry
+ * modes (hb = HB(DOFH,NE)); NULL keeps a field.  WETDRY keeps reading the
+ * nodal depths DP of the setup.
+ *
+ * dgswem_cuda_state_save / _load: copy the current state (ZE/QX/QY, WDFLG)
+ * to / from device slot `slot` (allocated on first save; checkpoints).
+ *
+ * dgswem_cuda_gauges: ng gauge points, each in element elem[g] (1-based
+ * input id) with ZE basis values phi[3g..3g+2] at the point (1 and the
+ * corner-map combinations of its barycentric weights); dgswem_cuda_gauge_eta
+ * evaluates ZE of the current state there.
+ *
+ * Discrete adjoint of DG_HYDRO_TIMESTEP (NLEQ=1, ICS=1, land and ocean
+ * edges, no slope limiter, no WETDRY, linear / quadratic / Manning friction;
+ * DGSWEM_ERR_ARG otherwise; FP64 handles only):
+ *   dgswem_cuda_adjoint_begin   zero the state cotangent and the gradients
+ *   dgswem_cuda_adjoint_seed    add w[g] * dZE(gauge g)/dq to the cotangent of
+ *                               the state the next adjoint step ends at
+ *   dgswem_cuda_adjoint_step    with the state before step `it` loaded,
+ *                               recompute step `it` (the handle ends at the
+ *                               state after it) and carry the cotangent back
+ *                               through it, adding that step's parameter
+ *                               gradient
+ *   dgswem_cuda_adjoint_read    gradients w.r.t. nbar (NE, input order) and HB
+ *                               (HB(DOFH,NE)), and the current state
+ *                               cotangent (ZE/QX/QY(DOFH,NE)); NULL skips. */
+int dgswem_cuda_set_params(dgswem_cuda* h, const double* nbar, const double* hb);
+int dgswem_cuda_state_save(dgswem_cuda* h, int slot);
+int dgswem_cuda_state_load(dgswem_cuda* h, int slot);
+int dgswem_cuda_gauges(dgswem_cuda* h, int ng, const int* elem, const double* phi);
+int dgswem_cuda_gauge_eta(dgswem_cuda* h, double* eta);
+int dgswem_cuda_adjoint_begin(dgswem_cuda* h);
+int dgswem_cuda_adjoint_seed(dgswem_cuda* h, const double* w);
+int dgswem_cuda_adjoint_step(dgswem_cuda* h, int it);
+int dgswem_cuda_adjoint_read(dgswem_cuda* h, double* g_nbar, double* g_hb, double* lam_ze, double* lam_qx,
+                             double* lam_qy);
+/* The two passes of a gauge-misfit gradient with sqrt(N)-style checkpoints,
+ * each one call.  dgswem_cuda_misfit_forward runs steps it0 .. it0+nsteps-1
+ * from the current state, saving the state every `every` steps in slots
+ * 0, 1, .. and writing ZE at the gauges after each step to eta[k*ng + g].
+ * dgswem_cuda_adjoint_sweep (after it, same it0 / nsteps / every) zeroes the
+ * gradients and carries w[k*ng + g] (the misfit's derivative with respect to
+ * ZE at gauge g after step k) back to the initial state: per segment it
+ * re-runs the steps from the checkpoint keeping their stage states (slots
+ * from nseg on, and `every` x (NRK-1) stage buffers), then steps back.
+ * Read the result with dgswem_cuda_adjoint_read. */
+int dgswem_cuda_misfit_forward(dgswem_cuda* h, int it0, int nsteps, int every, double* eta);
+int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, const double* w);
+
 /* ---- standalone input path (no Fortran host) ------------------------------
  * Reads fort.14, fort.15, fort.dg (and fort.13 when NWP>0) from `dir` and runs
  * the setup the reference does in READ_INPUT + PREP_DG, producing a
