@@ -71,6 +71,7 @@ SIGNATURES = {
     "dgswem_cuda_kernel_launches": (C.c_longlong, [C.c_void_p]),
     "dgswem_cuda_last_error": (C.c_int, [C.c_char_p, C.c_int]),
     "dgswem_cuda_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dgswem_cuda_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "dgswem_cuda_stream": (C.c_void_p, [C.c_void_p]),
     "dgswem_cuda_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "dgswem_cuda_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong)]),

@@ -245,6 +245,20 @@ struct dgswem_cuda {
   // state slots of dgswem_cuda_state_save / _load (checkpoints)
   std::vector<DevBuf<double>> slot_q;
   std::vector<DevBuf<int>> slot_wd;
+  // CUDA graphs of graph_steps steps (dgswem_cuda_set_graph): two graphs
+  // that differ only in the pinned buffer their first node copies the
+  // chunk's stage forcing and ramps from, so that the host fills one while
+  // the other runs
+  int graph_steps = 0, graph_next = 0;
+  bool graph_ready = false;
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  double* gbuf_host[2] = {nullptr, nullptr};
+  size_t gbuf_bytes = 0;
+  cudaEvent_t gdone[2] = {nullptr, nullptr};
+  DevBuf<double> gbuf_dev;
+  double* graph_q0 = nullptr;      // buffer that held the state at capture
+  long long graph_launches = 0;    // kernels per graph
 };
 
 namespace {
@@ -824,7 +838,7 @@ void stage_forcing(const dgswem_cuda* h, double timedg, double rampdg, double* o
 
 // One RK stage: the stage kernel writes stage buffer irk for the owned
 // elements (launch_stage_rhs), then the limiter and WETDRY (launch_limit).
-void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing) {
+void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, const double* ramp = nullptr) {
   const int nrk = h->nrk;
   StageArgs A{};
   A.m = h->mesh;
@@ -846,6 +860,7 @@ void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing) {
   A.rout = h->keep_rhs[irk - 1] ? h->rhs[irk - 1].p : nullptr;
   A.wd = h->wd.p;
   stage_clock(h, it, irk, &A.timedg, &A.rampdg);
+  A.ramp = ramp;
   A.ocean_zg = forcing;
   A.flow_qn = forcing ? forcing + (size_t)h->amig.size() * h->needs * 2 : nullptr;
   A.wsx = h->wsx.p;
@@ -898,8 +913,109 @@ void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
   launch_limit(h, irk);
 }
 
+// ---- CUDA graphs of whole steps ----
+// A graph holds graph_steps (even) steps: one host-to-device copy of the
+// chunk's stage blocks (the host forcing of the stage, then RAMPDG) and the
+// stage kernels, which read the ramp and forcing from that block.  An even
+// step count brings the swapped stage buffers back to the captured
+// arrangement.
+size_t graph_block(const dgswem_cuda* h) { return h->forcing_per_stage + 1; }
+
+void graph_release(dgswem_cuda* h) {
+  for (int b = 0; b < 2; ++b) {
+    if (h->gexec[b]) cudaGraphExecDestroy(h->gexec[b]);
+    if (h->graph[b]) cudaGraphDestroy(h->graph[b]);
+    h->gexec[b] = nullptr;
+    h->graph[b] = nullptr;
+  }
+  h->graph_ready = false;
+}
+
+void graph_fill(dgswem_cuda* h, double* buf, int it0) {
+  const int nrk = h->nrk;
+  const size_t blk = graph_block(h);
+  for (int i = 0; i < h->graph_steps; ++i)
+    for (int irk = 1; irk <= nrk; ++irk) {
+      double timedg, rampdg;
+      stage_clock(h, it0 + i, irk, &timedg, &rampdg);
+      double* o = buf + ((size_t)i * nrk + (irk - 1)) * blk;
+      if (h->forcing_per_stage) stage_forcing(h, timedg, rampdg, o);
+      o[h->forcing_per_stage] = rampdg;
+    }
+}
+
+void graph_capture(dgswem_cuda* h) {
+  graph_release(h);
+  const int m = h->graph_steps, nrk = h->nrk;
+  const size_t blk = graph_block(h), len = (size_t)m * nrk * blk, bytes = len * sizeof(double);
+  h->gbuf_dev.ensure(len);
+  for (int b = 0; b < 2; ++b) {
+    if (h->gdone[b]) DG_CUDA(cudaEventSynchronize(h->gdone[b]));
+    if (h->gbuf_bytes < bytes && h->gbuf_host[b]) {
+      cudaFreeHost(h->gbuf_host[b]);
+      h->gbuf_host[b] = nullptr;
+    }
+    if (!h->gbuf_host[b]) DG_CUDA(cudaMallocHost(&h->gbuf_host[b], bytes));
+    if (!h->gdone[b]) DG_CUDA(cudaEventCreateWithFlags(&h->gdone[b], cudaEventDisableTiming));
+  }
+  h->gbuf_bytes = std::max(h->gbuf_bytes, bytes);
+  const long long l0 = h->launches;
+  h->graph_q0 = h->q[0].p;
+  for (int b = 0; b < 2; ++b) {
+    DG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
+    try {
+      DG_CUDA(cudaMemcpyAsync(h->gbuf_dev.p, h->gbuf_host[b], bytes, cudaMemcpyHostToDevice, h->stream));
+      for (int i = 0; i < m; ++i) {
+        for (int irk = 1; irk <= nrk; ++irk) {
+          const double* sb = h->gbuf_dev.p + ((size_t)i * nrk + (irk - 1)) * blk;
+          launch_stage_rhs(h, 0, irk, h->forcing_per_stage ? sb : nullptr, sb + h->forcing_per_stage);
+          launch_limit(h, irk);
+        }
+        std::swap(h->q[0], h->q[nrk]);
+      }
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(h->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      h->launches = l0;
+      throw;
+    }
+    DG_CUDA(cudaStreamEndCapture(h->stream, &h->graph[b]));
+    DG_CUDA(cudaGraphInstantiate(&h->gexec[b], h->graph[b], 0));
+  }
+  h->graph_launches = (h->launches - l0) / 2;
+  h->launches = l0;
+  h->graph_ready = true;
+}
+
+// Steps it0 .. it0+n-1 through the graphs, as many whole graphs as fit;
+// returns the steps done.
+int run_steps_graph(dgswem_cuda* h, int it0, int n) {
+  const int m = h->graph_steps, nrk = h->nrk;
+  if (m < 2 || h->prof_on || n < m) return 0;
+  if (!h->graph_ready) graph_capture(h);
+  if (h->q[0].p != h->graph_q0) {  // the state sits in the other buffer: move it where the graphs read it
+    DG_CUDA(cudaMemcpyAsync(h->q[nrk].p, h->q[0].p, 9 * (size_t)h->ne * sizeof(double), cudaMemcpyDeviceToDevice,
+                            h->stream));
+    std::swap(h->q[0], h->q[nrk]);
+  }
+  int done = 0, b = h->graph_next;
+  for (; done + m <= n; done += m, b ^= 1) {
+    DG_CUDA(cudaEventSynchronize(h->gdone[b]));  // buffer b free again
+    graph_fill(h, h->gbuf_host[b], it0 + done);
+    DG_CUDA(cudaGraphLaunch(h->gexec[b], h->stream));
+    DG_CUDA(cudaEventRecord(h->gdone[b], h->stream));
+    h->launches += h->graph_launches;
+  }
+  h->graph_next = b;
+  return done;
+}
+
 void run_steps(dgswem_cuda* h, int it0, int n) {
   const int nrk = h->nrk;
+  const int by_graph = run_steps_graph(h, it0, n);
+  it0 += by_graph;
+  n -= by_graph;
   for (int done = 0; done < n;) {
     const int m = std::min(n - done, h->chunk_steps > 0 ? h->chunk_steps : n);
     const double* dev = nullptr;
@@ -1239,6 +1355,11 @@ void dgswem_cuda_destroy(dgswem_cuda* h) {
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   if (h->forcing_copied) cudaEventDestroy(h->forcing_copied);
   if (h->forcing_host) cudaFreeHost(h->forcing_host);
+  graph_release(h);
+  for (int b = 0; b < 2; ++b) {
+    if (h->gdone[b]) cudaEventDestroy(h->gdone[b]);
+    if (h->gbuf_host[b]) cudaFreeHost(h->gbuf_host[b]);
+  }
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -1477,6 +1598,19 @@ int dgswem_cuda_halo_unpack(dgswem_cuda* h, int kind, int peer, int irk, const d
 }
 
 long long dgswem_cuda_kernel_launches(const dgswem_cuda* h) { return h ? h->launches : -1; }
+
+int dgswem_cuda_set_graph(dgswem_cuda* h, int steps) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (steps != 0 && (steps < 2 || steps % 2 != 0))
+      throw Failure(DGSWEM_ERR_ARG, "steps per graph must be 0 (off) or an even number >= 2");
+    DG_CUDA(cudaSetDevice(h->device));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_release(h);
+    h->graph_steps = steps;
+    h->graph_next = 0;
+  });
+}
 
 int dgswem_cuda_set_stream(dgswem_cuda* h, void* stream) {
   return guarded([&]() {

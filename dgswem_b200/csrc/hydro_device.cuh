@@ -209,6 +209,7 @@ struct StageArgs {
   double a[kMaxStages], b[kMaxStages];      // ATVD(irk,I), BTVD(irk,I)*DT
   const int* __restrict__ wd;               // WDFLG (read)
   double timedg, rampdg;
+  const double* __restrict__ ramp;          // RAMPDG of this stage in device memory (graph replays), or null: rampdg
   const double* __restrict__ ocean_zg;      // [(f*NEEDS + L)*2 + ipt] EMO*RFF*COS(ARGJ-EFA)
   const double* __restrict__ flow_qn;       // [(f*NFEDS + L)*3 + point] QNAM*RFF*COS(ARG)
   const double* __restrict__ wsx;           // nodal met forcing (already ramped), or null

@@ -30,6 +30,10 @@ typedef double real;
 #endif
 __constant__ BasisT<real> cBasisR;  // cBasis in that type
 
+// RAMPDG of the stage: from device memory in a replayed CUDA graph (whose
+// kernel arguments are fixed at capture), else the launch argument
+__device__ __forceinline__ double stage_ramp(const StageArgs& A) { return A.ramp ? *A.ramp : A.rampdg; }
+
 // Element geometry rows in the arithmetic type
 __device__ __forceinline__ const real* egeo_r(const MeshView& m) {
 #ifdef DGSWEM_MIXED
@@ -240,7 +244,7 @@ __device__ __forceinline__ void ghost_state(const StageArgs& A, unsigned kind, i
       qne = -(xi * nx + yi * ny);
       qte = xi * tx + yi * ty;
     } else {
-      qne = (real)A.rampdg * (real)A.m.ebcfsp[list] * subsup * sqrt(subsup * real(P.g));
+      qne = (real)stage_ramp(A) * (real)A.m.ebcfsp[list] * subsup * sqrt(subsup * real(P.g));
       qte = 0;
     }
     xx = (ty * qne - ny * qte) / (nx * ty - ny * tx);
@@ -309,12 +313,12 @@ __device__ __noinline__ void ibarrier_side(const StageArgs& A, int seg, int side
       const double ssf = 2.0 * abovef / 3.0, ssb = 2.0 * aboveb / 3.0;
       if (abovef > aboveb && abovef > 0.01) {
         weir = 1;
-        qfn = (aboveb > ssf) ? A.rampdg * m.ibcfsb[seg] * aboveb * sqrt(2.0 * P.g * (abovef - aboveb))
-                             : A.rampdg * m.ibcfsp[seg] * ssf * sqrt(ssf * P.g);
+        qfn = (aboveb > ssf) ? stage_ramp(A) * m.ibcfsb[seg] * aboveb * sqrt(2.0 * P.g * (abovef - aboveb))
+                             : stage_ramp(A) * m.ibcfsp[seg] * ssf * sqrt(ssf * P.g);
       } else if (aboveb > abovef && aboveb > 0.01) {
         weir = -1;
-        qbn = (abovef > ssb) ? A.rampdg * m.ibcfsb[seg] * abovef * sqrt(2.0 * P.g * (aboveb - abovef))
-                             : A.rampdg * m.ibcfsp[seg] * ssb * sqrt(ssb * P.g);
+        qbn = (abovef > ssb) ? stage_ramp(A) * m.ibcfsb[seg] * abovef * sqrt(2.0 * P.g * (aboveb - abovef))
+                             : stage_ramp(A) * m.ibcfsp[seg] * ssb * sqrt(ssb * P.g);
       }
     }
     Flux3 fb{0, 0, 0}, ff{0, 0, 0};
@@ -517,7 +521,7 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<r
       dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
       dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
     }
-    const real fw = real(1) / f1, r = (real)A.rampdg;
+    const real fw = real(1) / f1, r = (real)stage_ramp(A);
     const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
     const real wx0 = r * (real)A.wsx[n0], wx1 = r * (real)A.wsx[n1], wx2 = r * (real)A.wsx[n2];
     const real wy0 = r * (real)A.wsy[n0], wy1 = r * (real)A.wsy[n1], wy2 = r * (real)A.wsy[n2];

@@ -159,6 +159,11 @@ class HydroStep:
         default stream), e.g. ``torch.cuda.Stream().cuda_stream``."""
         _abi.check(self._lib.dgswem_cuda_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 
+    def set_graph(self, steps: int) -> None:
+        """dgswem_cuda_set_graph: replay whole steps of ``run`` as CUDA graphs
+        of ``steps`` (even) steps; 0 turns graphs off."""
+        _abi.check(self._lib.dgswem_cuda_set_graph(self._h, int(steps)))
+
     @property
     def stream_handle(self) -> int:
         return int(self._lib.dgswem_cuda_stream(self._h) or 0)

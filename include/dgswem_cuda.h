@@ -220,6 +220,14 @@ int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, d
 /* Number of kernels the library launched since create (for accounting). */
 long long dgswem_cuda_kernel_launches(const dgswem_cuda* h);
 
+/* Run the whole-step chunks of dgswem_cuda_run as CUDA graphs of `steps`
+ * steps (even, >= 2; 0: off, the default): the chunk's stage kernels and one
+ * copy of its host forcing and ramps are captured once, then replayed, so a
+ * chunk costs one graph launch instead of 3 x NRK kernel launches per step.
+ * Results are bit-identical to the launches without graphs.  Not while
+ * per-kernel profiling is on.  No counterpart in the reference. */
+int dgswem_cuda_set_graph(dgswem_cuda* h, int steps);
+
 /* Launch on the caller's CUDA stream (a cudaStream_t passed as void*, used
  * as given: NULL is the CUDA default stream).  dgswem_cuda_stream() returns
  * the stream in use, so a caller can restore the library's own stream.
