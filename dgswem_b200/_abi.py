@@ -91,6 +91,8 @@ SIGNATURES = {
     "dgswem_cuda_adjoint_read": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "dgswem_cuda_misfit_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp]),
     "dgswem_cuda_adjoint_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp]),
+    "dgswem_cuda_limit_state": (C.c_int, [C.c_void_p]),
+    "dgswem_cuda_limiter_vjp": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]),
 }
 
 _lib = None

@@ -11,8 +11,9 @@
 // Manning floor CF, the friction cap 0.9/DT, the ocean depth-positivity fix).
 //
 // Scope: NLEQ=1 (finite amplitude), ICS=1, land and ocean edges (any other
-// kind is rejected before launch), no slope limiter and no WETDRY (the host
-// rejects them: their frozen-branch adjoints are not built), linear,
+// kind is rejected before launch), slope limiter 5 with its branches frozen
+// at the forward's (node_arg .. elem_bound_scatter below), no WETDRY (the
+// host rejects it: its frozen-branch adjoint is not built), linear,
 // quadratic or Manning friction (not hybrid), NWS 0/1.
 //
 // Deterministic without atomics: edge_vjp evaluates each edge point once
@@ -346,6 +347,183 @@ __global__ void __launch_bounds__(128) elem_vjp(const __grid_constant__ AdjArgs 
   for (int c = 0; c < 9; ++c) A.lam[(size_t)c * ne + e] += lam9[c];
   for (int k = 0; k < 3; ++k) A.g_hb[(size_t)k * ne + e] += ghb[k];
   if (A.g_n) A.g_n[e] += gn;
+}
+
+// ---- slope limiter 5 with frozen branches (slopelimiter.F:3259-3781) ----
+// The forward limiter maps the stage kernel's output q (pre-limiter) to the
+// stage state: per element and variable, vertex values clamped to the node
+// min / max of the element means over each node's star, three
+// mean-preserving redistribution sweeps, modes 2-3 rebuilt (mode 1 kept).
+// With its decisions frozen (which clamp, the sweep signs, the counts of
+// positive differences, which of the two limits each reduction takes) it is
+// linear in q and in the node bounds; the bounds are the means of the first
+// star element that attains them.
+
+// Node min / max of the element means (as node_minmax) and the first star
+// element attaining each: arg[(2 var + {0 min, 1 max}) * NP + n].
+__global__ void node_arg(const MeshView m, const double* __restrict__ q, double* __restrict__ mm,
+                         int* __restrict__ arg) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= m.np) return;
+  const int ne = m.ne, np = m.np;
+  for (int var = 0; var < 3; ++var) {
+    double vmin = 99999., vmax = -99999.;
+    int amin = -1, amax = -1;
+    for (int p = m.star_ptr[n]; p < m.star_ptr[n + 1]; ++p) {
+      const int e = m.star[p];
+      const double t = q[(size_t)(3 * var) * ne + e];
+      if (t < vmin) { vmin = t; amin = e; }
+      if (t > vmax) { vmax = t; amax = e; }
+    }
+    mm[(size_t)(2 * var) * np + n] = vmin;
+    mm[(size_t)(2 * var + 1) * np + n] = vmax;
+    arg[(size_t)(2 * var) * np + n] = amin;
+    arg[(size_t)(2 * var + 1) * np + n] = amax;
+  }
+}
+
+__device__ __forceinline__ double div_count(double x, int kdp) {
+  if (kdp <= 1) return x;
+  if (kdp == 2) return x * 0.5;
+  return x / 3.0;
+}
+
+// Per element: replay of the limiter on the pre-limiter state q, then its
+// reverse mode.  lam (in place): the cotangent of the limited state on
+// entry, of the pre-limiter state on exit (without the bound terms);
+// lb[e*18 + (var*3 + a)*2 + {0 min, 1 max}]: the cotangent of vertex a's
+// bounds.
+__global__ void __launch_bounds__(128) limit_vjp(const MeshView m, const double* __restrict__ q,
+                                                 const double* __restrict__ mm, double* __restrict__ lam,
+                                                 double* __restrict__ lb) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ne = m.ne, np = m.np;
+  if (e >= ne) return;
+  int nd[3];
+  for (int v = 0; v < 3; ++v) nd[v] = m.nm[(size_t)v * ne + e];
+  for (int var = 0; var < 3; ++var) {
+    double z[3];
+    for (int k = 0; k < 3; ++k) z[k] = q[(size_t)(3 * var + k) * ne + e];
+    double vmin[3], vmax[3], vx[3];
+    int clamp[3];  // 0 none, 1 to max, 2 to min
+    for (int a = 0; a < 3; ++a) {
+      vmin[a] = mm[(size_t)(2 * var) * np + nd[a]];
+      vmax[a] = mm[(size_t)(2 * var + 1) * np + nd[a]];
+      const double v = z[0] + cB.phi_corner[a][1] * z[1] + cB.phi_corner[a][2] * z[2];
+      const double c1 = fmin(v, vmax[a]);
+      vx[a] = fmax(c1, vmin[a]);
+      clamp[a] = vx[a] != c1 ? 2 : (c1 != v ? 1 : 0);
+    }
+    // forward sweeps, recording the decisions
+    double sgn[3];
+    bool pos[3][3], to_max[3][3];
+    int kd[3][3];
+    for (int w = 0; w < 3; ++w) {
+      const double sumloc = (vx[0] + vx[1] + vx[2]) / 3.0;
+      double sumdif = (sumloc - z[0]) * 3.0;
+      const double s = copysign(1.0, sumdif);
+      sgn[w] = s;
+      double dif[3];
+      for (int a = 0; a < 3; ++a) dif[a] = (vx[a] - z[0]) * s;
+      int kdp = (dif[0] > 0) + (dif[1] > 0) + (dif[2] > 0);
+      for (int k = 0; k < 3; ++k) {
+        double redfac = 0.0;
+        pos[w][k] = dif[k] > 0;
+        kd[w][k] = kdp;
+        if (pos[w][k]) {
+          redfac = div_count(sumdif * s, kdp);
+          kdp = kdp - 1;
+        }
+        const double redmax = s > 0 ? vx[k] - vmin[k] : vmax[k] - vx[k];
+        to_max[w][k] = !(redfac <= redmax);  // fmin(redfac, redmax) took redmax
+        redfac = fmin(redfac, redmax);
+        sumdif = sumdif - redfac * s;
+        vx[k] = vx[k] - redfac * s;
+      }
+    }
+    // reverse: outputs z0 (kept), z1, z2 from vx
+    const size_t c0 = (size_t)(3 * var) * ne + e;
+    const double l0 = lam[c0], l1 = lam[c0 + ne], l2 = lam[c0 + 2 * (size_t)ne];
+    double dz[3] = {l0, 0.0, 0.0}, dvx[3], dmin[3] = {0, 0, 0}, dmax[3] = {0, 0, 0};
+    dvx[0] = -(1.0 / 6.0) * l1 - 0.5 * l2;
+    dvx[1] = -(1.0 / 6.0) * l1 + 0.5 * l2;
+    dvx[2] = (1.0 / 3.0) * l1;
+    for (int w = 2; w >= 0; --w) {
+      const double s = sgn[w];
+      double dsum = 0.0;  // cotangent of sumdif along the sweep
+      for (int k = 2; k >= 0; --k) {
+        const double dred = -s * dsum - s * dvx[k];
+        if (to_max[w][k]) {
+          if (s > 0) { dvx[k] += dred; dmin[k] -= dred; }
+          else { dmax[k] += dred; dvx[k] -= dred; }
+        } else if (pos[w][k]) {
+          const int d = kd[w][k];
+          dsum += (d <= 1 ? 1.0 : (d == 2 ? 0.5 : 1.0 / 3.0)) * s * dred;
+        }
+      }
+      // sumdif = (vx0 + vx1 + vx2)/3*3 - 3 z0 at the sweep's start
+      for (int a = 0; a < 3; ++a) dvx[a] += dsum;
+      dz[0] -= 3.0 * dsum;
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (clamp[a] == 1) dmax[a] += dvx[a];
+      else if (clamp[a] == 2) dmin[a] += dvx[a];
+      else {
+        dz[0] += dvx[a];
+        dz[1] += cB.phi_corner[a][1] * dvx[a];
+        dz[2] += cB.phi_corner[a][2] * dvx[a];
+      }
+      lb[(size_t)e * 18 + (var * 3 + a) * 2] = dmin[a];
+      lb[(size_t)e * 18 + (var * 3 + a) * 2 + 1] = dmax[a];
+    }
+    lam[c0] = dz[0];
+    lam[c0 + ne] = dz[1];
+    lam[c0 + 2 * (size_t)ne] = dz[2];
+  }
+}
+
+// Per node: the cotangents of its bounds, summed over its star in star order.
+__global__ void node_bound_gather(const MeshView m, const double* __restrict__ lb, double* __restrict__ nb) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= m.np) return;
+  const int ne = m.ne, np = m.np;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int p = m.star_ptr[n]; p < m.star_ptr[n + 1]; ++p) {
+    const int e = m.star[p];
+    const int a = m.nm[e] == n ? 0 : (m.nm[(size_t)ne + e] == n ? 1 : 2);
+    for (int var = 0; var < 3; ++var) {
+      acc[2 * var] += lb[(size_t)e * 18 + (var * 3 + a) * 2];
+      acc[2 * var + 1] += lb[(size_t)e * 18 + (var * 3 + a) * 2 + 1];
+    }
+  }
+  for (int r = 0; r < 6; ++r) nb[(size_t)r * np + n] = acc[r];
+}
+
+// Per element: the node-bound cotangents of the nodes whose min / max it
+// attains, added to its mean (mode 1) of that variable.
+__global__ void elem_bound_scatter(const MeshView m, const int* __restrict__ arg, const double* __restrict__ nb,
+                                   double* __restrict__ lam) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ne = m.ne, np = m.np;
+  if (e >= ne) return;
+  double add[3] = {0, 0, 0};
+  for (int v = 0; v < 3; ++v) {
+    const int n = m.nm[(size_t)v * ne + e];
+    if (v == 1 && n == m.nm[e]) continue;  // a node listed twice counts once
+    if (v == 2 && (n == m.nm[e] || n == m.nm[(size_t)ne + e])) continue;
+    for (int r = 0; r < 6; ++r)
+      if (arg[(size_t)r * np + n] == e) add[r / 2] += nb[(size_t)r * np + n];
+  }
+  for (int var = 0; var < 3; ++var) lam[(size_t)(3 * var) * ne + e] += add[var];
+}
+
+void launch_limit_vjp(const MeshView& m, const double* qpre, double* mm, int* arg, double* lam, double* lb,
+                      double* nb, cudaStream_t s) {
+  const unsigned gn = (unsigned)((m.np + 127) / 128), ge = (unsigned)((m.ne + 127) / 128);
+  node_arg<<<gn, 128, 0, s>>>(m, qpre, mm, arg);
+  limit_vjp<<<ge, 128, 0, s>>>(m, qpre, mm, lam, lb);
+  node_bound_gather<<<gn, 128, 0, s>>>(m, lb, nb);
+  elem_bound_scatter<<<ge, 128, 0, s>>>(m, arg, nb, lam);
 }
 
 // lam_I += a_I lam_j, nu_I += b_I lam_j for I < n, over all 9*NE values

@@ -237,6 +237,14 @@ struct dgswem_cuda {
   // (dgswem_cuda_adjoint_sweep)
   std::vector<DevBuf<double>> adj_stage;
   DevBuf<double> adj_forc;
+  // limiter reverse mode: pre-limiter stage outputs (segment: every x NRK;
+  // step-wise: NRK), node bounds / their elements, bound cotangents
+  std::vector<DevBuf<double>> adj_pre, adj_pre_step;
+  DevBuf<double> adj_mm, adj_lb, adj_nb;
+  DevBuf<int> adj_arg;
+  // when set, launch_stage copies each stage kernel's output (before the
+  // limiter) to keep_pre[irk - 1]
+  double* const* keep_pre = nullptr;
   // gauges: device element, ZE basis values, values / weights; grouped by
   // element (CSR over distinct elements, gauges in input order) for the seed
   int ngauge = 0, ngroup = 0;
@@ -910,6 +918,9 @@ void launch_limit(dgswem_cuda* h, int irk) {
 // into pinned memory and copied with one transfer ahead of its kernels.
 void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
   launch_stage_rhs(h, it, irk, forcing);
+  if (h->keep_pre)
+    DG_CUDA(cudaMemcpyAsync(h->keep_pre[irk - 1], h->q[irk].p, 9 * (size_t)h->ne * sizeof(double),
+                            cudaMemcpyDeviceToDevice, h->stream));
   launch_limit(h, irk);
 }
 
@@ -1082,7 +1093,6 @@ void adjoint_prepare(dgswem_cuda* h) {
   if (h->v == &kMixed) no("the mixed-precision form (FP64 handles only)");
   if (!(h->ph.nleq == 1.0 && h->ph.leq == 0.0)) no("NLEQ=0 (linearised) runs");
   if (h->ph.ics != 1) no("ICS=2");
-  if (h->slopeflag != 0) no("the slope limiter (its frozen-branch adjoint is not built)");
   if (h->nolifa >= 2) no("WETDRY (its frozen-branch adjoint is not built)");
   if (h->nfeds > 0 || h->nreds > 0 || h->mesh.nebseg > 0 || h->mesh.nibseg > 0)
     no("flow, radiation or barrier boundaries");
@@ -1098,6 +1108,14 @@ void adjoint_prepare(dgswem_cuda* h) {
     h->adj_gn.alloc((size_t)h->ne);
     h->adj_ghb.alloc(3 * (size_t)h->ne);
     h->adj_eb.alloc(36 * (size_t)h->ne);
+    if (h->slopeflag != 0) {
+      h->adj_mm.alloc(6 * (size_t)h->np);
+      h->adj_nb.alloc(6 * (size_t)h->np);
+      h->adj_arg.alloc(6 * (size_t)h->np);
+      h->adj_lb.alloc(18 * (size_t)h->ne);
+      h->adj_pre_step.resize(h->nrk);
+      for (auto& b : h->adj_pre_step) b.alloc(n9);
+    }
     // slots of edges in no list are never written: zero once
     DG_CUDA(cudaMemset(h->adj_eb.p, 0, 36 * (size_t)h->ne * sizeof(double)));
     std::vector<unsigned> info(h->ne);
@@ -1121,9 +1139,11 @@ void adjoint_prepare(dgswem_cuda* h) {
 }
 
 // Carry the state cotangent adj_lam[nrk] back through step `it`, whose stage
-// I state is stage[I-1] and stage forcing `forcing` (nrk blocks of
-// forcing_per_stage, or null); adds the step's parameter gradient.
-void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const double* forcing) {
+// I state is stage[I-1], stage forcing `forcing` (nrk blocks of
+// forcing_per_stage, or null) and, with the limiter, stage kernel outputs
+// before the limiter pre[irk-1]; adds the step's parameter gradient.
+void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const double* forcing,
+                    const double* const* pre) {
   const int nrk = h->nrk;
   const size_t n9 = 9 * (size_t)h->ne;
   for (int I = 0; I < nrk; ++I) {
@@ -1153,6 +1173,11 @@ void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const do
     }
     if (j >= 2) {
       const int irk = j - 1;
+      if (h->slopeflag != 0) {  // stage state j is the limited output of stage irk's kernel
+        adj::launch_limit_vjp(h->mesh, pre[irk - 1], h->adj_mm.p, h->adj_arg.p, h->adj_lam[j - 1].p, h->adj_lb.p,
+                              h->adj_nb.p, h->stream);
+        for (int k = 0; k < 4; ++k) check_launch(h, "limit_vjp");
+      }
       SspAdjArgs b{};
       b.lam_j = h->adj_lam[j - 1].p;
       b.n = irk;
@@ -1772,11 +1797,21 @@ int dgswem_cuda_adjoint_step(dgswem_cuda* h, int it) {
     DG_CUDA(cudaSetDevice(h->device));
     // recompute step `it` from the loaded state: stage I's state is q[I-1]
     // (I >= 2) and q[nrk] (I = 1, swapped there at the end of the step)
-    run_steps(h, it, 1);
     const int nrk = h->nrk;
-    std::vector<const double*> st(nrk);
+    std::vector<double*> pre(nrk, nullptr);
+    if (h->slopeflag != 0)
+      for (int I = 0; I < nrk; ++I) pre[I] = h->adj_pre_step[I].p;
+    h->keep_pre = h->slopeflag != 0 ? pre.data() : nullptr;
+    try {
+      run_steps(h, it, 1);
+    } catch (...) {
+      h->keep_pre = nullptr;
+      throw;
+    }
+    h->keep_pre = nullptr;
+    std::vector<const double*> st(nrk), pc(pre.begin(), pre.end());
     for (int I = 1; I <= nrk; ++I) st[I - 1] = I == 1 ? h->q[nrk].p : h->q[I - 1].p;
-    adjoint_stages(h, it, st.data(), h->forcing_per_stage ? h->forcing_dev.p : nullptr);
+    adjoint_stages(h, it, st.data(), h->forcing_per_stage ? h->forcing_dev.p : nullptr, pc.data());
   });
 }
 
@@ -1830,7 +1865,13 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
         if (!b.p) b.alloc(n9);
     }
     if (fstep) h->adj_forc.ensure(fstep * seg_steps);
-    std::vector<const double*> st(nrk);
+    if (h->slopeflag != 0 && h->adj_pre.size() < (size_t)seg_steps * nrk) {
+      h->adj_pre.resize((size_t)seg_steps * nrk);
+      for (auto& b : h->adj_pre)
+        if (!b.p) b.alloc(n9);
+    }
+    std::vector<const double*> st(nrk), pc(nrk, nullptr);
+    std::vector<double*> keep(nrk, nullptr);
     for (int seg = nseg - 1; seg >= 0; --seg) {
       const int k0 = seg * every, k1 = std::min(k0 + every, nsteps);
       // forward over the segment, keeping each step's start state, stage
@@ -1839,7 +1880,17 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
       for (int k = k0; k < k1; ++k) {
         const int j = k - k0;
         save_slot(h, nseg + j);
-        run_steps(h, it0 + k, 1);
+        if (h->slopeflag != 0) {
+          for (int I = 0; I < nrk; ++I) keep[I] = h->adj_pre[(size_t)j * nrk + I].p;
+          h->keep_pre = keep.data();
+        }
+        try {
+          run_steps(h, it0 + k, 1);
+        } catch (...) {
+          h->keep_pre = nullptr;
+          throw;
+        }
+        h->keep_pre = nullptr;
         for (int I = 2; I <= nrk; ++I)
           DG_CUDA(cudaMemcpyAsync(h->adj_stage[(size_t)j * (nrk - 1) + (I - 2)].p, h->q[I - 1].p,
                                   n9 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -1853,7 +1904,9 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
         if (ng > 0) seed_gauges(h, h->w_rec.p + (size_t)(k - 1) * ng);
         st[0] = h->slot_q[nseg + j].p;
         for (int I = 2; I <= nrk; ++I) st[I - 1] = h->adj_stage[(size_t)j * (nrk - 1) + (I - 2)].p;
-        adjoint_stages(h, it0 + k - 1, st.data(), fstep ? h->adj_forc.p + (size_t)j * fstep : nullptr);
+        if (h->slopeflag != 0)
+          for (int I = 0; I < nrk; ++I) pc[I] = h->adj_pre[(size_t)j * nrk + I].p;
+        adjoint_stages(h, it0 + k - 1, st.data(), fstep ? h->adj_forc.p + (size_t)j * fstep : nullptr, pc.data());
       }
     }
     DG_CUDA(cudaStreamSynchronize(h->stream));
@@ -1882,6 +1935,45 @@ int dgswem_cuda_adjoint_read(dgswem_cuda* h, double* g_nbar, double* g_hb, doubl
         if (lam_qy) lam_qy[3 * e + k] = lam[(size_t)(6 + k) * ne + i];
       }
     }
+  });
+}
+
+int dgswem_cuda_limit_state(dgswem_cuda* h) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "limit_state needs the whole mesh (a handle of dgswem_cuda_create)");
+    DG_CUDA(cudaSetDevice(h->device));
+    launch_limit(h, 0);  // the stage path's SLOPELIMITER5 (+ WETDRY) on the current state
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int dgswem_cuda_limiter_vjp(dgswem_cuda* h, const double* lam_ze, const double* lam_qx, const double* lam_qy,
+                            double* out_ze, double* out_qx, double* out_qy) {
+  return guarded([&]() {
+    if (!h || !lam_ze || !lam_qx || !lam_qy || !out_ze || !out_qx || !out_qy)
+      throw Failure(DGSWEM_ERR_ARG, "null argument");
+    if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "limiter_vjp needs the whole mesh");
+    if (h->slopeflag == 0) throw Failure(DGSWEM_ERR_ARG, "the deck has no slope limiter (SLOPEFLAG = 0)");
+    DG_CUDA(cudaSetDevice(h->device));
+    adjoint_prepare(h);
+    const int ne = h->ne;
+    const size_t n9 = 9 * (size_t)ne;
+    std::vector<double> lam(n9);
+    const double* src[3] = {lam_ze, lam_qx, lam_qy};
+    for (int var = 0; var < 3; ++var)
+      for (int i = 0; i < ne; ++i)
+        for (int k = 0; k < 3; ++k) lam[(size_t)(3 * var + k) * ne + i] = src[var][3 * (size_t)h->perm_h[i] + k];
+    DG_CUDA(cudaMemcpy(h->adj_lam[0].p, lam.data(), n9 * sizeof(double), cudaMemcpyHostToDevice));
+    adj::launch_limit_vjp(h->mesh, h->q[0].p, h->adj_mm.p, h->adj_arg.p, h->adj_lam[0].p, h->adj_lb.p, h->adj_nb.p,
+                          h->stream);
+    for (int k = 0; k < 4; ++k) check_launch(h, "limit_vjp");
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    DG_CUDA(cudaMemcpy(lam.data(), h->adj_lam[0].p, n9 * sizeof(double), cudaMemcpyDeviceToHost));
+    double* dst[3] = {out_ze, out_qx, out_qy};
+    for (int var = 0; var < 3; ++var)
+      for (int i = 0; i < ne; ++i)
+        for (int k = 0; k < 3; ++k) dst[var][3 * (size_t)h->perm_h[i] + k] = lam[(size_t)(3 * var + k) * ne + i];
   });
 }
 

@@ -294,6 +294,11 @@ namespace adj {
 void set_basis(const BasisP1& b);
 void launch_rhs_vjp(const AdjArgs& a, cudaStream_t s);
 void launch_ssp_adj(const SspAdjArgs& a, cudaStream_t s);
+// Reverse mode of SLOPELIMITER5 with frozen branches at pre-limiter state
+// qpre: lam (9*NE, in place) from the limited state's cotangent to the
+// pre-limiter state's.  Scratch: mm (6*NP), arg (6*NP), lb (18*NE), nb (6*NP).
+void launch_limit_vjp(const MeshView& m, const double* qpre, double* mm, int* arg, double* lam, double* lb,
+                      double* nb, cudaStream_t s);
 // eta[slot*ng + g] = sum_k phi[g*3+k] * q[k*NE + elem[g]] (ZE at gauge points)
 void launch_gauge_eval(const double* q, int ne, const int* elem, const double* phi, int ng, double* eta,
                        cudaStream_t s);
