@@ -20,8 +20,9 @@ The "ensemble" object is the batched configuration: 256 seeded members of
 5k-200k elements (about 13.5M in all) advanced by one handle in mixed
 precision, with the batched-vs-one-at-a-time rate of its first 16 members.
 The "adjoint" object times the discrete adjoint (gradient of a gauge misfit
-w.r.t. Manning n and bathymetry) against the forward on a 1M-element basin and
-gives its central finite-difference check.
+w.r.t. Manning n and bathymetry) against the forward on the 1M-element wet/dry
+sloping beach, 2000 steps, and gives its central finite-difference check on a
+10k-element smooth subcase.
 """
 from __future__ import annotations
 
@@ -266,22 +267,23 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
 def adjoint_arm(args, device: int) -> dict:
     """Discrete adjoint of the FP64 step (gradient of a 64-gauge elevation
     misfit w.r.t. the element-mean Manning n and the bathymetry modes, sqrt(N)
-    state checkpoints), on an always-wet smooth basin of 998,560 elements --
-    the adjoint covers no limiter and no WETDRY, so the wet/dry sloping beach
-    of the adjoint configuration is replaced by this basin of the same size.
-    Observations: a forward run with Manning n 20 % larger.  Reports the
-    forward and gradient times (CUDA events on the handle's stream, both
-    including the host's per-step gauge reads) and a central finite-difference
-    check on the 10,112-element basin."""
+    state checkpoints, the limiter's and WETDRY's branches frozen at the
+    forward's) on the adjoint configuration: the wet/dry sloping beach of
+    999,040 elements (limiter 5, nodal Manning n), 2000 steps, observations
+    from a forward run with Manning n 20 % larger; the tide is ramped over
+    0.002 days so that the misfit sees it within the run.  Reports the forward
+    and gradient times (CUDA events on the handle's stream, both including the
+    host's gauge reads) and a central finite-difference check on the
+    10,112-element smooth always-wet subcase."""
     import torch
     from dgswem_b200 import Deck, decks
     from dgswem_b200.adjoint import GaugeMisfitProblem, element_manning, locate_gauges
     n = args.adjoint_steps
-    path = decks.smooth_basin(Path(args.workdir) / "adjoint_basin_1M", nx=1580, ny=316, lx=100e3, ly=20e3,
-                              dt=0.25, nsteps=n, dramp=0.005)
+    path = decks.sloping_beach(Path(args.workdir) / "adjoint_beach_1M", nx=1580, ny=316, lx=100e3, ly=20e3,
+                               dt=0.5, nsteps=n, dramp=0.002)
     deck = Deck(path)
     rng = np.random.default_rng(20261203)
-    xy = np.column_stack([rng.uniform(500.0, 4000.0, 64), rng.uniform(1e3, 19e3, 64)])
+    xy = np.column_stack([rng.uniform(500.0, 8000.0, 64), rng.uniform(1e3, 19e3, 64)])
     elem, phi = locate_gauges(deck, xy)
     n0 = element_manning(deck)
     truth = GaugeMisfitProblem(deck, elem, phi, n, device=device)
@@ -337,8 +339,8 @@ def adjoint_arm(args, device: int) -> dict:
     ad = float(g1 @ dn + np.sum(g2 * dh))
     p.close()
     d.close()
-    return {"workload": f"smooth always-wet basin 100x20 km, {ne} elements, FP64, Manning n, 64 gauges, "
-                        f"{n} steps, checkpoints every {math.ceil(math.sqrt(n))} steps",
+    return {"workload": f"wet/dry sloping beach 100x20 km, {ne} elements, FP64, limiter 5, WETDRY, Manning n, "
+                        f"64 gauges, {n} steps, checkpoints every {math.ceil(math.sqrt(n))} steps",
             "steps": n, "forward_ms": ms_f, "gradient_ms": ms_b, "gradient_over_forward": ms_b / ms_f,
             "misfit": j, "grad_norm": {"nbar": float(np.linalg.norm(gn)), "hb": float(np.linalg.norm(ghb))},
             "fd_check": {"elements": 10112, "steps": 300, "eps": eps, "adjoint": ad, "central_fd": fd,
@@ -431,7 +433,7 @@ def main(argv=None):
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=40)
-    ap.add_argument("--adjoint-steps", type=int, default=1000, help="steps of the adjoint arm (0: skip)")
+    ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
     ap.add_argument("--mixed-err-steps", type=int, default=200,
                     help="steps of the mixed-vs-FP64 error comparison")
     args = ap.parse_args(argv)

@@ -15,9 +15,9 @@ sqrt(N) checkpoints plus NRK*sqrt(N) states of one segment.  ``GaugeMisfit``
 wraps both as a ``torch.autograd.Function``.
 
 No counterpart in the reference.  The adjoint covers NLEQ=1, ICS=1, land and
-ocean edges, linear / quadratic / Manning friction and slope limiter 5 with
-its branches frozen at the forward's, without WETDRY
-(``dgswem_cuda_adjoint_begin`` rejects the rest).
+ocean edges, linear / quadratic / Manning friction, slope limiter 5 and WETDRY
+with their branches frozen at the forward's (``dgswem_cuda_adjoint_begin``
+rejects the rest).
 """
 from __future__ import annotations
 

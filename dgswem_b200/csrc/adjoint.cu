@@ -11,10 +11,11 @@
 // Manning floor CF, the friction cap 0.9/DT, the ocean depth-positivity fix).
 //
 // Scope: NLEQ=1 (finite amplitude), ICS=1, land and ocean edges (any other
-// kind is rejected before launch), slope limiter 5 with its branches frozen
-// at the forward's (node_arg .. elem_bound_scatter below), no WETDRY (the
-// host rejects it: its frozen-branch adjoint is not built), linear,
-// quadratic or Manning friction (not hybrid), NWS 0/1.
+// kind is rejected before launch), slope limiter 5 and WETDRY with their
+// branches frozen at the forward's (node_arg .. elem_bound_scatter below;
+// the stage's dry elements lose their volume terms and the dry-side edge
+// rules replay the forward's choice), linear, quadratic or Manning friction
+// (not hybrid), NWS 0/1.
 //
 // Deterministic without atomics: edge_vjp evaluates each edge point once
 // and writes each side's trace cotangents to that element's own slots of a
@@ -98,6 +99,34 @@ __device__ void llf_vjp(const double a[4], const double b[4], double nx, double 
     d[k][2] += dqy;
     d[k][3] += dh;
   }
+}
+
+// Mass flux F of the LLF at traces a (in) and b (ex): the value whose size
+// and sign select internal_edge_hydro.F's dry-side rules.
+__device__ double llf_mass(const double a[4], const double b[4], double nx, double ny, double G) {
+  double eig = 0.0;
+  const double* s[2] = {a, b};
+  for (int k = 0; k < 2; ++k) {
+    const double H = s[k][0] + s[k][3];
+    const double un = (s[k][1] * nx + s[k][2] * ny) / H, c = sqrt(G * H * (ny * ny + nx * nx));
+    eig = fmax(eig, fmax(fabs(un) + c, fabs(un)));
+  }
+  return 0.5 * ((a[1] + b[1]) * nx + (a[2] + b[2]) * ny) - 0.5 * eig * (b[0] - a[0]);
+}
+
+// Momentum (qx, qy) reflected across the edge (normal component negated,
+// tangential kept: land_edge_hydro.F:201-218) and the transpose of that map
+// applied to cotangents (dx, dy), added to (ax, ay).
+__device__ __forceinline__ void reflect(double nx, double ny, double qx, double qy, double& rx, double& ry) {
+  const double tx = -ny, ty = nx, qn = qx * nx + qy * ny, qt = qx * tx + qy * ty;
+  rx = (ty * (-qn) - ny * qt) / (nx * ty - ny * tx);
+  ry = (-tx * (-qn) + nx * qt) / (nx * ty - ny * tx);
+}
+__device__ __forceinline__ void reflect_t(double nx, double ny, double dx, double dy, double& ax, double& ay) {
+  const double tx = -ny, ty = nx, den = 1.0 / (nx * ty - ny * tx);
+  const double dqne = (ty * dx - tx * dy) * den, dqte = (-ny * dx + nx * dy) * den;
+  ax += nx * (-dqne) + tx * dqte;
+  ay += ny * (-dqne) + ty * dqte;
 }
 
 // Reverse mode of the volume fluxes and sources at area point i of element e
@@ -229,27 +258,77 @@ __global__ void __launch_bounds__(256) edge_vjp(const __grid_constant__ AdjArgs 
   const double nx = eg(EGeo::kNx + l, e), ny = eg(EGeo::kNy + l, e);
   if (kind == kInterior) {  // e is the in side
     const int ex = m.link[(size_t)l * ne + e], lx = (int)ei_nled(info, l);
-    double qi[9], qx[9], hi[3], hx[3];
-    for (int c = 0; c < 9; ++c) { qi[c] = A.q[(size_t)c * ne + e]; qx[c] = A.q[(size_t)c * ne + ex]; }
-    for (int k = 0; k < 3; ++k) { hi[k] = m.hb[(size_t)k * ne + e]; hx[k] = m.hb[(size_t)k * ne + ex]; }
-    double ta[4], tb[4], c[3], da[4], db[4];
-    trace(qi, hi, l, I, ta);
-    trace(qx, hx, lx, 2 - I, tb);
-    const double efi = eg(EGeo::kEdfac + l, e), efx = eg(EGeo::kEdfac + lx, ex);
-    for (int v = 0; v < 3; ++v) {
-      double cv = 0.0;
-      for (int k = 0; k < 3; ++k)
-        cv += -efi * cB.edgeq[l][I][k] * A.nu[(size_t)(3 * v + k) * ne + e] +
-              efx * cB.edgeq[lx][2 - I][k] * A.nu[(size_t)(3 * v + k) * ne + ex];
-      c[v] = cv;
-    }
-    llf_vjp(ta, tb, nx, ny, P.g, c, da, db);
     double* oi = A.eb + (size_t)e * 36 + (3 * l + I) * 4;
     double* ox = A.eb + (size_t)ex * 36 + (3 * lx + (2 - I)) * 4;
+    const int wi = A.wd[e], wx = A.wd[ex];
+    double da[4] = {0, 0, 0, 0}, db[4] = {0, 0, 0, 0};
+    if (wi != 0 || wx != 0) {  // an edge between two dry elements adds nothing
+      double qi[9], qx[9], hi[3], hx[3];
+      for (int c = 0; c < 9; ++c) { qi[c] = A.q[(size_t)c * ne + e]; qx[c] = A.q[(size_t)c * ne + ex]; }
+      for (int k = 0; k < 3; ++k) { hi[k] = m.hb[(size_t)k * ne + e]; hx[k] = m.hb[(size_t)k * ne + ex]; }
+      double ta[4], tb[4];
+      trace(qi, hi, l, I, ta);
+      trace(qx, hx, lx, 2 - I, tb);
+      const double efi = eg(EGeo::kEdfac + l, e), efx = eg(EGeo::kEdfac + lx, ex);
+      // cotangents of F, G_in, H_in, G_ex, H_ex (the in side's sums subtract,
+      // the ex side's add)
+      double cF = 0, cGi = 0, cHi = 0, cGx = 0, cHx = 0;
+      for (int k = 0; k < 3; ++k) {
+        const double wi_k = efi * cB.edgeq[l][I][k], wx_k = efx * cB.edgeq[lx][2 - I][k];
+        cF += -wi_k * A.nu[(size_t)k * ne + e] + wx_k * A.nu[(size_t)k * ne + ex];
+        cGi -= wi_k * A.nu[(size_t)(3 + k) * ne + e];
+        cHi -= wi_k * A.nu[(size_t)(6 + k) * ne + e];
+        cGx += wx_k * A.nu[(size_t)(3 + k) * ne + ex];
+        cHx += wx_k * A.nu[(size_t)(6 + k) * ne + ex];
+      }
+      double F0 = 0.0;
+      const bool one_dry = wi == 0 || wx == 0;
+      if (one_dry) F0 = llf_mass(ta, tb, nx, ny, P.g);
+      if (!(one_dry && fabs(F0) > 1.0e-8)) {
+        const double c[3] = {cF, cGi + cGx, cHi + cHx};
+        llf_vjp(ta, tb, nx, ny, P.g, c, da, db);
+      } else {  // internal_edge_hydro.F:212-302 with the forward's choice
+        const bool in_dry = wi == 0;
+        const bool refl = in_dry ? F0 > 0.0 : F0 < 0.0;
+        if (refl) {
+          // the wet side's state on both sides, its momentum reflected on the dry side
+          const double* w = in_dry ? tb : ta;
+          double rx, ry;
+          reflect(nx, ny, w[1], w[2], rx, ry);
+          const double wr[4] = {w[0], rx, ry, w[3]};
+          const double c[3] = {cF, in_dry ? cGx : cGi, in_dry ? cHx : cHi};
+          double dra[4], drb[4];
+          llf_vjp(in_dry ? wr : ta, in_dry ? tb : wr, nx, ny, P.g, c, dra, drb);
+          double* dw = in_dry ? db : da;
+          const double* dref = in_dry ? dra : drb;
+          const double* dself = in_dry ? drb : dra;
+          dw[0] += dself[0] + dref[0];
+          dw[3] += dself[3] + dref[3];
+          dw[1] += dself[1];
+          dw[2] += dself[2];
+          reflect_t(nx, ny, dref[1], dref[2], dw[1], dw[2]);
+        } else {
+          // F and the wet side's momentum flux from the flux at G; the dry
+          // side's momentum flux re-evaluated with G = 0
+          const double cf[3] = {cF, in_dry ? cGx : cGi, in_dry ? cHx : cHi};
+          const double cr[3] = {0.0, in_dry ? cGi : cGx, in_dry ? cHi : cHx};
+          double d1[4], d2[4], d3[4], d4[4];
+          llf_vjp(ta, tb, nx, ny, P.g, cf, d1, d2);
+          llf_vjp(ta, tb, nx, ny, 0.0, cr, d3, d4);
+          for (int k = 0; k < 4; ++k) { da[k] = d1[k] + d3[k]; db[k] = d2[k] + d4[k]; }
+        }
+      }
+    }
     for (int k = 0; k < 4; ++k) { oi[k] = da[k]; ox[k] = db[k]; }
     return;
   }
-  // land or ocean (other kinds are rejected before launch)
+  // land or ocean (other kinds are rejected before launch); a dry element
+  // takes no boundary flux
+  if (A.wd[e] == 0) {
+    double* o = A.eb + (size_t)e * 36 + (3 * l + I) * 4;
+    for (int k = 0; k < 4; ++k) o[k] = 0.0;
+    return;
+  }
   double q[9], hb[3];
   for (int c = 0; c < 9; ++c) q[c] = A.q[(size_t)c * ne + e];
   for (int k = 0; k < 3; ++k) hb[k] = m.hb[(size_t)k * ne + e];
@@ -316,7 +395,8 @@ __global__ void __launch_bounds__(128) elem_vjp(const __grid_constant__ AdjArgs 
   auto eg = [&](int r, int el) { return m.egeo[(size_t)r * ne + el]; };
   const double geo[4] = {eg(EGeo::kDrdx, e), eg(EGeo::kDsdx, e), eg(EGeo::kDrdy, e), eg(EGeo::kDsdy, e)};
   const double nbar = m.manning ? eg(EGeo::kNbar, e) : 0.0;
-  for (int i = 0; i < 3; ++i) {
+  const int nvol = A.wd[e] != 0 ? 3 : 0;  // a dry element has no volume terms
+  for (int i = 0; i < nvol; ++i) {
     double dv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int k = 1; k < 3; ++k) {
       const double dpx = cB.drphi[k][i] * geo[0] + cB.dsphi[k][i] * geo[1];
@@ -388,98 +468,209 @@ __device__ __forceinline__ double div_count(double x, int kdp) {
   return x / 3.0;
 }
 
-// Per element: replay of the limiter on the pre-limiter state q, then its
-// reverse mode.  lam (in place): the cotangent of the limited state on
-// entry, of the pre-limiter state on exit (without the bound terms);
-// lb[e*18 + (var*3 + a)*2 + {0 min, 1 max}]: the cotangent of vertex a's
-// bounds.
-__global__ void __launch_bounds__(128) limit_vjp(const MeshView m, const double* __restrict__ q,
+// Reverse mode of WETDRY (wetdry.F:61-548) for element e with its branches
+// frozen, at its input q (the limited state) and input flag wd_in: lam from
+// the cotangent of WETDRY's output to that of its input; ghb1 / ghb2 += the
+// terms of the flattening (ZE modes 2-3 set to -HB modes 2-3).  The nodal
+// depths DP are constants here.
+__device__ void wetdry_vjp(const MeshView& m, const Physics& ph, int e, int wd_in, const double q[9], double lam[9],
+                           double& ghb1, double& ghb2) {
+  const int ne = m.ne;
+  const double H0 = ph.h0, ZERO = 1.0e-6, c13 = 1.0 / 3.0, c16 = 1.0 / 6.0;
+  double dpn[3];
+  for (int v = 0; v < 3; ++v) dpn[v] = m.dp[m.nm[(size_t)v * ne + e]];
+  const double dpe_min = fmin(fmin(dpn[0], dpn[1]), dpn[2]);
+  int ndry = 0, hmax_i = 0;
+  double hmax = ZERO, ht[3], zn[3];
+  for (int v = 0; v < 3; ++v) {
+    zn[v] = q[0] + cB.phi_corner[v][1] * q[1] + cB.phi_corner[v][2] * q[2];
+    ht[v] = dpn[v] + zn[v];
+    if (ht[v] > hmax) { hmax_i = v; hmax = ht[v]; }
+    if (ht[v] <= H0 + ZERO) ++ndry;
+  }
+  const double dp_avg = c13 * (dpn[0] + dpn[1] + dpn[2]);
+  if (ndry == 0) {
+    if (wd_in == 1) return;  // unchanged
+    // the element check alone: momentum zeroed if the highest vertex is too low
+    if (!(zn[hmax_i] > (-dpe_min + H0)))
+      for (int c = 3; c < 9; ++c) lam[c] = 0.0;
+    return;
+  }
+  const double ht_avg = q[0] + dp_avg;
+  if (ndry == 3 || ht_avg <= H0 + ZERO) {  // flatten: ZE1 = ht_avg - dp_avg, ZE2,3 = -HB2,3, no momentum
+    ghb1 -= lam[1];
+    ghb2 -= lam[2];
+    if (ht_avg < ZERO) lam[0] = 0.0;
+    lam[1] = 0.0;
+    lam[2] = 0.0;
+    for (int c = 3; c < 9; ++c) lam[c] = 0.0;
+    return;
+  }
+  // case 3B: replay, recording the branches
+  int l2h[3] = {0, 1, 2};
+  for (int k1 = 0; k1 < 3; ++k1)
+    for (int k2 = k1; k2 < 3; ++k2)
+      if (ht[l2h[k1]] > ht[l2h[k2]]) { const int t = l2h[k1]; l2h[k1] = l2h[k2]; l2h[k2] = t; }
+  double dh[3];
+  const bool b0 = H0 >= ht[l2h[0]];
+  dh[l2h[0]] = fmax(H0, ht[l2h[0]]) - ht[l2h[0]];
+  const bool b1 = H0 >= ht[l2h[1]] - 0.5 * dh[l2h[0]];
+  dh[l2h[1]] = fmax(H0, ht[l2h[1]] - 0.5 * dh[l2h[0]]) - ht[l2h[1]];
+  dh[l2h[2]] = -dh[l2h[0]] - dh[l2h[1]];
+  int nd2 = 0;
+  double hmax2 = 0.0, hh[3];
+  bool dry[3];
+  for (int v = 0; v < 3; ++v) {
+    hh[v] = ht[v] + dh[v];
+    if (hh[v] > hmax2) { hmax_i = v; hmax2 = hh[v]; }
+    dry[v] = hh[v] <= H0 + 1.0e-10;
+    if (dry[v]) ++nd2;
+  }
+  const bool keep_mom = (hh[hmax_i] - dpn[hmax_i]) > (-dpe_min + H0);
+  // reverse: momentum (rebuilt from wet vertices plus the dry vertices' share)
+  double din[9] = {lam[0], 0, 0, 0, 0, 0, 0, 0, 0};
+  if (keep_mom && nd2 < 3) {
+    for (int w = 0; w < 2; ++w) {  // QX modes 3..5, QY modes 6..8
+      const double* dq = lam + 3 + 3 * w;
+      const double dqh[3] = {c13 * dq[0] - c16 * dq[1] - 0.5 * dq[2], c13 * dq[0] - c16 * dq[1] + 0.5 * dq[2],
+                             c13 * dq[0] + c13 * dq[1]};
+      double ds = 0.0;
+      for (int v = 0; v < 3; ++v)
+        if (!dry[v]) ds += dqh[v];
+      for (int v = 0; v < 3; ++v) {
+        const double dn = dry[v] ? ds / (3.0 - (double)nd2) : dqh[v];
+        din[3 + 3 * w] += dn;
+        din[4 + 3 * w] += cB.phi_corner[v][1] * dn;
+        din[5 + 3 * w] += cB.phi_corner[v][2] * dn;
+      }
+    }
+  }
+  // elevation: ZE2,3 from the vertex elevations hh - DP, ZE1 kept
+  const double dzh[3] = {-c16 * lam[1] - 0.5 * lam[2], -c16 * lam[1] + 0.5 * lam[2], c13 * lam[1]};
+  double dht[3], ddh[3];
+  for (int v = 0; v < 3; ++v) { dht[v] = dzh[v]; ddh[v] = dzh[v]; }
+  ddh[l2h[0]] -= ddh[l2h[2]];
+  ddh[l2h[1]] -= ddh[l2h[2]];
+  if (b1) dht[l2h[1]] -= ddh[l2h[1]];
+  else ddh[l2h[0]] += -0.5 * ddh[l2h[1]];
+  if (b0) dht[l2h[0]] -= ddh[l2h[0]];
+  for (int v = 0; v < 3; ++v) {
+    din[0] += dht[v];
+    din[1] += cB.phi_corner[v][1] * dht[v];
+    din[2] += cB.phi_corner[v][2] * dht[v];
+  }
+  for (int c = 0; c < 9; ++c) lam[c] = din[c];
+}
+
+// Per element: replay of the limiter (slopeflag) and WETDRY (wetdry) on the
+// pre-limiter state q, then their reverse modes.  lam (in place): the
+// cotangent of the stage state on entry, of the pre-limiter state on exit
+// (without the bound terms); lb[e*18 + (var*3 + a)*2 + {0 min, 1 max}]: the
+// cotangent of vertex a's bounds; g_hb += WETDRY's HB terms.
+__global__ void __launch_bounds__(128) limit_vjp(const MeshView m, const Physics ph, int slopeflag, int wetdry,
+                                                 const int* __restrict__ wd, const double* __restrict__ q,
                                                  const double* __restrict__ mm, double* __restrict__ lam,
-                                                 double* __restrict__ lb) {
+                                                 double* __restrict__ lb, double* __restrict__ g_hb) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const int ne = m.ne, np = m.np;
   if (e >= ne) return;
   int nd[3];
   for (int v = 0; v < 3; ++v) nd[v] = m.nm[(size_t)v * ne + e];
-  for (int var = 0; var < 3; ++var) {
-    double z[3];
-    for (int k = 0; k < 3; ++k) z[k] = q[(size_t)(3 * var + k) * ne + e];
-    double vmin[3], vmax[3], vx[3];
-    int clamp[3];  // 0 none, 1 to max, 2 to min
-    for (int a = 0; a < 3; ++a) {
-      vmin[a] = mm[(size_t)(2 * var) * np + nd[a]];
-      vmax[a] = mm[(size_t)(2 * var + 1) * np + nd[a]];
-      const double v = z[0] + cB.phi_corner[a][1] * z[1] + cB.phi_corner[a][2] * z[2];
-      const double c1 = fmin(v, vmax[a]);
-      vx[a] = fmax(c1, vmin[a]);
-      clamp[a] = vx[a] != c1 ? 2 : (c1 != v ? 1 : 0);
-    }
-    // forward sweeps, recording the decisions
-    double sgn[3];
-    bool pos[3][3], to_max[3][3];
-    int kd[3][3];
-    for (int w = 0; w < 3; ++w) {
-      const double sumloc = (vx[0] + vx[1] + vx[2]) / 3.0;
-      double sumdif = (sumloc - z[0]) * 3.0;
-      const double s = copysign(1.0, sumdif);
-      sgn[w] = s;
-      double dif[3];
-      for (int a = 0; a < 3; ++a) dif[a] = (vx[a] - z[0]) * s;
-      int kdp = (dif[0] > 0) + (dif[1] > 0) + (dif[2] > 0);
-      for (int k = 0; k < 3; ++k) {
-        double redfac = 0.0;
-        pos[w][k] = dif[k] > 0;
-        kd[w][k] = kdp;
-        if (pos[w][k]) {
-          redfac = div_count(sumdif * s, kdp);
-          kdp = kdp - 1;
-        }
-        const double redmax = s > 0 ? vx[k] - vmin[k] : vmax[k] - vx[k];
-        to_max[w][k] = !(redfac <= redmax);  // fmin(redfac, redmax) took redmax
-        redfac = fmin(redfac, redmax);
-        sumdif = sumdif - redfac * s;
-        vx[k] = vx[k] - redfac * s;
-      }
-    }
-    // reverse: outputs z0 (kept), z1, z2 from vx
-    const size_t c0 = (size_t)(3 * var) * ne + e;
-    const double l0 = lam[c0], l1 = lam[c0 + ne], l2 = lam[c0 + 2 * (size_t)ne];
-    double dz[3] = {l0, 0.0, 0.0}, dvx[3], dmin[3] = {0, 0, 0}, dmax[3] = {0, 0, 0};
-    dvx[0] = -(1.0 / 6.0) * l1 - 0.5 * l2;
-    dvx[1] = -(1.0 / 6.0) * l1 + 0.5 * l2;
-    dvx[2] = (1.0 / 3.0) * l1;
-    for (int w = 2; w >= 0; --w) {
-      const double s = sgn[w];
-      double dsum = 0.0;  // cotangent of sumdif along the sweep
-      for (int k = 2; k >= 0; --k) {
-        const double dred = -s * dsum - s * dvx[k];
-        if (to_max[w][k]) {
-          if (s > 0) { dvx[k] += dred; dmin[k] -= dred; }
-          else { dmax[k] += dred; dvx[k] -= dred; }
-        } else if (pos[w][k]) {
-          const int d = kd[w][k];
-          dsum += (d <= 1 ? 1.0 : (d == 2 ? 0.5 : 1.0 / 3.0)) * s * dred;
-        }
-      }
-      // sumdif = (vx0 + vx1 + vx2)/3*3 - 3 z0 at the sweep's start
-      for (int a = 0; a < 3; ++a) dvx[a] += dsum;
-      dz[0] -= 3.0 * dsum;
-    }
-    for (int a = 0; a < 3; ++a) {
-      if (clamp[a] == 1) dmax[a] += dvx[a];
-      else if (clamp[a] == 2) dmin[a] += dvx[a];
-      else {
-        dz[0] += dvx[a];
-        dz[1] += cB.phi_corner[a][1] * dvx[a];
-        dz[2] += cB.phi_corner[a][2] * dvx[a];
-      }
-      lb[(size_t)e * 18 + (var * 3 + a) * 2] = dmin[a];
-      lb[(size_t)e * 18 + (var * 3 + a) * 2 + 1] = dmax[a];
-    }
-    lam[c0] = dz[0];
-    lam[c0 + ne] = dz[1];
-    lam[c0 + 2 * (size_t)ne] = dz[2];
+  double ql[9], l9[9];
+  for (int c = 0; c < 9; ++c) {
+    ql[c] = q[(size_t)c * ne + e];
+    l9[c] = lam[(size_t)c * ne + e];
   }
+  // limiter replay, keeping its decisions
+  int clamp[3][3];
+  double sgn[3][3];
+  bool pos[3][3][3], to_max[3][3][3];
+  int kd[3][3][3];
+  if (slopeflag != 0) {
+    for (int var = 0; var < 3; ++var) {
+      const double* z = ql + 3 * var;
+      double vmin[3], vmax[3], vx[3];
+      for (int a = 0; a < 3; ++a) {
+        vmin[a] = mm[(size_t)(2 * var) * np + nd[a]];
+        vmax[a] = mm[(size_t)(2 * var + 1) * np + nd[a]];
+        const double v = z[0] + cB.phi_corner[a][1] * z[1] + cB.phi_corner[a][2] * z[2];
+        const double c1 = fmin(v, vmax[a]);
+        vx[a] = fmax(c1, vmin[a]);
+        clamp[var][a] = vx[a] != c1 ? 2 : (c1 != v ? 1 : 0);
+      }
+      for (int w = 0; w < 3; ++w) {
+        const double sumloc = (vx[0] + vx[1] + vx[2]) / 3.0;
+        double sumdif = (sumloc - z[0]) * 3.0;
+        const double s = copysign(1.0, sumdif);
+        sgn[var][w] = s;
+        double dif[3];
+        for (int a = 0; a < 3; ++a) dif[a] = (vx[a] - z[0]) * s;
+        int kdp = (dif[0] > 0) + (dif[1] > 0) + (dif[2] > 0);
+        for (int k = 0; k < 3; ++k) {
+          double redfac = 0.0;
+          pos[var][w][k] = dif[k] > 0;
+          kd[var][w][k] = kdp;
+          if (pos[var][w][k]) {
+            redfac = div_count(sumdif * s, kdp);
+            kdp = kdp - 1;
+          }
+          const double redmax = s > 0 ? vx[k] - vmin[k] : vmax[k] - vx[k];
+          to_max[var][w][k] = !(redfac <= redmax);
+          redfac = fmin(redfac, redmax);
+          sumdif = sumdif - redfac * s;
+          vx[k] = vx[k] - redfac * s;
+        }
+      }
+      ql[3 * var + 1] = -(1.0 / 6.0 * (vx[0] + vx[1])) + 1.0 / 3.0 * vx[2];
+      ql[3 * var + 2] = -(.5 * vx[0]) + .5 * vx[1];
+    }
+  }
+  if (wetdry != 0) {
+    double g1 = 0.0, g2 = 0.0;
+    wetdry_vjp(m, ph, e, wd[e], ql, l9, g1, g2);
+    g_hb[(size_t)ne + e] += g1;
+    g_hb[(size_t)2 * ne + e] += g2;
+  }
+  if (slopeflag != 0) {
+    for (int var = 0; var < 3; ++var) {
+      const double l0 = l9[3 * var], l1 = l9[3 * var + 1], l2 = l9[3 * var + 2];
+      double dz[3] = {l0, 0.0, 0.0}, dvx[3], dmin[3] = {0, 0, 0}, dmax[3] = {0, 0, 0};
+      dvx[0] = -(1.0 / 6.0) * l1 - 0.5 * l2;
+      dvx[1] = -(1.0 / 6.0) * l1 + 0.5 * l2;
+      dvx[2] = (1.0 / 3.0) * l1;
+      for (int w = 2; w >= 0; --w) {
+        const double s = sgn[var][w];
+        double dsum = 0.0;  // cotangent of sumdif along the sweep
+        for (int k = 2; k >= 0; --k) {
+          const double dred = -s * dsum - s * dvx[k];
+          if (to_max[var][w][k]) {
+            if (s > 0) { dvx[k] += dred; dmin[k] -= dred; }
+            else { dmax[k] += dred; dvx[k] -= dred; }
+          } else if (pos[var][w][k]) {
+            const int d = kd[var][w][k];
+            dsum += (d <= 1 ? 1.0 : (d == 2 ? 0.5 : 1.0 / 3.0)) * s * dred;
+          }
+        }
+        for (int a = 0; a < 3; ++a) dvx[a] += dsum;  // sumdif = vx0 + vx1 + vx2 - 3 z0 at the sweep's start
+        dz[0] -= 3.0 * dsum;
+      }
+      for (int a = 0; a < 3; ++a) {
+        if (clamp[var][a] == 1) dmax[a] += dvx[a];
+        else if (clamp[var][a] == 2) dmin[a] += dvx[a];
+        else {
+          dz[0] += dvx[a];
+          dz[1] += cB.phi_corner[a][1] * dvx[a];
+          dz[2] += cB.phi_corner[a][2] * dvx[a];
+        }
+        lb[(size_t)e * 18 + (var * 3 + a) * 2] = dmin[a];
+        lb[(size_t)e * 18 + (var * 3 + a) * 2 + 1] = dmax[a];
+      }
+      l9[3 * var] = dz[0];
+      l9[3 * var + 1] = dz[1];
+      l9[3 * var + 2] = dz[2];
+    }
+  }
+  for (int c = 0; c < 9; ++c) lam[(size_t)c * ne + e] = l9[c];
 }
 
 // Per node: the cotangents of its bounds, summed over its star in star order.
@@ -517,20 +708,31 @@ __global__ void elem_bound_scatter(const MeshView m, const int* __restrict__ arg
   for (int var = 0; var < 3; ++var) lam[(size_t)(3 * var) * ne + e] += add[var];
 }
 
-void launch_limit_vjp(const MeshView& m, const double* qpre, double* mm, int* arg, double* lam, double* lb,
-                      double* nb, cudaStream_t s) {
+void launch_limit_vjp(const MeshView& m, const Physics& ph, int slopeflag, int wetdry, const int* wd,
+                      const double* qpre, double* mm, int* arg, double* lam, double* lb, double* nb, double* g_hb,
+                      cudaStream_t s) {
   const unsigned gn = (unsigned)((m.np + 127) / 128), ge = (unsigned)((m.ne + 127) / 128);
-  node_arg<<<gn, 128, 0, s>>>(m, qpre, mm, arg);
-  limit_vjp<<<ge, 128, 0, s>>>(m, qpre, mm, lam, lb);
-  node_bound_gather<<<gn, 128, 0, s>>>(m, lb, nb);
-  elem_bound_scatter<<<ge, 128, 0, s>>>(m, arg, nb, lam);
+  if (slopeflag != 0) node_arg<<<gn, 128, 0, s>>>(m, qpre, mm, arg);
+  limit_vjp<<<ge, 128, 0, s>>>(m, ph, slopeflag, wetdry, wd, qpre, mm, lam, lb, g_hb);
+  if (slopeflag != 0) {
+    node_bound_gather<<<gn, 128, 0, s>>>(m, lb, nb);
+    elem_bound_scatter<<<ge, 128, 0, s>>>(m, arg, nb, lam);
+  }
 }
 
 // lam_I += a_I lam_j, nu_I += b_I lam_j for I < n, over all 9*NE values
+// (first: lam_I = a_I lam_j, nu_I = b_I lam_j)
 __global__ void ssp_adj(const __grid_constant__ SspAdjArgs A) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.len) return;
   const double l = A.lam_j[i];
+  if (A.first) {
+    for (int I = 0; I < A.n; ++I) {
+      A.lam[I][i] = A.a[I] != 0.0 ? A.a[I] * l : 0.0;
+      A.nu[I][i] = A.b[I] != 0.0 ? A.b[I] * l : 0.0;
+    }
+    return;
+  }
   for (int I = 0; I < A.n; ++I) {
     if (A.a[I] != 0.0) A.lam[I][i] += A.a[I] * l;
     if (A.b[I] != 0.0) A.nu[I][i] += A.b[I] * l;

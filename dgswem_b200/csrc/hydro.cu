@@ -245,6 +245,10 @@ struct dgswem_cuda {
   // when set, launch_stage copies each stage kernel's output (before the
   // limiter) to keep_pre[irk - 1]
   double* const* keep_pre = nullptr;
+  // when set, launch_stage copies WDFLG as each stage kernel reads it to
+  // keep_wd[irk - 1]
+  int* const* keep_wd = nullptr;
+  std::vector<DevBuf<int>> adj_wd, adj_wd_step;  // per segment step x NRK / per NRK
   // gauges: device element, ZE basis values, values / weights; grouped by
   // element (CSR over distinct elements, gauges in input order) for the seed
   int ngauge = 0, ngroup = 0;
@@ -917,6 +921,9 @@ void launch_limit(dgswem_cuda* h, int irk) {
 // Steps it0 .. it0+n-1: the host forcing of each chunk of steps is computed
 // into pinned memory and copied with one transfer ahead of its kernels.
 void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
+  if (h->keep_wd)
+    DG_CUDA(cudaMemcpyAsync(h->keep_wd[irk - 1], h->wd.p, (size_t)h->ne * sizeof(int), cudaMemcpyDeviceToDevice,
+                            h->stream));
   launch_stage_rhs(h, it, irk, forcing);
   if (h->keep_pre)
     DG_CUDA(cudaMemcpyAsync(h->keep_pre[irk - 1], h->q[irk].p, 9 * (size_t)h->ne * sizeof(double),
@@ -1093,7 +1100,6 @@ void adjoint_prepare(dgswem_cuda* h) {
   if (h->v == &kMixed) no("the mixed-precision form (FP64 handles only)");
   if (!(h->ph.nleq == 1.0 && h->ph.leq == 0.0)) no("NLEQ=0 (linearised) runs");
   if (h->ph.ics != 1) no("ICS=2");
-  if (h->nolifa >= 2) no("WETDRY (its frozen-branch adjoint is not built)");
   if (h->nfeds > 0 || h->nreds > 0 || h->mesh.nebseg > 0 || h->mesh.nibseg > 0)
     no("flow, radiation or barrier boundaries");
   if (h->ph.iflinbf == 0 && h->ph.ifhybf == 1) no("hybrid friction");
@@ -1108,7 +1114,7 @@ void adjoint_prepare(dgswem_cuda* h) {
     h->adj_gn.alloc((size_t)h->ne);
     h->adj_ghb.alloc(3 * (size_t)h->ne);
     h->adj_eb.alloc(36 * (size_t)h->ne);
-    if (h->slopeflag != 0) {
+    if (h->slopeflag != 0 || h->nolifa >= 2) {
       h->adj_mm.alloc(6 * (size_t)h->np);
       h->adj_nb.alloc(6 * (size_t)h->np);
       h->adj_arg.alloc(6 * (size_t)h->np);
@@ -1116,6 +1122,8 @@ void adjoint_prepare(dgswem_cuda* h) {
       h->adj_pre_step.resize(h->nrk);
       for (auto& b : h->adj_pre_step) b.alloc(n9);
     }
+    h->adj_wd_step.resize(h->nrk);
+    for (auto& b : h->adj_wd_step) b.alloc((size_t)h->ne);
     // slots of edges in no list are never written: zero once
     DG_CUDA(cudaMemset(h->adj_eb.p, 0, 36 * (size_t)h->ne * sizeof(double)));
     std::vector<unsigned> info(h->ne);
@@ -1143,13 +1151,11 @@ void adjoint_prepare(dgswem_cuda* h) {
 // forcing_per_stage, or null) and, with the limiter, stage kernel outputs
 // before the limiter pre[irk-1]; adds the step's parameter gradient.
 void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const double* forcing,
-                    const double* const* pre) {
+                    const double* const* pre, const int* const* wdst) {
+  const bool limits = h->slopeflag != 0 || h->nolifa >= 2;
   const int nrk = h->nrk;
   const size_t n9 = 9 * (size_t)h->ne;
-  for (int I = 0; I < nrk; ++I) {
-    DG_CUDA(cudaMemsetAsync(h->adj_lam[I].p, 0, n9 * sizeof(double), h->stream));
-    DG_CUDA(cudaMemsetAsync(h->adj_nu[I].p, 0, n9 * sizeof(double), h->stream));
-  }
+  // the pass of j = nrk+1 assigns every lam_I / nu_I, I <= nrk (no zeroing)
   for (int j = nrk + 1; j >= 1; --j) {
     if (j <= nrk) {
       AdjArgs a{};
@@ -1165,6 +1171,7 @@ void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const do
       a.eb = h->adj_eb.p;
       a.edges = h->adj_edges.p;
       a.nedge = h->adj_nedge;
+      a.wd = wdst[j - 1];
       double timedg;
       stage_clock(h, it, j, &timedg, &a.rampdg);
       adj::launch_rhs_vjp(a, h->stream);
@@ -1173,14 +1180,16 @@ void adjoint_stages(dgswem_cuda* h, int it, const double* const* stage, const do
     }
     if (j >= 2) {
       const int irk = j - 1;
-      if (h->slopeflag != 0) {  // stage state j is the limited output of stage irk's kernel
-        adj::launch_limit_vjp(h->mesh, pre[irk - 1], h->adj_mm.p, h->adj_arg.p, h->adj_lam[j - 1].p, h->adj_lb.p,
-                              h->adj_nb.p, h->stream);
-        for (int k = 0; k < 4; ++k) check_launch(h, "limit_vjp");
+      if (limits) {  // stage state j is the limited / wet-dried output of stage irk's kernel
+        adj::launch_limit_vjp(h->mesh, h->ph, h->slopeflag, h->nolifa >= 2 ? 1 : 0, wdst[irk - 1], pre[irk - 1],
+                              h->adj_mm.p, h->adj_arg.p, h->adj_lam[j - 1].p, h->adj_lb.p, h->adj_nb.p,
+                              h->adj_ghb.p, h->stream);
+        for (int k = 0; k < (h->slopeflag != 0 ? 4 : 1); ++k) check_launch(h, "limit_vjp");
       }
       SspAdjArgs b{};
       b.lam_j = h->adj_lam[j - 1].p;
       b.n = irk;
+      b.first = j == nrk + 1;
       b.len = (long long)n9;
       for (int I = 1; I <= irk; ++I) {
         b.lam[I - 1] = h->adj_lam[I - 1].p;
@@ -1798,20 +1807,28 @@ int dgswem_cuda_adjoint_step(dgswem_cuda* h, int it) {
     // recompute step `it` from the loaded state: stage I's state is q[I-1]
     // (I >= 2) and q[nrk] (I = 1, swapped there at the end of the step)
     const int nrk = h->nrk;
+    const bool limits = h->slopeflag != 0 || h->nolifa >= 2;
     std::vector<double*> pre(nrk, nullptr);
-    if (h->slopeflag != 0)
-      for (int I = 0; I < nrk; ++I) pre[I] = h->adj_pre_step[I].p;
-    h->keep_pre = h->slopeflag != 0 ? pre.data() : nullptr;
+    std::vector<int*> wdk(nrk, nullptr);
+    for (int I = 0; I < nrk; ++I) {
+      if (limits) pre[I] = h->adj_pre_step[I].p;
+      wdk[I] = h->adj_wd_step[I].p;
+    }
+    h->keep_pre = limits ? pre.data() : nullptr;
+    h->keep_wd = wdk.data();
     try {
       run_steps(h, it, 1);
     } catch (...) {
       h->keep_pre = nullptr;
+      h->keep_wd = nullptr;
       throw;
     }
     h->keep_pre = nullptr;
+    h->keep_wd = nullptr;
     std::vector<const double*> st(nrk), pc(pre.begin(), pre.end());
+    std::vector<const int*> wc(wdk.begin(), wdk.end());
     for (int I = 1; I <= nrk; ++I) st[I - 1] = I == 1 ? h->q[nrk].p : h->q[I - 1].p;
-    adjoint_stages(h, it, st.data(), h->forcing_per_stage ? h->forcing_dev.p : nullptr, pc.data());
+    adjoint_stages(h, it, st.data(), h->forcing_per_stage ? h->forcing_dev.p : nullptr, pc.data(), wc.data());
   });
 }
 
@@ -1865,13 +1882,21 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
         if (!b.p) b.alloc(n9);
     }
     if (fstep) h->adj_forc.ensure(fstep * seg_steps);
-    if (h->slopeflag != 0 && h->adj_pre.size() < (size_t)seg_steps * nrk) {
+    const bool limits = h->slopeflag != 0 || h->nolifa >= 2;
+    if (limits && h->adj_pre.size() < (size_t)seg_steps * nrk) {
       h->adj_pre.resize((size_t)seg_steps * nrk);
       for (auto& b : h->adj_pre)
         if (!b.p) b.alloc(n9);
     }
+    if (h->adj_wd.size() < (size_t)seg_steps * nrk) {
+      h->adj_wd.resize((size_t)seg_steps * nrk);
+      for (auto& b : h->adj_wd)
+        if (!b.p) b.alloc((size_t)h->ne);
+    }
     std::vector<const double*> st(nrk), pc(nrk, nullptr);
+    std::vector<const int*> wc(nrk, nullptr);
     std::vector<double*> keep(nrk, nullptr);
+    std::vector<int*> keepw(nrk, nullptr);
     for (int seg = nseg - 1; seg >= 0; --seg) {
       const int k0 = seg * every, k1 = std::min(k0 + every, nsteps);
       // forward over the segment, keeping each step's start state, stage
@@ -1880,17 +1905,21 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
       for (int k = k0; k < k1; ++k) {
         const int j = k - k0;
         save_slot(h, nseg + j);
-        if (h->slopeflag != 0) {
-          for (int I = 0; I < nrk; ++I) keep[I] = h->adj_pre[(size_t)j * nrk + I].p;
-          h->keep_pre = keep.data();
+        for (int I = 0; I < nrk; ++I) {
+          if (limits) keep[I] = h->adj_pre[(size_t)j * nrk + I].p;
+          keepw[I] = h->adj_wd[(size_t)j * nrk + I].p;
         }
+        h->keep_pre = limits ? keep.data() : nullptr;
+        h->keep_wd = keepw.data();
         try {
           run_steps(h, it0 + k, 1);
         } catch (...) {
           h->keep_pre = nullptr;
+          h->keep_wd = nullptr;
           throw;
         }
         h->keep_pre = nullptr;
+        h->keep_wd = nullptr;
         for (int I = 2; I <= nrk; ++I)
           DG_CUDA(cudaMemcpyAsync(h->adj_stage[(size_t)j * (nrk - 1) + (I - 2)].p, h->q[I - 1].p,
                                   n9 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -1904,9 +1933,12 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
         if (ng > 0) seed_gauges(h, h->w_rec.p + (size_t)(k - 1) * ng);
         st[0] = h->slot_q[nseg + j].p;
         for (int I = 2; I <= nrk; ++I) st[I - 1] = h->adj_stage[(size_t)j * (nrk - 1) + (I - 2)].p;
-        if (h->slopeflag != 0)
-          for (int I = 0; I < nrk; ++I) pc[I] = h->adj_pre[(size_t)j * nrk + I].p;
-        adjoint_stages(h, it0 + k - 1, st.data(), fstep ? h->adj_forc.p + (size_t)j * fstep : nullptr, pc.data());
+        for (int I = 0; I < nrk; ++I) {
+          if (limits) pc[I] = h->adj_pre[(size_t)j * nrk + I].p;
+          wc[I] = h->adj_wd[(size_t)j * nrk + I].p;
+        }
+        adjoint_stages(h, it0 + k - 1, st.data(), fstep ? h->adj_forc.p + (size_t)j * fstep : nullptr, pc.data(),
+                       wc.data());
       }
     }
     DG_CUDA(cudaStreamSynchronize(h->stream));
@@ -1954,7 +1986,8 @@ int dgswem_cuda_limiter_vjp(dgswem_cuda* h, const double* lam_ze, const double* 
     if (!h || !lam_ze || !lam_qx || !lam_qy || !out_ze || !out_qx || !out_qy)
       throw Failure(DGSWEM_ERR_ARG, "null argument");
     if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "limiter_vjp needs the whole mesh");
-    if (h->slopeflag == 0) throw Failure(DGSWEM_ERR_ARG, "the deck has no slope limiter (SLOPEFLAG = 0)");
+    if (h->slopeflag == 0 && h->nolifa < 2)
+      throw Failure(DGSWEM_ERR_ARG, "the deck has neither the slope limiter nor WETDRY");
     DG_CUDA(cudaSetDevice(h->device));
     adjoint_prepare(h);
     const int ne = h->ne;
@@ -1965,9 +1998,9 @@ int dgswem_cuda_limiter_vjp(dgswem_cuda* h, const double* lam_ze, const double* 
       for (int i = 0; i < ne; ++i)
         for (int k = 0; k < 3; ++k) lam[(size_t)(3 * var + k) * ne + i] = src[var][3 * (size_t)h->perm_h[i] + k];
     DG_CUDA(cudaMemcpy(h->adj_lam[0].p, lam.data(), n9 * sizeof(double), cudaMemcpyHostToDevice));
-    adj::launch_limit_vjp(h->mesh, h->q[0].p, h->adj_mm.p, h->adj_arg.p, h->adj_lam[0].p, h->adj_lb.p, h->adj_nb.p,
-                          h->stream);
-    for (int k = 0; k < 4; ++k) check_launch(h, "limit_vjp");
+    adj::launch_limit_vjp(h->mesh, h->ph, h->slopeflag, h->nolifa >= 2 ? 1 : 0, h->wd.p, h->q[0].p, h->adj_mm.p,
+                          h->adj_arg.p, h->adj_lam[0].p, h->adj_lb.p, h->adj_nb.p, h->adj_ghb.p, h->stream);
+    for (int k = 0; k < (h->slopeflag != 0 ? 4 : 1); ++k) check_launch(h, "limit_vjp");
     DG_CUDA(cudaStreamSynchronize(h->stream));
     DG_CUDA(cudaMemcpy(lam.data(), h->adj_lam[0].p, n9 * sizeof(double), cudaMemcpyDeviceToHost));
     double* dst[3] = {out_ze, out_qx, out_qy};

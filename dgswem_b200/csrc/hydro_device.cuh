@@ -279,6 +279,7 @@ struct AdjArgs {
   double* eb;                           // 36*NE scratch: edge-point trace cotangents
   const int* __restrict__ edges;        // (element, local edge) pairs: interior edges from the in side, boundary edges
   int nedge;
+  const int* __restrict__ wd;           // WDFLG the stage kernel read (dry elements: no volume terms, dry-side edge rules)
 };
 // One stage of the reverse SSP-RK accumulation: lam_I += a_I lam_j and
 // nu_I += b_I lam_j for I < n (b_I already times DT).
@@ -288,17 +289,21 @@ struct SspAdjArgs {
   double* nu[kMaxStages];
   double a[kMaxStages], b[kMaxStages];
   int n;
+  int first;  // the step's first pass (j = NRK+1): assign instead of add (no zeroing beforehand)
   long long len;
 };
 namespace adj {
 void set_basis(const BasisP1& b);
 void launch_rhs_vjp(const AdjArgs& a, cudaStream_t s);
 void launch_ssp_adj(const SspAdjArgs& a, cudaStream_t s);
-// Reverse mode of SLOPELIMITER5 with frozen branches at pre-limiter state
-// qpre: lam (9*NE, in place) from the limited state's cotangent to the
-// pre-limiter state's.  Scratch: mm (6*NP), arg (6*NP), lb (18*NE), nb (6*NP).
-void launch_limit_vjp(const MeshView& m, const double* qpre, double* mm, int* arg, double* lam, double* lb,
-                      double* nb, cudaStream_t s);
+// Reverse mode of the stage's SLOPELIMITER5 (slopeflag) and WETDRY (wetdry)
+// with frozen branches at pre-limiter state qpre and input flags wd: lam
+// (9*NE, in place) from the cotangent of the limited / wet-dried state to
+// the pre-limiter state's; g_hb += the HB terms of WETDRY's flattening.
+// Scratch: mm (6*NP), arg (6*NP), lb (18*NE), nb (6*NP).
+void launch_limit_vjp(const MeshView& m, const Physics& ph, int slopeflag, int wetdry, const int* wd,
+                      const double* qpre, double* mm, int* arg, double* lam, double* lb, double* nb, double* g_hb,
+                      cudaStream_t s);
 // eta[slot*ng + g] = sum_k phi[g*3+k] * q[k*NE + elem[g]] (ZE at gauge points)
 void launch_gauge_eval(const double* q, int ne, const int* elem, const double* phi, int ng, double* eta,
                        cudaStream_t s);

@@ -265,8 +265,8 @@ int dgswem_cuda_last_error(char* buf, int buflen);
  * evaluates ZE of the current state there.
  *
  * Discrete adjoint of DG_HYDRO_TIMESTEP (NLEQ=1, ICS=1, land and ocean
- * edges, slope limiter 5 with its branches frozen at the forward's, no
- * WETDRY, linear / quadratic / Manning friction; DGSWEM_ERR_ARG otherwise;
+ * edges, slope limiter 5 and WETDRY with their branches frozen at the
+ * forward's, linear / quadratic / Manning friction; DGSWEM_ERR_ARG otherwise;
  * FP64 handles only):
  *   dgswem_cuda_adjoint_begin   zero the state cotangent and the gradients
  *   dgswem_cuda_adjoint_seed    add w[g] * dZE(gauge g)/dq to the cotangent of
@@ -300,12 +300,13 @@ int dgswem_cuda_adjoint_read(dgswem_cuda* h, double* g_nbar, double* g_hb, doubl
  * from nseg on, and `every` x (NRK-1) stage buffers), then steps back.
  * Read the result with dgswem_cuda_adjoint_read. */
 int dgswem_cuda_misfit_forward(dgswem_cuda* h, int it0, int nsteps, int every, double* eta);
-/* Building blocks of the limiter's reverse mode.  dgswem_cuda_limit_state
- * applies the stage path's SLOPELIMITER5 (and WETDRY when on) to the current
- * state in place.  dgswem_cuda_limiter_vjp returns, at the current state as
- * the limiter's input, the transpose of the limiter with its branches frozen
- * applied to the cotangents lam_* of its output (ZE/QX/QY(DOFH,NE) in, the
- * same layout out); needs SLOPEFLAG != 0 and the adjoint's scope. */
+/* Building blocks of the reverse mode.  dgswem_cuda_limit_state applies the
+ * stage path's SLOPELIMITER5 and WETDRY (those the deck turns on) to the
+ * current state in place.  dgswem_cuda_limiter_vjp returns, at the current
+ * state and WDFLG as their input, the transpose of the two with their
+ * branches frozen applied to the cotangents lam_* of their output
+ * (ZE/QX/QY(DOFH,NE) in, the same layout out); needs SLOPEFLAG != 0 or
+ * WETDRY, and the adjoint's scope. */
 int dgswem_cuda_limit_state(dgswem_cuda* h);
 int dgswem_cuda_limiter_vjp(dgswem_cuda* h, const double* lam_ze, const double* lam_qx, const double* lam_qy,
                             double* out_ze, double* out_qx, double* out_qy);

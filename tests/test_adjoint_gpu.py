@@ -125,12 +125,12 @@ def test_torch_autograd_function(problem):
     np.testing.assert_array_equal(hb.grad.numpy(), ghb)
 
 
-def test_adjoint_rejects_limiter_and_wetdry(built, scratch):
-    path = decks.sloping_beach(scratch / "adj_rej", nx=20, ny=4, lx=1000.0, ly=200.0, nsteps=2)
-    with HydroStep(Deck(path)) as hs:
-        import ctypes as C  # noqa: F401
-        with pytest.raises(DgswemError, match="slope limiter|WETDRY"):
-            from dgswem_b200 import _abi
+def test_adjoint_rejects_barriers(built):
+    """The wetdry golden deck has barrier edges, which the adjoint does not cover."""
+    from conftest import golden_dir
+    from dgswem_b200 import _abi
+    with HydroStep(Deck(golden_dir("wetdry"))) as hs:
+        with pytest.raises(DgswemError, match="barrier"):
             _abi.check(hs._lib.dgswem_cuda_adjoint_begin(hs._h))
 
 
@@ -220,3 +220,111 @@ def test_limiter_is_active(limiter_problem, tmp_path_factory):
     p2.close()
     d2.close()
     assert np.abs(eta - eta_lim).max() > 1e-9
+
+
+def test_wetdry_reverse_mode_dot_product(built, scratch):
+    """WETDRY after the limiter (the stage path's limit_wetdry) against
+    central differences of the forward, as the limiter's dot-product test, at
+    a seeded state whose vertex depths straddle H0 on a sloping beach (all-wet,
+    flattened and partially wet elements; random input flags)."""
+    from dgswem_b200 import _abi
+    from dgswem_b200.adjoint import _dp
+    path = decks.sloping_beach(scratch / "wdvjp", nx=16, ny=4, lx=800.0, ly=200.0, nsteps=2)
+    deck = Deck(path)
+    ne, npn = deck.s.ne, deck.s.np
+    nm = deck.int_array("nm", 3 * ne).reshape(3, ne) - 1
+    dp = deck.real_array("dp", npn)
+    with HydroStep(deck) as hs:
+        rng = np.random.default_rng(31)
+        dpe = (dp[nm[0]] + dp[nm[1]] + dp[nm[2]]) / 3.0
+        ze = np.stack([-dpe + rng.uniform(-0.3, 0.6, ne), 0.1 * rng.standard_normal(ne),
+                       0.1 * rng.standard_normal(ne)], 1)
+        x = [np.ascontiguousarray(ze), np.ascontiguousarray(0.2 * rng.standard_normal((ne, 3))),
+             np.ascontiguousarray(0.2 * rng.standard_normal((ne, 3)))]
+        wd = rng.integers(0, 2, ne).astype(np.int32)
+        mu = [np.ascontiguousarray(rng.standard_normal((ne, 3))) for _ in range(3)]
+        d = [rng.standard_normal((ne, 3)) for _ in range(3)]
+        g = [np.empty((ne, 3)) for _ in range(3)]
+        hs.set_state(*x, wd)
+        _abi.check(hs._lib.dgswem_cuda_limiter_vjp(hs._h, *[_dp(m) for m in mu], *[_dp(a) for a in g]))
+        eps = 1e-6  # the ZE modes are ~20 m (-DP): a smaller step drowns in rounding
+        out = []
+        for sgn in (1.0, -1.0):
+            hs.set_state(*(np.ascontiguousarray(x[v] + sgn * eps * d[v]) for v in range(3)), wd)
+            _abi.check(hs._lib.dgswem_cuda_limit_state(hs._h))
+            out.append(hs.state())
+        assert np.array_equal(out[0][3], out[1][3])  # no flag flipped inside the step
+        lhs = sum(float(np.sum((out[0][v] - out[1][v]) / (2 * eps) * mu[v])) for v in range(3))
+        rhs = sum(float(np.sum(d[v] * g[v])) for v in range(3))
+        print(f"wetdry dot product: FD {lhs:.10e} reverse {rhs:.10e} rel {abs(lhs - rhs) / abs(rhs):.2e}")
+        assert abs(lhs - rhs) <= 1e-6 * abs(rhs)
+        # WETDRY acted: some elements were flattened or wetted / dried
+        hs.set_state(*x, wd)
+        _abi.check(hs._lib.dgswem_cuda_limit_state(hs._h))
+        y = hs.state()
+        assert not np.array_equal(y[3], wd) and np.abs(y[1] - x[1]).max() > 1e-3
+    deck.close()
+
+
+@pytest.fixture(scope="module")
+def wetdry_problem(tmp_path_factory):
+    """The sloping beach (config 2 physics: WETDRY, limiter 5, nodal Manning n)
+    at a state with moving fronts: a 1 m tide ramped over 0.002 days, 600
+    steps from cold start (the wave reaches and runs up the shore), then a
+    3-step misfit at gauges around the shoreline, observations from Manning
+    n x 1.5."""
+    from dgswem_b200 import _abi
+    from dgswem_b200 import build
+    build.build_library()
+    path = decks.sloping_beach(tmp_path_factory.mktemp("adjwd") / "beach", nx=60, ny=12, lx=3000.0, ly=600.0,
+                               nsteps=700, dt=0.5, dramp=0.002)
+    deck = Deck(path)
+    rng = np.random.default_rng(9)
+    elem, phi = locate_gauges(deck, np.column_stack([rng.uniform(2300.0, 2800.0, 16), rng.uniform(50.0, 550.0, 16)]))
+    n0 = element_manning(deck)
+    hb0 = deck.real_array("hb", 3 * deck.s.ne).reshape(deck.s.ne, 3)
+
+    def warmed(nbar):
+        p = GaugeMisfitProblem(deck, elem, phi, 3, it0=601)
+        p.set_params(nbar=nbar)
+        p.hs.run(1, 600)
+        _abi.check(p.hs._lib.dgswem_cuda_state_save(p.hs._h, 0))
+        return p
+    t = warmed(1.5 * n0)
+    obs = t.run()
+    t.close()
+    prob = warmed(n0)
+    prob.obs = obs
+    yield deck, prob, n0, hb0
+    prob.close()
+    deck.close()
+
+
+def test_wetdry_adjoint_matches_short_central_difference(wetdry_problem):
+    """Gradient of the 3-step misfit through the whole wet/dry chain (dry
+    elements' volume terms masked, dry-side edge rules, limiter, WETDRY, all
+    frozen at the forward's branches) against a central difference of step
+    1e-7 in a random Manning direction, small enough that no branch of the 3
+    steps changes."""
+    deck, prob, n0, hb0 = wetdry_problem
+    prob.set_params(n0, hb0)
+    prob.forward()
+    gn, ghb = prob.gradient()
+    dn = n0 * np.random.default_rng(3).standard_normal(deck.s.ne)
+    eps = 1e-7
+    fd = (misfit(prob, n0 + eps * dn, hb0) - misfit(prob, n0 - eps * dn, hb0)) / (2 * eps)
+    ad = float(gn @ dn)
+    print(f"wetdry 3 steps: adjoint {ad:.10e} central FD {fd:.10e} J {misfit(prob, n0, hb0):.3e}")
+    assert fd != 0.0
+    assert abs(ad - fd) <= 1e-5 * abs(fd)
+    prob.set_params(n0, hb0)
+
+
+def test_wetdry_adjoint_stepwise_matches_sweep(wetdry_problem):
+    deck, prob, n0, hb0 = wetdry_problem
+    prob.set_params(n0, hb0)
+    prob.forward()
+    gn, ghb = prob.gradient()
+    gn2, ghb2 = prob.gradient_stepwise()
+    np.testing.assert_array_equal(gn2, gn)
+    np.testing.assert_array_equal(ghb2, ghb)
