@@ -30,7 +30,9 @@ SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_stri
 HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
+# host code is compiled with OpenMP (the deck reader's tables, the edge search,
+# the device numbering and geometry table use all host threads)
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2,-fopenmp", "--expt-relaxed-constexpr"]
 
 
 def nvcc() -> str:
@@ -69,7 +71,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
-    link = [nvcc(), "-ccbin", host_cxx(), "-shared", *ARCH, "-o", str(out), *objs]
+    link = [nvcc(), "-ccbin", host_cxx(), "-shared", "-Xcompiler", "-fopenmp", *ARCH, "-o", str(out), *objs]
     subprocess.run(link, check=True)
     return out
 

@@ -64,6 +64,26 @@ class ListStream {
     return true;
   }
   const std::string& path() const { return path_; }
+  // random access to the records (for parsing tables in parallel)
+  size_t pos() const { return next_; }
+  size_t remaining() const { return rec_.size() - next_; }
+  std::string_view rec(size_t i) const { return std::string_view(buf_.data() + rec_[i].first, rec_[i].second); }
+  void seek(size_t i) { next_ = i; }
+  // the first n fields of one record (false if it has fewer: the READ would
+  // continue on the next record)
+  static bool split_fields(std::string_view s, size_t n, std::string_view* out) {
+    size_t got = 0, i = 0, len = s.size();
+    while (i < len && got < n) {
+      while (i < len && (std::isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
+      if (i >= len || s[i] == '/') break;
+      size_t j = i;
+      while (j < len && !std::isspace((unsigned char)s[j]) && s[j] != ',' && s[j] != '/') ++j;
+      out[got++] = s.substr(i, j - i);
+      i = j;
+      if (i < len && s[i] == '/') break;
+    }
+    return got == n;
+  }
   std::vector<std::string> records() const {
     std::vector<std::string> out;
     out.reserve(rec_.size());
@@ -161,6 +181,43 @@ std::string trimmed(const std::string& s) {
   if (b == std::string::npos) return std::string();
   size_t e = s.find_last_not_of(" \t");
   return s.substr(b, e - b + 1);
+}
+
+// A table of `count` READs of `nf` fields starting at the stream's position,
+// one record each in well-formed decks: parsed by `row(i, fields)` on all
+// host threads (rows must write disjoint outputs); if a record has fewer
+// fields or `row` throws, the whole table is parsed again sequentially, which
+// reports the error as the one-READ-at-a-time reading would.
+template <int NF, typename Row>
+void parse_table(ListStream& f, int count, Row row) {
+  const size_t r0 = f.pos();
+  int bad = 0;
+  if (f.remaining() >= (size_t)count) {
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int i = 0; i < count; ++i) {
+      if (bad) continue;
+      std::string_view t[NF];
+      if (!ListStream::split_fields(f.rec(r0 + i), NF, t)) {
+        bad = 1;
+        continue;
+      }
+      try {
+        row(i, t);
+      } catch (...) {
+        bad = 1;
+      }
+    }
+    if (!bad) {
+      f.seek(r0 + count);
+      return;
+    }
+  }
+  f.seek(r0);
+  for (int i = 0; i < count; ++i) {
+    std::string_view t[NF];
+    f.read_fields(NF, t);
+    row(i, t);
+  }
 }
 
 // One land/flow/barrier boundary segment of fort.14 after READ_INPUT's
@@ -279,17 +336,15 @@ void read_fort13(const std::string& dir, dgswem_deck* d) {
       found = true;
       d->manning.assign(d->s.np, defaults[name]);
     }
-    for (int i = 0; i < count; ++i) {
-      if (!take) {
-        f.record_view();
-        continue;
-      }
-      std::string_view t[2];
-      f.read_fields(2, t);
+    if (!take) {
+      for (int i = 0; i < count; ++i) f.record_view();
+      continue;
+    }
+    parse_table<2>(f, count, [&](int, const std::string_view* t) {
       int node = ListStream::as_int(t[0]);
       if (node < 1 || node > d->s.np) throw dgswem::Failure(DGSWEM_ERR_IO, "fort.13 node out of range");
       d->manning[node - 1] = ListStream::as_real(t[1]);
-    }
+    });
   }
   if (!found) throw dgswem::Failure(DGSWEM_ERR_IO, "fort.13 has no mannings_n_at_sea_floor data");
 }
@@ -352,9 +407,7 @@ void read_fort14_15(const std::string& dir, dgswem_deck* d, Fort15* p) {
   }
   const int np = s.np, ne = s.ne;
   d->x.assign(np, 0.0); d->y.assign(np, 0.0); d->dp.assign(np, 0.0); d->sfea.assign(np, 0.0);
-  for (int i = 0; i < np; ++i) {
-    std::string_view t[4];
-    f14.read_fields(4, t);
+  parse_table<4>(f14, np, [&](int, const std::string_view* t) {
     int id = ListStream::as_int(t[0]);
     if (id < 1 || id > np) throw dgswem::Failure(DGSWEM_ERR_IO, "node number out of range in fort.14");
     double a = ListStream::as_real(t[1]), b = ListStream::as_real(t[2]);
@@ -369,13 +422,11 @@ void read_fort14_15(const std::string& dir, dgswem_deck* d, Fort15* p) {
       d->sfea[id - 1] = phi;
     }
     d->dp[id - 1] = ListStream::as_real(t[3]);
-  }
+  });
   if (s.nolifa <= 1)
     for (double& v : d->dp) v = std::max(v, s.h0);  // read_input.F:1356
   d->nm.assign(3 * (size_t)ne, 0);
-  for (int i = 0; i < ne; ++i) {
-    std::string_view t[5];
-    f14.read_fields(5, t);
+  parse_table<5>(f14, ne, [&](int, const std::string_view* t) {
     int id = ListStream::as_int(t[0]);
     if (id < 1 || id > ne) throw dgswem::Failure(DGSWEM_ERR_IO, "element number out of range in fort.14");
     for (int v = 0; v < 3; ++v) {
@@ -383,7 +434,7 @@ void read_fort14_15(const std::string& dir, dgswem_deck* d, Fort15* p) {
       if (n < 1 || n > np) throw dgswem::Failure(DGSWEM_ERR_IO, "connectivity refers to a missing node");
       d->nm[(id - 1) + (size_t)ne * v] = n;
     }
-  }
+  });
   for (int e = 0; e < ne; ++e) {  // read_input.F:1406-1419
     const double* X = d->x.data();
     const double* Y = d->y.data();
@@ -645,6 +696,29 @@ void build_edges(dgswem_deck* d, const Fort15& p) {
   d->neled.assign(3 * (size_t)ne, 0);
   d->nedno.clear();
   d->nedel.clear();
+  // the first other element of node a's star (in star order) holding local
+  // edge l's node pair, and its local edge: a function of the mesh alone,
+  // found for every (element, edge) in parallel
+  std::vector<int> match(3 * (size_t)ne, -1);
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < ne; ++e)
+    for (int l = 0; l < 3; ++l) {
+      const int a = NM(e, (l + 1) % 3), b = NM(e, (l + 2) % 3);
+      for (int q = node_first[a - 1]; q < node_first[a]; ++q) {
+        const int o = node_elems[q];
+        if (o == e) continue;
+        int hit = -1;
+        for (int m = 0; m < 3 && hit < 0; ++m) {
+          const int c1 = NM(o, (m + 1) % 3), c2 = NM(o, (m + 2) % 3);
+          if ((c1 == a && c2 == b) || (c1 == b && c2 == a)) hit = m;
+        }
+        if (hit >= 0) {
+          match[l + 3 * (size_t)e] = 3 * o + hit;
+          break;
+        }
+      }
+    }
+  // edge ids in the order of first visit (create_edge_data.F:85-138)
   int nedges = 0;
   for (int e = 0; e < ne; ++e) {
     for (int l = 0; l < 3; ++l) {
@@ -656,21 +730,13 @@ void build_edges(dgswem_deck* d, const Fort15& p) {
       d->nedno.push_back(b);
       d->nedel.push_back(e + 1);
       d->nedel.push_back(0);
-      bool matched = false;
-      for (int q = node_first[a - 1]; q < node_first[a] && !matched; ++q) {
-        int o = node_elems[q];
-        if (o == e) continue;
-        for (int m = 0; m < 3; ++m) {
-          int c1 = NM(o, (m + 1) % 3), c2 = NM(o, (m + 2) % 3);
-          if ((c1 == a && c2 == b) || (c1 == b && c2 == a)) {
-            if (d->neled[m + 3 * (size_t)o] != 0)
-              throw dgswem::Failure(DGSWEM_ERR_IO, "possible duplicate element " + std::to_string(o + 1));
-            d->neled[m + 3 * (size_t)o] = id;
-            d->nedel[2 * (size_t)(id - 1) + 1] = o + 1;
-            matched = true;
-            break;
-          }
-        }
+      const int mt = match[l + 3 * (size_t)e];
+      if (mt >= 0) {
+        const int o = mt / 3, m = mt % 3;
+        if (d->neled[m + 3 * (size_t)o] != 0)
+          throw dgswem::Failure(DGSWEM_ERR_IO, "possible duplicate element " + std::to_string(o + 1));
+        d->neled[m + 3 * (size_t)o] = id;
+        d->nedel[2 * (size_t)(id - 1) + 1] = o + 1;
       }
     }
   }

@@ -655,6 +655,7 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& pl
   {
     std::vector<double> eg((size_t)EGeo::kRows * nl, 0.0);
     auto at = [&](int r, int e) -> double& { return eg[(size_t)r * nl + e]; };
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < nl; ++e) {
       double xs[3], ys[3];
       for (int v = 0; v < 3; ++v) {

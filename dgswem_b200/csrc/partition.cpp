@@ -5,6 +5,7 @@
 #include "partition.h"
 
 #include <algorithm>
+#include <parallel/algorithm>
 #include <cstdint>
 #include <string>
 
@@ -32,6 +33,7 @@ std::vector<int> morton_order(const std::vector<double>& px, const std::vector<d
     return r;
   };
   std::vector<uint64_t> key(n);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; ++i) {
     const int g = grouped ? group[i] : 0;
     const double span = std::max(std::max(x1[g] - x0[g], y1[g] - y0[g]), 1e-300);
@@ -41,9 +43,13 @@ std::vector<int> morton_order(const std::vector<double>& px, const std::vector<d
   }
   std::vector<int> perm(n);
   for (int i = 0; i < n; ++i) perm[i] = i;
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+  // (group, key, index) is a strict total order, so the parallel sort gives
+  // the stable sort's permutation
+  __gnu_parallel::sort(perm.begin(), perm.end(), [&](int a, int b) {
     const int ga = grouped ? group[a] : 0, gb = grouped ? group[b] : 0;
-    return ga != gb ? ga < gb : key[a] < key[b];
+    if (ga != gb) return ga < gb;
+    if (key[a] != key[b]) return key[a] < key[b];
+    return a < b;
   });
   return perm;
 }
