@@ -13,6 +13,11 @@ DG_HYDRO_TIMESTEP over the whole mesh.  The deck is generated (seeded) into
 Multi-GPU (torchrun): each rank steps its own replica of the basin; the path
 has no data exchange between independent meshes (weak scaling, replicas only).
 
+Each handle's tile and limiter block shapes are picked after warm-up by the
+library's autotuner (whole steps with each shape, the state restored
+afterwards; "tiles" objects give the picks and per-shape times);
+--no-autotune keeps the default shapes.
+
 The line's "mixed" object is the mixed-precision form (FP32 edge, volume and
 limiter terms; FP64 state, SSP combination and wet/dry) on the same deck: its
 rate, its speed-up over the FP64 line and its error against the FP64 form.
@@ -158,6 +163,19 @@ def mass(deck, ze) -> float:
     return float(np.sum((ze[:, 0] + hb[:, 0]) * areas * 0.5))
 
 
+def autotune(h, args, it: int) -> dict | None:
+    """Tile and limiter block shapes picked by the library's autotuner
+    (dgswem_cuda_autotune: whole steps from step ``it`` with each shape,
+    state restored), with its per-shape milliseconds per step; None with
+    --no-autotune (the default shapes)."""
+    if args.no_autotune:
+        return None
+    t0 = time.perf_counter()
+    r = h.autotune(it=it, steps=args.tune_steps, reps=3, cached=True)
+    r["tune_s"] = time.perf_counter() - t0
+    return r
+
+
 def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
     """The mixed-precision form (DGSWEM_CUDA_MIXED) on the same deck: its rate
     (same timing rules as the FP64 line), per-kernel times, and its error
@@ -169,6 +187,7 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
     hm = HydroStep(deck, device=device, mixed=True)
     hm.set_stream(stream.cuda_stream)
     hm.run(1, args.warmup)
+    tiles = autotune(hm, args, args.warmup + 1)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -205,7 +224,7 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
     return {"value": value, "unit": "DOF-stage/s", "ms_per_step": ms / args.steps,
             "dtype": "f32 edge/volume/limiter terms, f64 state, SSP, wet/dry",
             "per_kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items() if v[1]},
-            "err_vs_fp64": err}
+            "tiles": tiles, "err_vs_fp64": err}
 
 
 def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
@@ -238,20 +257,22 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
             ens.hs.set_stream(stream.cuda_stream)
             ens.set_met(wsx, wsy, pr)
             ens.run(1, w)
+            tiles = autotune(ens.hs, args, w + 1)
             l0 = ens.hs.kernel_launches
             ms = timed(ens.run, w + 1)
-            return ms, ens.hs.kernel_launches - l0, ens.total_elements, ens.nrk
+            return ms, ens.hs.kernel_launches - l0, ens.total_elements, ens.nrk, tiles
 
-    ms, launches, ne_tot, nrk = batched(ds, *met)
+    ms, launches, ne_tot, nrk, tiles = batched(ds, *met)
     ms = max_over_ranks(ms, world, dist, "cuda")
     sub = min(16, len(ds))
-    ms_sub, _, ne_sub, _ = batched(ds[:sub], *(f[:sub] for f in met))
+    ms_sub, _, ne_sub, _, _ = batched(ds[:sub], *(f[:sub] for f in met))
     ms_one = 0.0
     for i in range(sub):
         with HydroStep(ds[i], device=device, mixed=True) as hs:
             hs.set_stream(stream.cuda_stream)
             hs.set_met(met[0][i], met[1][i], met[2][i])
             hs.run(1, w)
+            autotune(hs, args, w + 1)
             ms_one += timed(hs.run, w + 1)
     rate = lambda ne, t: DOFS_PER_ELEMENT * ne * nrk * k / (t / 1e3)  # noqa: E731
     for d in ds:
@@ -259,7 +280,7 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
     return {"members": len(specs), "elements": int(ne_tot), "steps": k, "warmup": w,
             "value": whole_job_rate(world, ne_tot, nrk, k, ms), "unit": "DOF-stage/s",
             "ms_per_step": ms / k, "dtype": "mixed (f32 edge/volume/limiter, f64 state/SSP/wet-dry)",
-            "gpu_launches": int(launches), "deck_write_read_s": t_decks,
+            "gpu_launches": int(launches), "deck_write_read_s": t_decks, "tiles": tiles,
             "subset16": {"elements": int(ne_sub), "batched_rate": rate(ne_sub, ms_sub),
                          "one_at_a_time_rate": rate(ne_sub, ms_one), "batching_speedup": ms_one / ms_sub}}
 
@@ -431,6 +452,8 @@ def main(argv=None):
     ap.add_argument("--ref-max-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default tile / limiter block shapes")
+    ap.add_argument("--tune-steps", type=int, default=10, help="steps per shape timing of the autotuner")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=40)
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
@@ -468,8 +491,9 @@ def main(argv=None):
     torch.cuda.set_stream(stream)
     hs.set_stream(stream.cuda_stream)
 
-    # warm-up
+    # warm-up, then the shapes (each timing restores the state)
     hs.run(1, args.warmup)
+    tiles = autotune(hs, args, args.warmup + 1)
     torch.cuda.synchronize()
     it0 = args.warmup + 1
 
@@ -539,6 +563,7 @@ def main(argv=None):
         "config": workload_config(args, ne, nrk),
         "gpu_launches": int(launches),
         "setup_s": {"deck_read": t_setup1 - t_setup0, "device_create": t_setup2 - t_setup1},
+        "tiles": tiles,
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes,

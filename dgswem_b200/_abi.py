@@ -12,6 +12,10 @@ from pathlib import Path
 # DGSWEM_CUDA_LIB points at another build of the same library
 LIB_PATH = Path(os.environ.get("DGSWEM_CUDA_LIB", Path(__file__).resolve().parent / "lib" / "libdgswem_cuda.so"))
 
+# dgswem_cuda.h constants
+MAX_SHAPES = 8        # DGSWEM_CUDA_MAX_SHAPES
+TUNE_CACHED = 1       # DGSWEM_CUDA_TUNE_CACHED
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
@@ -72,6 +76,10 @@ SIGNATURES = {
     "dgswem_cuda_last_error": (C.c_int, [C.c_char_p, C.c_int]),
     "dgswem_cuda_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dgswem_cuda_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
+    "dgswem_cuda_shapes": (C.c_int, [_ip, _ip, _ip, _ip, _ip, _ip]),
+    "dgswem_cuda_set_shapes": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dgswem_cuda_get_shapes": (C.c_int, [C.c_void_p, _ip, _ip]),
+    "dgswem_cuda_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]),
     "dgswem_cuda_stream": (C.c_void_p, [C.c_void_p]),
     "dgswem_cuda_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "dgswem_cuda_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong)]),

@@ -5,7 +5,9 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -141,10 +143,10 @@ struct DevBuf {
 struct Variant {
   unsigned real_bytes;
   void (*set_basis)(const BasisP1&);
-  void (*stage)(const StageArgs&, bool, unsigned, size_t, cudaStream_t);
+  void (*stage)(const StageArgs&, bool, int, unsigned, size_t, cudaStream_t);
   void (*ibarrier)(const StageArgs&, bool, cudaStream_t);
   void (*node_minmax)(const LimitArgs&, unsigned, cudaStream_t);
-  void (*limit_wetdry)(const LimitArgs&, unsigned, cudaStream_t);
+  void (*limit_wetdry)(const LimitArgs&, int, cudaStream_t);
   void (*modal2nodal)(const MeshView&, const double*, const int*, double, double, double*, double*,
                       double*, int*, unsigned, cudaStream_t);
   void (*f2s)(const double*, double*, int, int, const int*, unsigned, cudaStream_t);
@@ -201,6 +203,9 @@ struct dgswem_cuda {
   DevBuf<unsigned> einfo, eslot, tile_tasks;
   DevBuf<int> tile_elem_ptr, tile_task_ptr, tile_halo_ptr, tile_halo;
   int ntile = 0;
+  // shape of the stage tiles (kTileShapes) and of the limiter blocks
+  // (kLimitBlocks): the defaults, or set / picked by dgswem_cuda_autotune
+  int tile_shape = kDefaultTileShape, limit_shape = kDefaultLimitShape;
   DevBuf<double> emo_dg, efa_dg, qnam_dg, qnph_dg, ebht, ebcfsp, ibht, ibcfsb, ibcfsp;
   DevBuf<double> wsx, wsy, pr, minmax, staging;
   std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
@@ -333,20 +338,23 @@ struct LaunchTimer {
 
 unsigned grid_for(int n, int block) { return (unsigned)((n + block - 1) / block); }
 
-// Stage tile plan: for each tile of kTile consecutive elements, the edge
-// tasks it evaluates and the out-of-tile neighbours (halo) they read.  Edge
-// ownership: a boundary edge of a listed kind and an internal-barrier side
-// belong to their element; an interior edge inside the tile is evaluated once,
-// by its in side NEDEL(1); an interior edge to another tile is evaluated by
-// both tiles, each for its own element, in the reference's in/ex orientation.
-// Tasks: interior edges in element order, then the boundary kinds grouped, so
-// that a warp's tasks mostly take one branch.
-// Tiles cover the first n_tiled elements (the owned ones); `ne` is the row
-// stride of link (all local elements, ghosts included).
+// Stage tile plan of the handle's tile shape (h->tile_shape): for each tile
+// of consecutive elements, the edge tasks it evaluates and the out-of-tile
+// neighbours (halo) they read.  Edge ownership: a boundary edge of a listed
+// kind and an internal-barrier side belong to their element; an interior
+// edge inside the tile is evaluated once, by its in side NEDEL(1); an
+// interior edge to another tile is evaluated by both tiles, each for its own
+// element, in the reference's in/ex orientation.  Tasks: interior edges in
+// element order, then the boundary kinds grouped, so that a warp's tasks
+// mostly take one branch.  Tiles cover the first n_tiled elements (the owned
+// ones); `ne` is the row stride of link (all local elements, ghosts
+// included).  Tiles are cut sequentially, then planned in parallel (each
+// writes only its own elements' eslot).
 void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>& link,
                      const std::vector<unsigned>& einfo) {
-  // Tiles: consecutive elements, at most kTile of them and at most
-  // kStageThreads edge tasks (one pass of the block over its tasks).  An
+  const TileShape shape = kTileShapes[h->tile_shape];
+  // Tiles: consecutive elements, at most shape.tile of them and at most
+  // shape.threads edge tasks (one pass of the block over its tasks).  An
   // element adds a task per listed boundary edge and per interior edge whose
   // neighbour is not already in the tile.
   std::vector<int> elem_ptr(1, 0);
@@ -363,7 +371,7 @@ void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>
         }
         ++add;
       }
-      if (e - t0 == kTile || count + add > kStageThreads) {
+      if (e - t0 == shape.tile || count + add > shape.threads) {
         elem_ptr.push_back(e);
         t0 = e;
         count = 0;
@@ -375,81 +383,103 @@ void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>
     elem_ptr.push_back(n_tiled);
   }
   const int ntile = (int)elem_ptr.size() - 1;
-  std::vector<int> task_ptr(ntile + 1, 0), halo_ptr(ntile + 1, 0), halo;
-  std::vector<unsigned> tasks;  // (word, list) pairs
+  std::vector<std::vector<unsigned>> ttasks(ntile);  // (word, list) pairs per tile
+  std::vector<std::vector<int>> thalo(ntile);
   std::vector<unsigned> eslot(ne, 0u);
-  std::vector<int> hl;
+  int max_halo = 0, max_tasks = 0;
   struct Task {
     unsigned word, list;
     int el, led;
   };
-  std::vector<Task> tt;
-  int max_halo = 0, max_tasks = 0;
-  for (int t = 0; t < ntile; ++t) {
-    const int t0 = elem_ptr[t], t1 = elem_ptr[t + 1];
-    hl.clear();
-    for (int e = t0; e < t1; ++e)
-      for (int l = 0; l < 3; ++l)
-        if (ei_kind(einfo[e], l) == kInterior) {
-          const int nb = link[(size_t)l * ne + e];
-          if (nb < t0 || nb >= t1) hl.push_back(nb);
-        }
-    std::sort(hl.begin(), hl.end());
-    hl.erase(std::unique(hl.begin(), hl.end()), hl.end());
-    auto slot = [&](int g) -> unsigned {
-      if (g >= t0 && g < t1) return (unsigned)(g - t0);
-      return (unsigned)(kTile + (std::lower_bound(hl.begin(), hl.end(), g) - hl.begin()));
-    };
-    tt.clear();
-    for (int pass = 0; pass < 2; ++pass)  // interior edges, then boundary kinds
-      for (unsigned want = pass == 0 ? (unsigned)kInterior : 1u; want <= (pass == 0 ? 0u : 6u); ++want)
-        for (int e = t0; e < t1; ++e)
-          for (int l = 0; l < 3; ++l) {
-            const unsigned info = einfo[e], kind = ei_kind(info, l);
-            if (kind != want) continue;
-            const int lk = link[(size_t)l * ne + e];
-            unsigned w = kind << TaskBits::kKind, list = 0;
-            if (kind == kInterior) {
-              const bool local = lk >= t0 && lk < t1, in_side = ei_flag(info, l) != 0;
-              if (local && !in_side) continue;  // the in side's task
-              const unsigned nled = ei_nled(info, l);
-              if (in_side)
-                w |= (unsigned)l << TaskBits::kLedIn | nled << TaskBits::kLedEx | slot(e) << TaskBits::kInSlot |
-                     slot(lk) << TaskBits::kExSlot;
-              else
-                w |= nled << TaskBits::kLedIn | (unsigned)l << TaskBits::kLedEx | 1u << TaskBits::kFlip |
-                     slot(lk) << TaskBits::kInSlot | slot(e) << TaskBits::kExSlot;
-            } else {
-              w |= (unsigned)l << TaskBits::kLedIn | slot(e) << TaskBits::kInSlot;
-              list = kind == kIBarrier ? (unsigned)lk * 2u + (ei_flag(info, l) ? 0u : 1u) : (unsigned)lk;
-            }
-            tt.push_back({w, list, e, l});
+#pragma omp parallel
+  {
+    std::vector<int> hl;
+    std::vector<Task> tt;
+#pragma omp for schedule(dynamic, 64) reduction(max : max_halo, max_tasks)
+    for (int t = 0; t < ntile; ++t) {
+      const int t0 = elem_ptr[t], t1 = elem_ptr[t + 1];
+      hl.clear();
+      for (int e = t0; e < t1; ++e)
+        for (int l = 0; l < 3; ++l)
+          if (ei_kind(einfo[e], l) == kInterior) {
+            const int nb = link[(size_t)l * ne + e];
+            if (nb < t0 || nb >= t1) hl.push_back(nb);
           }
-    for (int e = t0; e < t1; ++e) eslot[e] = kNoTask | kNoTask << 10 | kNoTask << 20;
-    auto set_slot = [&](int e, int l, unsigned ti) {
-      eslot[e] = (eslot[e] & ~(kNoTask << (10 * l))) | ti << (10 * l);
-    };
-    for (size_t i = 0; i < tt.size(); ++i) set_slot(tt[i].el, tt[i].led, (unsigned)i);
-    for (int e = t0; e < t1; ++e)  // shared edges inside the tile: the in side's task
-      for (int l = 0; l < 3; ++l) {
-        const unsigned info = einfo[e];
-        if (ei_kind(info, l) != kInterior || ei_flag(info, l)) continue;
-        const int nb = link[(size_t)l * ne + e];
-        if (nb < t0 || nb >= t1) continue;
-        set_slot(e, l, (eslot[nb] >> (10 * ei_nled(info, l))) & kNoTask);
+      std::sort(hl.begin(), hl.end());
+      hl.erase(std::unique(hl.begin(), hl.end()), hl.end());
+      auto slot = [&](int g) -> unsigned {
+        if (g >= t0 && g < t1) return (unsigned)(g - t0);
+        return (unsigned)(shape.tile + (std::lower_bound(hl.begin(), hl.end(), g) - hl.begin()));
+      };
+      tt.clear();
+      for (int pass = 0; pass < 2; ++pass)  // interior edges, then boundary kinds
+        for (unsigned want = pass == 0 ? (unsigned)kInterior : 1u; want <= (pass == 0 ? 0u : 6u); ++want)
+          for (int e = t0; e < t1; ++e)
+            for (int l = 0; l < 3; ++l) {
+              const unsigned info = einfo[e], kind = ei_kind(info, l);
+              if (kind != want) continue;
+              const int lk = link[(size_t)l * ne + e];
+              unsigned w = kind << TaskBits::kKind, list = 0;
+              if (kind == kInterior) {
+                const bool local = lk >= t0 && lk < t1, in_side = ei_flag(info, l) != 0;
+                if (local && !in_side) continue;  // the in side's task
+                const unsigned nled = ei_nled(info, l);
+                if (in_side)
+                  w |= (unsigned)l << TaskBits::kLedIn | nled << TaskBits::kLedEx | slot(e) << TaskBits::kInSlot |
+                       slot(lk) << TaskBits::kExSlot;
+                else
+                  w |= nled << TaskBits::kLedIn | (unsigned)l << TaskBits::kLedEx | 1u << TaskBits::kFlip |
+                       slot(lk) << TaskBits::kInSlot | slot(e) << TaskBits::kExSlot;
+              } else {
+                w |= (unsigned)l << TaskBits::kLedIn | slot(e) << TaskBits::kInSlot;
+                list = kind == kIBarrier ? (unsigned)lk * 2u + (ei_flag(info, l) ? 0u : 1u) : (unsigned)lk;
+              }
+              tt.push_back({w, list, e, l});
+            }
+      for (int e = t0; e < t1; ++e) eslot[e] = kNoTask | kNoTask << 10 | kNoTask << 20;
+      auto set_slot = [&](int e, int l, unsigned ti) {
+        eslot[e] = (eslot[e] & ~(kNoTask << (10 * l))) | ti << (10 * l);
+      };
+      for (size_t i = 0; i < tt.size(); ++i) set_slot(tt[i].el, tt[i].led, (unsigned)i);
+      for (int e = t0; e < t1; ++e)  // shared edges inside the tile: the in side's task
+        for (int l = 0; l < 3; ++l) {
+          const unsigned info = einfo[e];
+          if (ei_kind(info, l) != kInterior || ei_flag(info, l)) continue;
+          const int nb = link[(size_t)l * ne + e];
+          if (nb < t0 || nb >= t1) continue;
+          set_slot(e, l, (eslot[nb] >> (10 * ei_nled(info, l))) & kNoTask);
+        }
+      std::vector<unsigned>& out = ttasks[t];
+      out.reserve(2 * tt.size());
+      for (const Task& k : tt) {
+        out.push_back(k.word);
+        out.push_back(k.list);
       }
-    for (const Task& k : tt) {
-      tasks.push_back(k.word);
-      tasks.push_back(k.list);
+      thalo[t] = hl;
+      max_halo = std::max(max_halo, (int)hl.size());
+      max_tasks = std::max(max_tasks, (int)tt.size());
     }
-    halo.insert(halo.end(), hl.begin(), hl.end());
-    task_ptr[t + 1] = task_ptr[t] + (int)tt.size();
-    halo_ptr[t + 1] = halo_ptr[t] + (int)hl.size();
-    max_halo = std::max(max_halo, (int)hl.size());
-    max_tasks = std::max(max_tasks, (int)tt.size());
   }
-  if (max_halo + kTile > 512 || max_tasks >= (int)kNoTask)
+  if (max_halo + shape.tile > kMaxTileSlots || max_tasks >= (int)kNoTask)
     throw Failure(DGSWEM_ERR_ARG, "stage tile plan exceeds the task word's slot range");
+  const size_t stage_smem = stage_layout(shape.tile, max_halo, std::max(max_tasks, 1), h->v->real_bytes).bytes;
+  int dev_smem = 0;
+  DG_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+  if (stage_smem > (size_t)dev_smem)
+    throw Failure(DGSWEM_ERR_ARG, "stage tile needs " + std::to_string(stage_smem) +
+                                      " bytes of shared memory, the device allows " + std::to_string(dev_smem));
+  std::vector<int> task_ptr(ntile + 1, 0), halo_ptr(ntile + 1, 0), halo;
+  std::vector<unsigned> tasks;
+  for (int t = 0; t < ntile; ++t) {
+    task_ptr[t + 1] = task_ptr[t] + (int)ttasks[t].size() / 2;
+    halo_ptr[t + 1] = halo_ptr[t] + (int)thalo[t].size();
+  }
+  tasks.reserve(2 * (size_t)task_ptr[ntile]);
+  halo.reserve((size_t)halo_ptr[ntile]);
+  for (int t = 0; t < ntile; ++t) {
+    tasks.insert(tasks.end(), ttasks[t].begin(), ttasks[t].end());
+    halo.insert(halo.end(), thalo[t].begin(), thalo[t].end());
+  }
   h->ntile = ntile;
   h->tile_elem_ptr.upload(elem_ptr);
   h->tile_task_ptr.upload(task_ptr);
@@ -457,14 +487,16 @@ void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>
   h->tile_tasks.upload(tasks.empty() ? std::vector<unsigned>(2, 0u) : tasks);
   h->tile_halo.upload(halo.empty() ? std::vector<int>(1, 0) : halo);
   h->eslot.upload(eslot);
-  h->mesh.max_halo = max_halo;
-  h->mesh.max_tasks = max_tasks;
-  h->stage_smem = stage_layout(max_halo, std::max(max_tasks, 1), h->v->real_bytes).bytes;
-  int dev_smem = 0;
-  DG_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-  if (h->stage_smem > (size_t)dev_smem)
-    throw Failure(DGSWEM_ERR_ARG, "stage tile needs " + std::to_string(h->stage_smem) +
-                                      " bytes of shared memory, the device allows " + std::to_string(dev_smem));
+  h->stage_smem = stage_smem;
+  MeshView& m = h->mesh;
+  m.max_halo = max_halo;
+  m.max_tasks = max_tasks;
+  m.tile_elem_ptr = h->tile_elem_ptr.p;
+  m.tile_task_ptr = h->tile_task_ptr.p;
+  m.tile_tasks = reinterpret_cast<const uint2*>(h->tile_tasks.p);
+  m.tile_halo_ptr = h->tile_halo_ptr.p;
+  m.tile_halo = h->tile_halo.p;
+  m.eslot = h->eslot.p;
 }
 
 // Device element and node order: elements sorted along a Morton (Z-order)
@@ -746,12 +778,6 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& pl
   m.hb = h->hb.p; m.egeo = h->egeo.p; m.egeof = h->egeof.p; m.cori = h->cori.p; m.fric = h->fric.p; m.manning = h->manning.p;
   m.sfac_area = h->sfac_area.p; m.sfac_edge = h->sfac_edge.p;
   m.star_ptr = h->star_ptr.p; m.star = h->star.p; m.node_perm = h->node_perm.p;
-  m.tile_elem_ptr = h->tile_elem_ptr.p;
-  m.tile_task_ptr = h->tile_task_ptr.p;
-  m.tile_tasks = reinterpret_cast<const uint2*>(h->tile_tasks.p);
-  m.tile_halo_ptr = h->tile_halo_ptr.p;
-  m.tile_halo = h->tile_halo.p;
-  m.eslot = h->eslot.p;
   m.needs = s->needs; m.nfeds = s->nfeds; m.nebseg = s->nebseg; m.nibseg = s->nibseg;
   m.nbfr = h->amig.empty() ? 0 : nbfr;
   m.nffr = h->famig.empty() ? 0 : nffr;
@@ -889,7 +915,7 @@ void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, co
   }
   {
     LaunchTimer t(h, 0);
-    h->v->stage(A, nonlin, (unsigned)h->ntile, h->stage_smem, h->stream);
+    h->v->stage(A, nonlin, h->tile_shape, (unsigned)h->ntile, h->stage_smem, h->stream);
     t.done();
   }
 }
@@ -914,7 +940,7 @@ void launch_limit(dgswem_cuda* h, int irk) {
       t.done();
     }
     LaunchTimer t(h, 2);
-    h->v->limit_wetdry(L, grid_for(h->n_own, kPointBlock), h->stream);
+    h->v->limit_wetdry(L, h->limit_shape, h->stream);
     t.done();
   }
 }
@@ -1644,6 +1670,223 @@ int dgswem_cuda_set_graph(dgswem_cuda* h, int steps) {
     graph_release(h);
     h->graph_steps = steps;
     h->graph_next = 0;
+  });
+}
+
+namespace {
+
+// Rebuilds the stage tile plan for tile shape `shape` from the device copies
+// of the edge graph (link, einfo); on failure (the shape's plan does not fit
+// the task word or shared memory) the current plan stays.  Captured graphs
+// hold the old plan's launches: released.
+void replan(dgswem_cuda* h, int shape) {
+  DG_CUDA(cudaStreamSynchronize(h->stream));
+  graph_release(h);
+  std::vector<int> link(3 * (size_t)h->ne);
+  std::vector<unsigned> info(h->ne);
+  DG_CUDA(cudaMemcpy(link.data(), h->link.p, link.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  DG_CUDA(cudaMemcpy(info.data(), h->einfo.p, info.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  const int old = h->tile_shape;
+  h->tile_shape = shape;
+  try {
+    build_tile_plan(h, h->n_own, h->ne, link, info);
+  } catch (...) {
+    h->tile_shape = old;  // the plan is uploaded only after every check passed
+    throw;
+  }
+}
+
+// Mesh signature of the autotuner's cache: the variant, the device, the
+// element / node counts and a hash of the edge graph (FNV-1a over einfo and
+// link) and of the physics switches that decide which kernels run.
+uint64_t tune_signature(dgswem_cuda* h) {
+  std::vector<int> link(3 * (size_t)h->ne);
+  std::vector<unsigned> info(h->ne);
+  DG_CUDA(cudaMemcpy(link.data(), h->link.p, link.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  DG_CUDA(cudaMemcpy(info.data(), h->einfo.p, info.size() * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  uint64_t x = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      x ^= (v >> (8 * b)) & 0xffu;
+      x *= 1099511628211ull;
+    }
+  };
+  mix((uint64_t)(uintptr_t)h->v);
+  mix((uint64_t)h->device);
+  mix((uint64_t)h->ne);
+  mix((uint64_t)h->np);
+  mix((uint64_t)h->nrk);
+  mix((uint64_t)h->slopeflag);
+  mix((uint64_t)h->nolifa);
+  mix((uint64_t)(h->ph.nleq == 1.0 && h->ph.leq == 0.0));
+  mix((uint64_t)(h->mesh.sfac_edge != nullptr));
+  for (unsigned v : info) mix(v);
+  for (int v : link) mix((uint64_t)(unsigned)v);
+  return x;
+}
+
+struct TuneResult {
+  int tile_shape, limit_shape;
+  double ms_tile[kNumTileShapes], ms_limit[kNumLimitShapes];
+};
+std::mutex g_tune_lock;
+std::map<uint64_t, TuneResult> g_tune_cache;
+
+}  // namespace
+
+static_assert(kNumTileShapes <= DGSWEM_CUDA_MAX_SHAPES && kNumLimitShapes <= DGSWEM_CUDA_MAX_SHAPES,
+              "shape lists fit the C-ABI arrays");
+
+int dgswem_cuda_shapes(int* n_tile, int* tile_elems, int* tile_threads, int* n_limit, int* limit_threads,
+                       int* limit_blocks_per_sm) {
+  return guarded([&]() {
+    if (n_tile) *n_tile = kNumTileShapes;
+    if (n_limit) *n_limit = kNumLimitShapes;
+    for (int i = 0; i < kNumTileShapes; ++i) {
+      if (tile_elems) tile_elems[i] = kTileShapes[i].tile;
+      if (tile_threads) tile_threads[i] = kTileShapes[i].threads;
+    }
+    for (int i = 0; i < kNumLimitShapes; ++i) {
+      if (limit_threads) limit_threads[i] = kLimitBlocks[i];
+      if (limit_blocks_per_sm) limit_blocks_per_sm[i] = kLimitMinBlocks[i];
+    }
+  });
+}
+
+int dgswem_cuda_set_shapes(dgswem_cuda* h, int tile_shape, int limit_shape) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (tile_shape < -1 || tile_shape >= kNumTileShapes || limit_shape < -1 || limit_shape >= kNumLimitShapes)
+      throw Failure(DGSWEM_ERR_ARG, "shape index out of range");
+    DG_CUDA(cudaSetDevice(h->device));
+    if (tile_shape >= 0 && tile_shape != h->tile_shape) replan(h, tile_shape);
+    if (limit_shape >= 0) h->limit_shape = limit_shape;
+  });
+}
+
+int dgswem_cuda_get_shapes(const dgswem_cuda* h, int* tile_shape, int* limit_shape) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (tile_shape) *tile_shape = h->tile_shape;
+    if (limit_shape) *limit_shape = h->limit_shape;
+  });
+}
+
+int dgswem_cuda_autotune(dgswem_cuda* h, int it, int steps, int reps, int flags, double* ms_tile,
+                         double* ms_limit) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (steps < 1 || reps < 1 || it < 1) throw Failure(DGSWEM_ERR_ARG, "autotune: it, steps and reps must be >= 1");
+    if (h->nparts != 1)
+      throw Failure(DGSWEM_ERR_ARG, "autotune times whole steps of a handle of dgswem_cuda_create");
+    DG_CUDA(cudaSetDevice(h->device));
+    DG_CUDA(cudaStreamSynchronize(h->stream));
+    const uint64_t sig = tune_signature(h);
+    TuneResult r{};
+    bool cached = false;
+    if (flags & DGSWEM_CUDA_TUNE_CACHED) {
+      std::lock_guard<std::mutex> g(g_tune_lock);
+      auto f = g_tune_cache.find(sig);
+      if (f != g_tune_cache.end()) {
+        r = f->second;
+        cached = true;
+      }
+    }
+    if (!cached) {
+      // the state the steps start from: kept, restored before each timing
+      // and at the end (the stage buffers other than q[0] and the limiter's
+      // node bounds are scratch of every step)
+      const size_t n9 = 9 * (size_t)h->ne;
+      DevBuf<double> q0;
+      DevBuf<int> wd0;
+      DevBuf<unsigned> err0;
+      q0.alloc(n9);
+      wd0.alloc((size_t)h->ne);
+      err0.alloc(1);
+      DG_CUDA(cudaMemcpyAsync(q0.p, h->q[0].p, n9 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      DG_CUDA(cudaMemcpyAsync(wd0.p, h->wd.p, (size_t)h->ne * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+      DG_CUDA(cudaMemcpyAsync(err0.p, h->err.p, sizeof(unsigned), cudaMemcpyDeviceToDevice, h->stream));
+      auto restore = [&]() {
+        DG_CUDA(cudaMemcpyAsync(h->q[0].p, q0.p, n9 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        DG_CUDA(cudaMemcpyAsync(h->wd.p, wd0.p, (size_t)h->ne * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+        DG_CUDA(cudaMemcpyAsync(h->err.p, err0.p, sizeof(unsigned), cudaMemcpyDeviceToDevice, h->stream));
+      };
+      const int graph_steps = h->graph_steps;
+      const bool prof_on = h->prof_on;
+      const int tile0 = h->tile_shape, limit0 = h->limit_shape;
+      h->graph_steps = 0;
+      h->prof_on = false;
+      cudaEvent_t ev[2] = {nullptr, nullptr};
+      auto time_steps = [&]() -> double {
+        restore();
+        run_steps(h, it, 1);  // warm-up (first launch of the shape's kernels)
+        double best = 0.0;
+        for (int k = 0; k < reps; ++k) {
+          restore();
+          DG_CUDA(cudaEventRecord(ev[0], h->stream));
+          run_steps(h, it, steps);
+          DG_CUDA(cudaEventRecord(ev[1], h->stream));
+          DG_CUDA(cudaEventSynchronize(ev[1]));
+          float ms = 0.f;
+          DG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+          const double per = (double)ms / steps;
+          if (k == 0 || per < best) best = per;
+        }
+        return best;
+      };
+      try {
+        for (auto& e : ev) DG_CUDA(cudaEventCreate(&e));
+        r.tile_shape = -1;
+        for (int s = 0; s < kNumTileShapes; ++s) {
+          r.ms_tile[s] = -1.0;
+          try {
+            replan(h, s);
+          } catch (const Failure& f) {
+            if (f.code != DGSWEM_ERR_ARG) throw;
+            continue;  // the shape's plan does not fit: not timed
+          }
+          r.ms_tile[s] = time_steps();
+          if (r.tile_shape < 0 || r.ms_tile[s] < r.ms_tile[r.tile_shape]) r.tile_shape = s;
+        }
+        if (r.tile_shape < 0) throw Failure(DGSWEM_ERR_ARG, "autotune: no tile shape fits the mesh");
+        if (h->tile_shape != r.tile_shape) replan(h, r.tile_shape);
+        const bool limiter = h->slopeflag != 0 || h->nolifa >= 2;
+        r.limit_shape = limit0;
+        for (int s = 0; s < kNumLimitShapes; ++s) r.ms_limit[s] = -1.0;
+        if (limiter) {
+          for (int s = 0; s < kNumLimitShapes; ++s) {
+            h->limit_shape = s;
+            r.ms_limit[s] = time_steps();
+            if (s == 0 || r.ms_limit[s] < r.ms_limit[r.limit_shape]) r.limit_shape = s;
+          }
+        }
+        restore();
+      } catch (...) {
+        for (auto& e : ev)
+          if (e) cudaEventDestroy(e);
+        h->graph_steps = graph_steps;
+        h->prof_on = prof_on;
+        try {
+          restore();
+          h->limit_shape = limit0;
+          if (h->tile_shape != tile0) replan(h, tile0);
+        } catch (...) {
+        }
+        throw;
+      }
+      for (auto& e : ev) cudaEventDestroy(e);
+      h->graph_steps = graph_steps;
+      h->prof_on = prof_on;
+      DG_CUDA(cudaStreamSynchronize(h->stream));
+      std::lock_guard<std::mutex> g(g_tune_lock);
+      g_tune_cache[sig] = r;
+    }
+    if (h->tile_shape != r.tile_shape) replan(h, r.tile_shape);
+    h->limit_shape = r.limit_shape;
+    if (ms_tile)
+      for (int s = 0; s < kNumTileShapes; ++s) ms_tile[s] = r.ms_tile[s];
+    if (ms_limit)
+      for (int s = 0; s < kNumLimitShapes; ++s) ms_limit[s] = r.ms_limit[s];
   });
 }
 

@@ -10,7 +10,7 @@
 //                      or index into the boundary list of that edge's kind
 //   einfo[e]           packed edge kinds, processing order, orientation bits
 //   hb[k*NE + e]       bathymetry modes HB(k,e)
-//   stage tile plan    per tile of up to kTile consecutive elements: its edge tasks
+//   stage tile plan    per tile of consecutive elements (TileShape): its edge tasks
 //                      (uint2 each, interior edges first, then boundary kinds)
 //                      and its halo (out-of-tile neighbours, global ids);
 //                      eslot[e] names the task of each local edge
@@ -96,7 +96,8 @@ struct MeshView {
   const double* __restrict__ ibht;
   const double* __restrict__ ibcfsb;
   const double* __restrict__ ibcfsp;
-  // stage tile plan (built once at create from the edge graph)
+  // stage tile plan (built at create from the edge graph, rebuilt when the
+  // tile shape changes)
   int max_halo, max_tasks;                // largest halo / task list of a tile
   const int* __restrict__ tile_elem_ptr;  // [ntile+1] first element of each tile
   const int* __restrict__ tile_task_ptr;  // [ntile+1] offsets into tile_tasks
@@ -106,20 +107,32 @@ struct MeshView {
   const unsigned* __restrict__ eslot;     // task of local edge l: bits 10l..10l+9
 };
 
-// Stage tiles: up to kTile consecutive elements and kStageThreads edge tasks
-// per block of kStageThreads.
-#ifndef DGSWEM_TILE
-#define DGSWEM_TILE 128
-#endif
-#ifndef DGSWEM_STAGE_THREADS
-#define DGSWEM_STAGE_THREADS 384
-#endif
-constexpr int kTile = DGSWEM_TILE;
-constexpr int kStageThreads = DGSWEM_STAGE_THREADS;
+// Stage tile shapes the stage kernel is compiled in: a tile of up to `tile`
+// consecutive elements and `threads` edge tasks per block of `threads`.
+// Every shape gives the same results bit for bit (each edge point's flux is
+// evaluated in the reference's in/ex orientation whichever tile evaluates
+// it, and each element's sums keep the reference's order); the autotuner
+// (dgswem_cuda_autotune) picks the fastest for a mesh.  `tile` is a multiple
+// of 32 (phase 3 keeps an area point per warp) and `threads` a multiple of
+// `tile` above it (phase 1 copies rows by whole groups of `tile` threads).
+struct TileShape {
+  int tile, threads;
+};
+constexpr int kNumTileShapes = 4;
+constexpr TileShape kTileShapes[kNumTileShapes] = {{128, 384}, {64, 192}, {64, 256}, {256, 768}};
+constexpr int kDefaultTileShape = 0;
+// Block sizes of the limiter / WETDRY element kernel (limit_wetdry), each
+// compiled for 1024 resident threads per SM except the last (768: more
+// registers per thread)
+constexpr int kNumLimitShapes = 3;
+constexpr int kLimitBlocks[kNumLimitShapes] = {256, 128, 256};
+constexpr int kLimitMinBlocks[kNumLimitShapes] = {4, 8, 3};
+constexpr int kDefaultLimitShape = 0;
 constexpr unsigned kNoTask = 1023u;
+constexpr int kMaxTileSlots = 512;  // tile + halo rows addressable by a task word's 9-bit slots
 
 // Task word of the tile plan.  Slots index the tile's shared-memory element
-// rows: 0..kTile-1 the tile's own elements, kTile+j halo element j.
+// rows: 0..tile-1 the tile's own elements, tile+j halo element j.
 struct TaskBits {
   static constexpr int kKind = 0;     // 3 bits, EdgeKind
   static constexpr int kLedIn = 3;    // 2 bits, local edge of the in side
@@ -163,24 +176,26 @@ struct StageLayout {
   unsigned qs, geo, qf, vol, res, wd, gid, tdry, info, bytes;
 };
 __host__ __device__ inline unsigned align16(unsigned x) { return (x + 15u) & ~15u; }
-// rb: bytes of the arithmetic type of the edge and volume terms (8: FP64
-// kernels; 4: mixed precision, which adds the FP32 slot copy qf)
-__host__ __device__ inline StageLayout stage_layout(int max_halo, int max_tasks, unsigned rb) {
+// tile: elements per tile of the shape; rb: bytes of the arithmetic type of
+// the edge and volume terms (8: FP64 kernels; 4: mixed precision, which adds
+// the FP32 slot copy qf)
+__host__ __device__ inline StageLayout stage_layout(int tile, int max_halo, int max_tasks, unsigned rb) {
   StageLayout L;
-  const unsigned S = kTile + (unsigned)max_halo;
+  const unsigned nt = (unsigned)tile;
+  const unsigned S = nt + (unsigned)max_halo;
   const unsigned T = (unsigned)max_tasks;
   L.qs = align16(rb == 8u ? (unsigned)sizeof(BasisT<double>) : (unsigned)sizeof(BasisT<float>));
   // qs[S][kQStride]: ZE, QX, QY, HB modes (mixed: the tile's own slots only,
   // for the FP64 SSP combination; the edge and volume terms read qf)
-  L.geo = L.qs + kQStride * (rb == 8u ? S : (unsigned)kTile) * 8u;
-  L.qf = L.geo + kGeoRows * kTile * rb;        // geo[kGeoRows][kTile] in the arithmetic type
+  L.geo = L.qs + kQStride * (rb == 8u ? S : nt) * 8u;
+  L.qf = L.geo + kGeoRows * nt * rb;           // geo[kGeoRows][tile] in the arithmetic type
   L.vol = L.qf + (rb == 8u ? 0u : kQfStride * S * 4u);  // qf[S][kQfStride] (mixed only)
-  L.res = L.vol + kVolRows * 3u * kTile * rb;  // vol[kVolRows][3][kTile]
+  L.res = L.vol + kVolRows * 3u * nt * rb;     // vol[kVolRows][3][tile]
   L.wd = L.res + 15u * T * rb;                 // res[task][point][5]
   L.gid = align16(L.wd + S * 4u);              // wd[S]
   L.tdry = align16(L.gid + (unsigned)max_halo * 4u);
   L.info = align16(L.tdry + T * 4u);          // einfo, eslot of the tile's elements
-  L.bytes = align16(L.info + 2u * kTile * 4u);
+  L.bytes = align16(L.info + 2u * nt * 4u);
   return L;
 }
 
@@ -238,10 +253,11 @@ struct LimitArgs {
 #define DGSWEM_DECLARE_LAUNCHERS(NS)                                                           \
   namespace NS {                                                                               \
   void set_basis(const BasisP1& b);                                                            \
-  void launch_stage(const StageArgs& a, bool nonlin, unsigned grid, size_t smem, cudaStream_t s); \
+  void launch_stage(const StageArgs& a, bool nonlin, int shape, unsigned grid, size_t smem,       \
+                    cudaStream_t s);                                                           \
   void launch_ibarrier(const StageArgs& a, bool nonlin, cudaStream_t s);                       \
   void launch_node_minmax(const LimitArgs& a, unsigned grid, cudaStream_t s);                  \
-  void launch_limit_wetdry(const LimitArgs& a, unsigned grid, cudaStream_t s);                 \
+  void launch_limit_wetdry(const LimitArgs& a, int shape, cudaStream_t s);                      \
   void launch_modal2nodal(const MeshView& m, const double* q, const int* wd, double nleq,      \
                           double leq, double* eta2, double* uu2, double* vv2, int* nodecode,   \
                           unsigned grid, cudaStream_t s);                                      \

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 
 // ---------------------------------------------------------------------------
 // Tile stage kernel.  Block b owns tile b of the tile plan built at create:
-// up to kTile consecutive elements, and for them the edge
+// up to kTile consecutive elements (the shape's tile), and for them the edge
 // tasks the tile evaluates (boundary edges, edges to out-of-tile elements,
 // shared interior edges once) and the halo of out-of-tile neighbours those
 // tasks read.  Four phases separated by barriers, each spread over all
@@ -389,10 +389,15 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 // internal_edge_hydro.F, *_edge_hydro.F, rhs_dg_hydro.F, DG_hydro_timestep.F:238-290
 // ---------------------------------------------------------------------------
 
-// resident stage blocks per SM the register allocation targets
-#ifndef DGSWEM_STAGE_MIN_BLOCKS
-#define DGSWEM_STAGE_MIN_BLOCKS 2
+// resident stage threads per SM the register allocation targets (FP64: two
+// blocks of 384, at most 85 registers a thread); a shape of T threads per
+// block is compiled for that many over T resident blocks
+#ifndef DGSWEM_STAGE_RESIDENT_THREADS
+#define DGSWEM_STAGE_RESIDENT_THREADS 768
 #endif
+constexpr int stage_min_blocks(int threads) {
+  return DGSWEM_STAGE_RESIDENT_THREADS / threads > 0 ? DGSWEM_STAGE_RESIDENT_THREADS / threads : 1;
+}
 
 // The 12 modal values (ZE, QX, QY, HB modes, contiguous) of shared-memory
 // slot `slot` in the arithmetic type: the FP64 slots qs (stride kQStride),
@@ -449,7 +454,7 @@ __device__ __forceinline__ void trace_depth(const Physics& P, real z, real w, re
 // vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  C: the basis
 // tables in shared memory (I is a runtime index); qt: the slots in the
 // arithmetic type.
-template <bool kNonlin, bool kSph>
+template <bool kNonlin, bool kSph, int kTile>
 __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<real>& C, const real* qt,
                                               const real* geo, int I, int el, int e, real out[8]) {
   const MeshView& m = A.m;
@@ -535,11 +540,11 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<r
   out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
 }
 
-template <bool kNonlin, bool kSph>
+template <bool kNonlin, bool kSph, int kTile>
 __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisT<real>& C, const real* qt,
                                              const real* geo, real* vol, int I, int el, int e) {
   real v[8];
-  volume_values<kNonlin, kSph>(A, C, qt, geo, I, el, e, v);
+  volume_values<kNonlin, kSph, kTile>(A, C, qt, geo, I, el, e, v);
 #pragma unroll
   for (int r = 0; r < 8; ++r) vol[(r * 3 + I) * kTile + el] = v[r];
 }
@@ -554,7 +559,7 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisT<re
 // whole warp.  The sums are in the arithmetic type, the SSP combination in
 // FP64 (in the mixed variant: the RHS rounded to FP32, the stage states and
 // their combination FP64).
-template <bool kNonlin>
+template <bool kNonlin, int kTile>
 __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisT<real>& B, const double* qs,
                                              const real* geo, const real* vol, const real* res,
                                              const int* tdry, const unsigned* sinfo, const int* wds, int tbeg,
@@ -693,8 +698,10 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisT<re
   if (bad) atomicOr(A.err, 1u);
 }
 
-template <bool kNonlin, bool kSph>
-__global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_p1(const __grid_constant__ StageArgs A) {
+template <bool kNonlin, bool kSph, int kTile, int kStageThreads>
+__global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads))
+    stage_p1(const __grid_constant__ StageArgs A) {
+  static_assert(kTile % 32 == 0 && kStageThreads % kTile == 0 && kStageThreads > kTile, "tile shape");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const MeshView& m = A.m;
   const Physics& P = A.ph;
@@ -705,7 +712,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   const int n = m.tile_elem_ptr[tile + 1] - tile0;
   const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
   const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
-  const StageLayout L = stage_layout(m.max_halo, m.max_tasks, (unsigned)sizeof(real));
+  const StageLayout L = stage_layout(kTile, m.max_halo, m.max_tasks, (unsigned)sizeof(real));
   BasisT<real>& B = *reinterpret_cast<BasisT<real>*>(smem_raw);
   double* qs = reinterpret_cast<double*>(smem_raw + L.qs);
   real* geo = reinterpret_cast<real*>(smem_raw + L.geo);
@@ -969,7 +976,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int i = w / kTile, el = w - i * kTile;
     if (el >= n || wds[el] == 0) continue;
-    volume_point<kNonlin, kSph>(A, B, qt, geo, vol, i, el, tile0 + el);
+    volume_point<kNonlin, kSph, kTile>(A, B, qt, geo, vol, i, el, tile0 + el);
   }
   __syncthreads();
 
@@ -977,7 +984,7 @@ __global__ void __launch_bounds__(kStageThreads, DGSWEM_STAGE_MIN_BLOCKS) stage_
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int var = w / kTile, el = w - var * kTile;
     if (el >= n) continue;
-    sum_variable<kNonlin>(A, B, qs, geo, vol, res, tdry, sinfo, wds, tbeg, var, el, tile0 + el);
+    sum_variable<kNonlin, kTile>(A, B, qs, geo, vol, res, tdry, sinfo, wds, tbeg, var, el, tile0 + el);
   }
 }
 
@@ -1015,10 +1022,12 @@ __device__ __forceinline__ real div_count(real x, int kdp) {
 // by wetdry.F:61-548 for the same element.  The limiter arithmetic is in the
 // arithmetic type (FP32 in the mixed variant, on deviations from the element
 // mean, which it does not change), WETDRY in FP64.
-// 4 resident blocks of 256 per SM (64 registers, no spills): more warps to
-// cover the limiter's dependent FP64 chains than the 3 blocks an unbounded
-// allocation allows
-__global__ void __launch_bounds__(256, 4) limit_wetdry(const __grid_constant__ LimitArgs L) {
+// Compiled per limiter shape (kLimitBlocks / kLimitMinBlocks): 1024 resident
+// threads per SM (64 registers, no spills: more warps to cover the
+// limiter's dependent FP64 chains than an unbounded allocation allows) in
+// blocks of 256 or 128, or 768 (85 registers).
+template <int kBlock, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_constant__ LimitArgs L) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const int ne = L.m.ne, np = L.m.np;
   if (e >= L.ne_act) return;

@@ -8,7 +8,7 @@
 #define DGSWEM_FAST_MATH 1
 #define DGSWEM_MIXED 1
 // FP32 terms need fewer registers and a smaller tile in shared memory:
-// three resident stage blocks per SM (56 registers)
-#define DGSWEM_STAGE_MIN_BLOCKS 3
+// 1152 resident stage threads per SM (three blocks of 384, 56 registers)
+#define DGSWEM_STAGE_RESIDENT_THREADS 1152
 #include "hydro_kernels.cuh"
 #include "kernel_launch.inc"

@@ -70,6 +70,11 @@ class Ensemble:
     def synchronize(self) -> None:
         self.hs.synchronize()
 
+    def autotune(self, it: int = 1, steps: int = 10, reps: int = 3, cached: bool = True) -> dict:
+        """Tile and limiter block shapes for the merged mesh, timed over all
+        members' whole steps (HydroStep.autotune); the states stay as they were."""
+        return self.hs.autotune(it, steps, reps, cached)
+
     # -- results per member -------------------------------------------------------
     def _split_elems(self, arrays):
         return [tuple(a[self.elem_off[i]:self.elem_off[i + 1]] for a in arrays) for i in range(len(self))]

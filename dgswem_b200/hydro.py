@@ -164,6 +164,49 @@ class HydroStep:
         of ``steps`` (even) steps; 0 turns graphs off."""
         _abi.check(self._lib.dgswem_cuda_set_graph(self._h, int(steps)))
 
+    # ---- tile / block shapes and the autotuner ----
+    @staticmethod
+    def shapes() -> dict:
+        """dgswem_cuda_shapes: the stage tile shapes ``(elements, threads)``
+        and the limiter shapes ``(threads, resident blocks per SM)`` the
+        kernels are compiled for."""
+        lib = _abi.load()
+        nt, nl = C.c_int(), C.c_int()
+        te = np.zeros(_abi.MAX_SHAPES, np.int32)
+        tt = np.zeros(_abi.MAX_SHAPES, np.int32)
+        lt = np.zeros(_abi.MAX_SHAPES, np.int32)
+        lb = np.zeros(_abi.MAX_SHAPES, np.int32)
+        _abi.check(lib.dgswem_cuda_shapes(C.byref(nt), _iptr(te), _iptr(tt), C.byref(nl), _iptr(lt), _iptr(lb)))
+        return {"tile": [(int(te[i]), int(tt[i])) for i in range(nt.value)],
+                "limiter": [(int(lt[i]), int(lb[i])) for i in range(nl.value)]}
+
+    def set_shapes(self, tile: int = -1, limiter: int = -1) -> None:
+        """dgswem_cuda_set_shapes: stage tile shape / limiter block by index
+        into ``shapes()`` (-1 keeps the current one)."""
+        _abi.check(self._lib.dgswem_cuda_set_shapes(self._h, int(tile), int(limiter)))
+
+    def get_shapes(self) -> tuple[int, int]:
+        t, l = C.c_int(), C.c_int()
+        _abi.check(self._lib.dgswem_cuda_get_shapes(self._h, C.byref(t), C.byref(l)))
+        return t.value, l.value
+
+    def autotune(self, it: int = 1, steps: int = 10, reps: int = 3, cached: bool = True) -> dict:
+        """dgswem_cuda_autotune: time ``steps`` steps from step ``it`` with
+        every tile shape, then every limiter block, keep the fastest; the
+        state is left as it was.  Returns the picked indices and the
+        milliseconds per step of each shape (None: not timed)."""
+        sh = self.shapes()
+        mt = np.zeros(_abi.MAX_SHAPES, np.float64)
+        ml = np.zeros(_abi.MAX_SHAPES, np.float64)
+        flags = _abi.TUNE_CACHED if cached else 0
+        _abi.check(self._lib.dgswem_cuda_autotune(self._h, int(it), int(steps), int(reps), flags, _dptr(mt),
+                                                  _dptr(ml)))
+        t, l = self.get_shapes()
+        fix = lambda v: None if v < 0 else float(v)  # noqa: E731
+        return {"tile": t, "limiter": l, "tile_shape": sh["tile"][t], "limiter_shape": sh["limiter"][l],
+                "ms_tile": [fix(mt[i]) for i in range(len(sh["tile"]))],
+                "ms_limiter": [fix(ml[i]) for i in range(len(sh["limiter"]))]}
+
     @property
     def stream_handle(self) -> int:
         return int(self._lib.dgswem_cuda_stream(self._h) or 0)

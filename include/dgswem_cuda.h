@@ -228,6 +228,38 @@ long long dgswem_cuda_kernel_launches(const dgswem_cuda* h);
  * per-kernel profiling is on.  No counterpart in the reference. */
 int dgswem_cuda_set_graph(dgswem_cuda* h, int steps);
 
+/* ---- tile and block shapes, autotuner ------------------------------------
+ * The stage kernel is compiled for several tile shapes (elements per tile,
+ * threads per block) and the limiter / WETDRY kernel for several block
+ * sizes; every shape gives bit-identical results.  dgswem_cuda_shapes lists
+ * them (arrays of up to DGSWEM_CUDA_MAX_SHAPES entries, any may be NULL;
+ * a limiter shape is its threads per block and the resident blocks per SM
+ * its registers were allocated for).
+ * dgswem_cuda_set_shapes selects one of each by index (-1 keeps the current
+ * one) and rebuilds the stage tile plan; DGSWEM_ERR_ARG if the tile shape's
+ * plan does not fit the mesh (the current plan stays).  Captured CUDA graphs
+ * are released.
+ *
+ * dgswem_cuda_autotune times `steps` whole steps from step `it` (forcing of
+ * steps it..it+steps-1), best of `reps`, with each tile shape, then with
+ * each limiter block size under the fastest tile shape, every timing from
+ * the handle's current state; it restores that state (ZE, QX, QY, WDFLG and
+ * the NaN flag) and keeps the fastest shapes.  ms_tile / ms_limit (NULL or
+ * arrays of the shape counts) receive milliseconds per step, -1 for a shape
+ * not timed (its plan does not fit, or no limiter / WETDRY runs).  With
+ * DGSWEM_CUDA_TUNE_CACHED a result measured earlier in this process for the
+ * same mesh signature (variant, device, sizes, edge graph, physics
+ * switches) is reused without timing.  Whole-mesh handles only
+ * (dgswem_cuda_create).  No counterpart in the reference. */
+#define DGSWEM_CUDA_MAX_SHAPES 8
+#define DGSWEM_CUDA_TUNE_CACHED 1
+int dgswem_cuda_shapes(int* n_tile, int* tile_elems, int* tile_threads, int* n_limit, int* limit_threads,
+                       int* limit_blocks_per_sm);
+int dgswem_cuda_set_shapes(dgswem_cuda* h, int tile_shape, int limit_shape);
+int dgswem_cuda_get_shapes(const dgswem_cuda* h, int* tile_shape, int* limit_shape);
+int dgswem_cuda_autotune(dgswem_cuda* h, int it, int steps, int reps, int flags, double* ms_tile,
+                         double* ms_limit);
+
 /* Launch on the caller's CUDA stream (a cudaStream_t passed as void*, used
  * as given: NULL is the CUDA default stream).  dgswem_cuda_stream() returns
  * the stream in use, so a caller can restore the library's own stream.
