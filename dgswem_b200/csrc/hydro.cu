@@ -1357,7 +1357,7 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     h->wd.alloc(nl);
     h->wd_staging.alloc(s->ne);
     h->nodecode.alloc(s->np);
-    h->minmax.alloc(6 * npl);
+    h->minmax.alloc(6 * (size_t)npl);
     h->err.alloc(1);
     DG_CUDA(cudaMemset(h->err.p, 0, sizeof(unsigned)));
     if (s->nws == 1) {

@@ -238,7 +238,7 @@ struct LimitArgs {
   MeshView m;
   Physics ph;
   double* q;                 // stage output, limited / wet-dried in place
-  double* minmax;            // [6*NP]: zmin zmax qxmin qxmax qymin qymax
+  double* minmax;            // [6*NP]: (min, max) pairs of ZE, QX, QY means per node
   int* wd;                   // WDFLG (read + write)
   int slopeflag, wetdry;
   int ne_act;                // elements limited / wet-dried: the owned ones (the first ne_act)

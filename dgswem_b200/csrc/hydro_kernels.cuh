@@ -988,7 +988,11 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   }
 }
 
-// slopelimiter.F:3300-3404: min/max of element means over each node's star
+// slopelimiter.F:3300-3404: min/max of element means over each node's star,
+// stored as (min, max) pairs per variable, minmax[(var*NP + n)*2 + {0,1}]:
+// the limiter pass gathers a node's bounds of a variable with one 16-byte
+// load (one sector; six separate arrays took two 8-byte loads from two
+// sectors), and this pass writes three coalesced pair arrays.
 __global__ void node_minmax(const __grid_constant__ LimitArgs L) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= L.m.np) return;
@@ -1000,13 +1004,16 @@ __global__ void node_minmax(const __grid_constant__ LimitArgs L) {
     zmin = fmin(zmin, zt); xmin = fmin(xmin, xt); ymin = fmin(ymin, yt);
     zmax = fmax(zmax, zt); xmax = fmax(xmax, xt); ymax = fmax(ymax, yt);
   }
-  const int np = L.m.np;
-  L.minmax[n] = zmin;
-  L.minmax[(size_t)np + n] = zmax;
-  L.minmax[(size_t)2 * np + n] = xmin;
-  L.minmax[(size_t)3 * np + n] = xmax;
-  L.minmax[(size_t)4 * np + n] = ymin;
-  L.minmax[(size_t)5 * np + n] = ymax;
+  const size_t np = (size_t)L.m.np;
+  double2* o = reinterpret_cast<double2*>(L.minmax);
+  o[n] = make_double2(zmin, zmax);
+  o[np + n] = make_double2(xmin, xmax);
+  o[2 * np + n] = make_double2(ymin, ymax);
+}
+
+// bounds (min, max) of variable var at node nd
+__device__ __forceinline__ double2 node_bounds(const double* minmax, int np, int nd, int var) {
+  return reinterpret_cast<const double2*>(minmax)[(size_t)var * np + nd];
 }
 
 // x / d for the redistribution divisor d = max(1, kdp) in {1, 2, 3}: x / 1
@@ -1052,8 +1059,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
       real vmin[3], vmax[3], vx[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        vmin[a] = (real)(L.minmax[(size_t)(2 * var) * np + nd[a]] - zc[0]);
-        vmax[a] = (real)(L.minmax[(size_t)(2 * var + 1) * np + nd[a]] - zc[0]);
+        const double2 bd = node_bounds(L.minmax, np, nd[a], var);
+        vmin[a] = (real)(bd.x - zc[0]);
+        vmax[a] = (real)(bd.y - zc[0]);
         vx[a] = (real)(B.phi_corner[a][1] * zc[1] + B.phi_corner[a][2] * zc[2]);
         vx[a] = fmax(fmin(vx[a], vmax[a]), vmin[a]);
       }
@@ -1062,8 +1070,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
       real vmin[3], vmax[3], vx[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        vmin[a] = L.minmax[(size_t)(2 * var) * np + nd[a]];
-        vmax[a] = L.minmax[(size_t)(2 * var + 1) * np + nd[a]];
+        const double2 bd = node_bounds(L.minmax, np, nd[a], var);
+        vmin[a] = bd.x;
+        vmax[a] = bd.y;
         vx[a] = zc[0] + B.phi_corner[a][1] * zc[1] + B.phi_corner[a][2] * zc[2];
         vx[a] = fmax(fmin(vx[a], vmax[a]), vmin[a]);
       }
