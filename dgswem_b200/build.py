@@ -60,7 +60,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     inputs = [CSRC / s for s, _ in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "dgswem_cuda.h"]
     if not force and not _stale(out, inputs):
         return out
-    objs = []
+    objs, cmds = [], []
     build = PKG / "_build"
     build.mkdir(exist_ok=True)
     for src, extra in SOURCES:
@@ -69,8 +69,14 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
                "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units compile independently: one nvcc per unit at once
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c, check=False), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     link = [nvcc(), "-ccbin", host_cxx(), "-shared", "-Xcompiler", "-fopenmp", *ARCH, "-o", str(out), *objs]
     subprocess.run(link, check=True)
     return out

