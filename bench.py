@@ -21,6 +21,8 @@ afterwards; "tiles" objects give the picks and per-shape times);
 The line's "mixed" object is the mixed-precision form (FP32 edge, volume and
 limiter terms; FP64 state, SSP combination and wet/dry) on the same deck: its
 rate, its speed-up over the FP64 line and its error against the FP64 form.
+The "config3" object is the 8M-element quarter annulus with wind (config 3
+at p=1): FP64 and mixed rates and the mixed form's error against FP64.
 The "ensemble" object is the batched configuration: 256 seeded members of
 5k-200k elements (about 13.5M in all) advanced by one handle in mixed
 precision, with the batched-vs-one-at-a-time rate of its first 16 members.
@@ -225,6 +227,71 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
             "dtype": "f32 edge/volume/limiter terms, f64 state, SSP, wet/dry",
             "per_kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items() if v[1]},
             "tiles": tiles, "err_vs_fp64": err}
+
+
+def config3_arm(args, stream, device: int, world: int, dist) -> dict:
+    """Config 3 at p=1: the quarter annulus of config 1 refined to
+    ``--config3-nr`` x ``--config3-nth`` cells (8M triangles by default),
+    h = 3.048 (r / 60.96 km)^2 m, M2 tide of 0.3048 m on the outer arc,
+    linear friction tau = 1e-4 1/s, dt = 0.5 s, and a uniform wind stress of
+    0.1 Pa at 30 degrees (NWS=1: WSX2 = tau/rho0 cos 30, WSY2 = tau/rho0
+    sin 30, PR2 = 0).  FP64 and mixed rates with the FP64 line's timing
+    rules, and the mixed form's error against the FP64 form after
+    ``--config3-err-steps`` steps from the same state.  The reference's p=2
+    path is broken (p=2 is not on the device), so this is the p=1 half of
+    the configuration."""
+    import torch
+    from dgswem_b200 import Deck, HydroStep, decks
+    nr, nth = args.config3_nr, args.config3_nth
+    t0 = time.perf_counter()
+    path = decks.quarter_annulus(Path(args.workdir) / f"config3_{nr}x{nth}", nr=nr, nth=nth, nsteps=5000,
+                                 dt=0.5, nws=1)
+    t_write = time.perf_counter() - t0
+    deck = Deck(path)
+    npn = deck.s.np
+    tau_rho = 0.1 / 1000.0
+    met = (np.full(npn, tau_rho * math.cos(math.radians(30.0))), np.full(npn, tau_rho * math.sin(math.radians(30.0))),
+           np.zeros(npn))
+    k, w = args.config3_steps, args.warmup
+    out = {"workload": f"quarter annulus {nr}x{nth} cells, {deck.s.ne} elements, FP64/mixed DG p=1, SSP-RK(2,2), "
+                       "linear friction, wind 0.1 Pa at 30 degrees (NWS=1), dt=0.5 s",
+           "elements": int(deck.s.ne), "steps": k, "warmup": w, "deck_write_s": t_write}
+    states = {}
+    for name, kw in (("fp64", {}), ("mixed", {"mixed": True})):
+        with HydroStep(deck, device=device, **kw) as h:
+            h.set_stream(stream.cuda_stream)
+            h.set_met(*met)
+            h.run(1, w)
+            tiles = autotune(h, args, w + 1)
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.run(w + 1, k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+            out[name] = {"value": whole_job_rate(world, deck.s.ne, deck.s.nrk, k, ms), "unit": "DOF-stage/s",
+                         "ms_per_step": ms / k,
+                         "tile_shape": tiles["tile_shape"] if tiles else None}
+        with HydroStep(deck, device=device, **kw) as h:
+            h.set_stream(stream.cuda_stream)
+            h.set_met(*met)
+            h.run(1, args.config3_err_steps)
+            h.synchronize()
+            states[name] = (h.state(), h.modal2nodal())
+    (sf, nf), (sm, nmx) = states["fp64"], states["mixed"]
+    mf, mm = mass(deck, sf[0]), mass(deck, sm[0])
+    out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["mixed"]["err_vs_fp64"] = {
+        "steps": args.config3_err_steps,
+        "eta_nodal_linf_m": float(np.abs(nmx[0] - nf[0]).max()),
+        "ze_mean_linf_m": float(np.abs(sm[0][:, 0] - sf[0][:, 0]).max()),
+        "vel_nodal_linf_ms": float(max(np.abs(nmx[1] - nf[1]).max(), np.abs(nmx[2] - nf[2]).max())),
+        "mass_rel": (mm - mf) / mf}
+    deck.close()
+    return out
 
 
 def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
@@ -454,6 +521,11 @@ def main(argv=None):
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tile / limiter block shapes")
     ap.add_argument("--tune-steps", type=int, default=10, help="steps per shape timing of the autotuner")
+    ap.add_argument("--config3-steps", type=int, default=100,
+                    help="timed steps of the 8M-element config-3 annulus with wind (0: skip)")
+    ap.add_argument("--config3-nr", type=int, default=1000)
+    ap.add_argument("--config3-nth", type=int, default=4000)
+    ap.add_argument("--config3-err-steps", type=int, default=200)
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=40)
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
@@ -583,6 +655,8 @@ def main(argv=None):
         mixed = mixed_arm(deck, stream, args, world, dist if world > 1 else None, local)
         mixed["speedup_vs_fp64"] = mixed["value"] / value
         line["mixed"] = mixed
+    if args.config3_steps > 0:
+        line["config3"] = config3_arm(args, stream, local, world, dist if world > 1 else None)
     if args.ensemble_members > 0:
         line["ensemble"] = ensemble_arm(args, stream, local, world, dist if world > 1 else None)
     if args.adjoint_steps > 0 and world == 1:

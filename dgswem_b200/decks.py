@@ -17,7 +17,9 @@ edge neighbours sit a few hundred entries apart in every array.
 """
 from __future__ import annotations
 
+import io
 import math
+import os
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -65,6 +67,29 @@ def _fmt(v: float) -> str:
     return repr(float(v))
 
 
+def _savetxt_chunk(args) -> str:
+    arr, fmt = args
+    buf = io.StringIO()
+    np.savetxt(buf, arr, fmt=fmt)
+    return buf.getvalue()
+
+
+def _savetxt(f, arr, fmt, rows_per_chunk: int = 250_000) -> None:
+    """np.savetxt of ``arr`` into ``f``; tables of more than a million rows
+    are formatted in chunks on spawned worker processes (the same text)."""
+    n = len(arr)
+    workers = min(16, os.cpu_count() or 1)
+    if n <= 1_000_000 or workers < 2:
+        np.savetxt(f, arr, fmt=fmt)
+        return
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    chunks = [(arr[i:i + rows_per_chunk], fmt) for i in range(0, n, rows_per_chunk)]
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as pool:
+        for text in pool.map(_savetxt_chunk, chunks):
+            f.write(text)
+
+
 def write_deck(path, x, y, dp, elems, open_segs, land_segs, ctl: Controls, emo=None, efa=None,
                manning=None, flow=None):
     """Write fort.14, fort.15, fort.dg (and fort.13 when ``manning`` is given).
@@ -80,8 +105,8 @@ def write_deck(path, x, y, dp, elems, open_segs, land_segs, ctl: Controls, emo=N
     ids = np.arange(1, npn + 1)
     with open(path / "fort.14", "w") as f:
         f.write(f"{ctl.title}\n{ne} {npn}\n")
-        np.savetxt(f, np.column_stack([ids, x, y, dp]), fmt=["%d", "%.10f", "%.10f", "%.10f"])
-        np.savetxt(f, np.column_stack([np.arange(1, ne + 1), np.full(ne, 3), elems]), fmt="%d")
+        _savetxt(f, np.column_stack([ids, x, y, dp]), fmt=["%d", "%.10f", "%.10f", "%.10f"])
+        _savetxt(f, np.column_stack([np.arange(1, ne + 1), np.full(ne, 3), elems]), fmt="%d")
         neta = sum(len(s) for s in open_segs)
         f.write(f"{len(open_segs)} ! NOPE\n{neta} ! NETA\n")
         for s in open_segs:

@@ -60,3 +60,21 @@ def test_partition_handle_rejects_whole_mesh_calls(built, scratch):
             hs.timestep(1)
         with pytest.raises(DgswemError, match="whole mesh"):
             hs.modal2nodal()
+
+
+def test_partitions_with_other_tile_shapes(built):
+    """Each partition's tile plan rebuilt for another tile and limiter shape
+    (dgswem_cuda_set_shapes on a partition handle: tiles cover its owned
+    elements) still reproduces the single-handle run bit for bit."""
+    from conftest import golden_dir
+    deck = Deck(golden_dir("wetdry"))
+    with HydroStep(deck) as hs:
+        hs.run(1, 80)
+        ref = hs.state()
+    nshape = len(HydroStep.shapes()["tile"])
+    with PartitionedRun(deck, 3) as pr:
+        for i, p in enumerate(pr.parts):
+            p.set_shapes((i + 1) % nshape, i % len(HydroStep.shapes()["limiter"]))
+        pr.run(1, 80)
+        got = pr.state()
+    check_equal(ref, got)
