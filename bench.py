@@ -100,6 +100,31 @@ def ensure_deck(workdir: Path, nx: int, ny: int, rank: int, world: int, dist=Non
     return path
 
 
+def rank0_first(rank: int, world: int, dist, fn):
+    """fn() on rank 0 first -- it writes decks into the shared work directory
+    -- then, after a barrier, on the other ranks, which find the decks
+    complete and only open them (no two ranks write the same files); every
+    rank gets fn's result."""
+    out = fn() if rank == 0 else None
+    if world > 1 and dist is not None:
+        dist.barrier()
+    if rank != 0:
+        out = fn()
+    return out
+
+
+def config3_deck(workdir, nr: int, nth: int) -> Path:
+    """The config-3 quarter annulus (nr x nth cells, dt = 0.5 s, NWS=1) under
+    workdir, written unless complete."""
+    from dgswem_b200 import decks
+    path = Path(workdir) / f"config3_{nr}x{nth}"
+    done = path / ".complete"
+    if not done.exists():
+        decks.quarter_annulus(path, nr=nr, nth=nth, nsteps=5000, dt=0.5, nws=1)
+        done.write_text("ok\n")
+    return path
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -241,11 +266,10 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     path is broken (p=2 is not on the device), so this is the p=1 half of
     the configuration."""
     import torch
-    from dgswem_b200 import Deck, HydroStep, decks
+    from dgswem_b200 import Deck, HydroStep
     nr, nth = args.config3_nr, args.config3_nth
     t0 = time.perf_counter()
-    path = decks.quarter_annulus(Path(args.workdir) / f"config3_{nr}x{nth}", nr=nr, nth=nth, nsteps=5000,
-                                 dt=0.5, nws=1)
+    path = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth))
     t_write = time.perf_counter() - t0
     deck = Deck(path)
     npn = deck.s.np
@@ -306,7 +330,9 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
     from dgswem_b200.ensemble import Ensemble, make_members
     specs = decks.ensemble_specs(args.ensemble_members)
     t0 = time.perf_counter()
-    ds, met = make_members(Path(args.workdir) / "ensemble", specs, workers=min(16, os.cpu_count() or 1))
+    ds, met = rank0_first(rank_env()[0], world, dist,
+                          lambda: make_members(Path(args.workdir) / "ensemble", specs,
+                                               workers=min(16, os.cpu_count() or 1)))
     t_decks = time.perf_counter() - t0
     k, w = args.ensemble_steps, args.warmup
 

@@ -21,6 +21,16 @@ def main(rank: int, world: int, port: int, workdir: str, out: str) -> int:
     import bench
     path = bench.ensure_deck(Path(workdir), 6, 3, rank, world, dist)
     slowest = bench.max_over_ranks(10.0 * (rank + 1), world, dist, "cpu")
+    # decks of the config-3 and ensemble arms: rank 0 writes, the others open
+    from dgswem_b200 import Deck, decks
+    from dgswem_b200.ensemble import make_members
+    c3 = bench.rank0_first(rank, world, dist, lambda: bench.config3_deck(workdir, 4, 8))
+    d3 = Deck(c3)
+    c3_ne = d3.s.ne
+    d3.close()
+    specs = decks.ensemble_specs(3, seed=4, ne_min=100, ne_max=300)
+    ens, _ = bench.rank0_first(rank, world, dist, lambda: make_members(Path(workdir) / "ens", specs, nsteps=2))
+    ens_ne = [d.s.ne for d in ens]
     args = SimpleNamespace(workdir=workdir, nx=6, ny=3, steps=2, warmup=1, ref_max_steps=2, gpus=world)
     buf = io.StringIO()
     with contextlib.redirect_stdout(buf):
@@ -28,7 +38,8 @@ def main(rank: int, world: int, port: int, workdir: str, out: str) -> int:
     dist.barrier()
     dist.destroy_process_group()
     Path(out).write_text(json.dumps({"rank": rank, "deck": str(path), "complete": (path / ".complete").exists(),
-                                     "slowest": slowest, "rc": rc, "stdout": buf.getvalue()}))
+                                     "slowest": slowest, "rc": rc, "stdout": buf.getvalue(),
+                                     "config3_ne": c3_ne, "ensemble_ne": ens_ne}))
     return 0
 
 

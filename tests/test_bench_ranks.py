@@ -34,6 +34,9 @@ def test_bench_two_gloo_ranks(built, tmp_path):
     line = json.loads(res[0]["stdout"].strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+    # the config-3 and ensemble decks: written once by rank 0, read by both
+    assert res[0]["config3_ne"] == res[1]["config3_ne"] == 2 * 4 * 8
+    assert res[0]["ensemble_ne"] == res[1]["ensemble_ne"] and len(res[0]["ensemble_ne"]) == 3
 
 
 def test_whole_job_rate_counts_every_rank():
