@@ -9,8 +9,11 @@
  * build may contract a*b+c, so agreement with its golden files is at print
  * precision, not bitwise).
  *
- * Scope (the parity path): p=1 (p=2 generalised as in the p-generic boundary
- * code, unpinned), LLF flux (numerical_flux.F:750-1022, the flux the
+ * Scope (the parity path): p=1; p=2 generalised as in the p-generic boundary
+ * code -- the interior-edge sums run over every mode, where the reference's
+ * internal_edge_hydro.F:306-318,337-345 sum modes 1-3 only (its p=2 defect,
+ * which makes the higher modes unstable) -- and checked by its convergence
+ * order, not pinned to the reference; LLF flux (numerical_flux.F:750-1022, the flux the
  * reference compiles with _FLUX=2), SSP-RK (RKSSP), SLOPELIMITER5, WETDRY,
  * ocean/land/flow/radiation/external-barrier/internal-barrier edges, NWS=0/1,
  * rainfall=0/1, ICS=1/2, NOLIBF=0/1/2, Manning n from fort.13.
@@ -186,7 +189,7 @@ struct Model {
 
   // state: ZE[(s*NE + e)*dofh + k], s = 0..NRK  (reference stage s+1)
   std::vector<double> ZE, QX, QY, RHS_ZE, RHS_QX, RHS_QY, HB;
-  std::vector<double> ze_edge, qx_edge, qy_edge;  // [(e*3+slot)*3 + k]
+  std::vector<double> ze_edge, qx_edge, qy_edge;  // [(e*3+slot)*dofh + k]
   std::vector<int> WDFLG, NODECODE;
   std::vector<double> WSX2, WSY2, PR2, WSX_BASE, WSY_BASE, PR_BASE;
   // node star in element order: star[star_ptr[n] .. star_ptr[n+1])
@@ -1043,7 +1046,7 @@ void Model::prep_dg() {
   RHS_ZE.assign((size_t)NRK * NE * dofh, 0.0);
   RHS_QX = RHS_ZE; RHS_QY = RHS_ZE;
   HB.assign((size_t)NE * dofh, 0.0);
-  ze_edge.assign((size_t)NE * 9, 0.0); qx_edge = ze_edge; qy_edge = ze_edge;
+  ze_edge.assign((size_t)NE * 3 * dofh, 0.0); qx_edge = ze_edge; qy_edge = ze_edge;
   WDFLG.assign(NE, 1);
   NODECODE.assign(NP, 1);
   WSX2.assign(NP, 0.0); WSY2.assign(NP, 0.0); PR2.assign(NP, 0.0);
@@ -1483,7 +1486,9 @@ void Model::internal_edges() {
     int led_in = NEDSD[2 * ged], led_ex = NEDSD[2 * ged + 1];
     int el_in = NEDEL[2 * ged], el_ex = NEDEL[2 * ged + 1];
     if (WDFLG[el_in] == 0 && WDFLG[el_ex] == 0) continue;
-    double rin[3][3] = {{0}}, rex[3][3] = {{0}};  // [var][k]
+    // [var][k]; every mode (the reference sums modes 1-3 only, which is its
+    // p=2 defect; at p=1 the loops are the same)
+    double rin[3][6] = {{0}}, rex[3][6] = {{0}};
     double nx = COSNX[ged], ny = SINNX[ged], tx = -ny, ty = nx;
     double edfac_in = XLEN[ged] / AREAS[el_in], edfac_ex = XLEN[ged] / AREAS[el_ex];
     for (int i = 0; i < NEGP; ++i) {
@@ -1533,7 +1538,7 @@ void Model::internal_edges() {
           }
         }
       }
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < dofh; ++k) {
         double w_in = edfac_in * edgeq(k, gp_in, led_in);
         double w_ex = edfac_ex * edgeq(k, gp_ex, led_ex);
         rin[0][k] = rin[0][k] - w_in * f_hat_o;
@@ -1549,13 +1554,13 @@ void Model::internal_edges() {
       if (ELEM_EDGE[3 * el_ex + k] == ged) ind_ex = k;
       if (ELEM_EDGE[3 * el_in + k] == ged) ind_in = k;
     }
-    for (int k = 0; k < 3; ++k) {
-      ze_edge[((size_t)el_ex * 3 + ind_ex) * 3 + k] = rex[0][k];
-      qx_edge[((size_t)el_ex * 3 + ind_ex) * 3 + k] = rex[1][k];
-      qy_edge[((size_t)el_ex * 3 + ind_ex) * 3 + k] = rex[2][k];
-      ze_edge[((size_t)el_in * 3 + ind_in) * 3 + k] = rin[0][k];
-      qx_edge[((size_t)el_in * 3 + ind_in) * 3 + k] = rin[1][k];
-      qy_edge[((size_t)el_in * 3 + ind_in) * 3 + k] = rin[2][k];
+    for (int k = 0; k < dofh; ++k) {
+      ze_edge[((size_t)el_ex * 3 + ind_ex) * dofh + k] = rex[0][k];
+      qx_edge[((size_t)el_ex * 3 + ind_ex) * dofh + k] = rex[1][k];
+      qy_edge[((size_t)el_ex * 3 + ind_ex) * dofh + k] = rex[2][k];
+      ze_edge[((size_t)el_in * 3 + ind_in) * dofh + k] = rin[0][k];
+      qx_edge[((size_t)el_in * 3 + ind_in) * dofh + k] = rin[1][k];
+      qy_edge[((size_t)el_in * 3 + ind_in) * dofh + k] = rin[2][k];
     }
   }
 }
@@ -1565,19 +1570,20 @@ void Model::add_internal_flux() {
   const int s = IRK - 1;
 #pragma omp parallel for schedule(static)
   for (int l = 0; l < NE; ++l) {
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < dofh; ++k) {
       double zs = 0.0, xs = 0.0, ys = 0.0;
       for (int i = 0; i < 3; ++i) {
-        zs = zs + ze_edge[((size_t)l * 3 + i) * 3 + k];
-        xs = xs + qx_edge[((size_t)l * 3 + i) * 3 + k];
-        ys = ys + qy_edge[((size_t)l * 3 + i) * 3 + k];
+        zs = zs + ze_edge[((size_t)l * 3 + i) * dofh + k];
+        xs = xs + qx_edge[((size_t)l * 3 + i) * dofh + k];
+        ys = ys + qy_edge[((size_t)l * 3 + i) * dofh + k];
       }
       rze(s, l, k) = rze(s, l, k) + zs;
       rqx(s, l, k) = rqx(s, l, k) + xs;
       rqy(s, l, k) = rqy(s, l, k) + ys;
     }
-    for (int i = 0; i < 9; ++i) {
-      ze_edge[(size_t)l * 9 + i] = 0.0; qx_edge[(size_t)l * 9 + i] = 0.0; qy_edge[(size_t)l * 9 + i] = 0.0;
+    for (int i = 0; i < 3 * dofh; ++i) {
+      ze_edge[(size_t)l * 3 * dofh + i] = 0.0; qx_edge[(size_t)l * 3 * dofh + i] = 0.0;
+      qy_edge[(size_t)l * 3 * dofh + i] = 0.0;
     }
   }
 }
@@ -2085,6 +2091,13 @@ int orc_get_real_table(const orc_model* h, const char* which, double* out, int c
   else if (w == "X") v = &m.X;
   else if (w == "Y") v = &m.Y;
   else if (w == "HB") v = &m.HB;
+  // basis and area rule (p-generic): PHI_AREA[k*NAGP + i], the reference
+  // triangle's area points and weights (weights sum to 2), M_INV per mode
+  else if (w == "PHI_AREA") v = &m.PHI_AREA;
+  else if (w == "XAGP") v = &m.XAGP;
+  else if (w == "YAGP") v = &m.YAGP;
+  else if (w == "WAGP") v = &m.WAGP;
+  else if (w == "M_INV") v = &m.M_INV;
   else return -1;
   int n = (int)v->size();
   if (out) std::memcpy(out, v->data(), (size_t)std::min(n, cap) * sizeof(double));

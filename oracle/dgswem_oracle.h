@@ -53,8 +53,10 @@ void orc_set_met(orc_model* m, const double* wsx, const double* wsy, const doubl
  * "NEDSD" (2*nedges), "NIEDN","NLEDN","NEEDN","NFEDN","NREDN","NEBSEGN",
  * "NIBSEGN" (2*nibseg), "ELEM_EDGE" (3*ne).  Returns the element count. */
 int orc_get_int_table(const orc_model* m, const char* which, int* out, int cap);
-/* Real edge tables: "XLEN","COSNX","SINNX" (nedges), "AREAS" (ne),
- * "DP" (np), "X","Y" (np). */
+/* Real tables: "XLEN","COSNX","SINNX" (nedges), "AREAS" (ne), "DP" (np),
+ * "X","Y" (np), "HB" (dofh*ne); basis and area rule: "PHI_AREA"
+ * (dofh*NAGP, [k*NAGP + i]), "XAGP","YAGP","WAGP" (NAGP, reference
+ * triangle (-1,-1),(1,-1),(-1,1), weights summing to 2), "M_INV" (dofh). */
 int orc_get_real_table(const orc_model* m, const char* which, double* out, int cap);
 
 /* Full reference-style run writing fort.63 (elevation) to out_path. */
