@@ -26,8 +26,9 @@ LIBNAME = "libdgswem_cuda.so"
 # approximate ones (the flags do not change FP64 operations)
 SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_strict.cu", ["-fmad=false"]),
            ("kernels_mixed.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
-           ("adjoint.cu", ["-fmad=true"]), ("deck.cpp", []), ("partition.cpp", [])]
-HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
+           ("adjoint.cu", ["-fmad=true"]), ("kernels_p2_fast.cu", ["-fmad=true"]),
+           ("kernels_p2_strict.cu", ["-fmad=false"]), ("deck.cpp", []), ("partition.cpp", [])]
+HEADERS = ["hydro_device.cuh", "hydro_kernels.cuh", "hydro_p2.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # host code is compiled with OpenMP (the deck reader's tables, the edge search,
@@ -57,7 +58,8 @@ def _stale(target: Path, inputs) -> bool:
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     LIBDIR.mkdir(exist_ok=True)
     out = LIBDIR / LIBNAME
-    inputs = [CSRC / s for s, _ in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "dgswem_cuda.h"]
+    inputs = [CSRC / s for s, _ in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "dgswem_cuda.h",
+                                                                            Path(__file__)]
     if not force and not _stale(out, inputs):
         return out
     objs, cmds = [], []

@@ -926,11 +926,13 @@ extern "C" int dgswem_deck_open(const char* dir, dgswem_deck** out) {
     read_fort_dg(root, d.get());
     read_fort14_15(root, d.get(), &p);
     if (d->pl != d->ph) throw dgswem::Failure(DGSWEM_ERR_ARG, "p-adaptivity (pl != ph) is not supported");
-    if (d->ph != 1) throw dgswem::Failure(DGSWEM_ERR_ARG, "only p = 1 is supported by the device path");
+    if (d->ph != 1 && d->ph != 2) throw dgswem::Failure(DGSWEM_ERR_ARG, "only p = 1 and p = 2 are supported");
+    if (d->ph == 2 && (d->s.slopeflag != 0 || d->s.nolifa >= 2))
+      throw dgswem::Failure(DGSWEM_ERR_ARG, "the slope limiter and wetting/drying are p = 1 only, as in the reference");
     if (d->modal_ic != 0) throw dgswem::Failure(DGSWEM_ERR_ARG, "modal_ic != 0 is not supported by the deck reader");
     if (d->artdif != 0 || d->sedflag != 0)
       throw dgswem::Failure(DGSWEM_ERR_ARG, "artificial diffusion / sediment are not on this path");
-    d->s.dofh = 3;
+    d->s.dofh = (d->ph + 1) * (d->ph + 2) / 2;
     rk_tables(d.get());
     d->s.nrk = d->rk_stage;
     build_edges(d.get(), p);

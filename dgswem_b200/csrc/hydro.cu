@@ -98,6 +98,133 @@ static BasisP1 make_basis_p1() {
   return B;
 }
 
+// Orthogonal basis of degree <= 2 on the reference triangle and its r/s
+// derivatives at (X, Y), in the hierarchical order (P, Q-P), Q = 0..D,
+// P = 0..Q (orthogonal_basis_v1.F:50-244: the Jacobi-type recurrences in P
+// and Q, values below 1e-15 set to 0).
+static void ortho_basis_p2(double X, double Y, double* b, double* d1, double* d2) {
+  constexpr int D = 2;
+  double PHI[D + 1][D + 1] = {}, DP1[D + 1][D + 1] = {}, DP2[D + 1][D + 1] = {};
+  PHI[0][0] = 1.0;
+  PHI[1][0] = (1.0 + 2.0 * X + Y) / 2.0;
+  DP1[1][0] = 1.0;
+  DP2[1][0] = 1.0 / 2.0;
+  for (int P = 1; P <= D - 1; ++P) {
+    const double w = (1.0 - Y) / 2.0;
+    const double a = (2.0 * P + 1.0) / (P + 1.0), c = P / (P + 1.0);
+    PHI[P + 1][0] = a * PHI[1][0] * PHI[P][0] - c * (w * w) * PHI[P - 1][0];
+    DP1[P + 1][0] = a * (DP1[1][0] * PHI[P][0] + PHI[1][0] * DP1[P][0]) - c * (w * w) * DP1[P - 1][0];
+    DP2[P + 1][0] = a * (DP2[1][0] * PHI[P][0] + PHI[1][0] * DP2[P][0]) -
+                    c * ((Y - 1) / 2 * PHI[P - 1][0] + (w * w) * DP2[P - 1][0]);
+  }
+  for (int P = 0; P <= D - 1; ++P) {
+    const double f = (1.0 + 2.0 * P + (3.0 + 2.0 * P) * Y) / 2.0;
+    PHI[P][1] = PHI[P][0] * f;
+    DP1[P][1] = DP1[P][0] * f;
+    DP2[P][1] = DP2[P][0] * f + PHI[P][0] * (3.0 + 2.0 * P) / 2.0;
+  }
+  for (int Q = 1; Q <= D - 1; ++Q)
+    for (int P = 0; P <= D - Q - 1; ++P) {
+      const double AQ = (2.0 * Q + 2.0 + 2.0 * P) * (2.0 * Q + 3.0 + 2.0 * P) / (2.0 * Q + 2.0) / (Q + 2.0 + 2.0 * P);
+      const double t = 2.0 * P + 1.0;
+      const double BQ = (t * t) * (2.0 * Q + 2.0 + 2.0 * P) / (2.0 * Q + 2.0) / (2.0 * Q + 2.0 * P + 1.0) /
+                        (Q + 2.0 + 2.0 * P);
+      const double CQ = (Q + 2.0 * P + 1.0) * Q * (2.0 * Q + 3.0 + 2.0 * P) / (Q + 1.0) / (Q + 2.0 + 2.0 * P) /
+                        (2.0 * Q + 2.0 * P + 1.0);
+      PHI[P][Q + 1] = (AQ * Y + BQ) * PHI[P][Q] - CQ * PHI[P][Q - 1];
+      DP1[P][Q + 1] = (AQ * Y + BQ) * DP1[P][Q] - CQ * DP1[P][Q - 1];
+      DP2[P][Q + 1] = (AQ * Y + BQ) * DP2[P][Q] + AQ * PHI[P][Q] - CQ * DP2[P][Q - 1];
+    }
+  int k = 0;
+  for (int Q = 0; Q <= D; ++Q)
+    for (int P = 0; P <= Q; ++P, ++k) {
+      const double v0 = PHI[P][Q - P], v1 = DP1[P][Q - P], v2 = DP2[P][Q - P];
+      b[k] = std::fabs(v0) < 1.0e-15 ? 0.0 : v0;
+      if (d1) d1[k] = std::fabs(v1) < 1.0e-15 ? 0.0 : v1;
+      if (d2) d2[k] = std::fabs(v2) < 1.0e-15 ? 0.0 : v2;
+    }
+}
+
+// p=2 tables: the six-point area rule of degree 4 (quadrature_v1.F:245-262,
+// 802-840: two orbits of barycentric points on the reference triangle
+// (-1,-1), (1,-1), (-1,1), weights doubled to its area 2), the four-point
+// Gauss-Lobatto edge rule (quad_rules_general.F: +-1, +-sqrt(1/5), weights
+// from the Legendre polynomial of degree 3), M_INV, PHI_EDGE and EDGEQ as
+// prep_DG.F:648-870 builds them.
+static BasisP2 make_basis_p2() {
+  BasisP2 B{};
+  const double V1[2] = {-1.0, -1.0}, V2[2] = {1.0, -1.0}, V3[2] = {-1.0, 1.0};
+  const double Av[2] = {0.4459484909159648863183292538830519, 0.0915762135097707434595714634022015};
+  const double Wv[2] = {0.2233815896780114656950070084331228, 0.1099517436553218676383263249002105};
+  double xa[kP2Agp], ya[kP2Agp];
+  int n = 0;
+  for (int o = 0; o < 2; ++o) {
+    const double a = Av[o], b = Av[o], c = 1.0 - (a + b);
+    const double tri[3][3] = {{a, b, c}, {b, c, a}, {c, a, b}};
+    for (int r = 0; r < 3; ++r, ++n) {
+      xa[n] = V1[0] * tri[r][0] + V2[0] * tri[r][1] + V3[0] * tri[r][2];
+      ya[n] = V1[1] * tri[r][0] + V2[1] * tri[r][1] + V3[1] * tri[r][2];
+      B.wagp[n] = 2.0 * Wv[o];
+    }
+  }
+  for (int i = 0; i < kP2Agp; ++i) {
+    double phi[kP2Modes], dr[kP2Modes], ds[kP2Modes];
+    ortho_basis_p2(xa[i], ya[i], phi, dr, ds);
+    for (int k = 0; k < kP2Modes; ++k) {
+      B.phi_area[k][i] = phi[k];
+      B.drphi[k][i] = dr[k];
+      B.dsphi[k][i] = ds[k];
+    }
+    B.psi[0][i] = -1.0 / 2.0 * (xa[i] + ya[i]);
+    B.psi[1][i] = 1.0 / 2.0 * (xa[i] + 1.0);
+    B.psi[2][i] = 1.0 / 2.0 * (ya[i] + 1.0);
+  }
+  {
+    const double sq = std::sqrt(1.0 / 5.0), nrl = 2.0;
+    B.xegp[0] = -1.0; B.xegp[1] = -sq; B.xegp[2] = sq; B.xegp[3] = 1.0;
+    B.wegp[0] = 2.0 / ((nrl + 1.0) * (nrl + 2.0));
+    B.wegp[3] = B.wegp[0];
+    for (int m = 1; m <= 2; ++m) {
+      const double x = B.xegp[m];
+      double pm1 = 1.0, pc = x;
+      for (int q = 1; q <= 2; ++q) {
+        const double pn = ((2.0 * q + 1.0) * x * pc - q * pm1) / (q + 1.0);
+        pm1 = pc;
+        pc = pn;
+      }
+      B.wegp[m] = 2.0 / ((nrl + 1.0) * (nrl + 2.0) * pc * pc);
+    }
+  }
+  {
+    int k = 0;
+    for (int J = 0; J <= 2; ++J)
+      for (int I = 0; I <= J; ++I, ++k) {
+        const int JJ = J - I;
+        B.m_inv[k] = (2.0 * I + 1.0) * (2.0 * JJ + 2.0 * I + 2.0) / 4.0;
+      }
+  }
+  for (int l = 0; l < 3; ++l)
+    for (int q = 0; q < kP2Egp; ++q) {
+      const double t = B.xegp[q];
+      const double px = l == 0 ? -t : (l == 1 ? -1.0 : t);
+      const double py = l == 0 ? t : (l == 1 ? -t : -1.0);
+      double phi[kP2Modes];
+      ortho_basis_p2(px, py, phi, nullptr, nullptr);
+      for (int k = 0; k < kP2Modes; ++k) {
+        B.phi_edge[l][q][k] = phi[k];
+        B.edgeq[l][q][k] = 2.0 * B.m_inv[k] * phi[k] * B.wegp[q];
+      }
+    }
+  const double vx[3] = {-1.0, 1.0, -1.0}, vy[3] = {-1.0, -1.0, 1.0};
+  for (int v = 0; v < 3; ++v) ortho_basis_p2(vx[v], vy[v], B.phi_corner[v], nullptr, nullptr);
+  for (int k = 0; k < kP2Modes; ++k)
+    for (int i = 0; i < kP2Agp; ++i) {
+      B.mw[k][i] = B.m_inv[k] * B.wagp[i];
+      B.srfac[k][i] = B.m_inv[k] * B.wagp[i] * B.phi_area[k][i];
+    }
+  return B;
+}
+
 // Owning device allocation; movable, not copyable (a copy would free the
 // buffer twice).
 template <typename T>
@@ -168,6 +295,19 @@ static const Variant kMixed = {4, mixed::set_basis, mixed::launch_stage, mixed::
                                mixed::launch_fortran_to_soa, mixed::launch_soa_to_fortran,
                                mixed::launch_gather_int, mixed::launch_halo};
 
+// Launchers of the p=2 stage (kernels_p2_fast.cu / kernels_p2_strict.cu)
+struct P2Variant {
+  void (*set_basis)(const BasisP2&);
+  void (*stage)(const P2Args&, bool, cudaStream_t);
+  void (*modal2nodal)(const MeshView&, const double*, double, double, double*, double*, double*, int*,
+                      cudaStream_t);
+  void (*layout)(bool, const double*, double*, int, int, const int*, cudaStream_t);
+};
+static const P2Variant kFastP2 = {fast_p2::set_basis_p2, fast_p2::launch_p2_stage, fast_p2::launch_p2_modal2nodal,
+                                  fast_p2::launch_p2_layout};
+static const P2Variant kStrictP2 = {strict_p2::set_basis_p2, strict_p2::launch_p2_stage,
+                                    strict_p2::launch_p2_modal2nodal, strict_p2::launch_p2_layout};
+
 }  // namespace dgswem
 
 using namespace dgswem;
@@ -206,6 +346,14 @@ struct dgswem_cuda {
   // shape of the stage tiles (kTileShapes) and of the limiter blocks
   // (kLimitBlocks): the defaults, or set / picked by dgswem_cuda_autotune
   int tile_shape = kDefaultTileShape, limit_shape = kDefaultLimitShape;
+  // modes per variable: 3 (p=1) or 6 (p=2: the p=2 launchers, an edge list of
+  // interior edges from the in side and land / ocean edges, and the
+  // edge-point flux slots, 36 per element)
+  int dofh = 3;
+  const P2Variant* v2 = nullptr;
+  DevBuf<int> p2_edges;
+  DevBuf<double> p2_ef;
+  int p2_nedge = 0;
   DevBuf<double> emo_dg, efa_dg, qnam_dg, qnph_dg, ebht, ebcfsp, ibht, ibcfsb, ibcfsp;
   DevBuf<double> wsx, wsy, pr, minmax, staging;
   std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
@@ -279,6 +427,12 @@ struct dgswem_cuda {
 };
 
 namespace {
+
+// Entry points of the p=1 path only (the limiter and its reverse mode, the
+// adjoint, state slots, partitions, tile shapes, graphs)
+void need_p1(const dgswem_cuda* h, const char* what) {
+  if (h && h->dofh != 3) throw Failure(DGSWEM_ERR_ARG, std::string(what) + " is p=1 only");
+}
 
 void check_launch(dgswem_cuda* h, const char* what = "kernel") {
   ++h->launches;
@@ -656,9 +810,9 @@ void build_layout(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& pl
   h->x.upload(xd);
   h->y.upload(yd);
   h->dp.upload(node_permuted(s->dp));
-  std::vector<double> hb(3 * (size_t)nl);
+  std::vector<double> hb((size_t)h->dofh * nl);
   for (int i = 0; i < nl; ++i)
-    for (int k = 0; k < 3; ++k) hb[(size_t)k * nl + i] = s->hb[k + (size_t)s->dofh * perm[i]];
+    for (int k = 0; k < h->dofh; ++k) hb[(size_t)k * nl + i] = s->hb[k + (size_t)s->dofh * perm[i]];
   h->hb.upload(hb);
   // per-element coefficients: a scalar when uniform
   auto uniform = [&](const double* a, double* val) {
@@ -815,13 +969,17 @@ void build_halo(dgswem_cuda* h, const dgswem_cuda_setup* s, const PartPlan& plan
 // local elements' device state (stage buffer 1) and WDFLG.
 void upload_state(dgswem_cuda* h, const double* ze, const double* qx, const double* qy, const int* wdflg) {
   const int nl = h->ne, ng = h->ne_glob;
-  h->staging.ensure(3 * (size_t)ng);
+  const size_t dofh = (size_t)h->dofh;
+  h->staging.ensure(dofh * ng);
   const double* src[3] = {ze, qx, qy};
   for (int var = 0; var < 3; ++var) {
     if (!src[var]) continue;
-    DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], 3 * (size_t)ng * sizeof(double), cudaMemcpyHostToDevice,
+    DG_CUDA(cudaMemcpyAsync(h->staging.p, src[var], dofh * ng * sizeof(double), cudaMemcpyHostToDevice,
                             h->stream));
-    h->v->f2s(h->staging.p, h->q[0].p, nl, var, h->perm.p, grid_for(nl, kPointBlock), h->stream);
+    if (h->v2)
+      h->v2->layout(true, h->staging.p, h->q[0].p, nl, var, h->perm.p, h->stream);
+    else
+      h->v->f2s(h->staging.p, h->q[0].p, nl, var, h->perm.p, grid_for(nl, kPointBlock), h->stream);
     check_launch(h, "fortran_to_soa");
   }
   if (wdflg) {
@@ -877,7 +1035,45 @@ void stage_forcing(const dgswem_cuda* h, double timedg, double rampdg, double* o
 
 // One RK stage: the stage kernel writes stage buffer irk for the owned
 // elements (launch_stage_rhs), then the limiter and WETDRY (launch_limit).
+// The p=2 stage: edge kernel, then element kernel (SSP combination included).
+void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing) {
+  const int nrk = h->nrk;
+  P2Args A{};
+  A.m = h->mesh;
+  A.ph = h->ph;
+  A.irk = irk;
+  A.qin = h->q[irk - 1].p;
+  A.qout = h->q[irk].p;
+  for (int I = 1; I <= irk; ++I) {
+    A.qhist[I - 1] = h->q[I - 1].p;
+    A.rhist[I - 1] = h->rhs[I - 1].p;
+    A.a[I - 1] = h->atvd[(size_t)(irk - 1) * nrk + (I - 1)];
+    A.b[I - 1] = h->btvd[(size_t)(irk - 1) * nrk + (I - 1)] * h->dtdp;
+  }
+  A.rout = h->keep_rhs[irk - 1] ? h->rhs[irk - 1].p : nullptr;
+  double timedg;
+  stage_clock(h, it, irk, &timedg, &A.rampdg);
+  A.ocean_zg = forcing;
+  A.wsx = h->wsx.p;
+  A.wsy = h->wsy.p;
+  A.pr = h->pr.p;
+  A.ef = h->p2_ef.p;
+  A.edges = h->p2_edges.p;
+  A.nedge = h->p2_nedge;
+  A.ne_act = h->n_own;
+  A.err = h->err.p;
+  const bool nonlin = h->ph.nleq == 1.0 && h->ph.leq == 0.0;
+  LaunchTimer t(h, 0);
+  h->v2->stage(A, nonlin, h->stream);
+  ++h->launches;  // two kernels
+  t.done();
+}
+
 void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, const double* ramp = nullptr) {
+  if (h->v2) {
+    launch_stage_p2(h, it, irk, forcing);
+    return;
+  }
   const int nrk = h->nrk;
   StageArgs A{};
   A.m = h->mesh;
@@ -922,6 +1118,7 @@ void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, co
 
 // SLOPELIMITER5 and WETDRY on stage buffer irk (owned elements)
 void launch_limit(dgswem_cuda* h, int irk) {
+  if (h->v2) return;  // neither limiter nor WETDRY at p=2
   const bool wetdry = h->nolifa >= 2;
   if (h->slopeflag != 0 || wetdry) {
     LimitArgs L{};
@@ -1281,7 +1478,17 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     if (flags & ~(DGSWEM_CUDA_STRICT | DGSWEM_CUDA_MIXED)) throw Failure(DGSWEM_ERR_ARG, "unknown flags");
     if ((flags & DGSWEM_CUDA_STRICT) && (flags & DGSWEM_CUDA_MIXED))
       throw Failure(DGSWEM_ERR_ARG, "DGSWEM_CUDA_STRICT and DGSWEM_CUDA_MIXED exclude each other");
-    if (s->dofh != 3) throw Failure(DGSWEM_ERR_ARG, "only p=1 (DOFH=3) is implemented on the device");
+    if (s->dofh != 3 && s->dofh != kP2Modes)
+      throw Failure(DGSWEM_ERR_ARG, "DOFH must be 3 (p=1) or 6 (p=2)");
+    if (s->dofh == kP2Modes) {
+      if (nparts != 1) throw Failure(DGSWEM_ERR_ARG, "p=2 runs on a whole-mesh handle (dgswem_cuda_create)");
+      if (flags & DGSWEM_CUDA_MIXED) throw Failure(DGSWEM_ERR_ARG, "the mixed-precision form is p=1 only");
+      if (s->slopeflag != 0) throw Failure(DGSWEM_ERR_ARG, "the slope limiter is p=1 only, as in the reference");
+      if (s->nolifa >= 2) throw Failure(DGSWEM_ERR_ARG, "wetting and drying are p=1 only, as in the reference");
+      if (s->ics != 1) throw Failure(DGSWEM_ERR_ARG, "p=2 supports ICS=1");
+      if (s->nfeds || s->nreds || s->nebseg || s->nibseg)
+        throw Failure(DGSWEM_ERR_ARG, "p=2 supports land and ocean boundaries (no flow, radiation or barriers)");
+    }
     if (s->ne <= 0 || s->np <= 0 || s->nedges <= 0) throw Failure(DGSWEM_ERR_ARG, "empty mesh");
     if (s->nrk < 1 || s->nrk > kMaxStages) throw Failure(DGSWEM_ERR_ARG, "nrk out of range");
     if (s->nws != 0 && s->nws != 1) throw Failure(DGSWEM_ERR_ARG, "only NWS=0/1 are supported");
@@ -1295,6 +1502,8 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     std::unique_ptr<dgswem_cuda> h(new dgswem_cuda());
     h->device = device;
     h->v = (flags & DGSWEM_CUDA_STRICT) ? &kStrict : (flags & DGSWEM_CUDA_MIXED) ? &kMixed : &kFast;
+    h->dofh = s->dofh;
+    if (h->dofh == kP2Modes) h->v2 = (flags & DGSWEM_CUDA_STRICT) ? &kStrictP2 : &kFastP2;
     h->ne = s->ne;
     h->np = s->np;
     h->nrk = s->nrk;
@@ -1340,20 +1549,38 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
       kStrict.set_basis(B);
       kMixed.set_basis(B);
       adj::set_basis(B);
+      if (h->v2) h->v2->set_basis(make_basis_p2());
       DG_CUDA(cudaGetLastError());
     }
     const PartPlan plan = make_part_plan(s, part, nparts);
     build_layout(h.get(), s, plan);
     build_halo(h.get(), s, plan);
+    if (h->v2) {
+      std::vector<unsigned> info(h->ne);
+      DG_CUDA(cudaMemcpy(info.data(), h->einfo.p, h->ne * sizeof(unsigned), cudaMemcpyDeviceToHost));
+      std::vector<int> edges;
+      for (int e = 0; e < h->ne; ++e)
+        for (int l = 0; l < 3; ++l) {
+          const unsigned k = ei_kind(info[e], l);
+          if ((k == kInterior && ei_flag(info[e], l)) || k == kLand || k == kOcean) {
+            edges.push_back(e);
+            edges.push_back(l);
+          }
+        }
+      h->p2_nedge = (int)edges.size() / 2;
+      h->p2_edges.upload(edges.empty() ? std::vector<int>(2, 0) : edges);
+      h->p2_ef.alloc((size_t)3 * kP2Egp * 3 * h->ne);  // slots of edges in no list stay zero
+      DG_CUDA(cudaMemset(h->p2_ef.p, 0, h->p2_ef.n * sizeof(double)));
+    }
     const size_t nl = (size_t)h->ne, npl = (size_t)h->np;
     h->q.resize(s->nrk + 1);
     for (auto& b : h->q) {
-      b.alloc(9 * nl);
+      b.alloc(3 * (size_t)h->dofh * nl);
       DG_CUDA(cudaMemset(b.p, 0, b.n * sizeof(double)));
     }
     h->rhs.resize(s->nrk);
     for (int I = 0; I < s->nrk; ++I)
-      if (h->keep_rhs[I]) h->rhs[I].alloc(9 * nl);
+      if (h->keep_rhs[I]) h->rhs[I].alloc(3 * (size_t)h->dofh * nl);
     h->wd.alloc(nl);
     h->wd_staging.alloc(s->ne);
     h->nodecode.alloc(s->np);
@@ -1474,14 +1701,17 @@ int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* q
     double* dst[3] = {ze, qx, qy};
     if (h->nparts == 1) {  // every element is owned: scatter to input order on the device
       const int ne = h->ne;
-      h->staging.ensure(9 * (size_t)ne);
+      const size_t dofh = (size_t)h->dofh;
+      h->staging.ensure(3 * dofh * ne);
       for (int var = 0; var < 3; ++var) {
         if (!dst[var]) continue;
-        h->v->s2f(h->q[0].p, h->staging.p + (size_t)3 * ne * var, ne, var, h->inv.p, grid_for(ne, kPointBlock),
-                  h->stream);
+        double* sv = h->staging.p + dofh * ne * var;
+        if (h->v2)
+          h->v2->layout(false, h->q[0].p, sv, ne, var, h->inv.p, h->stream);
+        else
+          h->v->s2f(h->q[0].p, sv, ne, var, h->inv.p, grid_for(ne, kPointBlock), h->stream);
         check_launch(h, "soa_to_fortran");
-        DG_CUDA(cudaMemcpyAsync(dst[var], h->staging.p + (size_t)3 * ne * var, 3 * (size_t)ne * sizeof(double),
-                                cudaMemcpyDeviceToHost, h->stream));
+        DG_CUDA(cudaMemcpyAsync(dst[var], sv, dofh * ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       }
       if (wdflg) {
         h->v->gather_int(h->wd.p, h->wd_staging.p, h->inv.p, ne, grid_for(ne, kPointBlock), h->stream);
@@ -1543,8 +1773,12 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
     const int np = h->np;
     h->staging.ensure(4 * (size_t)np);
     double* d = h->staging.p;
-    h->v->modal2nodal(h->mesh, h->q[0].p, h->wd.p, h->ph.nleq, h->ph.leq, d, d + np, d + 2 * (size_t)np,
-                      h->nodecode.p, grid_for(np, kPointBlock), h->stream);
+    if (h->v2)
+      h->v2->modal2nodal(h->mesh, h->q[0].p, h->ph.nleq, h->ph.leq, d, d + np, d + 2 * (size_t)np, h->nodecode.p,
+                         h->stream);
+    else
+      h->v->modal2nodal(h->mesh, h->q[0].p, h->wd.p, h->ph.nleq, h->ph.leq, d, d + np, d + 2 * (size_t)np,
+                        h->nodecode.p, grid_for(np, kPointBlock), h->stream);
     check_launch(h, "modal2nodal");
     if (eta2) DG_CUDA(cudaMemcpyAsync(eta2, d, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (uu2) DG_CUDA(cudaMemcpyAsync(uu2, d + np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1557,6 +1791,7 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
 
 int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, double* vv2, int* nodecode) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_modal2nodal_noalloc");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "modal2nodal needs the whole mesh (a handle of dgswem_cuda_create)");
     const int np = h->np;
@@ -1582,6 +1817,7 @@ int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, d
 
 int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_stage_rhs");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (irk < 1 || irk > h->nrk) throw Failure(DGSWEM_ERR_ARG, "stage out of range");
     DG_CUDA(cudaSetDevice(h->device));
@@ -1602,6 +1838,7 @@ int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) {
 
 int dgswem_cuda_stage_limit(dgswem_cuda* h, int irk) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_stage_limit");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (irk < 1 || irk > h->nrk) throw Failure(DGSWEM_ERR_ARG, "stage out of range");
     DG_CUDA(cudaSetDevice(h->device));
@@ -1611,6 +1848,7 @@ int dgswem_cuda_stage_limit(dgswem_cuda* h, int irk) {
 
 int dgswem_cuda_step_end(dgswem_cuda* h) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_step_end");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     std::swap(h->q[0], h->q[h->nrk]);  // stage NRK+1 becomes stage 1
   });
@@ -1638,6 +1876,7 @@ int dgswem_cuda_halo_count(const dgswem_cuda* h, int kind, int peer, int* nsend,
 
 static int halo_copy(dgswem_cuda* h, int kind, int peer, int irk, double* buf, bool pack) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_halo_pack / _unpack");
     if (!h || !buf) throw Failure(DGSWEM_ERR_ARG, "null argument");
     if (kind != kHaloMeans && kind != kHaloFull) throw Failure(DGSWEM_ERR_ARG, "unknown halo kind");
     if (peer < 0 || peer >= h->nparts) throw Failure(DGSWEM_ERR_ARG, "peer out of range");
@@ -1665,6 +1904,7 @@ int dgswem_cuda_set_graph(dgswem_cuda* h, int steps) {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (steps != 0 && (steps < 2 || steps % 2 != 0))
       throw Failure(DGSWEM_ERR_ARG, "steps per graph must be 0 (off) or an even number >= 2");
+    if (steps != 0) need_p1(h, "dgswem_cuda_set_graph");
     DG_CUDA(cudaSetDevice(h->device));
     DG_CUDA(cudaStreamSynchronize(h->stream));
     graph_release(h);
@@ -1755,6 +1995,7 @@ int dgswem_cuda_shapes(int* n_tile, int* tile_elems, int* tile_threads, int* n_l
 
 int dgswem_cuda_set_shapes(dgswem_cuda* h, int tile_shape, int limit_shape) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_set_shapes");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (tile_shape < -1 || tile_shape >= kNumTileShapes || limit_shape < -1 || limit_shape >= kNumLimitShapes)
       throw Failure(DGSWEM_ERR_ARG, "shape index out of range");
@@ -1775,6 +2016,7 @@ int dgswem_cuda_get_shapes(const dgswem_cuda* h, int* tile_shape, int* limit_sha
 int dgswem_cuda_autotune(dgswem_cuda* h, int it, int steps, int reps, int flags, double* ms_tile,
                          double* ms_limit) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_autotune");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (steps < 1 || reps < 1 || it < 1) throw Failure(DGSWEM_ERR_ARG, "autotune: it, steps and reps must be >= 1");
     if (h->nparts != 1)
@@ -1930,6 +2172,7 @@ int dgswem_cuda_profile_read(dgswem_cuda* h, double* ms, long long* launches) {
 
 int dgswem_cuda_set_params(dgswem_cuda* h, const double* nbar, const double* hb) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_set_params");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "set_params needs the whole mesh (a handle of dgswem_cuda_create)");
     DG_CUDA(cudaSetDevice(h->device));
@@ -1958,6 +2201,7 @@ int dgswem_cuda_set_params(dgswem_cuda* h, const double* nbar, const double* hb)
 
 int dgswem_cuda_state_save(dgswem_cuda* h, int slot) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_state_save");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (slot < 0) throw Failure(DGSWEM_ERR_ARG, "negative state slot");
     DG_CUDA(cudaSetDevice(h->device));
@@ -1967,6 +2211,7 @@ int dgswem_cuda_state_save(dgswem_cuda* h, int slot) {
 
 int dgswem_cuda_state_load(dgswem_cuda* h, int slot) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_state_load");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     DG_CUDA(cudaSetDevice(h->device));
     load_slot(h, slot);
@@ -1975,6 +2220,7 @@ int dgswem_cuda_state_load(dgswem_cuda* h, int slot) {
 
 int dgswem_cuda_gauges(dgswem_cuda* h, int ng, const int* elem, const double* phi) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_gauges");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "gauges need the whole mesh (a handle of dgswem_cuda_create)");
     if (ng < 0 || (ng > 0 && (!elem || !phi))) throw Failure(DGSWEM_ERR_ARG, "gauges: bad arguments");
@@ -2025,6 +2271,7 @@ int dgswem_cuda_gauge_eta(dgswem_cuda* h, double* eta) {
 
 int dgswem_cuda_adjoint_begin(dgswem_cuda* h) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_adjoint_begin");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     DG_CUDA(cudaSetDevice(h->device));
     adjoint_prepare(h);
@@ -2033,6 +2280,7 @@ int dgswem_cuda_adjoint_begin(dgswem_cuda* h) {
 
 int dgswem_cuda_adjoint_seed(dgswem_cuda* h, const double* w) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_adjoint_seed");
     if (!h || !w) throw Failure(DGSWEM_ERR_ARG, "null argument");
     if (!h->adj_on) throw Failure(DGSWEM_ERR_ARG, "call dgswem_cuda_adjoint_begin first");
     DG_CUDA(cudaSetDevice(h->device));
@@ -2045,6 +2293,7 @@ int dgswem_cuda_adjoint_seed(dgswem_cuda* h, const double* w) {
 
 int dgswem_cuda_adjoint_step(dgswem_cuda* h, int it) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_adjoint_step");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (!h->adj_on) throw Failure(DGSWEM_ERR_ARG, "call dgswem_cuda_adjoint_begin first");
     DG_CUDA(cudaSetDevice(h->device));
@@ -2078,6 +2327,7 @@ int dgswem_cuda_adjoint_step(dgswem_cuda* h, int it) {
 
 int dgswem_cuda_misfit_forward(dgswem_cuda* h, int it0, int nsteps, int every, double* eta) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_misfit_forward");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (nsteps < 0 || every < 1) throw Failure(DGSWEM_ERR_ARG, "misfit_forward: bad step counts");
     DG_CUDA(cudaSetDevice(h->device));
@@ -2104,6 +2354,7 @@ int dgswem_cuda_misfit_forward(dgswem_cuda* h, int it0, int nsteps, int every, d
 
 int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, const double* w) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_adjoint_sweep");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (nsteps < 1 || every < 1) throw Failure(DGSWEM_ERR_ARG, "adjoint_sweep: bad step counts");
     DG_CUDA(cudaSetDevice(h->device));
@@ -2192,6 +2443,7 @@ int dgswem_cuda_adjoint_sweep(dgswem_cuda* h, int it0, int nsteps, int every, co
 int dgswem_cuda_adjoint_read(dgswem_cuda* h, double* g_nbar, double* g_hb, double* lam_ze, double* lam_qx,
                              double* lam_qy) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_adjoint_read");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (!h->adj_on) throw Failure(DGSWEM_ERR_ARG, "call dgswem_cuda_adjoint_begin first");
     DG_CUDA(cudaSetDevice(h->device));
@@ -2216,6 +2468,7 @@ int dgswem_cuda_adjoint_read(dgswem_cuda* h, double* g_nbar, double* g_hb, doubl
 
 int dgswem_cuda_limit_state(dgswem_cuda* h) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_limit_state");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "limit_state needs the whole mesh (a handle of dgswem_cuda_create)");
     DG_CUDA(cudaSetDevice(h->device));
@@ -2227,6 +2480,7 @@ int dgswem_cuda_limit_state(dgswem_cuda* h) {
 int dgswem_cuda_limiter_vjp(dgswem_cuda* h, const double* lam_ze, const double* lam_qx, const double* lam_qy,
                             double* out_ze, double* out_qx, double* out_qy) {
   return guarded([&]() {
+    need_p1(h, "dgswem_cuda_limiter_vjp");
     if (!h || !lam_ze || !lam_qx || !lam_qy || !out_ze || !out_qx || !out_qy)
       throw Failure(DGSWEM_ERR_ARG, "null argument");
     if (h->nparts != 1) throw Failure(DGSWEM_ERR_ARG, "limiter_vjp needs the whole mesh");

@@ -275,6 +275,53 @@ DGSWEM_DECLARE_LAUNCHERS(fast)
 DGSWEM_DECLARE_LAUNCHERS(strict)
 DGSWEM_DECLARE_LAUNCHERS(mixed)
 
+// ---- p=2 (hydro_p2.cuh, kernels_p2_fast.cu / kernels_p2_strict.cu) --------
+// Six modes per variable, the four-point Gauss-Lobatto edge rule and the
+// six-point area rule (quadrature_v1.F); FP64, no wet/dry, no limiter.
+constexpr int kP2Modes = 6, kP2Egp = 4, kP2Agp = 6;
+struct BasisP2 {
+  double phi_edge[3][kP2Egp][kP2Modes];  // [led][point][mode]
+  double edgeq[3][kP2Egp][kP2Modes];     // 2*M_INV*PHI_EDGE*WEGP
+  double phi_area[kP2Modes][kP2Agp];     // [mode][point]
+  double drphi[kP2Modes][kP2Agp], dsphi[kP2Modes][kP2Agp];
+  double phi_corner[3][kP2Modes];        // [vertex][mode]
+  double psi[3][kP2Agp];                 // linear nodal basis at the area points
+  double m_inv[kP2Modes], wagp[kP2Agp], wegp[kP2Egp], xegp[kP2Egp];
+  double mw[kP2Modes][kP2Agp];           // M_INV*WAGP
+  double srfac[kP2Modes][kP2Agp];        // M_INV*WAGP*PHI_AREA
+};
+struct P2Args {
+  MeshView m;   // hb: six rows; egeo; einfo / link for the edge kinds and neighbours
+  Physics ph;
+  int irk;
+  const double* __restrict__ qin;  // 18 rows (6*var + mode)
+  double* qout;
+  const double* qhist[kMaxStages];
+  const double* rhist[kMaxStages];
+  double* rout;
+  double a[kMaxStages], b[kMaxStages];
+  double rampdg;
+  const double* __restrict__ ocean_zg;
+  const double* __restrict__ wsx;
+  const double* __restrict__ wsy;
+  const double* __restrict__ pr;
+  double* ef;                      // [((e*3 + led)*4 + point)*3 + c] edge-point fluxes F, G, H per side
+  const int* __restrict__ edges;   // (element, local edge): interior edges from the in side, land and ocean edges
+  int nedge, ne_act;
+  unsigned* err;
+};
+#define DGSWEM_DECLARE_P2_LAUNCHERS(NS)                                                          \
+  namespace NS {                                                                                 \
+  void set_basis_p2(const BasisP2& b);                                                           \
+  void launch_p2_stage(const P2Args& a, bool nonlin, cudaStream_t s);                            \
+  void launch_p2_modal2nodal(const MeshView& m, const double* q, double nleq, double leq,         \
+                             double* eta2, double* uu2, double* vv2, int* nodecode, cudaStream_t s); \
+  void launch_p2_layout(bool to_device, const double* src, double* dst, int ne, int var,         \
+                        const int* map, cudaStream_t s);                                         \
+  }
+DGSWEM_DECLARE_P2_LAUNCHERS(fast_p2)
+DGSWEM_DECLARE_P2_LAUNCHERS(strict_p2)
+
 // ---- discrete adjoint (adjoint.cu) ----------------------------------------
 // Vector-Jacobian product of one RK stage's right-hand side L(q; n, HB) at
 // stage state q: lam += (dL/dq)^T nu, g_n += (dL/dnbar)^T nu (element-mean

@@ -1,0 +1,116 @@
+"""The p=2 device path (GPU) against the oracle's p=2, which is checked by
+its convergence order (test_oracle_p2_convergence.py): the strict variant
+bit for bit, the fast one within 1e-10 relative; its own convergence order;
+and the p=1-only features rejected on a p=2 handle."""
+import math
+
+import numpy as np
+import pytest
+
+from dgswem_b200 import Deck, HydroStep, decks
+from dgswem_b200._abi import DgswemError
+from oracle_lib import Oracle
+
+import test_oracle_p2_convergence as sw
+
+pytestmark = pytest.mark.gpu
+
+P2 = {"extra": {"pl": 2, "ph": 2}}
+
+
+def standing_wave_state(path, nx):
+    """The basin deck and the L2 projection of the standing wave (oracle tables)."""
+    x, y, elems = sw.basin(path, nx, 2)
+    orc = Oracle(path)
+    px, py, wphys, phi, wa = sw.area_points(orc, x, y, elems)
+    minv = orc.real_table("M_INV")
+    ze = (sw.A * np.cos(sw.K * px) * wa[None, :]) @ phi.T * minv[None, :]
+    return orc, ze, np.zeros_like(ze), (px, wphys, phi)
+
+
+def run_pair(path, nsteps, strict, state=None, met=None):
+    orc = Oracle(path)
+    with HydroStep(Deck(path), strict=strict) as hs:
+        assert hs.dofh == 6
+        if state is not None:
+            wd = np.ones(hs.ne, np.int32)
+            hs.set_state(state[0], state[1], state[1], wd)
+            orc.set_state(state[0], state[1], state[1], wd)
+        if met is not None:
+            hs.set_met(*met)
+            orc.set_met(*met)
+        hs.run(1, nsteps)
+        orc.run(1, nsteps)
+        hs.synchronize()
+        g, o = hs.state(), orc.state()
+        gn, on = hs.modal2nodal(), orc.modal2nodal()
+    orc.close()
+    return g, o, gn, on
+
+
+def decks_p2(scratch):
+    basin = scratch / "p2_basin"
+    orc, ze, zero, _ = standing_wave_state(basin, 16)
+    orc.close()
+    qa = decks.quarter_annulus(scratch / "p2_qa", nr=8, nth=16, nsteps=60, nolibf=1, cf=0.0025, **P2)
+    qa_lin = decks.quarter_annulus(scratch / "p2_qa_lin", nr=8, nth=16, nsteps=60, nolifa=0, nolica=0, nolicat=0,
+                                   nolibf=2, nws=1, **P2)
+    return [("standing wave, linear, SSP(3,3)", basin, 150, (ze, zero), None),
+            ("quarter annulus, tide, quadratic friction", qa, 60, None, None),
+            ("quarter annulus, linear, hybrid friction, wind", qa_lin, 60, None, "wind")]
+
+
+def wind(path):
+    d = Deck(path)
+    npn = d.s.np
+    d.close()
+    t = 0.1 / 1000.0
+    return np.full(npn, t * math.cos(0.5)), np.full(npn, t * math.sin(0.5)), np.zeros(npn)
+
+
+def test_p2_strict_bitwise_vs_oracle(built, scratch):
+    for name, path, n, state, met in decks_p2(scratch):
+        g, o, gn, on = run_pair(path, n, True, state, wind(path) if met else None)
+        assert np.abs(g[0]).max() > 0, name
+        for a, b, v in zip(g, o, ("ZE", "QX", "QY", "WDFLG")):
+            np.testing.assert_array_equal(a, b, err_msg=f"{name}: {v}")
+        for a, b, v in zip(gn, on, ("ETA2", "UU2", "VV2")):
+            np.testing.assert_array_equal(a, b, err_msg=f"{name}: {v}")
+
+
+def test_p2_fast_vs_oracle(built, scratch):
+    for name, path, n, state, met in decks_p2(scratch):
+        g, o, _, _ = run_pair(path, n, False, state, wind(path) if met else None)
+        for a, b, v in zip(g[:3], o[:3], ("ZE", "QX", "QY")):
+            scale = max(np.abs(b).max(), 1e-300)
+            assert np.abs(a - b).max() / scale <= 1e-10, f"{name}: {v}"
+
+
+def test_p2_convergence_order_on_device(built, scratch):
+    errs = []
+    for nx in (8, 16, 32):
+        path = scratch / f"p2_conv_{nx}"
+        orc, ze, zero, (px, wphys, phi) = standing_wave_state(path, nx)
+        orc.close()
+        with HydroStep(Deck(path)) as hs:
+            hs.set_state(ze, zero, zero, np.ones(hs.ne, np.int32))
+            hs.run(1, sw.NSTEPS)
+            z = hs.state()[0]
+        eta = sw.A * np.cos(sw.K * px) * math.cos(sw.OMEGA * sw.DT * sw.NSTEPS)
+        errs.append(math.sqrt(float(np.sum(wphys * (z @ phi - eta) ** 2))))
+    rates = [math.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert all(r > 2.6 for r in rates), (errs, rates)
+
+
+def test_p2_rejects_p1_only_features(built, scratch):
+    path = decks.quarter_annulus(scratch / "p2_rej", nr=4, nth=8, nsteps=2, **P2)
+    with HydroStep(Deck(path)) as hs:
+        for call in (lambda: hs.set_graph(2), lambda: hs.autotune(), lambda: hs.set_shapes(1, -1)):
+            with pytest.raises(DgswemError, match="p=1 only"):
+                call()
+        hs.set_graph(0)  # off is accepted
+    with pytest.raises(DgswemError, match="p=1 only"):
+        HydroStep(Deck(path), mixed=True)
+    lim = decks.quarter_annulus(scratch / "p2_lim", nr=4, nth=8, nsteps=2, slopeflag=5, **P2)
+    with pytest.raises(DgswemError, match="p = 1 only"):
+        Deck(lim)
