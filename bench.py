@@ -113,14 +113,14 @@ def rank0_first(rank: int, world: int, dist, fn):
     return out
 
 
-def config3_deck(workdir, nr: int, nth: int) -> Path:
-    """The config-3 quarter annulus (nr x nth cells, dt = 0.5 s, NWS=1) under
-    workdir, written unless complete."""
+def config3_deck(workdir, nr: int, nth: int, p: int = 1) -> Path:
+    """The config-3 quarter annulus (nr x nth cells, dt = 0.5 s, NWS=1, DG of
+    degree p) under workdir, written unless complete."""
     from dgswem_b200 import decks
-    path = Path(workdir) / f"config3_{nr}x{nth}"
+    path = Path(workdir) / (f"config3_{nr}x{nth}" + ("" if p == 1 else f"_p{p}"))
     done = path / ".complete"
     if not done.exists():
-        decks.quarter_annulus(path, nr=nr, nth=nth, nsteps=5000, dt=0.5, nws=1)
+        decks.quarter_annulus(path, nr=nr, nth=nth, nsteps=5000, dt=0.5, nws=1, extra={"pl": p, "ph": p})
         done.write_text("ok\n")
     return path
 
@@ -308,6 +308,35 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     (sf, nf), (sm, nmx) = states["fp64"], states["mixed"]
     mf, mm = mass(deck, sf[0]), mass(deck, sm[0])
     out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if args.config3_p2_steps > 0:
+        # the p=2 half: the same annulus at p=2 (18 DOFs per element), FP64
+        path2 = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth, p=2))
+        deck2 = Deck(path2)
+        k2 = args.config3_p2_steps
+        with HydroStep(deck2, device=device) as h:
+            h.set_stream(stream.cuda_stream)
+            h.set_met(*met)
+            h.run(1, w)
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.run(w + 1, k2)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms2 = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+            h.profile(True)
+            h.run(w + 1 + k2, 4)
+            prof = h.profile_read()
+            h.profile(False)
+            h.synchronize()
+        dofs = 3 * deck2.s.dofh
+        out["p2"] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
+                     "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
+                     "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
+                     "dtype": "f64", "kernels": "p2_edges + p2_elements per RK stage"}
+        deck2.close()
     out["mixed"]["err_vs_fp64"] = {
         "steps": args.config3_err_steps,
         "eta_nodal_linf_m": float(np.abs(nmx[0] - nf[0]).max()),
@@ -552,6 +581,7 @@ def main(argv=None):
     ap.add_argument("--config3-nr", type=int, default=1000)
     ap.add_argument("--config3-nth", type=int, default=4000)
     ap.add_argument("--config3-err-steps", type=int, default=200)
+    ap.add_argument("--config3-p2-steps", type=int, default=50, help="timed steps of the p=2 config-3 annulus (0: skip)")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=40)
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
