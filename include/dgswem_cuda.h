@@ -45,7 +45,7 @@ enum {
 typedef struct dgswem_cuda_setup {
   /* sizes */
   int ne, np;              /* elements, nodes                              */
-  int dofh;                /* modes per variable: 3 (p=1)                  */
+  int dofh;                /* modes per variable: 3 (p=1) or 6 (p=2)       */
   int nrk;                 /* RK stages (RK_STAGE)                         */
   int nedges;              /* NEDGES                                       */
   int nieds, nleds, needs, nfeds, nreds, nebseg, nibseg;
@@ -114,7 +114,13 @@ typedef struct dgswem_cuda dgswem_cuda;
 
 /* Copies the setup to GPU `device` and builds the device layout.
  * Replaces the state the reference keeps in module arrays after PREP_DG
- * (src/dgswem.F:196). */
+ * (src/dgswem.F:196).  DOFH = 6 makes a p=2 handle (FP64, fast or strict):
+ * no slope limiter and no wetting/drying (p=1 only in the reference), land,
+ * ocean and interior edges, ICS=1, a whole-mesh handle; its interior-edge
+ * sums run over all six modes (the reference's p=2 sums modes 1-3 only).
+ * State arrays are ZE/QX/QY(6, NE).  The adjoint, state slots, tile shapes,
+ * CUDA graphs and partitions are p=1 only and return DGSWEM_ERR_ARG on a
+ * p=2 handle. */
 int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
                        dgswem_cuda** out);
 
