@@ -380,8 +380,14 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
             ens.set_met(wsx, wsy, pr)
             ens.run(1, w)
             tiles = autotune(ens.hs, args, w + 1)
+            if args.ensemble_graph_steps:
+                ens.hs.set_graph(args.ensemble_graph_steps)
+                ens.run(w + 1, args.ensemble_graph_steps)  # capture, outside the timing
+                w1 = w + 1 + args.ensemble_graph_steps
+            else:
+                w1 = w + 1
             l0 = ens.hs.kernel_launches
-            ms = timed(ens.run, w + 1)
+            ms = timed(ens.run, w1)
             return ms, ens.hs.kernel_launches - l0, ens.total_elements, ens.nrk, tiles
 
     ms, launches, ne_tot, nrk, tiles = batched(ds, *met)
@@ -395,7 +401,12 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
             hs.set_met(met[0][i], met[1][i], met[2][i])
             hs.run(1, w)
             autotune(hs, args, w + 1)
-            ms_one += timed(hs.run, w + 1)
+            w1 = w + 1
+            if args.ensemble_graph_steps:
+                hs.set_graph(args.ensemble_graph_steps)
+                hs.run(w1, args.ensemble_graph_steps)
+                w1 += args.ensemble_graph_steps
+            ms_one += timed(hs.run, w1)
     rate = lambda ne, t: DOFS_PER_ELEMENT * ne * nrk * k / (t / 1e3)  # noqa: E731
     for d in ds:
         d.close()
@@ -403,6 +414,7 @@ def ensemble_arm(args, stream, device: int, world: int, dist) -> dict:
             "value": whole_job_rate(world, ne_tot, nrk, k, ms), "unit": "DOF-stage/s",
             "ms_per_step": ms / k, "dtype": "mixed (f32 edge/volume/limiter, f64 state/SSP/wet-dry)",
             "gpu_launches": int(launches), "deck_write_read_s": t_decks, "tiles": tiles,
+            "graph_steps": args.ensemble_graph_steps,
             "subset16": {"elements": int(ne_sub), "batched_rate": rate(ne_sub, ms_sub),
                          "one_at_a_time_rate": rate(ne_sub, ms_one), "batching_speedup": ms_one / ms_sub}}
 
@@ -584,6 +596,8 @@ def main(argv=None):
     ap.add_argument("--config3-p2-steps", type=int, default=50, help="timed steps of the p=2 config-3 annulus (0: skip)")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=40)
+    ap.add_argument("--ensemble-graph-steps", type=int, default=8,
+                    help="whole steps per CUDA graph in the ensemble arm (even; 0: plain launches)")
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
     ap.add_argument("--mixed-err-steps", type=int, default=200,
                     help="steps of the mixed-vs-FP64 error comparison")
