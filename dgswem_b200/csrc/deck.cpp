@@ -1124,12 +1124,12 @@ extern "C" int dgswem_deck_merge(const dgswem_cuda_setup* const* parts, int n, d
       append_offset(d->nredn, m->nredn, m->nreds, edoff, false);
       append_offset(d->nebsegn, m->nebsegn, m->nebseg, edoff, false);
       append_offset(d->nibsegn, m->nibsegn, 2 * (size_t)m->nibseg, edoff, true);
-      append(d->hb, m->hb, 3 * (size_t)m->ne);
+      append(d->hb, m->hb, (size_t)s0.dofh * m->ne);
       append(d->cori_el, m->cori_el, m->ne);
       append(d->fric_el, m->fric_el, m->ne);
-      append(d->ze, m->ze, 3 * (size_t)m->ne);
-      append(d->qx, m->qx, 3 * (size_t)m->ne);
-      append(d->qy, m->qy, 3 * (size_t)m->ne);
+      append(d->ze, m->ze, (size_t)s0.dofh * m->ne);
+      append(d->qx, m->qx, (size_t)s0.dofh * m->ne);
+      append(d->qy, m->qy, (size_t)s0.dofh * m->ne);
       append(d->wdflg, m->wdflg, m->ne);
       append(d->ebht, m->ebht, m->nebseg);
       append(d->ebcfsp, m->ebcfsp, m->nebseg);

@@ -69,3 +69,17 @@ def test_merge_rejects_incompatible_members(built, scratch):
         Deck.merge([Deck(a), Deck(c)])
     with pytest.raises(DgswemError, match="empty"):
         Deck.merge([])
+
+
+def test_merge_p2_members(built, scratch):
+    """p=2 members: six bathymetry modes per element carried over."""
+    p2 = {"extra": {"pl": 2, "ph": 2}}
+    a = decks.quarter_annulus(scratch / "p2m_a", nr=4, nth=8, nsteps=2, **p2)
+    b = decks.quarter_annulus(scratch / "p2m_b", nr=6, nth=6, nsteps=2, **p2)
+    da, db = Deck(a), Deck(b)
+    m = Deck.merge([da, db])
+    assert m.s.dofh == 6 and m.s.ne == da.s.ne + db.s.ne
+    hb = m.real_array("hb", 6 * m.s.ne)
+    np.testing.assert_array_equal(hb[:6 * da.s.ne], da.real_array("hb", 6 * da.s.ne))
+    np.testing.assert_array_equal(hb[6 * da.s.ne:], db.real_array("hb", 6 * db.s.ne))
+    m.close()

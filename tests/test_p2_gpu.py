@@ -114,3 +114,21 @@ def test_p2_rejects_p1_only_features(built, scratch):
     lim = decks.quarter_annulus(scratch / "p2_lim", nr=4, nth=8, nsteps=2, slopeflag=5, **P2)
     with pytest.raises(DgswemError, match="p = 1 only"):
         Deck(lim)
+
+
+def test_p2_ensemble_matches_members_alone(built, scratch):
+    from dgswem_b200 import Ensemble
+    paths = [decks.quarter_annulus(scratch / f"p2_ens_{i}", nr=4 + 2 * i, nth=8 + 4 * i, nsteps=40, nolibf=1,
+                                   cf=0.0025, **P2) for i in range(3)]
+    ds = [Deck(p) for p in paths]
+    with Ensemble(ds, mixed=False) as ens:
+        ens.run(1, 40)
+        ens.synchronize()
+        got = ens.states()
+    for i, d in enumerate(ds):
+        with HydroStep(d) as hs:
+            hs.run(1, 40)
+            want = hs.state()
+        for a, b, v in zip(got[i], want, ("ZE", "QX", "QY", "WDFLG")):
+            np.testing.assert_array_equal(a, b, err_msg=f"member {i} {v}")
+        assert want[0].shape[1] == 6
