@@ -1036,7 +1036,7 @@ void stage_forcing(const dgswem_cuda* h, double timedg, double rampdg, double* o
 // One RK stage: the stage kernel writes stage buffer irk for the owned
 // elements (launch_stage_rhs), then the limiter and WETDRY (launch_limit).
 // The p=2 stage: edge kernel, then element kernel (SSP combination included).
-void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing) {
+void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing, const double* ramp) {
   const int nrk = h->nrk;
   P2Args A{};
   A.m = h->mesh;
@@ -1053,6 +1053,7 @@ void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing) {
   A.rout = h->keep_rhs[irk - 1] ? h->rhs[irk - 1].p : nullptr;
   double timedg;
   stage_clock(h, it, irk, &timedg, &A.rampdg);
+  A.ramp = ramp;
   A.ocean_zg = forcing;
   A.wsx = h->wsx.p;
   A.wsy = h->wsy.p;
@@ -1071,7 +1072,7 @@ void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing) {
 
 void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, const double* ramp = nullptr) {
   if (h->v2) {
-    launch_stage_p2(h, it, irk, forcing);
+    launch_stage_p2(h, it, irk, forcing, ramp);
     return;
   }
   const int nrk = h->nrk;
@@ -1237,8 +1238,8 @@ int run_steps_graph(dgswem_cuda* h, int it0, int n) {
   if (m < 2 || h->prof_on || n < m) return 0;
   if (!h->graph_ready) graph_capture(h);
   if (h->q[0].p != h->graph_q0) {  // the state sits in the other buffer: move it where the graphs read it
-    DG_CUDA(cudaMemcpyAsync(h->q[nrk].p, h->q[0].p, 9 * (size_t)h->ne * sizeof(double), cudaMemcpyDeviceToDevice,
-                            h->stream));
+    DG_CUDA(cudaMemcpyAsync(h->q[nrk].p, h->q[0].p, 3 * (size_t)h->dofh * h->ne * sizeof(double),
+                            cudaMemcpyDeviceToDevice, h->stream));
     std::swap(h->q[0], h->q[nrk]);
   }
   int done = 0, b = h->graph_next;
@@ -1904,7 +1905,6 @@ int dgswem_cuda_set_graph(dgswem_cuda* h, int steps) {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (steps != 0 && (steps < 2 || steps % 2 != 0))
       throw Failure(DGSWEM_ERR_ARG, "steps per graph must be 0 (off) or an even number >= 2");
-    if (steps != 0) need_p1(h, "dgswem_cuda_set_graph");
     DG_CUDA(cudaSetDevice(h->device));
     DG_CUDA(cudaStreamSynchronize(h->stream));
     graph_release(h);

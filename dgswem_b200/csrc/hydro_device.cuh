@@ -301,6 +301,7 @@ struct P2Args {
   double* rout;
   double a[kMaxStages], b[kMaxStages];
   double rampdg;
+  const double* __restrict__ ramp;  // RAMPDG in device memory (graph replays), or null: rampdg
   const double* __restrict__ ocean_zg;
   const double* __restrict__ wsx;
   const double* __restrict__ wsy;

@@ -157,7 +157,7 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const double* q, cons
       dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
       dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
     }
-    const double fw = 1.0 / f1, r = A.rampdg;
+    const double fw = 1.0 / f1, r = A.ramp ? *A.ramp : A.rampdg;
     const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
     const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
     const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];

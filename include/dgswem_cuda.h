@@ -118,9 +118,8 @@ typedef struct dgswem_cuda dgswem_cuda;
  * no slope limiter and no wetting/drying (p=1 only in the reference), land,
  * ocean and interior edges, ICS=1, a whole-mesh handle; its interior-edge
  * sums run over all six modes (the reference's p=2 sums modes 1-3 only).
- * State arrays are ZE/QX/QY(6, NE).  The adjoint, state slots, tile shapes,
- * CUDA graphs and partitions are p=1 only and return DGSWEM_ERR_ARG on a
- * p=2 handle. */
+ * State arrays are ZE/QX/QY(6, NE).  The adjoint, state slots, tile shapes
+ * and partitions are p=1 only and return DGSWEM_ERR_ARG on a p=2 handle. */
 int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
                        dgswem_cuda** out);
 

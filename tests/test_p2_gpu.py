@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from dgswem_b200 import Deck, HydroStep, decks
+from dgswem_b200 import _abi
 from dgswem_b200._abi import DgswemError
 from oracle_lib import Oracle
 
@@ -105,10 +106,10 @@ def test_p2_convergence_order_on_device(built, scratch):
 def test_p2_rejects_p1_only_features(built, scratch):
     path = decks.quarter_annulus(scratch / "p2_rej", nr=4, nth=8, nsteps=2, **P2)
     with HydroStep(Deck(path)) as hs:
-        for call in (lambda: hs.set_graph(2), lambda: hs.autotune(), lambda: hs.set_shapes(1, -1)):
+        for call in (lambda: hs.autotune(), lambda: hs.set_shapes(1, -1),
+                     lambda: _abi.check(hs._lib.dgswem_cuda_state_save(hs._h, 0))):
             with pytest.raises(DgswemError, match="p=1 only"):
                 call()
-        hs.set_graph(0)  # off is accepted
     with pytest.raises(DgswemError, match="p=1 only"):
         HydroStep(Deck(path), mixed=True)
     lim = decks.quarter_annulus(scratch / "p2_lim", nr=4, nth=8, nsteps=2, slopeflag=5, **P2)
@@ -132,3 +133,24 @@ def test_p2_ensemble_matches_members_alone(built, scratch):
         for a, b, v in zip(got[i], want, ("ZE", "QX", "QY", "WDFLG")):
             np.testing.assert_array_equal(a, b, err_msg=f"member {i} {v}")
         assert want[0].shape[1] == 6
+
+
+def test_p2_graphs_match_launches(built, scratch):
+    """Whole-step CUDA graphs at p=2 (the wind ramp read from device memory
+    in the replays): bit-identical to launch-by-launch stepping."""
+    path = decks.quarter_annulus(scratch / "p2_graph", nr=6, nth=12, nsteps=60, nolibf=1, cf=0.0025, nws=1,
+                                 dramp=0.01, **P2)
+    met = wind(path)
+    out = []
+    for graph in (0, 6):
+        with HydroStep(Deck(path)) as hs:
+            hs.set_met(*met)
+            if graph:
+                hs.set_graph(graph)
+            hs.run(1, 25)
+            hs.timestep(26)
+            hs.run(27, 30)
+            hs.synchronize()
+            out.append(hs.state())
+    for a, b, v in zip(out[0], out[1], ("ZE", "QX", "QY", "WDFLG")):
+        np.testing.assert_array_equal(a, b, err_msg=v)
