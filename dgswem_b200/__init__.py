@@ -9,7 +9,8 @@ include/dgswem_cuda.h.
             hs.timestep(it)
         eta, uu, vv, nodecode = hs.modal2nodal()
 """
-from .hydro import Deck, DistributedPartition, HydroStep, PartitionedRun, run_case, write_fort63  # noqa: F401
+from .hydro import Deck, DistributedPartition, HydroStep, PartitionedRun, run_case, write_fort63, write_hotstart  # noqa: F401
 from .ensemble import Ensemble  # noqa: F401
 
-__all__ = ["Deck", "DistributedPartition", "Ensemble", "HydroStep", "PartitionedRun", "run_case", "write_fort63"]
+__all__ = ["Deck", "DistributedPartition", "Ensemble", "HydroStep", "PartitionedRun", "run_case", "write_fort63",
+           "write_hotstart"]

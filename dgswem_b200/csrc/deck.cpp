@@ -235,6 +235,7 @@ struct dgswem_deck {
   int nt = 0, noutge = 0, nspoolge = 0, ntcysge = 0, ntcyfge = 0;
   // fort.dg
   int ph = 1, pl = 1, rk_stage = 2, rk_order = 2, modal_ic = 0, artdif = 0, sedflag = 0;
+  int dghot = 0, dghotspool = 86400, hot_it = 0;  // DG hot start output switch / interval; ITHS read
   // storage the setup points into
   std::vector<double> atvd, btvd, dtvd;
   std::vector<int> nm, nedno, nedel, nedsd, neled;
@@ -284,7 +285,11 @@ void read_fort_dg(const std::string& dir, dgswem_deck* d) {
     d->rk_order = ListStream::as_int(rk[1]);
     f.read(1);
     d->modal_ic = f.integer();
-    f.read(2);
+    {
+      auto h = f.read(2);  // DGHOT, DGHOTSPOOL (read_fort_dg.F90:111)
+      d->dghot = ListStream::as_int(h[0]);
+      d->dghotspool = ListStream::as_int(h[1]);
+    }
     d->s.slopeflag = f.integer();
     d->sedflag = ListStream::as_int(f.read(4)[0]);
     f.read(1); f.read(1);
@@ -292,12 +297,12 @@ void read_fort_dg(const std::string& dir, dgswem_deck* d) {
     return;
   }
   // keyword format (read_fort_dg.F90:186-300), defaults of FORT_DG_SETUP
-  d->pl = 1; d->ph = 1; d->rk_stage = 2; d->rk_order = 2; d->modal_ic = 0;
+  d->pl = 1; d->ph = 1; d->rk_stage = 2; d->rk_order = 2; d->modal_ic = 0; d->dghot = 0; d->dghotspool = 86400;
   d->s.slopeflag = 5; d->s.rainfall = 0; d->artdif = 0; d->sedflag = 0;
   std::unordered_map<std::string, int*> ints = {
       {"pl", &d->pl}, {"ph", &d->ph}, {"rk_stage", &d->rk_stage}, {"rk_order", &d->rk_order},
       {"modal_ic", &d->modal_ic}, {"slopeflag", &d->s.slopeflag}, {"rainfall", &d->s.rainfall},
-      {"artdif", &d->artdif}, {"sedflag", &d->sedflag}};
+      {"artdif", &d->artdif}, {"sedflag", &d->sedflag}, {"dghot", &d->dghot}, {"dghotspool", &d->dghotspool}};
   for (const std::string& raw : f.records()) {
     std::string line = trimmed(raw);
     if (line.empty() || line[0] == '!') continue;
@@ -917,6 +922,59 @@ void build_element_data(dgswem_deck* d, const Fort15& p) {
 
 }  // namespace
 
+// DG hot start (prep_DG.F:1403-1445, MODAL_IC = 2): Hot_start.263 (PH, then
+// ZE(K,J) one per record), Hot_start.264 (PH PH, then QX(K,J) QY(K,J)) and
+// Hot_start.214 (ITHS ..., then HB(K,J) WDFLG(J)), records in the order J
+// = 1..NE, K = 1..DOFH, read list-directed (the items a record needs, the
+// rest of it skipped; D exponents accepted).  The modes replace the cold
+// start's ZE/QX/QY, HB and WDFLG.
+namespace {
+std::vector<std::vector<double>> hot_records(const std::string& path) {
+  std::ifstream in(path);
+  if (!in) throw dgswem::Failure(DGSWEM_ERR_IO, "cannot open " + path);
+  std::vector<std::vector<double>> recs;
+  std::string line;
+  while (std::getline(in, line)) {
+    for (char& c : line)
+      if (c == ',') c = ' ';
+      else if (c == 'D' || c == 'd') c = 'E';
+    std::vector<double> v;
+    const char* p = line.c_str();
+    char* end = nullptr;
+    for (;;) {
+      const double x = std::strtod(p, &end);
+      if (end == p) break;
+      v.push_back(x);
+      p = end;
+    }
+    if (!v.empty()) recs.push_back(std::move(v));
+  }
+  return recs;
+}
+}  // namespace
+
+static void read_hotstart(const std::string& root, dgswem_deck* d) {
+  const dgswem_cuda_setup& s = d->s;
+  const size_t ne = (size_t)s.ne, dofh = (size_t)s.dofh, n = ne * dofh;
+  auto r263 = hot_records(root + "/Hot_start.263");
+  auto r264 = hot_records(root + "/Hot_start.264");
+  auto r214 = hot_records(root + "/Hot_start.214");
+  if (r263.size() < n + 1 || r264.size() < n + 1 || r214.size() < n + 1)
+    throw dgswem::Failure(DGSWEM_ERR_IO, "DG hot start files hold fewer records than NE x DOFH");
+  if ((int)r263[0][0] != d->ph || r264[0].size() < 2 || (int)r264[0][0] != d->ph)
+    throw dgswem::Failure(DGSWEM_ERR_IO, "INCONSISTENCY IN P -- CHECK INPUT FILES (DG hot start)");
+  d->hot_it = (int)r214[0][0];
+  for (size_t i = 0; i < n; ++i) {
+    const auto &a = r263[i + 1], &b = r264[i + 1], &c = r214[i + 1];
+    if (b.size() < 2 || c.size() < 2) throw dgswem::Failure(DGSWEM_ERR_IO, "short DG hot start record");
+    d->ze[i] = a[0];
+    d->qx[i] = b[0];
+    d->qy[i] = b[1];
+    d->hb[i] = c[0];
+    d->wdflg[i / dofh] = (int)c[1];
+  }
+}
+
 extern "C" int dgswem_deck_open(const char* dir, dgswem_deck** out) {
   return dgswem::guarded([&]() {
     if (!dir || !out) throw dgswem::Failure(DGSWEM_ERR_ARG, "null argument");
@@ -929,7 +987,8 @@ extern "C" int dgswem_deck_open(const char* dir, dgswem_deck** out) {
     if (d->ph != 1 && d->ph != 2) throw dgswem::Failure(DGSWEM_ERR_ARG, "only p = 1 and p = 2 are supported");
     if (d->ph == 2 && (d->s.slopeflag != 0 || d->s.nolifa >= 2))
       throw dgswem::Failure(DGSWEM_ERR_ARG, "the slope limiter and wetting/drying are p = 1 only, as in the reference");
-    if (d->modal_ic != 0) throw dgswem::Failure(DGSWEM_ERR_ARG, "modal_ic != 0 is not supported by the deck reader");
+    if (d->modal_ic != 0 && d->modal_ic != 2)
+      throw dgswem::Failure(DGSWEM_ERR_ARG, "modal_ic must be 0 (cold start) or 2 (DG hot start)");
     if (d->artdif != 0 || d->sedflag != 0)
       throw dgswem::Failure(DGSWEM_ERR_ARG, "artificial diffusion / sediment are not on this path");
     d->s.dofh = (d->ph + 1) * (d->ph + 2) / 2;
@@ -937,6 +996,7 @@ extern "C" int dgswem_deck_open(const char* dir, dgswem_deck** out) {
     d->s.nrk = d->rk_stage;
     build_edges(d.get(), p);
     build_element_data(d.get(), p);
+    if (d->modal_ic == 2) read_hotstart(root, d.get());
     dgswem_cuda_setup& s = d->s;
     s.atvd = d->atvd.data();
     s.btvd = d->btvd.data();
@@ -998,6 +1058,10 @@ extern "C" int dgswem_deck_int(const dgswem_deck* d, const char* key, int* value
     else if (k == "ntcysge") *value = d->ntcysge;
     else if (k == "ntcyfge") *value = d->ntcyfge;
     else if (k == "noutge") *value = d->noutge;
+    else if (k == "dghot") *value = d->dghot;
+    else if (k == "dghotspool") *value = d->dghotspool;
+    else if (k == "modal_ic") *value = d->modal_ic;
+    else if (k == "hotstart_it") *value = d->hot_it;
     else throw dgswem::Failure(DGSWEM_ERR_ARG, "unknown deck key " + k);
   });
 }

@@ -164,6 +164,18 @@ class HydroStep:
         of ``steps`` (even) steps; 0 turns graphs off."""
         _abi.check(self._lib.dgswem_cuda_set_graph(self._h, int(steps)))
 
+    def write_hotstart(self, path, it: int, hb=None) -> None:
+        """The DG hot start of the current state at step ``it`` (write_hotstart):
+        HB from this handle's deck unless given."""
+        if hb is None:
+            if self._deck is None:
+                raise ValueError("hb is needed when the handle was not created from a Deck")
+            hb = self._deck.real_array("hb", self.dofh * self.ne).reshape(self.ne, self.dofh)
+        ze, qx, qy, wd = self.state()
+        s = self._deck.s if self._deck is not None else None
+        dtdp = s.dtdp if s is not None else 0.0
+        write_hotstart(path, {3: 1, 6: 2}[self.dofh], it, dtdp, ze, qx, qy, hb, wd)
+
     # ---- tile / block shapes and the autotuner ----
     @staticmethod
     def shapes() -> dict:
@@ -464,20 +476,29 @@ class DistributedPartition:
 
 
 def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False,
-             mixed: bool = False):
+             mixed: bool = False, hot_dir=None):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with
     DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  Returns the
-    list of (it, eta2) snapshots; writes them to ``out`` when given."""
+    list of (it, eta2) snapshots; writes them to ``out`` when given.  A deck
+    with MODAL_IC = 2 starts from its DG hot start at step ITHS + 1; with
+    DGHOT = 1 the DG hot start is written (to ``hot_dir``, the deck's
+    directory by default, as the reference does) every DGHOTSPOOL steps and
+    at the last step (write_results.F:1197-1240)."""
     deck = Deck(path)
     nt = deck.control("nt") if nsteps is None else nsteps
+    it0 = deck.control("hotstart_it") + 1 if deck.control("modal_ic") == 2 else 1
+    dghot, dghotspool = deck.control("dghot"), deck.control("dghotspool")
+    hot_dir = Path(path) if hot_dir is None else Path(hot_dir)
     nspool, ts, tf = deck.control("nspoolge"), deck.control("ntcysge"), deck.control("ntcyfge")
     noutge = deck.control("noutge")
     nolifa = deck.s.nolifa
     snaps = []
     with HydroStep(deck, device, strict=strict, mixed=mixed) as hs:
         count = 0
-        for it in range(1, nt + 1):
+        for it in range(it0, nt + 1):
             hs.timestep(it)
+            if dghot == 1 and (it % dghotspool == 0 or it == nt):
+                hs.write_hotstart(hot_dir, it)
             if noutge != 0 and ts < it <= tf:
                 count += 1
                 if count == nspool:
@@ -492,6 +513,30 @@ def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict:
         write_fort63(out, snaps, deck.s.np, deck.s.dtdp * nspool, nspool, deck.s.statim, deck.s.dtdp)
     deck.close()
     return snaps
+
+
+def write_hotstart(path, ph: int, it: int, dtdp: float, ze, qx, qy, hb, wdflg) -> None:
+    """DG hot start files in the reference's layout (write_results.F:1197-1240,
+    read back by prep_DG.F:1403-1445 with MODAL_IC = 2): Hot_start.263 holds
+    PH, then ZE(K,J) one per record; Hot_start.264 PH PH, then QX(K,J)
+    QY(K,J); Hot_start.214 IT DTDP, then HB(K,J) WDFLG(J); records in the
+    order J = 1..NE, K = 1..DOFH.  ze, qx, qy, hb: (ne, dofh) arrays; values
+    with 18 significant digits (exact round trip)."""
+    path = Path(path)
+    path.mkdir(parents=True, exist_ok=True)
+    ze, qx, qy, hb = (np.asarray(a, dtype=np.float64) for a in (ze, qx, qy, hb))
+    ne, dofh = ze.shape
+    with open(path / "Hot_start.263", "w") as f:
+        f.write(f" {ph}\n")
+        np.savetxt(f, ze.reshape(-1, 1), fmt=" %.17E")
+    with open(path / "Hot_start.264", "w") as f:
+        f.write(f" {ph} {ph}\n")
+        np.savetxt(f, np.column_stack([qx.ravel(), qy.ravel()]), fmt=" %.17E")
+    with open(path / "Hot_start.214", "w") as f:
+        f.write(f" {it} {dtdp:.17E}\n")
+        wd = np.repeat(np.asarray(wdflg, dtype=np.int64), dofh)
+        for h, w in zip(hb.ravel(), wd):
+            f.write(f" {h:.17E} {w}\n")
 
 
 def write_fort63(path, snaps, np_, dt_out, nspool, statim, dtdp):
