@@ -67,3 +67,28 @@ def test_deck_errors_are_status_codes(built, scratch):
     (bad / "fort.14").write_text("\n".join(text))
     with pytest.raises(DgswemError, match="clockwise"):
         Deck(bad)
+
+
+def test_p2_deck(built, scratch):
+    """fort.dg with pl = ph = 2: DOFH = 6, the bathymetry's six modes (the
+    linear nodal depth's modes 1-3, zeros above) equal to the oracle's, and
+    the edge tables of the same mesh; the limiter and wet/dry refused at p=2
+    as the reference has them at p=1 only."""
+    from dgswem_b200._abi import DgswemError
+    p2 = {"extra": {"pl": 2, "ph": 2}}
+    path = decks.quarter_annulus(scratch / "deck_p2", nr=4, nth=8, nsteps=2, **p2)
+    d = Deck(path)
+    ne = d.s.ne
+    assert d.s.dofh == 6
+    hb = d.real_array("hb", 6 * ne).reshape(ne, 6)
+    orc = Oracle(path)
+    assert orc.dofh == 6
+    np.testing.assert_array_equal(hb, orc.real_table("HB").reshape(ne, 6))
+    assert not hb[:, 3:].any()
+    np.testing.assert_array_equal(d.int_array("nedno", 2 * d.s.nedges), orc.int_table("NEDNO"))
+    orc.close()
+    d.close()
+    for kw in ({"slopeflag": 5}, {"nolifa": 2}):
+        bad = decks.quarter_annulus(scratch / f"deck_p2_{next(iter(kw))}", nr=4, nth=8, nsteps=2, **kw, **p2)
+        with pytest.raises(DgswemError, match="p = 1 only"):
+            Deck(bad)
