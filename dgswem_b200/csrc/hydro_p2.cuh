@@ -200,81 +200,99 @@ __global__ void __launch_bounds__(128, 3) p2_elements(const __grid_constant__ P2
     const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
     hyb = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
   }
-  double vol[kP2Agp][8];
-  for (int i = 0; i < kP2Agp; ++i) p2_volume<kNonlin>(A, q, hbe, drdx, dsdx, drdy, dsdy, hyb, e, i, vol[i]);
+  // all three variables' sums at once (no per-point volume array): each
+  // (variable, mode) sum takes the same terms in the same order as above
   const unsigned info = m.einfo[e];
+  double rhs[3][kP2Modes], isum[3][kP2Modes];
+#pragma unroll
+  for (int V = 0; V < 3; ++V)
+#pragma unroll
+    for (int k = 0; k < kP2Modes; ++k) { rhs[V][k] = 0.0; isum[V][k] = 0.0; }
+  for (int s = 0; s < 3; ++s) {
+    const int l = ei_order(info, s);
+    const unsigned kind = ei_kind(info, l);
+    if (kind == kNone) continue;
+    const double* ef = A.ef + (size_t)(e * 3 + l) * kP2Egp * 3;
+    if (kind == kInterior) {
+      const bool is_in = ei_flag(info, l) != 0;
+      const double edfac = m.egeo[(size_t)(EGeo::kEdfac + l) * ne + e];
+      double acc[3][kP2Modes];
+#pragma unroll
+      for (int V = 0; V < 3; ++V)
+#pragma unroll
+        for (int k = 0; k < kP2Modes; ++k) acc[V][k] = 0.0;
+      for (int I = 0; I < kP2Egp; ++I) {
+        const int j = is_in ? I : kP2Egp - 1 - I;
+        const double v0 = ef[j * 3], v1 = ef[j * 3 + 1], v2 = ef[j * 3 + 2];
+#pragma unroll
+        for (int k = 0; k < kP2Modes; ++k) {
+          const double wk = edfac * B.edgeq[l][j][k];
+          if (is_in) {
+            acc[0][k] = acc[0][k] - wk * v0;
+            acc[1][k] = acc[1][k] - wk * v1;
+            acc[2][k] = acc[2][k] - wk * v2;
+          } else {
+            acc[0][k] = acc[0][k] + wk * v0;
+            acc[1][k] = acc[1][k] + wk * v1;
+            acc[2][k] = acc[2][k] + wk * v2;
+          }
+        }
+      }
+#pragma unroll
+      for (int V = 0; V < 3; ++V)
+#pragma unroll
+        for (int k = 0; k < kP2Modes; ++k) isum[V][k] = isum[V][k] + acc[V][k];
+    } else {
+      const double areas = m.egeo[(size_t)EGeo::kAreas * ne + e];
+      const double xlen = m.egeo[(size_t)(EGeo::kXlen + l) * ne + e];
+      for (int I = 0; I < kP2Egp; ++I) {
+        const double v0 = ef[I * 3], v1 = ef[I * 3 + 1], v2 = ef[I * 3 + 2];
+#pragma unroll
+        for (int k = 0; k < kP2Modes; ++k) {
+          const double wk = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
+          rhs[0][k] = rhs[0][k] - wk * v0;
+          rhs[1][k] = rhs[1][k] - wk * v1;
+          rhs[2][k] = rhs[2][k] - wk * v2;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int V = 0; V < 3; ++V)
+#pragma unroll
+    for (int k = 0; k < kP2Modes; ++k) rhs[V][k] = rhs[V][k] + isum[V][k];  // add_internal_flux
+  if (P.rainfall == 1) {
+    const double src = 7.0556e-6;
+    for (int i = 0; i < kP2Agp; ++i)
+#pragma unroll
+      for (int k = 0; k < kP2Modes; ++k) rhs[0][k] = rhs[0][k] + B.srfac[k][i] * src;
+  }
+  for (int i = 0; i < kP2Agp; ++i) {
+    double vol[8];
+    p2_volume<kNonlin>(A, q, hbe, drdx, dsdx, drdy, dsdy, hyb, e, i, vol);
+    rhs[1][0] = rhs[1][0] + B.srfac[0][i] * vol[6];
+    rhs[2][0] = rhs[2][0] + B.srfac[0][i] * vol[7];
+#pragma unroll
+    for (int k = 1; k < kP2Modes; ++k) {
+      const double dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
+      const double dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
+      const double xf = B.mw[k][i] * dpx;
+      const double yf = B.mw[k][i] * dpy;
+      const double sr = B.srfac[k][i];
+      rhs[0][k] = rhs[0][k] + xf * vol[0] + yf * vol[1];
+      rhs[1][k] = rhs[1][k] + xf * vol[2] + yf * vol[3] + sr * vol[6];
+      rhs[2][k] = rhs[2][k] + xf * vol[4] + yf * vol[5] + sr * vol[7];
+    }
+  }
+  // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
   bool bad = false;
-  for (int V = 0; V < 3; ++V) {
-    double rhs[kP2Modes], isum[kP2Modes];
+  const bool hist0 = A.irk > 1;
 #pragma unroll
-    for (int k = 0; k < kP2Modes; ++k) { rhs[k] = 0.0; isum[k] = 0.0; }
-    for (int s = 0; s < 3; ++s) {
-      const int l = ei_order(info, s);
-      const unsigned kind = ei_kind(info, l);
-      if (kind == kNone) continue;
-      const double* ef = A.ef + (size_t)(e * 3 + l) * kP2Egp * 3 + V;
-      if (kind == kInterior) {
-        const bool is_in = ei_flag(info, l) != 0;
-        const double edfac = m.egeo[(size_t)(EGeo::kEdfac + l) * ne + e];
-        double acc[kP2Modes];
-#pragma unroll
-        for (int k = 0; k < kP2Modes; ++k) acc[k] = 0.0;
-        for (int I = 0; I < kP2Egp; ++I) {
-          const int j = is_in ? I : kP2Egp - 1 - I;
-          const double val = ef[j * 3];
-#pragma unroll
-          for (int k = 0; k < kP2Modes; ++k) {
-            const double wk = edfac * B.edgeq[l][j][k];
-            if (is_in)
-              acc[k] = acc[k] - wk * val;
-            else
-              acc[k] = acc[k] + wk * val;
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < kP2Modes; ++k) isum[k] = isum[k] + acc[k];
-      } else {
-        const double areas = m.egeo[(size_t)EGeo::kAreas * ne + e];
-        const double xlen = m.egeo[(size_t)(EGeo::kXlen + l) * ne + e];
-        for (int I = 0; I < kP2Egp; ++I) {
-          const double val = ef[I * 3];
-#pragma unroll
-          for (int k = 0; k < kP2Modes; ++k) {
-            const double wk = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
-            rhs[k] = rhs[k] - wk * val;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < kP2Modes; ++k) rhs[k] = rhs[k] + isum[k];  // add_internal_flux
-    if (V == 0 && P.rainfall == 1) {
-      const double src = 7.0556e-6;
-      for (int i = 0; i < kP2Agp; ++i)
-#pragma unroll
-        for (int k = 0; k < kP2Modes; ++k) rhs[k] = rhs[k] + B.srfac[k][i] * src;
-    }
-    for (int i = 0; i < kP2Agp; ++i) {
-      const double a = vol[i][2 * V], b = vol[i][2 * V + 1], vs = vol[i][V == 2 ? 7 : 6];
-      if (V != 0) rhs[0] = rhs[0] + B.srfac[0][i] * vs;
-#pragma unroll
-      for (int k = 1; k < kP2Modes; ++k) {
-        const double dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
-        const double dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
-        const double xf = B.mw[k][i] * dpx;
-        const double yf = B.mw[k][i] * dpy;
-        if (V == 0)
-          rhs[k] = rhs[k] + xf * a + yf * b;
-        else
-          rhs[k] = rhs[k] + xf * a + yf * b + B.srfac[k][i] * vs;
-      }
-    }
-    // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
-    const bool hist0 = A.irk > 1;
+  for (int V = 0; V < 3; ++V)
 #pragma unroll
     for (int k = 0; k < kP2Modes; ++k) {
       const int c = kP2Modes * V + k;
-      const double rk = rhs[k];
+      const double rk = rhs[V][k];
       if (A.rout) A.rout[(size_t)c * ne + e] = rk;
       const double qc = q[c];
       double acc = 0.0;
@@ -294,7 +312,6 @@ __global__ void __launch_bounds__(128, 3) p2_elements(const __grid_constant__ P2
       bad = bad || isnan(acc);
       A.qout[(size_t)c * ne + e] = acc;
     }
-  }
   if (bad) atomicOr(A.err, 1u);
 }
 
