@@ -175,10 +175,12 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const double* q, cons
 // right-hand side in the reference's order -- boundary edges by kind and
 // list, interior edges as the slot sum of add_internal_flux, rain, area
 // points -- then the SSP combination (DG_hydro_timestep.F:238-290) into
-// qout.  Every element is wet at p=2.  Compiled for three resident blocks
-// of 128 per SM (168 registers, a few dozen bytes of spills): latency bound
-// at the 7.7 warps per SM the unbounded 228-register allocation allows, it
-// is 5 % faster on the 8M-element annulus (4 blocks, 128 registers: no gain).
+// qout.  Every element is wet at p=2.  The three variables' sums are
+// accumulated together, each in that order, the volume terms of an area
+// point used as soon as they are formed.  Compiled for three resident
+// blocks of 128 per SM (168 registers, under 200 bytes of spills): latency
+// bound, it gains more from the warps than it loses to the spills (four
+// blocks, 128 registers: no gain).
 template <bool kNonlin>
 __global__ void __launch_bounds__(128, 3) p2_elements(const __grid_constant__ P2Args A) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
