@@ -177,12 +177,13 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const double* q, cons
 // points -- then the SSP combination (DG_hydro_timestep.F:238-290) into
 // qout.  Every element is wet at p=2.  The three variables' sums are
 // accumulated together, each in that order, the volume terms of an area
-// point used as soon as they are formed.  Compiled for three resident
-// blocks of 128 per SM (168 registers, under 200 bytes of spills): latency
-// bound, it gains more from the warps than it loses to the spills (four
-// blocks, 128 registers: no gain).
+// point used as soon as they are formed.  Compiled for four resident
+// blocks of 128 per SM (128 registers, about 500 bytes of spills to
+// L1-cached local memory): latency bound, it gains more from the warps than
+// it loses to the spills (8M-element step: 9.48 ms; three blocks, 168
+// registers: 10.20 ms; two blocks, 247 registers: 9.75 ms).
 template <bool kNonlin>
-__global__ void __launch_bounds__(128, 3) p2_elements(const __grid_constant__ P2Args A) {
+__global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2Args A) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= A.ne_act) return;
   const MeshView& m = A.m;
