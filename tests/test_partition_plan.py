@@ -15,7 +15,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from dgswem_b200 import Deck, _abi, decks
+from dgswem_b200 import Deck, _abi
 
 ROOT = Path(__file__).resolve().parents[1]
 
