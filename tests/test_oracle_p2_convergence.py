@@ -15,7 +15,7 @@ import math
 import numpy as np
 import pytest
 
-from dgswem_b200 import decks
+from dgswem_b200 import Deck, decks
 from oracle_lib import Oracle
 
 L, W, H, A, G = 10e3, 2.5e3, 10.0, 0.1, 9.81
@@ -82,3 +82,35 @@ def test_standing_wave_convergence_order(built, tmp_path, p):
     rates = [math.log2(errs[i] / errs[i + 1]) for i in range(2)]
     print(f"p={p} errors {errs} rates {rates}")
     assert all(r > p + 1 - 0.4 for r in rates), (errs, rates)
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_closed_basin_mass_conserved(built, tmp_path, p):
+    """Nonlinear equations (NOLIFA=1) in the closed basin from a Gaussian
+    bump: the water volume sum_e (ZE_1 + HB_1) * area stays constant to
+    round-off over 400 steps (mode 1 is the element mean)."""
+    path = tmp_path / f"mass_p{p}"
+    x, y, elems = basin(path, 16, p)
+    f15 = (path / "fort.15").read_text()
+    for key in ("NOLIFA", "NOLICA", "NOLICAT"):  # the full nonlinear equations
+        f15 = f15.replace(f"0 ! {key}\n", f"1 ! {key}\n")
+    (path / "fort.15").write_text(f15)
+    deck = Deck(path)
+    assert deck.s.nleq == 1.0 and deck.s.leq == 0.0
+    deck.close()
+    orc = Oracle(path)
+    px, py, wphys, phi, wa = area_points(orc, x, y, elems)
+    minv = orc.real_table("M_INV")
+    bump = 0.5 * np.exp(-(((px - 0.4 * L) / 1500.0) ** 2 + ((py - 0.5 * W) / 800.0) ** 2))
+    ze = (bump * wa[None, :]) @ phi.T * minv[None, :]
+    zero = np.zeros_like(ze)
+    orc.set_state(ze, zero, zero, np.ones(len(elems), np.int32))
+    area = np.sum(wphys, axis=1)
+    hb = orc.real_table("HB").reshape(len(elems), orc.dofh)
+    vol0 = float(np.sum((ze[:, 0] + hb[:, 0]) * area))
+    orc.run(1, NSTEPS)
+    z, qx, _, _ = orc.state()
+    orc.close()
+    vol1 = float(np.sum((z[:, 0] + hb[:, 0]) * area))
+    assert np.abs(qx).max() > 1e-4  # the bump spread
+    assert abs(vol1 - vol0) <= 1e-12 * vol0, (vol0, vol1)
