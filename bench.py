@@ -49,17 +49,21 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 DOFS_PER_ELEMENT = 9  # 3 variables x 3 modes at p=1
-# Algorithmic bytes per element and stage for stage_p1 (FP64, SSP(2,2),
-# averaged over its two stages): stage state in 72 + step-start state 36
-# (stage 2 only) + stage state out 72 + HB modes 24 + geometry table rows
-# copied to shared memory 112 (normals, Jacobian terms, XLEN/AREAS, mean
-# Manning n) + WDFLG 4 + edge info 8 + tile plan 14 (1.63 edge tasks of 8
-# bytes and 0.25 halo ids per element on the Morton-ordered mesh).
-STAGE_KERNEL_BYTES = 72 + 36 + 72 + 24 + 112 + 4 + 8 + 14
-# whole-stage algorithmic bytes (adds node_minmax: element means 24 + node
-# min/max 24; limit_wetdry: state 72 + 72, node ids 12, node min/max 24,
-# HB modes 16, WDFLG 4 + 4, nodal depth 4)
-STAGE_TOTAL_BYTES = STAGE_KERNEL_BYTES + 48 + 72 + 72 + 12 + 24 + 16 + 8 + 4
+# Algorithmic bytes per element and stage of the stage kernel (the model of
+# config 2 for the path): state 2.5 x 72 (stage state in and out, and the
+# step-start state on the second of two stages) + HB modes 24 + inverse
+# Jacobian and area 40 + neighbour element ids 12 + WDFLG read and write 8 +
+# Manning n 8.
+STAGE_KERNEL_BYTES = 2.5 * 72 + 24 + 40 + 12 + 8 + 8
+# the whole RK stage adds the limiter's node ids 12 and the node min/max
+# written and read back 24
+STEP_BYTES_PER_ELEMENT_STAGE = STAGE_KERNEL_BYTES + 12 + 24
+# what stage_p1 reads beyond that model, per element-stage: the geometry rows
+# it copies to shared memory (normals, Jacobian terms, XLEN/AREAS, mean
+# Manning n: 112 B where the model counts 40 + 8), the tile plan (1.63 edge
+# tasks of 8 bytes and 0.25 halo ids per element on the Morton-ordered mesh)
+# and the packed edge kinds / task slots
+STAGE_OVERHEAD_BYTES = {"geometry_rows_beyond_model": 112 - 48, "tile_plan": 14, "edge_info": 8}
 # DRAM bytes per element of one stage_p1 launch, dram__bytes_read.sum +
 # dram__bytes_write.sum from ncu on the same deck at 999,492 elements: the
 # mean of a stage-1 (291.6) and a stage-2 (364.0) launch; traffic grows with
@@ -206,9 +210,9 @@ def autotune(h, args, it: int) -> dict | None:
 def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
     """The mixed-precision form (DGSWEM_CUDA_MIXED) on the same deck: its rate
     (same timing rules as the FP64 line), per-kernel times, and its error
-    against the FP64 form after ``--mixed-err-steps`` steps from the initial
-    state (nodal elevation and velocity, element-mean elevation, total water
-    volume, wet/dry flags)."""
+    against the headline FP64 build after ``--mixed-err-steps`` steps from the
+    initial state (nodal elevation and velocity, element-mean elevation, total
+    water volume, wet/dry flags)."""
     import torch
     from dgswem_b200 import HydroStep
     hm = HydroStep(deck, device=device, mixed=True)
@@ -233,7 +237,7 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
     # error against the FP64 form, both from the deck's initial state
     n = args.mixed_err_steps
     outs = []
-    for kw in ({}, {"mixed": True}):
+    for kw in (variant_kwargs(args.variant), {"mixed": True}):
         with HydroStep(deck, device=device, **kw) as h:
             h.set_stream(stream.cuda_stream)
             h.run(1, n)
@@ -262,9 +266,9 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     0.1 Pa at 30 degrees (NWS=1: WSX2 = tau/rho0 cos 30, WSY2 = tau/rho0
     sin 30, PR2 = 0).  FP64 and mixed rates with the FP64 line's timing
     rules, and the mixed form's error against the FP64 form after
-    ``--config3-err-steps`` steps from the same state.  The reference's p=2
-    path is broken (p=2 is not on the device), so this is the p=1 half of
-    the configuration."""
+    ``--config3-err-steps`` steps from the same state.  With
+    ``--config3-p2-steps`` > 0 the same annulus at p=2 is timed too (FP64,
+    the p2_edges + p2_elements kernels): the "p2" object."""
     import torch
     from dgswem_b200 import Deck, HydroStep
     nr, nth = args.config3_nr, args.config3_nth
@@ -281,7 +285,7 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
                        "linear friction, wind 0.1 Pa at 30 degrees (NWS=1), dt=0.5 s",
            "elements": int(deck.s.ne), "steps": k, "warmup": w, "deck_write_s": t_write}
     states = {}
-    for name, kw in (("fp64", {}), ("mixed", {"mixed": True})):
+    for name, kw in (("fp64", variant_kwargs(args.variant)), ("mixed", {"mixed": True})):
         with HydroStep(deck, device=device, **kw) as h:
             h.set_stream(stream.cuda_stream)
             h.set_met(*met)
@@ -313,7 +317,7 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
         path2 = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth, p=2))
         deck2 = Deck(path2)
         k2 = args.config3_p2_steps
-        with HydroStep(deck2, device=device) as h:
+        with HydroStep(deck2, device=device, **variant_kwargs(args.variant)) as h:
             h.set_stream(stream.cuda_stream)
             h.set_met(*met)
             h.run(1, w)
@@ -511,18 +515,77 @@ def measured_peak():
 
 
 def cpu_baseline(path: Path, nsteps: int, threads: int):
-    """The FP64 oracle on the host cores (test-infrastructure CPU restatement)."""
+    """The FP64 oracle (test-infrastructure CPU restatement) on the host
+    cores: steps 1..nsteps of the deck from its initial state, the first one
+    untimed (first touch of the stage arrays).  Returns its rate over the
+    timed steps, their seconds, and the oracle's state after step nsteps --
+    the checker of the parity object."""
     sys.path.insert(0, str(ROOT / "tests"))
     from oracle_lib import Oracle
     orc = Oracle(path, threads=threads)
-    orc.step(1)  # warm-up (first-touch of the stage arrays)
+    orc.step(1)
     t0 = time.perf_counter()
-    for it in range(2, 2 + nsteps):
+    for it in range(2, nsteps + 1):
         orc.step(it)
     dt = time.perf_counter() - t0
     ne, nrk = orc.ne, orc.info("nrk")
+    state = orc.state()
     orc.close()
-    return DOFS_PER_ELEMENT * ne * nrk * nsteps / dt, dt
+    return DOFS_PER_ELEMENT * ne * nrk * (nsteps - 1) / dt, dt, state
+
+
+def parity(gpu_state, oracle_state, steps: int, variant: str) -> dict:
+    """The headline build's state after ``steps`` steps from the deck's
+    initial state against the oracle's: per variable the largest difference
+    relative to the variable's largest oracle coefficient, and how many
+    coefficients differ at all; wet/dry flags that differ."""
+    out = {"steps": steps, "variant": variant}
+    bitwise = True
+    for a, b, name in zip(gpu_state[:3], oracle_state[:3], ("ZE", "QX", "QY")):
+        out[f"{name}_max_rel"] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+        out[f"{name}_coefficients_differ"] = int((a != b).sum())
+        bitwise = bitwise and bool(np.array_equal(a, b))
+    out["max_rel"] = max(out[f"{v}_max_rel"] for v in ("ZE", "QX", "QY"))
+    out["wdflg_differ"] = int((gpu_state[3] != oracle_state[3]).sum())
+    out["bit_identical"] = bitwise and out["wdflg_differ"] == 0
+    return out
+
+
+VARIANT_TEXT = {"strict": "strict: FP64 without FMA contraction, the oracle's evaluation order (bit-identical to it)",
+                "fast": "fast: FP64 with FMA contraction"}
+
+
+def variant_kwargs(variant: str) -> dict:
+    return {"strict": True} if variant == "strict" else {}
+
+
+def other_variant_arm(deck, stream, args, world: int, dist, device: int) -> dict:
+    """The FP64 build the headline does not use, on the same deck and timing
+    rules (fewer steps): its rate, per-kernel times and shapes."""
+    import torch
+    from dgswem_b200 import HydroStep
+    other = "fast" if args.variant == "strict" else "strict"
+    with HydroStep(deck, device=device, **variant_kwargs(other)) as h:
+        h.set_stream(stream.cuda_stream)
+        h.run(1, args.warmup)
+        tiles = autotune(h, args, args.warmup + 1)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        k = args.other_variant_steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.run(args.warmup + 1, k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+        h.profile(True)
+        h.run(args.warmup + 1 + k, 10)
+        prof = h.profile_read()
+        h.profile(False)
+    return {"variant": VARIANT_TEXT[other], "value": whole_job_rate(world, deck.s.ne, deck.s.nrk, k, ms),
+            "unit": "DOF-stage/s", "steps": k, "ms_per_step": ms / k,
+            "per_kernel_ms": {n: v[0] / max(v[1], 1) for n, v in prof.items() if v[1]}, "tiles": tiles}
 
 
 def run_reference(args):
@@ -582,7 +645,13 @@ def main(argv=None):
     ap.add_argument("--ny", type=int, default=447)
     ap.add_argument("--workdir", default=os.environ.get("DGSWEM_BENCH_DIR", "/tmp/dgswem_b200_bench"))
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--cpu-steps", type=int, default=12, help="oracle steps in the cpu_baseline sample")
+    ap.add_argument("--variant", choices=["strict", "fast"], default="strict",
+                    help="FP64 kernel build of the headline: strict (no FMA contraction, bit-identical to the "
+                         "oracle) or fast (FMA contraction)")
+    ap.add_argument("--other-variant-steps", type=int, default=20,
+                    help="timed steps of the other FP64 build on the same deck (0: skip)")
+    ap.add_argument("--cpu-steps", type=int, default=12,
+                    help="oracle steps from the initial state: the cpu_baseline sample and the parity check")
     ap.add_argument("--ref-max-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision arm")
@@ -624,7 +693,8 @@ def main(argv=None):
     t_setup0 = time.perf_counter()
     deck = Deck(path)
     t_setup1 = time.perf_counter()
-    hs = HydroStep(deck, device=local)
+    vkw = variant_kwargs(args.variant)
+    hs = HydroStep(deck, device=local, **vkw)
     torch.cuda.synchronize()
     t_setup2 = time.perf_counter()
     ne, nrk = hs.ne, hs.nrk
@@ -673,6 +743,7 @@ def main(argv=None):
     achieved = STAGE_KERNEL_BYTES * ne / avg_stage_s / 1e9
     stage_total_ms = sum(v[0] for v in prof.values())
     stage_total_n = prof["stage_p1"][1]
+    step_achieved = STEP_BYTES_PER_ELEMENT_STAGE * ne * nrk / (ms_max / args.steps / 1e3) / 1e9
 
     # end to end through the C-ABI with host buffers: every step uploads the
     # state from pinned host memory, steps, and downloads the new state
@@ -710,20 +781,28 @@ def main(argv=None):
         "e2e": {"value": e2e_value, "unit": "DOF-stage/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes,
                 "how": "per step: upload ZE/QX/QY/WDFLG from pinned host memory, one hydro step, download"},
+        "variant": VARIANT_TEXT[args.variant],
         "roofline": {"bound": "hbm", "kernel": "stage_p1", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": STAGE_TRAFFIC_BYTES * ne,
                      "traffic_source": "ncu dram bytes per element of a stage-1 and a stage-2 launch (999,492 elements), "
                                        "scaled by the element count",
                      "algorithmic_bytes_per_element_stage": STAGE_KERNEL_BYTES,
+                     "overhead_bytes_per_element_stage": STAGE_OVERHEAD_BYTES,
                      "avg_launch_ms": avg_stage_s * 1e3,
+                     "whole_step": {"bytes_per_element_stage": STEP_BYTES_PER_ELEMENT_STAGE,
+                                    "achieved": step_achieved, "frac": step_achieved / peak,
+                                    "ms_per_step": ms_max / args.steps},
                      "stage_all_kernels_ms": stage_total_ms / max(stage_total_n, 1),
-                     "stage_all_kernels_frac": STAGE_TOTAL_BYTES * ne / (stage_total_ms / 1e3 / max(stage_total_n, 1)) / 1e9 / peak,
                      "per_kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items() if v[1]}},
     }
+    if args.other_variant_steps > 0:
+        line["other_variant"] = other_variant_arm(deck, stream, args, world, dist if world > 1 else None, local)
     if not args.no_mixed:
         mixed = mixed_arm(deck, stream, args, world, dist if world > 1 else None, local)
-        mixed["speedup_vs_fp64"] = mixed["value"] / value
+        mixed["speedup_vs_fp64"] = mixed["value"] / value  # against the headline FP64 build
+        if "other_variant" in line:
+            mixed["speedup_vs_other_fp64_build"] = mixed["value"] / line["other_variant"]["value"]
         line["mixed"] = mixed
     if args.config3_steps > 0:
         line["config3"] = config3_arm(args, stream, local, world, dist if world > 1 else None)
@@ -732,11 +811,21 @@ def main(argv=None):
     if args.adjoint_steps > 0 and world == 1:
         line["adjoint"] = adjoint_arm(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the checker: the headline build and the oracle from the deck's
+        # initial state for the same steps; the oracle's run is also the
+        # timed CPU baseline sample
+        k = args.cpu_steps
+        with HydroStep(deck, device=local, **vkw) as hp:
+            hp.set_stream(stream.cuda_stream)
+            hp.run(1, k)
+            hp.synchronize()
+            gstate = hp.state()
         threads = os.cpu_count() or 1
-        v, secs = cpu_baseline(path, args.cpu_steps, threads)
+        v, secs, ostate = cpu_baseline(path, k, threads)
         line["cpu_baseline"] = {"value": v, "unit": "DOF-stage/s", "cores": threads, "kind": "port",
-                                "sample": f"{args.cpu_steps} full hydro steps of the same {ne}-element deck "
+                                "sample": f"steps 2-{k} of the same {ne}-element deck from its initial state "
                                           f"({secs:.1f} s), FP64 oracle, OpenMP"}
+        line["parity"] = parity(gstate, ostate, k, args.variant)
     hs.close()
     deck.close()
     if rank == 0:

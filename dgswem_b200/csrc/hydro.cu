@@ -1476,9 +1476,10 @@ int dgswem_cuda_last_error(char* buf, int buflen) {
 
 static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int nparts, int device, int flags) {
   {
-    if (flags & ~(DGSWEM_CUDA_STRICT | DGSWEM_CUDA_MIXED)) throw Failure(DGSWEM_ERR_ARG, "unknown flags");
-    if ((flags & DGSWEM_CUDA_STRICT) && (flags & DGSWEM_CUDA_MIXED))
-      throw Failure(DGSWEM_ERR_ARG, "DGSWEM_CUDA_STRICT and DGSWEM_CUDA_MIXED exclude each other");
+    if (flags & ~(DGSWEM_CUDA_STRICT | DGSWEM_CUDA_MIXED | DGSWEM_CUDA_FAST))
+      throw Failure(DGSWEM_ERR_ARG, "unknown flags");
+    if (((flags & DGSWEM_CUDA_STRICT) != 0) + ((flags & DGSWEM_CUDA_MIXED) != 0) + ((flags & DGSWEM_CUDA_FAST) != 0) > 1)
+      throw Failure(DGSWEM_ERR_ARG, "DGSWEM_CUDA_STRICT, DGSWEM_CUDA_FAST and DGSWEM_CUDA_MIXED exclude each other");
     if (s->dofh != 3 && s->dofh != kP2Modes)
       throw Failure(DGSWEM_ERR_ARG, "DOFH must be 3 (p=1) or 6 (p=2)");
     if (s->dofh == kP2Modes) {
@@ -1502,9 +1503,10 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     DG_CUDA(cudaSetDevice(device));
     std::unique_ptr<dgswem_cuda> h(new dgswem_cuda());
     h->device = device;
-    h->v = (flags & DGSWEM_CUDA_STRICT) ? &kStrict : (flags & DGSWEM_CUDA_MIXED) ? &kMixed : &kFast;
+    // the strict kernels unless the fast or the mixed form is asked for
+    h->v = (flags & DGSWEM_CUDA_FAST) ? &kFast : (flags & DGSWEM_CUDA_MIXED) ? &kMixed : &kStrict;
     h->dofh = s->dofh;
-    if (h->dofh == kP2Modes) h->v2 = (flags & DGSWEM_CUDA_STRICT) ? &kStrictP2 : &kFastP2;
+    if (h->dofh == kP2Modes) h->v2 = (flags & DGSWEM_CUDA_FAST) ? &kFastP2 : &kStrictP2;
     h->ne = s->ne;
     h->np = s->np;
     h->nrk = s->nrk;

@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include "cr_math.cuh"
 #include "hydro_device.cuh"
 
 #ifndef DGSWEM_VARIANT
@@ -76,14 +77,16 @@ __device__ __forceinline__ void cp_async4_s(unsigned dst, const void* src) {
 }
 
 // DEPTH**(1.D0/3.D0) of the Manning friction (rhs_dg_hydro.F).  The strict
-// variant calls pow with the reference's exponent; the fast variant takes
-// the cube root, which differs from it by less than an ulp's worth of the
-// exponent's rounding (1/3 is not a double) and costs a fraction of pow.
+// variant takes the correctly rounded value of the reference's expression
+// (pow_third, cr_math.cuh: IEEE operations only, so the oracle's correctly
+// rounded evaluation gives the same bits); the fast variant takes the cube
+// root, which differs from it by less than an ulp's worth of the exponent's
+// rounding (1/3 is not a double) and costs a fraction of it.
 __device__ __forceinline__ double cube_root(double x) {
 #ifdef DGSWEM_FAST_MATH
   return cbrt(x);
 #else
-  return pow(x, 1.0 / 3.0);
+  return pow_third(x);
 #endif
 }
 __device__ __forceinline__ float cube_root(float x) { return cbrtf(x); }

@@ -18,7 +18,7 @@ from .hydro import Deck, HydroStep
 
 
 class Ensemble:
-    def __init__(self, decks, device: int = 0, mixed: bool = True, strict: bool = False):
+    def __init__(self, decks, device: int = 0, mixed: bool = True, strict: bool | None = None):
         self.members = list(decks)
         if not self.members:
             raise ValueError("empty ensemble")

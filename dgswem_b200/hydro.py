@@ -93,23 +93,25 @@ class HydroStep:
     DG_HYDRO_TIMESTEP).  ``setup`` is a ``Deck`` or a pointer to a filled
     ``dgswem_cuda_setup``."""
 
-    STRICT = 1  # DGSWEM_CUDA_STRICT
+    STRICT = 1  # DGSWEM_CUDA_STRICT (the default form)
     MIXED = 2   # DGSWEM_CUDA_MIXED
+    FAST = 4    # DGSWEM_CUDA_FAST
 
-    def __init__(self, setup, device: int = 0, strict: bool = False, part: int = 0, nparts: int = 1,
-                 mixed: bool = False):
-        """strict=True selects the kernels compiled without FMA contraction
-        (bitwise reproducible against the non-contracting FP64 oracle);
-        mixed=True the mixed-precision kernels (FP32 edge and volume
-        arithmetic, FP64 state, SSP combination, limiter and wet/dry); the
-        default is the FMA-contracted FP64 fast form.  nparts > 1 makes a
-        partition handle (dgswem_cuda_create_part), stepped by
-        ``PartitionedRun``."""
+    def __init__(self, setup, device: int = 0, strict: bool | None = None, part: int = 0, nparts: int = 1,
+                 mixed: bool = False, fast: bool = False):
+        """The kernels: strict (the default; compiled without FMA contraction,
+        bit-identical to the FP64 oracle), fast (``fast=True``, or
+        ``strict=False``: FMA contraction) or mixed (``mixed=True``: FP32
+        edge, volume and limiter arithmetic, FP64 state, SSP combination and
+        wet/dry).  nparts > 1 makes a partition handle
+        (dgswem_cuda_create_part), stepped by ``PartitionedRun``."""
         self._lib = _abi.load()
-        if strict and mixed:
-            raise ValueError("strict and mixed exclude each other")
-        self.strict = bool(strict)
+        fast = bool(fast) or (strict is False and not mixed)
+        if sum((bool(strict), fast, bool(mixed))) > 1:
+            raise ValueError("strict, fast and mixed exclude each other")
         self.mixed = bool(mixed)
+        self.fast = fast
+        self.strict = not (self.mixed or self.fast)
         self._deck = setup if isinstance(setup, Deck) else None
         sp = setup.setup if isinstance(setup, Deck) else setup
         s = sp.contents
@@ -117,7 +119,7 @@ class HydroStep:
         self.slopeflag = s.slopeflag
         self.part, self.nparts = int(part), int(nparts)
         h = C.c_void_p()
-        flags = self.STRICT if strict else (self.MIXED if mixed else 0)
+        flags = self.MIXED if self.mixed else (self.FAST if self.fast else 0)
         if self.nparts == 1:
             _abi.check(self._lib.dgswem_cuda_create(sp, int(device), flags, C.byref(h)))
         else:
@@ -323,7 +325,7 @@ class PartitionedRun:
 
     HALO_WIDTH = (3, 10)  # doubles per element of halo kinds 0 and 1
 
-    def __init__(self, setup, nparts: int, devices=None, strict: bool = False, mixed: bool = False):
+    def __init__(self, setup, nparts: int, devices=None, strict: bool | None = None, mixed: bool = False):
         import torch
         self._torch = torch
         self.nparts = int(nparts)
@@ -424,7 +426,7 @@ class DistributedPartition:
     produce its data; every rank issues the same sequence of exchanges (one
     batched send/receive per halo kind and stage)."""
 
-    def __init__(self, setup, strict: bool = False, group=None, mixed: bool = False):
+    def __init__(self, setup, strict: bool | None = None, group=None, mixed: bool = False):
         import torch
         import torch.distributed as dist
         self._torch, self._dist, self._group = torch, dist, group
@@ -475,7 +477,7 @@ class DistributedPartition:
         self.hs.step_end()
 
 
-def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool = False,
+def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool | None = None,
              mixed: bool = False, hot_dir=None):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with
     DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  Returns the

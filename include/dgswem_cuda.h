@@ -97,19 +97,29 @@ typedef struct dgswem_cuda_setup {
 
 typedef struct dgswem_cuda dgswem_cuda;
 
-/* dgswem_cuda_create flags.  Default (0): kernels compiled with fused
- * multiply-add contraction, the fast form.  DGSWEM_CUDA_STRICT: kernels
- * compiled with -fmad=false whose every product and sum is rounded
- * separately in the reference's evaluation order (bitwise reproducible
- * against a non-contracting FP64 CPU build except through pow()). */
+/* dgswem_cuda_create flags.  Default (0): the strict kernels, compiled with
+ * -fmad=false so that every product and sum is rounded separately in the
+ * reference's evaluation order, with the Manning depth factor
+ * DEPTH**(1.D0/3.D0) correctly rounded: bit-identical to a non-contracting
+ * FP64 CPU build of the reference path with correctly rounded pow (only the
+ * hybrid friction's general pow may differ in the last bit).
+ * DGSWEM_CUDA_STRICT names the default explicitly. */
 #define DGSWEM_CUDA_STRICT 1
+/* DGSWEM_CUDA_FAST: the same kernels compiled with fused multiply-add
+ * contraction and cbrt for the Manning factor.  About 9 % faster per step;
+ * results differ from the strict form by rounding, and the slope limiter's
+ * and WETDRY's branch decisions amplify that difference at their ties
+ * (1e-9..1e-5 relative after 10 steps of a wet/dry beach).  Excludes the
+ * other flags. */
+#define DGSWEM_CUDA_FAST 4
 /* DGSWEM_CUDA_MIXED: mixed precision.  The stage kernel's edge traces,
- * numerical fluxes, boundary ghost states, volume fluxes and sources and the
- * right-hand-side sums run in FP32; the state (ZE/QX/QY modes), the SSP-RK
- * combination (so the element-mean elevation accumulates across stages in
- * FP64), the ocean depth-positivity fix, the slope limiter and WETDRY stay
- * FP64.  Results differ from the FP64 forms by the FP32 rounding of the
- * right-hand side.  Excludes DGSWEM_CUDA_STRICT. */
+ * numerical fluxes, boundary ghost states, volume fluxes and sources, the
+ * right-hand-side sums and the slope limiter's clamp and redistribution
+ * sweeps (on deviations from the element mean) run in FP32; the state
+ * (ZE/QX/QY modes), the SSP-RK combination (so the element-mean elevation
+ * accumulates across stages in FP64), the ocean depth-positivity fix, the
+ * node min/max and WETDRY stay FP64.  Results differ from the FP64 forms by
+ * the FP32 rounding.  Excludes the other flags. */
 #define DGSWEM_CUDA_MIXED 2
 
 /* Copies the setup to GPU `device` and builds the device layout.

@@ -25,8 +25,11 @@
  */
 #include "dgswem_oracle.h"
 
+#include <quadmath.h>
+
 #include <algorithm>
 #include <cctype>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -48,6 +51,34 @@ static const double BARMIN = 0.01;                // global.F:89
 static const double R_EARTH = 6378206.4;          // dgswem.F:617
 
 struct Err : std::runtime_error { using std::runtime_error::runtime_error; };
+
+// DEPTH**(1.D0/3.D0) of the Manning friction (rhs_dg_hydro.F), correctly
+// rounded.  The reference's gfortran build calls the C library's pow, whose
+// result is within 0.52 ulp of x^c (c = RN(1/3)) but not always the nearest
+// double (about 1 evaluation in 1,200 of depths in [1e-3, 1e3] is one ulp
+// off); the oracle takes the nearest double, which pins the rounding of this
+// expression independently of any math library.  Method (Ziv's strategy):
+// d = pow(x, c); its relative error e is measured in x87 extended precision
+// (64-bit significand) from d^3 = x^(3c) (1 + 3e), x^(3c) = x (1 - 2^-54 ln x);
+// the nearest of d and its two neighbours is returned unless x^c lies within
+// 2^-60 relative of a midpoint, where the quadruple-precision pow decides.
+static_assert(LDBL_MANT_DIG == 64, "x87 extended precision expected");
+static double pow_third_cr(double x) {
+  const double d = std::pow(x, 1.0 / 3.0);
+  if (!(x > 0.0) || !(d < INFINITY) || !(d > 0.0)) return d;
+  const long double D = d;
+  const long double target = (long double)x * (1.0L - 0x1p-54L * (long double)std::log(x));
+  const long double e = ((D * D * D) / target - 1.0L) / 3.0L;  // d = x^c (1 + e)
+  const double up = std::nextafter(d, INFINITY), dn = std::nextafter(d, -INFINITY);
+  // d - x^c = e x^c ~ e d; midpoints at d + (up - d)/2 and d - (d - dn)/2
+  const long double dev = e * D;
+  const long double hu = 0.5L * ((long double)up - D), hd = 0.5L * (D - (long double)dn);
+  const long double tol = D * 0x1p-60L;
+  if (std::fabs(dev + hu) <= tol || std::fabs(dev - hd) <= tol) return (double)powq((__float128)x, (__float128)(1.0 / 3.0));
+  if (dev < -hu) return up;   // x^c above the upper midpoint
+  if (dev > hd) return dn;    // x^c below the lower midpoint
+  return d;
+}
 
 // ---------------------------------------------------------------- readers --
 // Fortran list-directed input: a READ takes the next record and, if it holds
@@ -1637,7 +1668,7 @@ void Model::rhs_dg_hydro() {
       double hx = HUV * sfq, hy = HVV + GH2;
       if (LoadManningsN) {
         double nb = (ManningsN[n1] + ManningsN[n2] + ManningsN[n3]) / 3.;
-        FRIC_EL[L] = G * (nb * nb) / std::pow(depth, 1.0 / 3.0);
+        FRIC_EL[L] = G * (nb * nb) / pow_third_cr(depth);
         if (FRIC_EL[L] < CF) FRIC_EL[L] = CF;
       }
       double tau = FRIC_EL[L];
@@ -1940,6 +1971,10 @@ struct orc_model {
 };
 
 extern "C" {
+
+void orc_pow_third(const double* xs, long n, double* out) {
+  for (long i = 0; i < n; ++i) out[i] = orc::pow_third_cr(xs[i]);
+}
 
 void orc_set_threads(int n) {
 #ifdef _OPENMP

@@ -59,6 +59,10 @@ int orc_get_int_table(const orc_model* m, const char* which, int* out, int cap);
  * triangle (-1,-1),(1,-1),(-1,1), weights summing to 2), "M_INV" (dofh). */
 int orc_get_real_table(const orc_model* m, const char* which, double* out, int cap);
 
+/* The Manning depth factor DEPTH**(1.D0/3.D0) as the oracle evaluates it
+ * (correctly rounded), over xs[0..n) into out. */
+void orc_pow_third(const double* xs, long n, double* out);
+
 /* Full reference-style run writing fort.63 (elevation) to out_path. */
 int orc_run_case(const char* dir, const char* out_path, char* err, int errlen);
 

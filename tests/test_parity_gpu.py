@@ -1,14 +1,16 @@
 """CUDA hydro step vs the FP64 oracle (GPU).
 
 Two kernel variants are checked:
-* strict (-fmad=false, the oracle's evaluation order): bit-for-bit equal to
-  the oracle on every deck whose physics avoids pow() (Manning n and hybrid
-  friction call pow on the device and on the host, which may differ in the
-  last bit); those decks are held to the FP64 bar below.
-* fast (FMA contraction): modal coefficients after N steps within 1e-10
-  relative (max |gpu - oracle| / max |oracle| per variable), the FP64 bar of
-  the drop-in, wherever the slope limiter does not meet its redistribution
-  ties (see test_fast_limiter_ties); integer wet/dry flags exactly.
+* strict (the drop-in default: -fmad=false, the oracle's evaluation order,
+  the Manning factor DEPTH**(1.D0/3.D0) correctly rounded on both sides):
+  bit-for-bit equal to the oracle on every deck except those with hybrid
+  friction, whose general pow() may differ in the last bit between the device
+  and the host C library; those are held to the FP64 bar below with
+  identical wet/dry flags.
+* fast (opt-in, FMA contraction): modal coefficients after N steps within
+  1e-10 relative (max |gpu - oracle| / max |oracle| per variable) wherever the
+  slope limiter and WETDRY do not meet their branch ties (see
+  test_fast_limiter_ties); integer wet/dry flags exactly.
 """
 import numpy as np
 import pytest
@@ -36,9 +38,10 @@ def scale_floors(deck):
 
 
 def run_both(path, nsteps, it0=1, met=None, strict=False):
+    """strict=False: the fast (FMA) build; True: the strict build."""
     deck = Deck(path)
     orc = Oracle(path, threads=4)
-    hs = HydroStep(deck, strict=strict)
+    hs = HydroStep(deck, strict=bool(strict))
     if met is not None:
         hs.set_met(*met)
         orc.set_met(*met)
@@ -161,12 +164,37 @@ RTOL_FAST_WETDRY = 1e-8
 
 @pytest.mark.parametrize("strict", [True, False])
 def test_sloping_beach_wetdry_manning(built, scratch, strict):
-    """Config 2 physics on a small mesh: wet/dry, limiter, nodal Manning n."""
+    """Config 2 physics on a small mesh: wet/dry, limiter, nodal Manning n.
+    Strict: bit for bit (the Manning factor is correctly rounded on both
+    sides)."""
     path = decks.sloping_beach(scratch / "sb_par", nx=60, ny=12, lx=3000.0, ly=600.0, nsteps=400, dt=0.5)
     _, _, g, o = run_both(path, 400, strict=strict)
     print("sloping beach: relative differences", [rel_err(a, b) for a, b in zip(g[:3], o[:3])])
-    check_state(g, o, rtol=RTOL if strict else RTOL_FAST_WETDRY)
+    if strict:
+        check_bitwise(g, o)
+    else:
+        check_state(g, o, rtol=RTOL_FAST_WETDRY)
     assert 0 < g[3].sum() < len(g[3])  # both wet and dry elements present
+
+
+def test_strict_sloping_beach_200k_bitwise(built, scratch):
+    """The bench configuration's physics (wet/dry, limiter 5, nodal Manning
+    n, M2 tide) on a 200k-element beach of the same 100 x 20 km basin,
+    50 steps: the strict build bit for bit (the Morton tile plan's halos and
+    task lists at a size where tiles carry the full task and halo caps)."""
+    path = decks.sloping_beach(scratch / "sb_200k", nx=707, ny=141, nsteps=50, dt=0.5)
+    _, _, g, o = run_both(path, 50, strict=True)
+    assert 0 < g[3].sum() < len(g[3])
+    check_bitwise(g, o)
+
+
+def test_quarter_annulus_config1_full_length_bitwise(built, scratch):
+    """Config 1 in full: the 1024-element tidal quarter annulus, SSP(2,2),
+    linear friction, dt = 10 s, all 4460 steps; the strict build bit for bit
+    against the oracle."""
+    path = decks.quarter_annulus(scratch / "qa1024_full", nsteps=4460)
+    _, _, g, o = run_both(path, 4460, strict=True)
+    check_bitwise(g, o)
 
 
 def test_wind_nws1(built, scratch):
