@@ -21,6 +21,10 @@ struct Failure : std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
+// The next MET_FORCING block of an NWS = 1 fort.22 reader (deck.cpp): NP
+// records into wsx2, wsy2, pr2 (input node order); throws Failure.
+void met_read_block(dgswem_met_reader* r, double* wsx2, double* wsy2, double* pr2);
+
 template <typename F>
 int guarded(F&& body) {
   try {

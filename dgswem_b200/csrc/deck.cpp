@@ -22,6 +22,7 @@
 #include <charconv>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -1234,3 +1235,99 @@ extern "C" int dgswem_deck_merge(const dgswem_cuda_setup* const* parts, int n, d
     *out = d.release();
   });
 }
+
+// ---- NWS = 1 meteorological forcing file (fort.22) -------------------------
+// met_forcing.F:49-66: every call of MET_FORCING -- once per RK stage,
+// DG_hydro_timestep.F:104 -- reads NP records `READ(22,*) NHG, WSX2(II),
+// WSY2(II), PR2(II)`, II = 1..NP, in input node order.  Each list-directed
+// READ starts a new record and takes four values, continuing on the
+// following lines if a line holds fewer; values after the fourth on its
+// last line are skipped.  Separators are blanks, tabs and commas; a D
+// exponent (1.0D-3) reads as E.
+struct dgswem_met_reader {
+  std::FILE* f = nullptr;
+  std::string path;
+  int np = 0;
+  long line = 0;  // lines consumed
+  long calls = 0; // blocks of NP records read
+  std::vector<char> buf;
+  ~dgswem_met_reader() {
+    if (f) std::fclose(f);
+  }
+  // the next line into buf (without its end of line); false at end of file
+  bool next_line() {
+    buf.clear();
+    int c;
+    bool any = false;
+    while ((c = std::fgetc(f)) != EOF) {
+      any = true;
+      if (c == '\n') break;
+      buf.push_back((char)c);
+    }
+    if (!any) return false;
+    ++line;
+    if (!buf.empty() && buf.back() == '\r') buf.pop_back();
+    buf.push_back(0);
+    return true;
+  }
+  // one list-directed READ of four values
+  void read_record(double v[4]) {
+    int got = 0;
+    while (got < 4) {
+      if (!next_line())
+        throw dgswem::Failure(DGSWEM_ERR_IO, path + ": end of file in record block " + std::to_string(calls + 1) +
+                                                 " (NP = " + std::to_string(np) + " records per MET_FORCING call)");
+      char* p = buf.data();
+      while (got < 4) {
+        while (*p == ' ' || *p == '\t' || *p == ',') ++p;
+        if (!*p) break;
+        char* q = p;
+        while (*q && *q != ' ' && *q != '\t' && *q != ',') {
+          if (*q == 'D' || *q == 'd') *q = 'E';
+          ++q;
+        }
+        const char end = *q;
+        *q = 0;
+        char* stop = nullptr;
+        const double x = std::strtod(p, &stop);
+        if (stop == p || *stop)
+          throw dgswem::Failure(DGSWEM_ERR_IO, path + ":" + std::to_string(line) + ": not a number: " + p);
+        v[got++] = x;
+        *q = end;
+        p = q;
+      }
+    }
+  }
+};
+
+extern "C" int dgswem_met_reader_open(const char* path, int np, dgswem_met_reader** out) {
+  return dgswem::guarded([&]() {
+    if (!path || !out || np <= 0) throw dgswem::Failure(DGSWEM_ERR_ARG, "bad arguments");
+    std::unique_ptr<dgswem_met_reader> r(new dgswem_met_reader());
+    r->path = path;
+    r->np = np;
+    r->f = std::fopen(path, "rb");
+    if (!r->f) throw dgswem::Failure(DGSWEM_ERR_IO, std::string("cannot open ") + path);
+    *out = r.release();
+  });
+}
+
+void dgswem::met_read_block(dgswem_met_reader* r, double* wsx2, double* wsy2, double* pr2) {
+  if (!r || !wsx2 || !wsy2 || !pr2) throw dgswem::Failure(DGSWEM_ERR_ARG, "null argument");
+  double v[4];
+  for (int i = 0; i < r->np; ++i) {
+    r->read_record(v);  // NHG (the node number) is read and not used, as in the reference
+    wsx2[i] = v[1];
+    wsy2[i] = v[2];
+    pr2[i] = v[3];
+  }
+  ++r->calls;
+}
+
+extern "C" int dgswem_met_reader_next(dgswem_met_reader* r, double* wsx2, double* wsy2, double* pr2) {
+  return dgswem::guarded([&]() { dgswem::met_read_block(r, wsx2, wsy2, pr2); });
+}
+
+extern "C" long dgswem_met_reader_calls(const dgswem_met_reader* r) { return r ? r->calls : -1; }
+
+extern "C" void dgswem_met_reader_close(dgswem_met_reader* r) { delete r; }

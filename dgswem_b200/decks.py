@@ -179,6 +179,21 @@ def write_deck(path, x, y, dp, elems, open_segs, land_segs, ctl: Controls, emo=N
     return path
 
 
+def write_fort22(path, blocks) -> Path:
+    """fort.22 of NWS = 1 (met_forcing.F:49-66): for each MET_FORCING call
+    (one per RK stage of every step, in order) a block of NP records
+    "NHG WSX2 WSY2 PR2"; ``blocks`` yields (wsx2, wsy2, pr2) arrays of NP
+    values in input node order.  Values with 17 significant digits (exact
+    round trip)."""
+    path = Path(path)
+    with open(path, "w") as f:
+        for wsx, wsy, pr in blocks:
+            n = len(wsx)
+            _savetxt(f, np.column_stack([np.arange(1, n + 1), wsx, wsy, pr]),
+                     fmt=["%d", "%.17E", "%.17E", "%.17E"])
+    return path
+
+
 def _grid_triangles(ni: int, nj: int) -> np.ndarray:
     """Node (i, j) -> i*(nj+1) + j + 1; two CCW triangles per cell, ordered
     column by column (j fastest)."""

@@ -223,6 +223,12 @@ struct Model {
   std::vector<double> ze_edge, qx_edge, qy_edge;  // [(e*3+slot)*dofh + k]
   std::vector<int> WDFLG, NODECODE;
   std::vector<double> WSX2, WSY2, PR2, WSX_BASE, WSY_BASE, PR_BASE;
+  // NWS = 1: unit 22 (fort.22 of the deck), read at every MET_FORCING call
+  // (met_forcing.F:49-66) unless the fields are given with orc_set_met
+  std::FILE* F22 = nullptr;
+  std::string F22_path;
+  void met_read_fort22();
+  ~Model() { if (F22) std::fclose(F22); }
   // node star in element order: star[star_ptr[n] .. star_ptr[n+1])
   std::vector<int> star_ptr, star;
 
@@ -1878,6 +1884,42 @@ void Model::wetdry() {
     if (setnode[J]) for (int a = 0; a < 3; ++a) NODECODE[NM[3 * J + a]] = 1;
 }
 
+// met_forcing.F:49-66: DO II = 1,NP: READ(22,*) NHG, WSX2(II), WSY2(II),
+// PR2(II).  Each READ begins a new record and takes four values from it and,
+// if it holds fewer, from the records that follow; what remains of its last
+// record is skipped.  Blanks, tabs and commas separate values; a Fortran D
+// exponent reads as E.
+void Model::met_read_fort22() {
+  WSX_BASE.resize(NP); WSY_BASE.resize(NP); PR_BASE.resize(NP);
+  std::string line;
+  for (int II = 0; II < NP; ++II) {
+    double v[4];
+    int got = 0;
+    while (got < 4) {
+      line.clear();
+      int c;
+      bool any = false;
+      while ((c = std::fgetc(F22)) != EOF && c != '\n') { any = true; line.push_back((char)c); }
+      if (!any && c == EOF) throw Err(F22_path + ": end of file (NWS = 1 reads NP records per stage)");
+      for (char& ch : line) {
+        if (ch == 'D' || ch == 'd') ch = 'E';
+        if (ch == ',' || ch == '\t' || ch == '\r') ch = ' ';
+      }
+      std::istringstream is(line);
+      std::string tok;
+      while (got < 4 && (is >> tok)) {
+        char* e = nullptr;
+        v[got] = std::strtod(tok.c_str(), &e);
+        if (e == tok.c_str() || *e) throw Err(F22_path + ": not a number: " + tok);
+        ++got;
+      }
+    }
+    WSX_BASE[II] = v[1];
+    WSY_BASE[II] = v[2];
+    PR_BASE[II] = v[3];
+  }
+}
+
 // DG_hydro_timestep.F:24-744
 void Model::step(int IT) {
   double ITDT = IT * DTDP;
@@ -1888,6 +1930,7 @@ void Model::step(int IT) {
     if (NRAMP == 1 || NRAMP == 2)
       RAMPDG = std::tanh((2.0 * ((IT - 1) + DTVD[IRK - 1]) * DTDP / 86400.0) / DRAMP);
     if (NRAMP == 3) throw Err("NRAMP = 3 not supported");
+    if (NWS == 1 && F22) met_read_fort22();
     if (NWS == 1)
       for (int n = 0; n < NP; ++n) {
         WSX2[n] = RAMPDG * (WSX_BASE.empty() ? 0.0 : WSX_BASE[n]);
@@ -1990,6 +2033,10 @@ orc_model* orc_open(const char* dir, char* err, int errlen) {
     h->m.read_fort_dg(dir);
     h->m.read_input(dir);
     h->m.prep_dg();
+    if (h->m.NWS == 1) {
+      h->m.F22_path = std::string(dir) + "/fort.22";
+      h->m.F22 = std::fopen(h->m.F22_path.c_str(), "rb");  // optional: orc_set_met gives the fields otherwise
+    }
   } catch (std::exception& e) {
     orc::copy_err(e.what(), err, errlen);
     delete h;
@@ -2081,6 +2128,7 @@ void orc_modal2nodal(const orc_model* h, double* eta2, double* uu2, double* vv2)
 
 void orc_set_met(orc_model* h, const double* wsx, const double* wsy, const double* pr) {
   orc::Model& m = h->m;
+  if (m.F22) { std::fclose(m.F22); m.F22 = nullptr; }  // the given fields replace the deck's fort.22
   m.WSX_BASE.assign(wsx, wsx + m.NP);
   m.WSY_BASE.assign(wsy, wsy + m.NP);
   m.PR_BASE.assign(pr, pr + m.NP);
