@@ -201,6 +201,28 @@ int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* q
 int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2,
                         const double* pr2);
 
+/* NWS = 1 from a fort.22 file, as MET_FORCING reads it (src/met_forcing.F:
+ * 49-66): before every RK stage (src/DG_hydro_timestep.F:104) the handle
+ * reads the next NP records "NHG, WSX2, WSY2, PR2" (list-directed, input node
+ * order) and uploads them; the stage kernel applies the stage's RAMPDG, the
+ * reference's RampMete.  From then on these fields replace those of
+ * dgswem_cuda_set_met; a NULL path detaches the file (the last fields stay).
+ * DGSWEM_ERR_IO when the file cannot be opened, ends inside a block or holds
+ * a value that is not a number (the step that needed it reports it).  While a
+ * file is attached, dgswem_cuda_run does not use CUDA graphs (the host reads
+ * between stages) and the discrete adjoint is not available.  A partition
+ * handle reads the whole mesh's NP records and keeps its own nodes'. */
+int dgswem_cuda_met_file(dgswem_cuda* h, const char* path);
+
+/* Host reader of the same records (no device): dgswem_met_reader_next fills
+ * the next MET_FORCING block, NP values of each field in input node order;
+ * dgswem_met_reader_calls counts the blocks read. */
+typedef struct dgswem_met_reader dgswem_met_reader;
+int dgswem_met_reader_open(const char* path, int np, dgswem_met_reader** out);
+int dgswem_met_reader_next(dgswem_met_reader* r, double* wsx2, double* wsy2, double* pr2);
+long dgswem_met_reader_calls(const dgswem_met_reader* r);
+void dgswem_met_reader_close(dgswem_met_reader* r);
+
 /* modal2nodal (src/write_results.F:14-170) on the device; results copied to
  * host arrays of NP entries (any may be NULL).  nodecode: 1 where a wet
  * element touches the node (the value WETDRY leaves in NODECODE). */
@@ -208,10 +230,14 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
                             int* nodecode);
 
 /* Largest NP that dgswem_cuda_modal2nodal_noalloc accepts: its static device
- * scratch holds ETA2, UU2 and VV2 for this many nodes (24 MiB). */
+ * scratch holds ETA2, UU2 and VV2 for this many nodes (24 MiB).  The CUDA
+ * loader reserves those 24 MiB on every device where the library's device
+ * code is loaded, whether or not dgswem_cuda_modal2nodal_noalloc is ever
+ * called (every rank of a partitioned run holds them too). */
 #define DGSWEM_CUDA_NOALLOC_MAX_NODES (1 << 20)
 
-/* dgswem_cuda_modal2nodal that allocates nothing.  No counterpart in the
+/* dgswem_cuda_modal2nodal that allocates nothing, for p=1 whole-mesh handles
+ * (a p=2 or a partition handle: DGSWEM_ERR_ARG).  No counterpart in the
  * reference (its modal2nodal fills the host arrays directly).  Same kernel and
  * same results as dgswem_cuda_modal2nodal, but the nodal scratch is a static
  * device array of DGSWEM_CUDA_NOALLOC_MAX_NODES nodes instead of the handle's
@@ -223,7 +249,10 @@ int dgswem_cuda_modal2nodal(dgswem_cuda* h, double* eta2, double* uu2, double* v
  * - NP > DGSWEM_CUDA_NOALLOC_MAX_NODES: DGSWEM_ERR_ARG, nothing launched.
  * - The first call on each device looks up the scratch's device address
  *   (cudaGetSymbolAddress, which may load the library's device module); make
- *   that first call before any stream capture.
+ *   that first call before any stream capture.  The address is kept for the
+ *   life of the process: it assumes the device's primary context is not
+ *   destroyed and recreated (cudaDeviceReset) between calls.
+ * - Any of the four outputs may be NULL (that copy is skipped).
  * - Nothing in the scratch has to start at zero: the kernel writes all NP
  *   entries of each nodal array before they are copied out.
  * - All handles on one device share the one scratch array: calls that overlap
