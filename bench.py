@@ -551,6 +551,52 @@ def parity(gpu_state, oracle_state, steps: int, variant: str) -> dict:
     return out
 
 
+def partitioned_arm(deck, args, world: int, dist, device: int) -> dict:
+    """The bench mesh split into ``world`` partitions, one per rank
+    (DistributedPartition: halos by NCCL send/receive between the stage
+    kernel and the limiter and after the limiter, as the reference's MPI
+    ghost updates), strong scaling: the whole job advances one mesh.  At
+    one rank the single partition runs through the same stage / limit entry
+    points with no exchange.  Timed with CUDA events on each rank's stream,
+    the slowest rank's time."""
+    import torch
+    from dgswem_b200 import DistributedPartition
+    if world == 1 and not dist.is_initialized():
+        # a one-rank group over gloo (no exchange happens) so that the
+        # driver's group calls are defined
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+        own_group = True
+    else:
+        own_group = False
+    stream = torch.cuda.current_stream()
+    dp = DistributedPartition(deck, **variant_kwargs(args.variant), transport="nccl")
+    info = dp.hs.part_info()
+    dp.run(1, args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    k = args.partition_steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dp.run(args.warmup + 1, k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dist if world > 1 else None, "cuda")
+    dp.close()
+    if own_group:
+        dist.destroy_process_group()
+    ne = deck.s.ne
+    return {"workload": f"the bench mesh ({ne} elements) split into {world} partition(s), one per GPU",
+            "scaling": "strong", "value": DOFS_PER_ELEMENT * ne * deck.s.nrk * k / (ms / 1e3),
+            "unit": "DOF-stage/s", "steps": k, "ms_per_step": ms / k,
+            "owned_elements_rank0": int(info["owned"]), "local_elements_rank0": int(info["local"]),
+            "transport": "nccl send/receive of packed halos" if world > 1 else "none (one partition)"}
+
+
 VARIANT_TEXT = {"strict": "strict: FP64 without FMA contraction, the oracle's evaluation order (bit-identical to it)",
                 "fast": "fast: FP64 with FMA contraction"}
 
@@ -650,6 +696,8 @@ def main(argv=None):
                          "oracle) or fast (FMA contraction)")
     ap.add_argument("--other-variant-steps", type=int, default=20,
                     help="timed steps of the other FP64 build on the same deck (0: skip)")
+    ap.add_argument("--partition-steps", type=int, default=20,
+                    help="timed steps of the partitioned arm: the bench mesh split over the ranks (0: skip)")
     ap.add_argument("--cpu-steps", type=int, default=12,
                     help="oracle steps from the initial state: the cpu_baseline sample and the parity check")
     ap.add_argument("--ref-max-steps", type=int, default=40)
@@ -798,6 +846,8 @@ def main(argv=None):
     }
     if args.other_variant_steps > 0:
         line["other_variant"] = other_variant_arm(deck, stream, args, world, dist if world > 1 else None, local)
+    if args.partition_steps > 0:
+        line["partitioned"] = partitioned_arm(deck, args, world, dist, local)
     if not args.no_mixed:
         mixed = mixed_arm(deck, stream, args, world, dist if world > 1 else None, local)
         mixed["speedup_vs_fp64"] = mixed["value"] / value  # against the headline FP64 build

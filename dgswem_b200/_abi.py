@@ -59,6 +59,11 @@ SIGNATURES = {
     "dgswem_cuda_upload_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_download_state": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_set_met": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "dgswem_cuda_met_file": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "dgswem_met_reader_open": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "dgswem_met_reader_next": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "dgswem_met_reader_calls": (C.c_long, [C.c_void_p]),
+    "dgswem_met_reader_close": (None, [C.c_void_p]),
     "dgswem_cuda_modal2nodal": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_modal2nodal_noalloc": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _ip]),
     "dgswem_cuda_create_part": (C.c_int, [C.POINTER(Setup), C.c_int, C.c_int, C.c_int, C.c_int,

@@ -98,4 +98,21 @@ DGSWEM_HD double pow_third(double x) {
   return ldexp(z + tail, q);
 }
 
+// x / 3, correctly rounded, without a division: q = RN(x t), t = RN(1/3);
+// r = x - 3q is exact (q is within 1 ulp of x/3, so r is a multiple of
+// ulp(q) no larger than 3 ulp(q)) and fma(r, t, q) = RN(q + r t) is within
+// 2^-53 ulp of x/3.  The exact quotient x/3 = M 2^e / 3 lies at least 1/6
+// ulp from every midpoint between doubles (its remainder in ulps is a
+// multiple of 1/3), so that rounding is the correctly rounded x/3 -- the IEEE
+// division's result -- for every finite x.  The sign is x's (a zero quotient
+// keeps the sign of x, as the division's does, which the sequence alone
+// would lose: fma(+0, t, -0) = +0).  Four instructions instead of a division
+// sequence.
+DGSWEM_HD double div3(double x) {
+  const double t = 1.0 / 3.0;
+  const double q = x * t;
+  const double r = fma(-q, 3.0, x);
+  return copysign(fma(r, t, q), x);
+}
+
 }  // namespace dgswem

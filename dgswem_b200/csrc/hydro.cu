@@ -414,6 +414,15 @@ struct dgswem_cuda {
   // that differ only in the pinned buffer their first node copies the
   // chunk's stage forcing and ramps from, so that the host fills one while
   // the other runs
+  // fort.22 of NWS = 1 read by the handle before every RK stage
+  // (dgswem_cuda_met_file): the reader, one block in input node order, and
+  // two pinned blocks in device node order, each free again once its event
+  // has completed
+  dgswem_met_reader* met = nullptr;
+  std::vector<double> met_in;
+  double* met_pin[2] = {nullptr, nullptr};
+  cudaEvent_t met_done[2] = {nullptr, nullptr};
+  int met_next = 0;
   int graph_steps = 0, graph_next = 0;
   bool graph_ready = false;
   cudaGraph_t graph[2] = {nullptr, nullptr};
@@ -1145,6 +1154,32 @@ void launch_limit(dgswem_cuda* h, int irk) {
 
 // Steps it0 .. it0+n-1: the host forcing of each chunk of steps is computed
 // into pinned memory and copied with one transfer ahead of its kernels.
+// MET_FORCING of NWS = 1 from the attached fort.22 (met_forcing.F:49-66):
+// the next NP records, in the device node order, copied to the nodal fields
+// the next stage kernel reads (stream-ordered after the previous stage's
+// kernels); the stage kernel applies RAMPDG.
+void met_stage(dgswem_cuda* h) {
+  const int np = h->np, ng = h->np_glob;
+  const int b = h->met_next;
+  DG_CUDA(cudaEventSynchronize(h->met_done[b]));  // pinned block b free again
+  h->met_in.resize(3 * (size_t)ng);
+  double* in = h->met_in.data();
+  met_read_block(h->met, in, in + ng, in + 2 * (size_t)ng);
+  double* o = h->met_pin[b];
+  for (int i = 0; i < np; ++i) {
+    const int n = h->node_perm_h[i];
+    o[i] = in[n];
+    o[(size_t)np + i] = in[(size_t)ng + n];
+    o[(size_t)2 * np + i] = in[(size_t)2 * ng + n];
+  }
+  const size_t bytes = (size_t)np * sizeof(double);
+  DG_CUDA(cudaMemcpyAsync(h->wsx.p, o, bytes, cudaMemcpyHostToDevice, h->stream));
+  DG_CUDA(cudaMemcpyAsync(h->wsy.p, o + np, bytes, cudaMemcpyHostToDevice, h->stream));
+  DG_CUDA(cudaMemcpyAsync(h->pr.p, o + 2 * (size_t)np, bytes, cudaMemcpyHostToDevice, h->stream));
+  DG_CUDA(cudaEventRecord(h->met_done[b], h->stream));
+  h->met_next = b ^ 1;
+}
+
 void launch_stage(dgswem_cuda* h, int it, int irk, const double* forcing) {
   if (h->keep_wd)
     DG_CUDA(cudaMemcpyAsync(h->keep_wd[irk - 1], h->wd.p, (size_t)h->ne * sizeof(int), cudaMemcpyDeviceToDevice,
@@ -1235,7 +1270,7 @@ void graph_capture(dgswem_cuda* h) {
 // returns the steps done.
 int run_steps_graph(dgswem_cuda* h, int it0, int n) {
   const int m = h->graph_steps, nrk = h->nrk;
-  if (m < 2 || h->prof_on || n < m) return 0;
+  if (m < 2 || h->prof_on || n < m || h->met) return 0;
   if (!h->graph_ready) graph_capture(h);
   if (h->q[0].p != h->graph_q0) {  // the state sits in the other buffer: move it where the graphs read it
     DG_CUDA(cudaMemcpyAsync(h->q[nrk].p, h->q[0].p, 3 * (size_t)h->dofh * h->ne * sizeof(double),
@@ -1277,8 +1312,10 @@ void run_steps(dgswem_cuda* h, int it0, int n) {
     }
     for (int i = 0; i < m; ++i) {
       const int it = it0 + done + i;
-      for (int irk = 1; irk <= nrk; ++irk)
+      for (int irk = 1; irk <= nrk; ++irk) {
+        if (h->met) met_stage(h);
         launch_stage(h, it, irk, dev ? dev + ((size_t)i * nrk + (irk - 1)) * h->forcing_per_stage : nullptr);
+      }
       std::swap(h->q[0], h->q[nrk]);  // stage NRK+1 becomes stage 1
     }
     done += m;
@@ -1294,14 +1331,16 @@ static __device__ __align__(256) double g_nodal_scratch[3 * kScratchNodes];
 
 // Device address of g_nodal_scratch on `device` (the current device), looked
 // up once per device ordinal under a lock; fixed-size table, no allocation.
+// Kept for the life of the process (the primary context is assumed not to be
+// reset between calls).
 constexpr int kMaxScratchDevices = 64;
 std::mutex g_scratch_lock;
 double* g_scratch_addr[kMaxScratchDevices] = {};
 
 double* nodal_scratch(int device) {
   if (device < 0 || device >= kMaxScratchDevices)
-    throw Failure(DGSWEM_ERR_ARG, "modal2nodal_noalloc: device ordinal " + std::to_string(device) + " >= " +
-                                      std::to_string(kMaxScratchDevices));
+    throw Failure(DGSWEM_ERR_ARG, "modal2nodal_noalloc: device ordinal " + std::to_string(device) +
+                                      " outside [0, " + std::to_string(kMaxScratchDevices) + ")");
   std::lock_guard<std::mutex> guard(g_scratch_lock);
   if (!g_scratch_addr[device]) {
     void* p = nullptr;
@@ -1328,6 +1367,7 @@ void adjoint_prepare(dgswem_cuda* h) {
   if (h->nfeds > 0 || h->nreds > 0 || h->mesh.nebseg > 0 || h->mesh.nibseg > 0)
     no("flow, radiation or barrier boundaries");
   if (h->ph.iflinbf == 0 && h->ph.ifhybf == 1) no("hybrid friction");
+  if (h->met) no("a fort.22 met file (give the fields with dgswem_cuda_set_met)");
   const size_t n9 = 9 * (size_t)h->ne;
   if (h->adj_lam.size() != (size_t)h->nrk + 1) {
     h->adj_lam.clear();
@@ -1646,6 +1686,11 @@ void dgswem_cuda_destroy(dgswem_cuda* h) {
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   if (h->forcing_copied) cudaEventDestroy(h->forcing_copied);
   if (h->forcing_host) cudaFreeHost(h->forcing_host);
+  if (h->met) dgswem_met_reader_close(h->met);
+  for (int b = 0; b < 2; ++b) {
+    if (h->met_done[b]) cudaEventDestroy(h->met_done[b]);
+    if (h->met_pin[b]) cudaFreeHost(h->met_pin[b]);
+  }
   graph_release(h);
   for (int b = 0; b < 2; ++b) {
     if (h->gdone[b]) cudaEventDestroy(h->gdone[b]);
@@ -1746,6 +1791,31 @@ int dgswem_cuda_download_state(dgswem_cuda* h, double* ze, double* qx, double* q
   });
 }
 
+int dgswem_cuda_met_file(dgswem_cuda* h, const char* path) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    if (h->nws != 1) throw Failure(DGSWEM_ERR_ARG, "a fort.22 met file needs NWS = 1");
+    need_p1(h, "dgswem_cuda_met_file");
+    DG_CUDA(cudaSetDevice(h->device));
+    if (h->met) {
+      dgswem_met_reader_close(h->met);
+      h->met = nullptr;
+    }
+    if (!path) return;
+    dgswem_met_reader* r = nullptr;
+    const int rc = dgswem_met_reader_open(path, h->np_glob, &r);
+    if (rc != DGSWEM_OK) throw Failure(rc, std::string("fort.22: cannot open ") + path);
+    h->met = r;
+    for (int b = 0; b < 2; ++b) {
+      if (!h->met_pin[b]) DG_CUDA(cudaMallocHost(&h->met_pin[b], 3 * (size_t)h->np * sizeof(double)));
+      if (!h->met_done[b]) {
+        DG_CUDA(cudaEventCreateWithFlags(&h->met_done[b], cudaEventDisableTiming));
+        DG_CUDA(cudaEventRecord(h->met_done[b], h->stream));
+      }
+    }
+  });
+}
+
 int dgswem_cuda_set_met(dgswem_cuda* h, const double* wsx2, const double* wsy2, const double* pr2) {
   return guarded([&]() {
     if (!h || !wsx2 || !wsy2 || !pr2) throw Failure(DGSWEM_ERR_ARG, "null argument");
@@ -1835,6 +1905,7 @@ int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) {
       DG_CUDA(cudaEventRecord(h->forcing_copied, h->stream));
       dev = h->forcing_dev.p;
     }
+    if (h->met) met_stage(h);
     launch_stage_rhs(h, it, irk, dev);
   });
 }

@@ -173,7 +173,7 @@ constexpr unsigned kQStride = 14;
 // that is conflict-free for 8 consecutive slots
 constexpr unsigned kQfStride = 12;
 struct StageLayout {
-  unsigned qs, geo, qf, vol, res, wd, gid, tdry, info, bytes;
+  unsigned qs, geo, qf, vol, res, wd, gid, tdry, info, tasks, bytes;
 };
 __host__ __device__ inline unsigned align16(unsigned x) { return (x + 15u) & ~15u; }
 // tile: elements per tile of the shape; rb: bytes of the arithmetic type of
@@ -195,7 +195,8 @@ __host__ __device__ inline StageLayout stage_layout(int tile, int max_halo, int 
   L.gid = align16(L.wd + S * 4u);              // wd[S]
   L.tdry = align16(L.gid + (unsigned)max_halo * 4u);
   L.info = align16(L.tdry + T * 4u);          // einfo, eslot of the tile's elements
-  L.bytes = align16(L.info + 2u * nt * 4u);
+  L.tasks = align16(L.info + 2u * nt * 4u);    // the tile's edge-task words (uint2)
+  L.bytes = align16(L.tasks + T * 8u);
   return L;
 }
 

@@ -552,21 +552,22 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisT<re
   for (int r = 0; r < 8; ++r) vol[(r * 3 + I) * kTile + el] = v[r];
 }
 
-// Phase 4 of the stage kernel for variable V of tile element el (global id
-// e): the right-hand side of the variable's three modes summed in the
+// Phase 4 of the stage kernel for mode K of tile element el (global id e):
+// the right-hand side of mode K of the three variables, each summed in the
 // reference's order -- boundary edges, interior edges in edge-number order
 // (the slot sum of add_internal_flux), rain, area points -- then the SSP
-// combination (DG_hydro_timestep.F:238-290) written to qout.  B is the
-// shared-memory copy of the basis (runtime-indexed tables), cBasisR the
-// constant-memory one (indices fixed by unrolled loops); V is the same for a
-// whole warp.  The sums are in the arithmetic type, the SSP combination in
-// FP64 (in the mixed variant: the RHS rounded to FP32, the stage states and
-// their combination FP64).
+// combination (DG_hydro_timestep.F:238-290) written to qout.  The edge and
+// area-point weights of mode K are formed once for the three variables.  B
+// is the shared-memory copy of the basis (runtime-indexed tables), cBasisR
+// the constant-memory one (K is the same for a whole warp, the point
+// indices are fixed by unrolled loops).  The sums are in the arithmetic
+// type, the SSP combination in FP64 (in the mixed variant: the RHS rounded
+// to FP32, the stage states and their combination FP64).
 template <bool kNonlin, int kTile>
-__device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisT<real>& B, const double* qs,
-                                             const real* geo, const real* vol, const real* res,
-                                             const int* tdry, const unsigned* sinfo, const int* wds, int tbeg,
-                                             int V, int el, int e) {
+__device__ __forceinline__ void sum_mode(const StageArgs& A, const BasisT<real>& B, const double* qs,
+                                         const real* geo, const real* vol, const real* res, const int* tdry,
+                                         const unsigned* sinfo, const int* wds, const uint2* stasks, int K, int el,
+                                         int e) {
   const BasisT<real>& C = cBasisR;
   const MeshView& m = A.m;
   const Physics& P = A.ph;
@@ -577,10 +578,10 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisT<re
   double h0q[3] = {0.0, 0.0, 0.0}, h0r[3] = {0.0, 0.0, 0.0};
   if (hist0) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const size_t c = (size_t)(3 * V + k) * ne + e;
-      if (A.a[0] != 0.0) h0q[k] = A.qhist[0][c];
-      if (A.b[0] != 0.0) h0r[k] = A.rhist[0][c];
+    for (int V = 0; V < 3; ++V) {
+      const size_t c = (size_t)(3 * V + K) * ne + e;
+      if (A.a[0] != 0.0) h0q[V] = A.qhist[0][c];
+      if (A.b[0] != 0.0) h0r[V] = A.rhist[0][c];
     }
   }
   const unsigned info = sinfo[el], slots = sinfo[kTile + el];
@@ -594,97 +595,89 @@ __device__ __forceinline__ void sum_variable(const StageArgs& A, const BasisT<re
     const int ti = (slots >> (10 * l)) & kNoTask;
     const real* r = res + (size_t)ti * 15;
     if (kind == kIBarrier) {
-      const double* o = A.ib_rhs + (size_t)m.tile_tasks[tbeg + ti].y * 9;
+      const double* o = A.ib_rhs + (size_t)stasks[ti].y * 9;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + (real)o[3 * V + k];
+      for (int V = 0; V < 3; ++V) rhs[V] = rhs[V] + (real)o[3 * V + K];
       continue;
     }
     if (kind == kInterior) {
       if (tdry[ti]) continue;
       const bool is_in = ei_flag(info, l) != 0;
-      const int comp = V == 0 ? 0 : (is_in ? V : V + 2);
+      const int c1 = is_in ? 1 : 3;  // G and H of this side: components c1, c1 + 1
       const real edfac = geo[(EGeo::kEdfac + l) * kTile + el];
       real acc[3] = {0, 0, 0};
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
         const int j = is_in ? I : 2 - I;
-        const real val = r[5 * I + comp];
+        const real wk = edfac * B.edgeq[l][j][K];
+        const real* rv = r + 5 * I;
+        const real val[3] = {rv[0], rv[c1], rv[c1 + 1]};
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const real wk = edfac * B.edgeq[l][j][k];
+        for (int V = 0; V < 3; ++V) {
           if (is_in)  // rhs_*_in(k) = rhs_*_in(k) - w_in * flux
-            acc[k] = acc[k] - wk * val;
+            acc[V] = acc[V] - wk * val[V];
           else        // rhs_*_ex(k) = rhs_*_ex(k) + w_ex * flux
-            acc[k] = acc[k] + wk * val;
+            acc[V] = acc[V] + wk * val[V];
         }
       }
 #pragma unroll
-      for (int k = 0; k < 3; ++k) isum[k] = isum[k] + acc[k];
+      for (int V = 0; V < 3; ++V) isum[V] = isum[V] + acc[V];
     } else {
       if (wde == 0) continue;
       const real areas = egeo_r(m)[(size_t)EGeo::kAreas * ne + e];
       const real xlen = egeo_r(m)[(size_t)(EGeo::kXlen + l) * ne + e];
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
-        const real val = r[5 * I + V];
+        const real wk = real(2) * C.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * C.wegp[I];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const real wk = real(2) * C.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * C.wegp[I];
-          rhs[k] = rhs[k] - wk * val;
-        }
+        for (int V = 0; V < 3; ++V) rhs[V] = rhs[V] - wk * r[5 * I + V];
       }
     }
   }
 #pragma unroll
-  for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + isum[k];  // add_internal_flux
-  if (V == 0 && P.rainfall == 1) {
+  for (int V = 0; V < 3; ++V) rhs[V] = rhs[V] + isum[V];  // add_internal_flux
+  if (P.rainfall == 1) {
     const real src = real(7.0556e-6);
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) rhs[k] = rhs[k] + C.srfac[k][i] * src;
+    for (int i = 0; i < 3; ++i) rhs[0] = rhs[0] + C.srfac[K][i] * src;
   }
   if (wde != 0) {
     const real drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
     const real drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
-    // flux pair of this variable: (fx, fy), (gx, gy) or (hx, hy); source sx / sy
-    const real* vx = vol + (2 * V) * 3 * kTile + el;
-    const real* vy = vx + 3 * kTile;
-    const real* vs = vol + (V == 2 ? 7 : 6) * 3 * kTile + el;
+    // vol rows: fx fy gx gy hx hy sx sy, each [point][tile]
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      const real a = vx[i * kTile], b = vy[i * kTile];
-      if (V != 0) {
-        const real sr0 = C.srfac[0][i];
-        rhs[0] = rhs[0] + sr0 * vs[i * kTile];
-      }
-#pragma unroll
-      for (int k = 1; k < 3; ++k) {
-        const real dpx = C.drphi[k][i] * drdx + C.dsphi[k][i] * dsdx;
-        const real dpy = C.drphi[k][i] * drdy + C.dsphi[k][i] * dsdy;
-        const real xf = C.mw[k][i] * dpx;
-        const real yf = C.mw[k][i] * dpy;
-        if (V == 0) {
-          rhs[k] = rhs[k] + xf * a + yf * b;
-        } else {
-          const real sr = C.srfac[k][i];
-          rhs[k] = rhs[k] + xf * a + yf * b + sr * vs[i * kTile];
-        }
+      const real sr = C.srfac[K][i];
+      const real sx = vol[(6 * 3 + i) * kTile + el], sy = vol[(7 * 3 + i) * kTile + el];
+      if (K == 0) {
+        rhs[1] = rhs[1] + sr * sx;
+        rhs[2] = rhs[2] + sr * sy;
+      } else {
+        const real dpx = C.drphi[K][i] * drdx + C.dsphi[K][i] * dsdx;
+        const real dpy = C.drphi[K][i] * drdy + C.dsphi[K][i] * dsdy;
+        const real xf = C.mw[K][i] * dpx;
+        const real yf = C.mw[K][i] * dpy;
+        const real fx = vol[(0 * 3 + i) * kTile + el], fy = vol[(1 * 3 + i) * kTile + el];
+        const real gx = vol[(2 * 3 + i) * kTile + el], gy = vol[(3 * 3 + i) * kTile + el];
+        const real hx = vol[(4 * 3 + i) * kTile + el], hy = vol[(5 * 3 + i) * kTile + el];
+        rhs[0] = rhs[0] + xf * fx + yf * fy;
+        rhs[1] = rhs[1] + xf * gx + yf * gy + sr * sx;
+        rhs[2] = rhs[2] + xf * hx + yf * hy + sr * sy;
       }
     }
   }
   // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
   bool bad = false;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const int c = 3 * V + k;
-    const double rk = (double)rhs[k];
+  for (int V = 0; V < 3; ++V) {
+    const int c = 3 * V + K;
+    const double rk = (double)rhs[V];
     if (A.rout) A.rout[(size_t)c * ne + e] = rk;
     const double qc = qs[el * kQStride + c];
     double acc = 0.0;
     if (hist0) {
-      if (A.a[0] != 0.0) acc = acc + A.a[0] * h0q[k];
-      if (A.b[0] != 0.0) acc = acc + A.b[0] * h0r[k];
+      if (A.a[0] != 0.0) acc = acc + A.a[0] * h0q[V];
+      if (A.b[0] != 0.0) acc = acc + A.b[0] * h0r[V];
     }
     for (int I = 1; I < A.irk; ++I) {
       const bool cur = I == A.irk - 1;
@@ -730,6 +723,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   int* gid = reinterpret_cast<int*>(smem_raw + L.gid);
   int* tdry = reinterpret_cast<int*>(smem_raw + L.tdry);
   unsigned* sinfo = reinterpret_cast<unsigned*>(smem_raw + L.info);  // [einfo | eslot][kTile]
+  uint2* stasks = reinterpret_cast<uint2*>(smem_raw + L.tasks);      // the tile's edge-task words
   {
     const real* src = reinterpret_cast<const real*>(&cBasisR);
     real* dst = reinterpret_cast<real*>(&B);
@@ -786,6 +780,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
             cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
         }
       }
+      for (int j = u; j < ntask; j += kU) cp_async8(stasks + j, m.tile_tasks + tbeg + j);
       for (int j = u; j < nh; j += kU) {
         const int g = m.tile_halo[hbeg + j];
         gid[j] = g;
@@ -855,6 +850,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
           cp_async4(sinfo + (r - 1) * kTile + w, (r == 1 ? m.einfo : m.eslot) + tile0 + w);
       }
     }
+    for (int j = tid; j < ntask; j += kStageThreads) cp_async8(stasks + j, m.tile_tasks + tbeg + j);
     for (int j = tid; j < nh; j += kStageThreads) {
       const int g = j == tid ? hg : m.tile_halo[hbeg + j];
       if (j != tid) gid[j] = g;
@@ -891,7 +887,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   // (the three points of a task on adjacent lanes: same slots, broadcast loads)
   for (int w = tid; w < 3 * ntask; w += kStageThreads) {
     const int ti = w / 3, I = w - 3 * ti;
-    const uint2 tk = m.tile_tasks[tbeg + ti];
+    const uint2 tk = stasks[ti];
     const unsigned fl = tk.x;
     const unsigned kind = fl & 7u;
     if (kind == kIBarrier) continue;  // ibarrier_sides, launched before this kernel
@@ -983,11 +979,11 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   }
   __syncthreads();
 
-  // ---- phase 4: per (element, variable) sums in the reference's order, SSP ----
+  // ---- phase 4: per (element, mode) sums in the reference's order, SSP ----
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
-    const int var = w / kTile, el = w - var * kTile;
+    const int K = w / kTile, el = w - K * kTile;
     if (el >= n) continue;
-    sum_variable<kNonlin, kTile>(A, B, qs, geo, vol, res, tdry, sinfo, wds, tbeg, var, el, tile0 + el);
+    sum_mode<kNonlin, kTile>(A, B, qs, geo, vol, res, tdry, sinfo, wds, stasks, K, el, tile0 + el);
   }
 }
 
@@ -1019,13 +1015,18 @@ __device__ __forceinline__ double2 node_bounds(const double* minmax, int np, int
   return reinterpret_cast<const double2*>(minmax)[(size_t)var * np + nd];
 }
 
+// x / 3 in the arithmetic type: the correctly rounded FP64 quotient without
+// a division (div3, cr_math.cuh), the FP32 division in the mixed variant
+__device__ __forceinline__ double third_of(double x) { return div3(x); }
+__device__ __forceinline__ float third_of(float x) { return x / 3.0f; }
+
 // x / d for the redistribution divisor d = max(1, kdp) in {1, 2, 3}: x / 1
 // and x / 2 are exact scalings (x * 0.5 is the same correctly rounded value
-// as x / 2), only d = 3 needs a division.
+// as x / 2), x / 3 the correctly rounded quotient.
 __device__ __forceinline__ real div_count(real x, int kdp) {
   if (kdp <= 1) return x;
   if (kdp == 2) return x * real(0.5);
-  return x / real(3);
+  return third_of(x);
 }
 
 // slopelimiter.F:3434-3779 (vertex clamp + 3 redistribution sweeps) followed
@@ -1082,7 +1083,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
 #endif
 #pragma unroll
       for (int sweep = 0; sweep < 3; ++sweep) {
-        const real sumloc = (vx[0] + vx[1] + vx[2]) / real(3);
+        const real sumloc = third_of(vx[0] + vx[1] + vx[2]);
         real sumdif = (sumloc - z0) * real(3);
         const real signdif = copysign(real(1), sumdif);
         real dif[3];
@@ -1146,16 +1147,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
           check = true;
         }
       } else {  // case 3B: move water to the dry vertices, momentum to the wet ones
-        int l2h[3] = {0, 1, 2};
-#pragma unroll
-        for (int k1 = 0; k1 < 3; ++k1)
-#pragma unroll
-          for (int k2 = k1; k2 < 3; ++k2)
-            if (ht[l2h[k1]] > ht[l2h[k2]]) { const int t = l2h[k1]; l2h[k1] = l2h[k2]; l2h[k2] = t; }
+        // vertices shallow -> deep: the reference's exchange sort of the
+        // index list (pairs (1,2), (1,3), (2,3) in that order, swapping when
+        // the first depth is larger), held as (depth, vertex) registers
+        double s0 = ht[0], s1 = ht[1], s2 = ht[2];
+        int j0 = 0, j1 = 1, j2 = 2;
+        if (s0 > s1) { const double t = s0; s0 = s1; s1 = t; const int u = j0; j0 = j1; j1 = u; }
+        if (s0 > s2) { const double t = s0; s0 = s2; s2 = t; const int u = j0; j0 = j2; j2 = u; }
+        if (s1 > s2) { const double t = s1; s1 = s2; s2 = t; const int u = j1; j1 = j2; j2 = u; }
+        const double d0 = fmax(H0, s0) - s0;
+        const double d1 = fmax(H0, s1 - 0.5 * d0) - s1;
+        const double d2 = -d0 - d1;
         double dh[3];
-        dh[l2h[0]] = fmax(H0, ht[l2h[0]]) - ht[l2h[0]];
-        dh[l2h[1]] = fmax(H0, ht[l2h[1]] - 0.5 * dh[l2h[0]]) - ht[l2h[1]];
-        dh[l2h[2]] = -dh[l2h[0]] - dh[l2h[1]];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) dh[v] = j0 == v ? d0 : (j1 == v ? d1 : d2);
         int nd2 = 0;
         double qxs = 0.0, qys = 0.0, hmax2 = 0.0, hh[3], qxn[3], qyn[3];
 #pragma unroll
@@ -1170,8 +1175,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
 #pragma unroll
           for (int c = 3; c < 9; ++c) q[c] = 0.0;
         } else {
-          qxs = qxs / (3.0 - (double)nd2);
-          qys = qys / (3.0 - (double)nd2);
+          // / (3 - nd2), nd2 in {0, 1, 2}: by 3 correctly rounded, by 2 and 1 exact
+          qxs = nd2 == 0 ? div3(qxs) : nd2 == 1 ? qxs * 0.5 : qxs;
+          qys = nd2 == 0 ? div3(qys) : nd2 == 1 ? qys * 0.5 : qys;
           double qxh[3], qyh[3];
 #pragma unroll
           for (int v = 0; v < 3; ++v) {
@@ -1194,7 +1200,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
       }
     }
     if (check) {
-      if (zh[hmax_i] > (-dpe_min + H0)) {
+      const double zmax = hmax_i == 0 ? zh[0] : (hmax_i == 1 ? zh[1] : zh[2]);
+      if (zmax > (-dpe_min + H0)) {
         wd = 1;
       } else {
 #pragma unroll

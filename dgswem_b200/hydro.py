@@ -88,6 +88,42 @@ class Deck:
         return np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0)
 
 
+class MetReader:
+    """Host reader of an NWS = 1 fort.22 (dgswem_met_reader): each ``next()``
+    is one MET_FORCING call's NP records (wsx2, wsy2, pr2) in input node
+    order (met_forcing.F:49-66)."""
+
+    def __init__(self, path, np_: int):
+        self._lib = _abi.load()
+        self.np = int(np_)
+        h = C.c_void_p()
+        _abi.check(self._lib.dgswem_met_reader_open(str(path).encode(), self.np, C.byref(h)))
+        self._h = h
+
+    def next(self):
+        w = [np.empty(self.np) for _ in range(3)]
+        _abi.check(self._lib.dgswem_met_reader_next(self._h, *[_dptr(a) for a in w]))
+        return tuple(w)
+
+    @property
+    def calls(self) -> int:
+        return int(self._lib.dgswem_met_reader_calls(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.dgswem_met_reader_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class HydroStep:
     """Device-resident DG hydro time step on one GPU (the drop-in for
     DG_HYDRO_TIMESTEP).  ``setup`` is a ``Deck`` or a pointer to a filled
@@ -287,6 +323,11 @@ class HydroStep:
     def halo_unpack(self, kind: int, peer: int, irk: int, dev_ptr: int) -> None:
         _abi.check(self._lib.dgswem_cuda_halo_unpack(self._h, int(kind), int(peer), int(irk), C.c_void_p(dev_ptr)))
 
+    def met_file(self, path) -> None:
+        """dgswem_cuda_met_file: read NWS = 1 fields from fort.22 before every
+        RK stage, as MET_FORCING does (None detaches the file)."""
+        _abi.check(self._lib.dgswem_cuda_met_file(self._h, None if path is None else str(path).encode()))
+
     def set_met(self, wsx2, wsy2, pr2) -> None:
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (wsx2, wsy2, pr2)]
         _abi.check(self._lib.dgswem_cuda_set_met(self._h, *[_dptr(v) for v in a]))
@@ -417,25 +458,41 @@ class PartitionedRun:
 
 
 class DistributedPartition:
-    """One partition per process and GPU (torch.distributed with NCCL): rank
-    r steps partition r of the group and moves its halos with NCCL
-    send/receive of the packed buffers that ``PartitionedRun`` moves by
-    device copies -- the reference's MPI ghost updates (messenger_elem.F)
-    over NVLink.  The handle launches on torch's current stream, so each
-    pack, transfer and unpack is stream-ordered after the kernels that
-    produce its data; every rank issues the same sequence of exchanges (one
-    batched send/receive per halo kind and stage)."""
+    """One partition per process (torch.distributed): rank r steps partition
+    r of the group and moves its halos -- the reference's MPI ghost updates
+    (messenger_elem.F:832-980, after the SSP update and after the limiter /
+    WETDRY, DG_hydro_timestep.F:493-514, 555-579) -- as the packed buffers
+    that ``PartitionedRun`` moves by device copies.
 
-    def __init__(self, setup, strict: bool | None = None, group=None, mixed: bool = False):
+    transport="nccl": the device buffers go by NCCL send/receive (one GPU
+    per rank, over NVLink); the handle launches on torch's current stream,
+    so every pack, transfer and unpack is stream-ordered after the kernels
+    that produce its data.  transport="host": the packed buffers are copied
+    to pinned host buffers and moved with the group's backend (gloo) --
+    for ranks that share a GPU or have no NCCL; each exchange synchronises
+    the stream before sending.  Every rank issues the same sequence of
+    exchanges (one per halo kind and stage); no kernel waits on another
+    rank."""
+
+    TRANSPORTS = ("nccl", "host")
+
+    def __init__(self, setup, strict: bool | None = None, group=None, mixed: bool = False,
+                 transport: str = "nccl"):
         import torch
         import torch.distributed as dist
+        if transport not in self.TRANSPORTS:
+            raise ValueError(f"transport must be one of {self.TRANSPORTS}")
         self._torch, self._dist, self._group = torch, dist, group
+        self.transport = transport
         self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
         dev = torch.cuda.current_device()
         self.hs = HydroStep(setup, device=dev, strict=strict, part=self.rank, nparts=self.world, mixed=mixed)
         self.hs.set_stream(torch.cuda.current_stream().cuda_stream)
         self.nrk, self.slopeflag = self.hs.nrk, self.hs.slopeflag
-        self.buf = {}  # (kind, peer) -> (send buffer, receive buffer, nsend, nrecv)
+        self.ne = self.hs.ne
+        # (kind, peer) -> (device send, device receive, nsend, nrecv, host send, host receive)
+        self.buf = {}
+        host = transport == "host"
         for kind in (0, 1):
             w = PartitionedRun.HALO_WIDTH[kind]
             for q in range(self.world):
@@ -443,28 +500,55 @@ class DistributedPartition:
                     continue
                 ns, nr = self.hs.halo_count(kind, q)
                 if ns or nr:
-                    self.buf[(kind, q)] = (torch.empty(max(ns, 1) * w, dtype=torch.float64, device=dev),
-                                           torch.empty(max(nr, 1) * w, dtype=torch.float64, device=dev), ns, nr)
+                    mk = lambda n, pin=False: torch.empty(max(n, 1) * w, dtype=torch.float64,  # noqa: E731
+                                                          **({"pin_memory": True} if pin else {"device": dev}))
+                    self.buf[(kind, q)] = (mk(ns), mk(nr), ns, nr, mk(ns, True) if host else None,
+                                           mk(nr, True) if host else None)
 
     def close(self):
         self.hs.close()
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def _exchange(self, kind: int, irk: int) -> None:
         dist = self._dist
-        ops = []
-        for (k, q), (snd, rcv, ns, nr) in self.buf.items():
-            if k != kind:
-                continue
+        bufs = [(q, b) for (k, q), b in sorted(self.buf.items()) if k == kind]
+        for q, (snd, _, ns, _, _, _) in bufs:
             if ns:
                 self.hs.halo_pack(kind, q, irk, snd.data_ptr())
-                ops.append(dist.P2POp(dist.isend, snd, q, self._group))
-            if nr:
-                ops.append(dist.P2POp(dist.irecv, rcv, q, self._group))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
+        if self.transport == "nccl":
+            ops = []
+            for q, (snd, rcv, ns, nr, _, _) in bufs:
+                if ns:
+                    ops.append(dist.P2POp(dist.isend, snd, q, self._group))
+                if nr:
+                    ops.append(dist.P2POp(dist.irecv, rcv, q, self._group))
+            if ops:
+                for req in dist.batch_isend_irecv(ops):
+                    req.wait()
+        else:
+            stream = self._torch.cuda.current_stream()
+            for q, (snd, _, ns, _, hsnd, _) in bufs:
+                if ns:
+                    hsnd.copy_(snd, non_blocking=True)
+            stream.synchronize()
+            reqs = []
+            for q, (_, _, ns, nr, hsnd, hrcv) in bufs:
+                if ns:
+                    reqs.append(dist.isend(hsnd, q, self._group))
+                if nr:
+                    reqs.append(dist.irecv(hrcv, q, self._group))
+            for req in reqs:
                 req.wait()
-        for (k, q), (_, rcv, _, nr) in self.buf.items():
-            if k == kind and nr:
+            for q, (_, rcv, _, nr, _, hrcv) in bufs:
+                if nr:
+                    rcv.copy_(hrcv, non_blocking=True)
+        for q, (_, rcv, _, nr, _, _) in bufs:
+            if nr:
                 self.hs.halo_unpack(kind, q, irk, rcv.data_ptr())
 
     def timestep(self, it: int) -> None:
@@ -476,11 +560,22 @@ class DistributedPartition:
             self._exchange(1, irk)
         self.hs.step_end()
 
+    def run(self, it0: int, nsteps: int) -> None:
+        for it in range(it0, it0 + nsteps):
+            self.timestep(it)
+
+    def owned_state(self):
+        """(ze, qx, qy, wdflg) in input numbering: this rank's owned
+        elements' rows, the others NaN / -1."""
+        return self.hs.state()
+
 
 def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict: bool | None = None,
              mixed: bool = False, hot_dir=None):
     """Run a deck like the reference program (dgswem.F:341-373 time loop with
-    DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  Returns the
+    DG_TIMESTEP and the fort.63 block of write_results.F:445-500).  NWS = 1
+    reads its wind stress and pressure from the deck's fort.22 at every RK
+    stage (met_forcing.F:49-66).  Returns the
     list of (it, eta2) snapshots; writes them to ``out`` when given.  A deck
     with MODAL_IC = 2 starts from its DG hot start at step ITHS + 1; with
     DGHOT = 1 the DG hot start is written (to ``hot_dir``, the deck's
@@ -496,6 +591,11 @@ def run_case(path, out=None, device: int = 0, nsteps: int | None = None, strict:
     nolifa = deck.s.nolifa
     snaps = []
     with HydroStep(deck, device, strict=strict, mixed=mixed) as hs:
+        if deck.s.nws == 1:
+            fort22 = Path(path) / "fort.22"
+            if not fort22.exists():
+                raise FileNotFoundError(f"{fort22}: NWS = 1 reads the met fields from fort.22 every stage")
+            hs.met_file(fort22)
         count = 0
         for it in range(it0, nt + 1):
             hs.timestep(it)

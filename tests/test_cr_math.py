@@ -1,4 +1,6 @@
-"""The Manning depth factor DEPTH**(1.D0/3.D0) (rhs_dg_hydro.F) in the strict
+"""Correctly rounded helpers of the strict kernels (cr_math.cuh).
+
+The Manning depth factor DEPTH**(1.D0/3.D0) (rhs_dg_hydro.F) in the strict
 kernels and in the oracle: both must give the correctly rounded double, so
 that the strict build and the oracle agree bit for bit on Manning decks.
 
@@ -36,6 +38,8 @@ def checker(tmp_path_factory):
                     "-o", str(out), "-lquadmath"], check=True)
     L = C.CDLL(str(out))
     L.cr_pow_third_eval.argtypes = [_dp, C.c_long, _dp, _dp, _dp]
+    L.cr_div3_mismatches.argtypes = [_dp, C.c_long]
+    L.cr_div3_mismatches.restype = C.c_long
     return L
 
 
@@ -81,3 +85,19 @@ def test_oracle_pow_third_correctly_rounded(checker):
     checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), ours.ctypes.data_as(_dp),
                               quad.ctypes.data_as(_dp), libm.ctypes.data_as(_dp))
     np.testing.assert_array_equal(orc, quad)
+
+
+def test_div3_is_the_ieee_quotient(checker):
+    """div3(x) and x / 3.0 bit for bit (signed zeros included) over random
+    bit patterns (every exponent, both signs, subnormals) and significands
+    at both ends of a binade."""
+    rng = np.random.default_rng(7)
+    bits = rng.integers(0, 2 ** 63, 4_000_000, dtype=np.int64) * rng.choice([1, -1], 4_000_000)
+    xs = bits.view(np.float64)
+    xs = xs[np.isfinite(xs)]
+    k = np.arange(1_000_000, dtype=np.float64)
+    edges = np.concatenate([np.ldexp(1.0 + k * 2.0 ** -52, (k % 200 - 100).astype(int)),
+                            np.ldexp(2.0 - (k + 1) * 2.0 ** -52, (k % 200 - 100).astype(int)),
+                            [0.0, -0.0, 5e-324, -5e-324, 1e-323, 3.0, 1.5, 2.0 ** -1022]])
+    xs = np.ascontiguousarray(np.concatenate([xs, edges]))
+    assert checker.cr_div3_mismatches(xs.ctypes.data_as(_dp), len(xs)) == 0
