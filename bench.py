@@ -602,7 +602,7 @@ VARIANT_TEXT = {"strict": "strict: FP64 without FMA contraction, the oracle's ev
 
 
 def variant_kwargs(variant: str) -> dict:
-    return {"strict": True} if variant == "strict" else {}
+    return {"strict": True} if variant == "strict" else {"fast": True}
 
 
 def other_variant_arm(deck, stream, args, world: int, dist, device: int) -> dict:

@@ -1,6 +1,7 @@
 // cr_math.cuh -- the correctly rounded value of DEPTH**(1.D0/3.D0), the
 // Manning depth factor of rhs_dg_hydro.F, computed with IEEE-754 basic
-// operations only (+, -, *, /, fma, and the exact frexp / ldexp), so that the
+// operations (+, -, *, /, fma, and the exact frexp / ldexp) and a
+// single-precision logarithm whose error the method absorbs, so that the
 // same source gives the same bits on the host and on the device.
 //
 // The exponent of the reference's expression is c = RN(1/3) = (1 - 2^-54)/3,
@@ -16,17 +17,21 @@
 //      exactly, t_h - m exact by Sterbenz's lemma), and one Newton step in
 //      double-double gives cbrt(m) = z - res y^2 / 3 (y^2 = 1 / z^2 to working
 //      precision);
-//   4. ln(x) = e' ln 2 + 2 atanh(s), s = (f' - 1) / (f' + 1), f' in [1/sqrt 2,
-//      sqrt 2), by its odd series (absolute error below 1e-14, which enters
-//      the result scaled by 2^-54 / 3);
+//   4. ln(x), which enters the result scaled by 2^-54 / 3: first from a
+//      single-precision logarithm, which decides the rounding unless the
+//      value lies within 2^-70 of a midpoint between doubles (checked from
+//      the exact rounding error of the final sum); then, in those rare
+//      cases, as e' ln 2 + 2 atanh(s), s = (f' - 1) / (f' + 1), f' in
+//      [1/sqrt 2, sqrt 2), by its odd series (absolute error below 1e-15);
 //   5. the double-double value times (1 - 2^-54 ln(x)/3) is rounded once to
 //      double and scaled by 2^q (exact).
 // The result differs from the correctly rounded x^c only when x^c lies within
 // about 2^-100 relative of a midpoint between two doubles.
 //
-// No library transcendental is called, so the strict kernels and the oracle
-// (which evaluates the same expression as a quadruple-precision pow rounded
-// to double) agree bit for bit.
+// The single-precision logarithm only chooses between the two evaluations
+// of step 4 (the device's and the host's may differ; the result does not),
+// so the strict kernels and the oracle (which evaluates the same expression
+// as a correctly rounded pow) agree bit for bit.
 #pragma once
 
 #include <cmath>
@@ -39,6 +44,35 @@
 
 namespace dgswem {
 
+// ln(x) = e' ln 2 + 2 atanh(s) for x = f 2^e, to 1e-15 absolute (step 4)
+DGSWEM_HD double ln_series(double f, int e) {
+  double fp = f;
+  int ep = e;
+  if (fp < 0.70710678118654752440) {
+    fp = fp + fp;
+    ep = ep - 1;
+  }
+  const double s = (fp - 1.0) / (fp + 1.0);
+  const double s2 = s * s;
+  double poly = 1.0 / 19.0;
+  poly = 1.0 / 17.0 + s2 * poly;
+  poly = 1.0 / 15.0 + s2 * poly;
+  poly = 1.0 / 13.0 + s2 * poly;
+  poly = 1.0 / 11.0 + s2 * poly;
+  poly = 1.0 / 9.0 + s2 * poly;
+  poly = 1.0 / 7.0 + s2 * poly;
+  poly = 1.0 / 5.0 + s2 * poly;
+  poly = 1.0 / 3.0 + s2 * poly;
+  const double lnf = 2.0 * s + 2.0 * s * (s2 * poly);
+  // ln 2 = hi + lo, hi with 21 trailing zero bits so that ep * hi is exact
+  const double ln2_hi = 0x1.62e42feep-1;
+  const double ln2_lo = 1.9082149292705877e-10;
+  return (double)ep * ln2_hi + ((double)ep * ln2_lo + lnf);
+}
+
+// kFastLog = false takes the series for ln(x) every time (the rare path
+// alone, for tests).
+template <bool kFastLog = true>
 DGSWEM_HD double pow_third(double x) {
   if (!(x > 0.0) || !(x < INFINITY)) {
     // pow(x, c) of a zero, negative, infinite or NaN base: 0, NaN, inf, NaN
@@ -69,31 +103,33 @@ DGSWEM_HD double pow_third(double x) {
   const double t_l = fma(p_h, z, -t_h);
   const double res = (t_h - m) + (t_l + p_l * z);
   const double corr = (res * y2) * third;  // cbrt(m) = z - corr
-  // step 4: ln(x), x = f' 2^e', f' in [1/sqrt 2, sqrt 2)
-  double fp = f;
-  int ep = e;
-  if (fp < 0.70710678118654752440) {
-    fp = fp + fp;
-    ep = ep - 1;
+  // steps 4-5, first with ln(x) from a single-precision logarithm (absolute
+  // error below 2^-20 for f in [0.5, 1)): delta is then known to 2^-75, and
+  // z + tail rounds to the same double as the exact value unless the exact
+  // value lies within 2^-70 (relative) of a midpoint between two doubles.
+  // s = RN(z + tail) and its rounding error err (exact, |tail| << z) show
+  // that distance: |err| far from half an ulp of s keeps s.  Otherwise --
+  // about once in 2^18 calls -- ln(x) to 1e-15 by its series.
+  const double k54 = 5.5511151231257827e-17 * third;  // 2^-54 / 3
+  if (kFastLog) {
+#if defined(__CUDA_ARCH__)
+    const float lnf_fast = __logf((float)f);
+#else
+    const float lnf_fast = std::log((float)f);
+#endif
+    const double lnx_fast = (double)e * 0.69314718055994531 + (double)lnf_fast;
+    const double delta_fast = lnx_fast * k54;
+    const double tail_fast = (-corr - z * delta_fast) + corr * delta_fast;
+    const double s = z + tail_fast;
+    const double err = tail_fast - (s - z);
+    int es;
+    const double fs = frexp(s, &es);                // s = fs 2^es, fs in [0.5, 1)
+    const double half_ulp = ldexp(1.0, es - 54);    // half an ulp of s
+    if (fs != 0.5 && fabs(fabs(err) - half_ulp) > s * 0x1p-70) return ldexp(s, q);
   }
-  const double s = (fp - 1.0) / (fp + 1.0);
-  const double s2 = s * s;
-  double poly = 1.0 / 19.0;
-  poly = 1.0 / 17.0 + s2 * poly;
-  poly = 1.0 / 15.0 + s2 * poly;
-  poly = 1.0 / 13.0 + s2 * poly;
-  poly = 1.0 / 11.0 + s2 * poly;
-  poly = 1.0 / 9.0 + s2 * poly;
-  poly = 1.0 / 7.0 + s2 * poly;
-  poly = 1.0 / 5.0 + s2 * poly;
-  poly = 1.0 / 3.0 + s2 * poly;
-  const double lnf = 2.0 * s + 2.0 * s * (s2 * poly);
-  // ln 2 = hi + lo, hi with 21 trailing zero bits so that ep * hi is exact
-  const double ln2_hi = 0x1.62e42feep-1;
-  const double ln2_lo = 1.9082149292705877e-10;
-  const double lnx = (double)ep * ln2_hi + ((double)ep * ln2_lo + lnf);
-  // step 5: delta = 2^-54 ln(x) / 3; (z - corr)(1 - delta), rounded once
-  const double delta = lnx * (5.5511151231257827e-17 * third);
+  // step 4-5 with ln(x) to 1e-15 (also when s is a power of two, whose ulp
+  // below is half the one above)
+  const double delta = ln_series(f, e) * k54;
   const double tail = (-corr - z * delta) + corr * delta;
   return ldexp(z + tail, q);
 }

@@ -11,10 +11,12 @@
 
 #include "cr_math.cuh"
 
-extern "C" void cr_pow_third_eval(const double* xs, long n, double* ours, double* quad, double* libm) {
+// ours: pow_third as the kernels call it (series = 0) or with the series
+// for ln(x) on every call (series = 1, the rare path alone)
+extern "C" void cr_pow_third_eval(const double* xs, long n, int series, double* ours, double* quad, double* libm) {
   for (long i = 0; i < n; ++i) {
     const double x = xs[i];
-    ours[i] = dgswem::pow_third(x);
+    ours[i] = series ? dgswem::pow_third<false>(x) : dgswem::pow_third(x);
     quad[i] = (double)powq((__float128)x, (__float128)(1.0 / 3.0));
     libm[i] = std::pow(x, 1.0 / 3.0);
   }

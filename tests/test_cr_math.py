@@ -37,7 +37,7 @@ def checker(tmp_path_factory):
                     str(ROOT / "dgswem_b200" / "csrc"), str(ROOT / "tests" / "native" / "cr_math_check.cpp"),
                     "-o", str(out), "-lquadmath"], check=True)
     L = C.CDLL(str(out))
-    L.cr_pow_third_eval.argtypes = [_dp, C.c_long, _dp, _dp, _dp]
+    L.cr_pow_third_eval.argtypes = [_dp, C.c_long, C.c_int, _dp, _dp, _dp]
     L.cr_div3_mismatches.argtypes = [_dp, C.c_long]
     L.cr_div3_mismatches.restype = C.c_long
     return L
@@ -55,10 +55,13 @@ def samples():
     ]).astype(np.float64)
 
 
-def test_pow_third_correctly_rounded(checker):
+@pytest.mark.parametrize("series", [0, 1])
+def test_pow_third_correctly_rounded(checker, series):
+    """series=0: as the kernels call it (single-precision log deciding the
+    rounding, series when undecided); series=1: the series every time."""
     xs = np.ascontiguousarray(samples())
     ours, quad, libm = (np.empty_like(xs) for _ in range(3))
-    checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), ours.ctypes.data_as(_dp),
+    checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), series, ours.ctypes.data_as(_dp),
                               quad.ctypes.data_as(_dp), libm.ctypes.data_as(_dp))
     np.testing.assert_array_equal(ours, quad)
     off = libm != quad
@@ -70,7 +73,7 @@ def test_pow_third_correctly_rounded(checker):
 def test_pow_third_special_values(checker):
     xs = np.array([0.0, -1.0, np.inf, np.nan])
     ours, quad, libm = (np.empty_like(xs) for _ in range(3))
-    checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), ours.ctypes.data_as(_dp),
+    checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), 0, ours.ctypes.data_as(_dp),
                               quad.ctypes.data_as(_dp), libm.ctypes.data_as(_dp))
     np.testing.assert_array_equal(ours, libm)  # 0, NaN, inf, NaN
 
@@ -82,7 +85,7 @@ def test_oracle_pow_third_correctly_rounded(checker):
     orc = np.empty_like(xs)
     L.orc_pow_third(xs.ctypes.data_as(_dp), len(xs), orc.ctypes.data_as(_dp))
     ours, quad, libm = (np.empty_like(xs) for _ in range(3))
-    checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), ours.ctypes.data_as(_dp),
+    checker.cr_pow_third_eval(xs.ctypes.data_as(_dp), len(xs), 0, ours.ctypes.data_as(_dp),
                               quad.ctypes.data_as(_dp), libm.ctypes.data_as(_dp))
     np.testing.assert_array_equal(orc, quad)
 
