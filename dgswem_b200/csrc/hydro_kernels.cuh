@@ -454,13 +454,12 @@ __device__ __forceinline__ void trace_depth(const Physics& P, real z, real w, re
 
 // Phase 3 of the stage kernel for area point I of tile element el (global
 // id e): volume fluxes and sources (rhs_dg_hydro.F:58-470) into
-// vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  I is a template
-// parameter (the point is the same for a whole warp), so the basis values
-// are constant-memory operands; qt: the slots in the arithmetic type.
-template <bool kNonlin, bool kSph, int kTile, int I>
-__device__ __forceinline__ void volume_values(const StageArgs& A, const real* qt, const real* geo, int el, int e,
-                                              real out[8]) {
-  const BasisT<real>& C = cBasisR;
+// vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  C: the basis
+// tables in shared memory (I is a runtime index); qt: the slots in the
+// arithmetic type.
+template <bool kNonlin, bool kSph, int kTile>
+__device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<real>& C, const real* qt,
+                                              const real* geo, int I, int el, int e, real out[8]) {
   const MeshView& m = A.m;
   const Physics& P = A.ph;
   const PhysR R = phys_r(A);
@@ -544,11 +543,11 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const real* qt
   out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
 }
 
-template <bool kNonlin, bool kSph, int kTile, int I>
-__device__ __forceinline__ void volume_point(const StageArgs& A, const real* qt, const real* geo, real* vol, int el,
-                                             int e) {
+template <bool kNonlin, bool kSph, int kTile>
+__device__ __forceinline__ void volume_point(const StageArgs& A, const BasisT<real>& C, const real* qt,
+                                             const real* geo, real* vol, int I, int el, int e) {
   real v[8];
-  volume_values<kNonlin, kSph, kTile, I>(A, qt, geo, el, e, v);
+  volume_values<kNonlin, kSph, kTile>(A, C, qt, geo, I, el, e, v);
 #pragma unroll
   for (int r = 0; r < 8; ++r) vol[(r * 3 + I) * kTile + el] = v[r];
 }
@@ -564,10 +563,11 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const real* qt,
 // indices are fixed by unrolled loops).  The sums are in the arithmetic
 // type, the SSP combination in FP64 (in the mixed variant: the RHS rounded
 // to FP32, the stage states and their combination FP64).
-template <bool kNonlin, int kTile, int K>
+template <bool kNonlin, int kTile>
 __device__ __forceinline__ void sum_mode(const StageArgs& A, const BasisT<real>& B, const double* qs,
                                          const real* geo, const real* vol, const real* res, const int* tdry,
-                                         const unsigned* sinfo, const int* wds, const uint2* stasks, int el, int e) {
+                                         const unsigned* sinfo, const int* wds, const uint2* stasks, int K, int el,
+                                         int e) {
   const BasisT<real>& C = cBasisR;
   const MeshView& m = A.m;
   const Physics& P = A.ph;
@@ -975,13 +975,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int i = w / kTile, el = w - i * kTile;
     if (el >= n || wds[el] == 0) continue;
-    // one instance per point: the point is the same for the whole warp
-    if (i == 0)
-      volume_point<kNonlin, kSph, kTile, 0>(A, qt, geo, vol, el, tile0 + el);
-    else if (i == 1)
-      volume_point<kNonlin, kSph, kTile, 1>(A, qt, geo, vol, el, tile0 + el);
-    else
-      volume_point<kNonlin, kSph, kTile, 2>(A, qt, geo, vol, el, tile0 + el);
+    volume_point<kNonlin, kSph, kTile>(A, B, qt, geo, vol, i, el, tile0 + el);
   }
   __syncthreads();
 
@@ -989,13 +983,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int K = w / kTile, el = w - K * kTile;
     if (el >= n) continue;
-    // one instance per mode: the mode is the same for the whole warp
-    if (K == 0)
-      sum_mode<kNonlin, kTile, 0>(A, B, qs, geo, vol, res, tdry, sinfo, wds, stasks, el, tile0 + el);
-    else if (K == 1)
-      sum_mode<kNonlin, kTile, 1>(A, B, qs, geo, vol, res, tdry, sinfo, wds, stasks, el, tile0 + el);
-    else
-      sum_mode<kNonlin, kTile, 2>(A, B, qs, geo, vol, res, tdry, sinfo, wds, stasks, el, tile0 + el);
+    sum_mode<kNonlin, kTile>(A, B, qs, geo, vol, res, tdry, sinfo, wds, stasks, K, el, tile0 + el);
   }
 }
 
