@@ -436,6 +436,54 @@ __device__ __forceinline__ void slot_trace(const BasisT<real>& B, const real* qt
   h = q[9] + q[10] * p1 + q[11] * p2;
 }
 
+// One Lobatto point of an interior edge in the reference's in/ex orientation
+// (internal_edge_hydro.F): the LLF flux of the two traces, then the dry-side
+// rules of :212-302 -> o[0..4] = F, G_in, H_in, G_ex, H_ex.
+template <bool kNonlin>
+__device__ __forceinline__ void interior_point(const Physics& P, real zi, real zx, real xi, real xx, real yi,
+                                           real yx, real hi, real hx, real hti, real htx, real sfi, real sfx,
+                                           real nx, real ny, int wd_in, int wd_ex, real* o) {
+  const Flux3T<real> f =
+      llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, sfi, sfx, nx, ny, real(P.g));
+  o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
+  if ((wd_in == 0 || wd_ex == 0) && fabs(f.f) > real(1.0e-8)) {
+    // internal_edge_hydro.F:212-302: mass flux out of / into a dry
+    // element.  The four cases re-evaluate the flux once with changed
+    // arguments: the dry side's state replaced by the wet side's with
+    // reflected momentum (outflow from a dry element), or gravity off
+    // (G = 0) for the dry side's momentum flux.
+    const bool in_dry = wd_in == 0;
+    const real F0 = f.f;
+    const real tx = -ny, ty = nx, den = nx * ty - ny * tx;
+    const bool reflect = in_dry ? F0 > real(0) : F0 < real(0);
+    // the wet side, whose momentum is reflected onto the dry side
+    const real qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
+    const real qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
+    const real qnr = -qnw, qtr = qtw;
+    const real qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
+    real a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
+    real a_hi = hi, a_hx = hx, a_ti = hti, a_tx = htx, a_si = sfi, a_sx = sfx, a_g = 0;
+    if (reflect) {
+      a_g = real(P.g);
+      if (in_dry) {
+        a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_ti = htx; a_si = sfx;
+      } else {
+        a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_tx = hti; a_sx = sfi;
+      }
+    }
+    const Flux3T<real> r = llf<kNonlin, real>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_ti, a_tx,
+                                              a_si, a_sx, nx, ny, a_g);
+    if (reflect) {
+      o[0] = r.f;
+      if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0; o[2] = 0; }
+      else        { o[1] = r.g; o[2] = r.h; o[3] = 0; o[4] = 0; }
+    } else {
+      if (in_dry) { o[1] = r.g; o[2] = r.h; }
+      else        { o[3] = r.g; o[4] = r.h; }
+    }
+  }
+}
+
 // Bathymetry hb and total depth ht at a trace point from elevation z and the
 // slot's fourth trace w: w is HB in the FP64 kernels; the mixed kernels'
 // FP32 slots hold the depth modes ZE + HB (summed in FP64, then rounded), so
@@ -452,29 +500,25 @@ __device__ __forceinline__ void trace_depth(const Physics& P, real z, real w, re
 #endif
 }
 
-// Phase 3 of the stage kernel for area point I of tile element el (global
-// id e): volume fluxes and sources (rhs_dg_hydro.F:58-470) into
-// vol[(v*3 + I)*kTile + el], v = fx fy gx gy hx hy sx sy.  C: the basis
-// tables in shared memory (I is a runtime index); qt: the slots in the
-// arithmetic type.
-template <bool kNonlin, bool kSph, int kTile>
-__device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<real>& C, const real* qt,
-                                              const real* geo, int I, int el, int e, real out[8]) {
+// Volume fluxes and sources at area point I of element e (rhs_dg_hydro.F:
+// 58-470) from the element's 12 slot values q (ZE, QX, QY modes, then HB or,
+// in the mixed variant, depth modes), its inverse Jacobian, element-mean
+// Manning n and hybrid friction factor: out = fx fy gx gy hx hy sx sy.
+template <bool kNonlin, bool kSph>
+__device__ __forceinline__ void volume_core(const StageArgs& A, const BasisT<real>& C, const real q[12], real drdx,
+                                            real dsdx, real drdy, real dsdy, real nbar, real hyb, int I, int e,
+                                            real out[8]) {
   const MeshView& m = A.m;
   const Physics& P = A.ph;
   const PhysR R = phys_r(A);
   const int ne = m.ne;
-  const int wde = 1;  // phase 3 runs for wet elements only
-  real q[12];
-  slot_values(qt, el, q);
+  const int wde = 1;  // volume terms are evaluated for wet elements only
 #ifdef DGSWEM_MIXED
   // the slot holds the depth modes ZE + HB (see trace_depth)
   const real hbe[3] = {q[9] - q[0], q[10] - q[1], q[11] - q[2]};
 #else
   const real* hbe = q + 9;
 #endif
-  const real drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
-  const real drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
   const real NLEQ = kNonlin ? real(1) : R.nleq, LEQ = kNonlin ? real(0) : R.leq;
   const real cori = m.cori ? (real)m.cori[e] : R.cori;
   real fric = m.fric ? (real)m.fric[e] : R.fric;
@@ -507,7 +551,6 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<r
   const real gx = (huu + gh2) * sfq, gy = huv;
   const real hx = huv * sfq, hy = hvv + gh2;
   if (m.manning) {
-    const real nbar = geo[EGeo::kNbar * kTile + el];
     fric = R.g * (nbar * nbar) / cube_root(depth);
     if (fric < R.cf) fric = R.cf;
   }
@@ -515,7 +558,7 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<r
   if (P.iflinbf == 0) {
     const real umag = sqrt(u * u + v * v);
     tau = tau * umag * fh;
-    if (P.ifhybf == 1) tau = tau * geo[SGeo::kHyb * kTile + el];
+    if (P.ifhybf == 1) tau = tau * hyb;
     tau = fmin(tau, R.tau_cap);
   }
   real sx = -(tau * uq) + fg * dhx * sfq + cori * vq;
@@ -541,6 +584,22 @@ __device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<r
   }
   out[0] = fx; out[1] = fy; out[2] = gx; out[3] = gy;
   out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
+}
+
+// Phase 3 of the stage kernel for area point I of tile element el (global
+// id e): volume_core on the element's shared-memory slot and geometry rows,
+// into vol[(v*3 + I)*kTile + el] by volume_point.  C: the basis tables in
+// shared memory (I is a runtime index); qt: the slots in the arithmetic type.
+template <bool kNonlin, bool kSph, int kTile>
+__device__ __forceinline__ void volume_values(const StageArgs& A, const BasisT<real>& C, const real* qt,
+                                              const real* geo, int I, int el, int e, real out[8]) {
+  real q[12];
+  slot_values(qt, el, q);
+  const real drdx = geo[EGeo::kDrdx * kTile + el], dsdx = geo[EGeo::kDsdx * kTile + el];
+  const real drdy = geo[EGeo::kDrdy * kTile + el], dsdy = geo[EGeo::kDsdy * kTile + el];
+  const real nbar = A.m.manning ? geo[EGeo::kNbar * kTile + el] : real(0);
+  const real hyb = (A.ph.iflinbf == 0 && A.ph.ifhybf == 1) ? geo[SGeo::kHyb * kTile + el] : real(0);
+  volume_core<kNonlin, kSph>(A, C, q, drdx, dsdx, drdy, dsdy, nbar, hyb, I, e, out);
 }
 
 template <bool kNonlin, bool kSph, int kTile>
@@ -915,45 +974,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
       trace_depth<kNonlin>(P, zx, wx, hx, htx);
       const real sfi = kSph ? (real)m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : real(1);
       const real sfx = kSph ? (real)m.sfac_edge[(size_t)(led_ex * 3 + gp_ex) * ne + gex] : real(1);
-      const Flux3T<real> f =
-          llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, sfi, sfx, nx, ny, real(P.g));
-      o[0] = f.f; o[1] = f.g; o[2] = f.h; o[3] = f.g; o[4] = f.h;
-      if ((wd_in == 0 || wd_ex == 0) && fabs(f.f) > real(1.0e-8)) {
-        // internal_edge_hydro.F:212-302: mass flux out of / into a dry
-        // element.  The four cases re-evaluate the flux once with changed
-        // arguments: the dry side's state replaced by the wet side's with
-        // reflected momentum (outflow from a dry element), or gravity off
-        // (G = 0) for the dry side's momentum flux.
-        const bool in_dry = wd_in == 0;
-        const real F0 = f.f;
-        const real tx = -ny, ty = nx, den = nx * ty - ny * tx;
-        const bool reflect = in_dry ? F0 > real(0) : F0 < real(0);
-        // the wet side, whose momentum is reflected onto the dry side
-        const real qxw = in_dry ? xx : xi, qyw = in_dry ? yx : yi;
-        const real qnw = qxw * nx + qyw * ny, qtw = qxw * tx + qyw * ty;
-        const real qnr = -qnw, qtr = qtw;
-        const real qxr = (ty * qnr - ny * qtr) / den, qyr = (-tx * qnr + nx * qtr) / den;
-        real a_zi = zi, a_zx = zx, a_xi = xi, a_xx = xx, a_yi = yi, a_yx = yx;
-        real a_hi = hi, a_hx = hx, a_ti = hti, a_tx = htx, a_si = sfi, a_sx = sfx, a_g = 0;
-        if (reflect) {
-          a_g = real(P.g);
-          if (in_dry) {
-            a_zi = zx; a_xi = qxr; a_yi = qyr; a_hi = hx; a_ti = htx; a_si = sfx;
-          } else {
-            a_zx = zi; a_xx = qxr; a_yx = qyr; a_hx = hi; a_tx = hti; a_sx = sfi;
-          }
-        }
-        const Flux3T<real> r = llf<kNonlin, real>(P, a_zi, a_zx, a_xi, a_xx, a_yi, a_yx, a_hi, a_hx, a_ti, a_tx,
-                                                  a_si, a_sx, nx, ny, a_g);
-        if (reflect) {
-          o[0] = r.f;
-          if (in_dry) { o[3] = r.g; o[4] = r.h; o[1] = 0; o[2] = 0; }
-          else        { o[1] = r.g; o[2] = r.h; o[3] = 0; o[4] = 0; }
-        } else {
-          if (in_dry) { o[1] = r.g; o[2] = r.h; }
-          else        { o[3] = r.g; o[4] = r.h; }
-        }
-      }
+      interior_point<kNonlin>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, sfi, sfx, nx, ny, wd_in, wd_ex, o);
     } else {
       if (wd_in == 0) continue;
       real zi, xi, yi, wi, zx, xx, yx, hi, hti;
