@@ -117,14 +117,17 @@ def rank0_first(rank: int, world: int, dist, fn):
     return out
 
 
-def config3_deck(workdir, nr: int, nth: int, p: int = 1) -> Path:
+def config3_deck(workdir, nr: int, nth: int, p: int = 1, dramp: float | None = None) -> Path:
     """The config-3 quarter annulus (nr x nth cells, dt = 0.5 s, NWS=1, DG of
-    degree p) under workdir, written unless complete."""
+    degree p; the tide and wind ramp over ``dramp`` days, the generator's two
+    days by default) under workdir, written unless complete."""
     from dgswem_b200 import decks
-    path = Path(workdir) / (f"config3_{nr}x{nth}" + ("" if p == 1 else f"_p{p}"))
+    path = Path(workdir) / (f"config3_{nr}x{nth}" + ("" if p == 1 else f"_p{p}") +
+                            ("" if dramp is None else f"_ramp{dramp:g}"))
     done = path / ".complete"
     if not done.exists():
-        decks.quarter_annulus(path, nr=nr, nth=nth, nsteps=5000, dt=0.5, nws=1, extra={"pl": p, "ph": p})
+        kw = {} if dramp is None else {"dramp": dramp}
+        decks.quarter_annulus(path, nr=nr, nth=nth, nsteps=5000, dt=0.5, nws=1, extra={"pl": p, "ph": p}, **kw)
         done.write_text("ok\n")
     return path
 
@@ -303,14 +306,23 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
             out[name] = {"value": whole_job_rate(world, deck.s.ne, deck.s.nrk, k, ms), "unit": "DOF-stage/s",
                          "ms_per_step": ms / k,
                          "tile_shape": tiles["tile_shape"] if tiles else None}
-        with HydroStep(deck, device=device, **kw) as h:
+    # the error comparison: both forms from the same initial state over
+    # --config3-err-steps steps of a copy of the deck whose tide and wind
+    # ramp up within the run (--config3-err-dramp days), so that the basin
+    # moves
+    epath = rank0_first(rank_env()[0], world, dist,
+                        lambda: config3_deck(args.workdir, nr, nth, dramp=args.config3_err_dramp))
+    edeck = Deck(epath)
+    for name, kw in (("fp64", variant_kwargs(args.variant)), ("mixed", {"mixed": True})):
+        with HydroStep(edeck, device=device, **kw) as h:
             h.set_stream(stream.cuda_stream)
             h.set_met(*met)
             h.run(1, args.config3_err_steps)
             h.synchronize()
             states[name] = (h.state(), h.modal2nodal())
     (sf, nf), (sm, nmx) = states["fp64"], states["mixed"]
-    mf, mm = mass(deck, sf[0]), mass(deck, sm[0])
+    mf, mm = mass(edeck, sf[0]), mass(edeck, sm[0])
+    edeck.close()
     out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     if args.config3_p2_steps > 0:
         # the p=2 half: the same annulus at p=2 (18 DOFs per element), FP64
@@ -342,7 +354,9 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
                      "dtype": "f64", "kernels": "p2_edges + p2_elements per RK stage"}
         deck2.close()
     out["mixed"]["err_vs_fp64"] = {
-        "steps": args.config3_err_steps,
+        "steps": args.config3_err_steps, "ramp_days": args.config3_err_dramp,
+        "fp64_eta_nodal_max_m": float(np.abs(nf[0]).max()),
+        "fp64_vel_nodal_max_ms": float(max(np.abs(nf[1]).max(), np.abs(nf[2]).max())),
         "eta_nodal_linf_m": float(np.abs(nmx[0] - nf[0]).max()),
         "ze_mean_linf_m": float(np.abs(sm[0][:, 0] - sf[0][:, 0]).max()),
         "vel_nodal_linf_ms": float(max(np.abs(nmx[1] - nf[1]).max(), np.abs(nmx[2] - nf[2]).max())),
@@ -438,7 +452,8 @@ def adjoint_arm(args, device: int) -> dict:
     from dgswem_b200 import Deck, decks
     from dgswem_b200.adjoint import GaugeMisfitProblem, element_manning, locate_gauges
     n = args.adjoint_steps
-    path = decks.sloping_beach(Path(args.workdir) / "adjoint_beach_1M", nx=1580, ny=316, lx=100e3, ly=20e3,
+    nx, ny = args.adjoint_nx, args.adjoint_ny
+    path = decks.sloping_beach(Path(args.workdir) / f"adjoint_beach_{nx}x{ny}", nx=nx, ny=ny, lx=100e3, ly=20e3,
                                dt=0.5, nsteps=n, dramp=0.002)
     deck = Deck(path)
     rng = np.random.default_rng(20261203)
@@ -709,13 +724,20 @@ def main(argv=None):
                     help="timed steps of the 8M-element config-3 annulus with wind (0: skip)")
     ap.add_argument("--config3-nr", type=int, default=1000)
     ap.add_argument("--config3-nth", type=int, default=4000)
-    ap.add_argument("--config3-err-steps", type=int, default=200)
+    ap.add_argument("--config3-err-steps", type=int, default=5000,
+                    help="steps of the config-3 mixed-vs-FP64 error comparison")
+    ap.add_argument("--config3-err-dramp", type=float, default=0.01,
+                    help="tide and wind ramp (days) of the error comparison's deck")
     ap.add_argument("--config3-p2-steps", type=int, default=50, help="timed steps of the p=2 config-3 annulus (0: skip)")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
-    ap.add_argument("--ensemble-steps", type=int, default=40)
+    ap.add_argument("--ensemble-steps", type=int, default=2000)
     ap.add_argument("--ensemble-graph-steps", type=int, default=8,
                     help="whole steps per CUDA graph in the ensemble arm (even; 0: plain launches)")
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
+    ap.add_argument("--adjoint-nx", type=int, default=1580, help="cells along the adjoint beach (x)")
+    ap.add_argument("--adjoint-ny", type=int, default=316, help="cells across the adjoint beach (y)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint arm (a driver for profiling its kernels) and print its object")
     ap.add_argument("--mixed-err-steps", type=int, default=200,
                     help="steps of the mixed-vs-FP64 error comparison")
     args = ap.parse_args(argv)
@@ -731,6 +753,11 @@ def main(argv=None):
 
     rank, world, local = rank_env()
     torch.cuda.set_device(local)
+    if args.adjoint_only:
+        Path(args.workdir).mkdir(parents=True, exist_ok=True)
+        if rank == 0:
+            print(json.dumps({"adjoint": adjoint_arm(args, local)}), flush=True)
+        return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     workdir = Path(args.workdir)
