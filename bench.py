@@ -325,34 +325,67 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     edeck.close()
     out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     if args.config3_p2_steps > 0:
-        # the p=2 half: the same annulus at p=2 (18 DOFs per element), FP64
+        # the p=2 half: the same annulus at p=2 (18 DOFs per element), the
+        # headline FP64 build and the mixed form (p2_edges + p2_elements)
         path2 = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth, p=2))
         deck2 = Deck(path2)
         k2 = args.config3_p2_steps
-        with HydroStep(deck2, device=device, **variant_kwargs(args.variant)) as h:
-            h.set_stream(stream.cuda_stream)
-            h.set_met(*met)
-            h.run(1, w)
-            torch.cuda.synchronize()
-            if world > 1:
-                dist.barrier()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            h.run(w + 1, k2)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms2 = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
-            h.profile(True)
-            h.run(w + 1 + k2, 4)
-            prof = h.profile_read()
-            h.profile(False)
-            h.synchronize()
         dofs = 3 * deck2.s.dofh
-        out["p2"] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
-                     "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
-                     "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
-                     "dtype": "f64", "kernels": "p2_edges + p2_elements per RK stage"}
+        for name, kw in (("p2", variant_kwargs(args.variant)), ("p2_mixed", {"mixed": True})):
+            with HydroStep(deck2, device=device, **kw) as h:
+                h.set_stream(stream.cuda_stream)
+                h.set_met(*met)
+                h.run(1, w)
+                torch.cuda.synchronize()
+                if world > 1:
+                    dist.barrier()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                h.run(w + 1, k2)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms2 = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+                h.profile(True)
+                h.run(w + 1 + k2, 4)
+                prof = h.profile_read()
+                h.profile(False)
+                h.synchronize()
+            out[name] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
+                         "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
+                         "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
+                         "dtype": "f64" if name == "p2" else "mixed (f32 traces/fluxes/volume/sums, f64 state/SSP)",
+                         "kernels": "p2_edges + p2_elements per RK stage"}
         deck2.close()
+        out["p2_mixed"]["speedup_vs_fp64"] = out["p2_mixed"]["value"] / out["p2"]["value"]
+        if args.config3_p2_err_steps > 0:
+            epath2 = rank0_first(rank_env()[0], world, dist,
+                                 lambda: config3_deck(args.workdir, nr, nth, p=2, dramp=args.config3_err_dramp))
+            edeck2 = Deck(epath2)
+            st2 = {}
+            for name, kw in (("fp64", variant_kwargs(args.variant)), ("mixed", {"mixed": True})):
+                with HydroStep(edeck2, device=device, **kw) as h:
+                    h.set_stream(stream.cuda_stream)
+                    h.set_met(*met)
+                    h.run(1, args.config3_p2_err_steps)
+                    h.synchronize()
+                    st2[name] = (h.state(), h.modal2nodal())
+            (pf_, pnf), (pm_, pnm) = st2["fp64"], st2["mixed"]
+            ne2 = edeck2.s.ne
+            nm2 = edeck2.int_array("nm", 3 * ne2).reshape(3, ne2) - 1
+            x2, y2 = edeck2.real_array("x", edeck2.s.np), edeck2.real_array("y", edeck2.s.np)
+            hb2 = edeck2.real_array("hb", 6 * ne2).reshape(ne2, 6)
+            a2, b2, c2 = nm2
+            ar2 = 0.5 * ((x2[a2] - x2[c2]) * (y2[b2] - y2[c2]) + (x2[c2] - x2[b2]) * (y2[a2] - y2[c2]))
+            vf, vm = np.sum((pf_[0][:, 0] + hb2[:, 0]) * ar2), np.sum((pm_[0][:, 0] + hb2[:, 0]) * ar2)
+            edeck2.close()
+            out["p2_mixed"]["err_vs_fp64"] = {
+                "steps": args.config3_p2_err_steps, "ramp_days": args.config3_err_dramp,
+                "fp64_eta_nodal_max_m": float(np.abs(pnf[0]).max()),
+                "fp64_vel_nodal_max_ms": float(max(np.abs(pnf[1]).max(), np.abs(pnf[2]).max())),
+                "eta_nodal_linf_m": float(np.abs(pnm[0] - pnf[0]).max()),
+                "ze_mean_linf_m": float(np.abs(pm_[0][:, 0] - pf_[0][:, 0]).max()),
+                "vel_nodal_linf_ms": float(max(np.abs(pnm[1] - pnf[1]).max(), np.abs(pnm[2] - pnf[2]).max())),
+                "mass_rel": (vm - vf) / vf}
     out["mixed"]["err_vs_fp64"] = {
         "steps": args.config3_err_steps, "ramp_days": args.config3_err_dramp,
         "fp64_eta_nodal_max_m": float(np.abs(nf[0]).max()),
@@ -726,6 +759,8 @@ def main(argv=None):
     ap.add_argument("--config3-nth", type=int, default=4000)
     ap.add_argument("--config3-err-steps", type=int, default=5000,
                     help="steps of the config-3 mixed-vs-FP64 error comparison")
+    ap.add_argument("--config3-p2-err-steps", type=int, default=5000,
+                    help="steps of the p=2 mixed-vs-FP64 error comparison (0: skip)")
     ap.add_argument("--config3-err-dramp", type=float, default=0.01,
                     help="tide and wind ramp (days) of the error comparison's deck")
     ap.add_argument("--config3-p2-steps", type=int, default=50, help="timed steps of the p=2 config-3 annulus (0: skip)")

@@ -27,7 +27,9 @@ LIBNAME = "libdgswem_cuda.so"
 SOURCES = [("hydro.cu", []), ("kernels_fast.cu", ["-fmad=true"]), ("kernels_strict.cu", ["-fmad=false"]),
            ("kernels_mixed.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
            ("adjoint.cu", ["-fmad=true"]), ("kernels_p2_fast.cu", ["-fmad=true"]),
-           ("kernels_p2_strict.cu", ["-fmad=false"]), ("deck.cpp", []), ("partition.cpp", [])]
+           ("kernels_p2_strict.cu", ["-fmad=false"]),
+           ("kernels_p2_mixed.cu", ["-fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]),
+           ("deck.cpp", []), ("partition.cpp", [])]
 HEADERS = ["cr_math.cuh", "hydro_device.cuh", "hydro_kernels.cuh", "hydro_p2.cuh", "kernel_launch.inc", "abi_util.h", "partition.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -295,7 +295,8 @@ static const Variant kMixed = {4, mixed::set_basis, mixed::launch_stage, mixed::
                                mixed::launch_fortran_to_soa, mixed::launch_soa_to_fortran,
                                mixed::launch_gather_int, mixed::launch_halo};
 
-// Launchers of the p=2 stage (kernels_p2_fast.cu / kernels_p2_strict.cu)
+// Launchers of the p=2 stage (kernels_p2_fast.cu / kernels_p2_strict.cu /
+// kernels_p2_mixed.cu)
 struct P2Variant {
   void (*set_basis)(const BasisP2&);
   void (*stage)(const P2Args&, bool, cudaStream_t);
@@ -307,6 +308,8 @@ static const P2Variant kFastP2 = {fast_p2::set_basis_p2, fast_p2::launch_p2_stag
                                   fast_p2::launch_p2_layout};
 static const P2Variant kStrictP2 = {strict_p2::set_basis_p2, strict_p2::launch_p2_stage,
                                     strict_p2::launch_p2_modal2nodal, strict_p2::launch_p2_layout};
+static const P2Variant kMixedP2 = {mixed_p2::set_basis_p2, mixed_p2::launch_p2_stage,
+                                   mixed_p2::launch_p2_modal2nodal, mixed_p2::launch_p2_layout};
 
 }  // namespace dgswem
 
@@ -1050,6 +1053,11 @@ void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing, con
   P2Args A{};
   A.m = h->mesh;
   A.ph = h->ph;
+  {
+    const Physics& p = h->ph;
+    A.pf = PhysF{(float)p.g, (float)p.nleq, (float)p.leq, (float)p.nleqg, (float)p.fg_l, (float)p.tau_cap,
+                 (float)p.cori, (float)p.fric, (float)p.cf};
+  }
   A.irk = irk;
   A.qin = h->q[irk - 1].p;
   A.qout = h->q[irk].p;
@@ -1524,7 +1532,6 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
       throw Failure(DGSWEM_ERR_ARG, "DOFH must be 3 (p=1) or 6 (p=2)");
     if (s->dofh == kP2Modes) {
       if (nparts != 1) throw Failure(DGSWEM_ERR_ARG, "p=2 runs on a whole-mesh handle (dgswem_cuda_create)");
-      if (flags & DGSWEM_CUDA_MIXED) throw Failure(DGSWEM_ERR_ARG, "the mixed-precision form is p=1 only");
       if (s->slopeflag != 0) throw Failure(DGSWEM_ERR_ARG, "the slope limiter is p=1 only, as in the reference");
       if (s->nolifa >= 2) throw Failure(DGSWEM_ERR_ARG, "wetting and drying are p=1 only, as in the reference");
       if (s->ics != 1) throw Failure(DGSWEM_ERR_ARG, "p=2 supports ICS=1");
@@ -1546,7 +1553,8 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     // the strict kernels unless the fast or the mixed form is asked for
     h->v = (flags & DGSWEM_CUDA_FAST) ? &kFast : (flags & DGSWEM_CUDA_MIXED) ? &kMixed : &kStrict;
     h->dofh = s->dofh;
-    if (h->dofh == kP2Modes) h->v2 = (flags & DGSWEM_CUDA_FAST) ? &kFastP2 : &kStrictP2;
+    if (h->dofh == kP2Modes)
+      h->v2 = (flags & DGSWEM_CUDA_FAST) ? &kFastP2 : (flags & DGSWEM_CUDA_MIXED) ? &kMixedP2 : &kStrictP2;
     h->ne = s->ne;
     h->np = s->np;
     h->nrk = s->nrk;

@@ -280,20 +280,24 @@ DGSWEM_DECLARE_LAUNCHERS(mixed)
 // Six modes per variable, the four-point Gauss-Lobatto edge rule and the
 // six-point area rule (quadrature_v1.F); FP64, no wet/dry, no limiter.
 constexpr int kP2Modes = 6, kP2Egp = 4, kP2Agp = 6;
-struct BasisP2 {
-  double phi_edge[3][kP2Egp][kP2Modes];  // [led][point][mode]
-  double edgeq[3][kP2Egp][kP2Modes];     // 2*M_INV*PHI_EDGE*WEGP
-  double phi_area[kP2Modes][kP2Agp];     // [mode][point]
-  double drphi[kP2Modes][kP2Agp], dsphi[kP2Modes][kP2Agp];
-  double phi_corner[3][kP2Modes];        // [vertex][mode]
-  double psi[3][kP2Agp];                 // linear nodal basis at the area points
-  double m_inv[kP2Modes], wagp[kP2Agp], wegp[kP2Egp], xegp[kP2Egp];
-  double mw[kP2Modes][kP2Agp];           // M_INV*WAGP
-  double srfac[kP2Modes][kP2Agp];        // M_INV*WAGP*PHI_AREA
+template <class T>
+struct BasisP2T {
+  T phi_edge[3][kP2Egp][kP2Modes];  // [led][point][mode]
+  T edgeq[3][kP2Egp][kP2Modes];     // 2*M_INV*PHI_EDGE*WEGP
+  T phi_area[kP2Modes][kP2Agp];     // [mode][point]
+  T drphi[kP2Modes][kP2Agp], dsphi[kP2Modes][kP2Agp];
+  T phi_corner[3][kP2Modes];        // [vertex][mode]
+  T psi[3][kP2Agp];                 // linear nodal basis at the area points
+  T m_inv[kP2Modes], wagp[kP2Agp], wegp[kP2Egp], xegp[kP2Egp];
+  T mw[kP2Modes][kP2Agp];           // M_INV*WAGP
+  T srfac[kP2Modes][kP2Agp];        // M_INV*WAGP*PHI_AREA
 };
+using BasisP2 = BasisP2T<double>;
+static_assert(sizeof(BasisP2T<float>) * 2 == sizeof(BasisP2), "p=2 basis tables are plain arrays");
 struct P2Args {
   MeshView m;   // hb: six rows; egeo; einfo / link for the edge kinds and neighbours
   Physics ph;
+  PhysF pf;     // ph rounded to FP32 (mixed precision)
   int irk;
   const double* __restrict__ qin;  // 18 rows (6*var + mode)
   double* qout;
@@ -308,6 +312,7 @@ struct P2Args {
   const double* __restrict__ wsy;
   const double* __restrict__ pr;
   double* ef;                      // [((e*3 + led)*4 + point)*3 + c] edge-point fluxes F, G, H per side
+                                   // (in the arithmetic type: FP32 in the mixed variant)
   const int* __restrict__ edges;   // (element, local edge): interior edges from the in side, land and ocean edges
   int nedge, ne_act;
   unsigned* err;
@@ -323,6 +328,7 @@ struct P2Args {
   }
 DGSWEM_DECLARE_P2_LAUNCHERS(fast_p2)
 DGSWEM_DECLARE_P2_LAUNCHERS(strict_p2)
+DGSWEM_DECLARE_P2_LAUNCHERS(mixed_p2)
 
 // ---- discrete adjoint (adjoint.cu) ----------------------------------------
 // Vector-Jacobian product of one RK stage's right-hand side L(q; n, HB) at

@@ -1,36 +1,52 @@
 // hydro_p2.cuh -- the p=2 stage (six modes per variable, four Gauss-Lobatto
-// points per edge, the six-point area rule), FP64: an edge kernel and an
-// element kernel per RK stage.  Included after hydro_kernels.cuh (its LLF
-// flux and depth) by kernels_p2_fast.cu / kernels_p2_strict.cu with
-// DGSWEM_VARIANT set.  The arithmetic follows the p=1 kernels term for term,
-// generalised over the modes and points as the reference's p-generic
-// boundary-edge code (land_edge_hydro.F:144,273) is; the interior-edge sums
-// run over every mode (the reference's internal_edge_hydro.F:306-318 sums
-// modes 1-3 only, its p=2 defect).  No wetting/drying and no slope limiter
-// at p=2 (both are p=1 only in the reference); land, ocean and interior
-// edges; ICS=1.
+// points per edge, the six-point area rule): an edge kernel and an element
+// kernel per RK stage.  Included after hydro_kernels.cuh (its LLF flux,
+// depth, trace_depth, the arithmetic type `real`) by kernels_p2_fast.cu /
+// kernels_p2_strict.cu (FP64) and kernels_p2_mixed.cu (edge traces, fluxes,
+// volume terms and right-hand-side sums in FP32; state, SSP combination and
+// the ocean depth-positivity fix in FP64, as at p=1) with DGSWEM_VARIANT set.
+// The arithmetic follows the p=1 kernels term for term, generalised over the
+// modes and points as the reference's p-generic boundary-edge code
+// (land_edge_hydro.F:144,273) is; the interior-edge sums run over every mode
+// (the reference's internal_edge_hydro.F:306-318 sums modes 1-3 only, its
+// p=2 defect).  No wetting/drying and no slope limiter at p=2 (both are p=1
+// only in the reference); land, ocean and interior edges; ICS=1.
 #pragma once
 
 namespace dgswem {
 namespace DGSWEM_VARIANT {
 
 __constant__ BasisP2 cB2;
+__constant__ BasisP2T<real> cB2R;  // cB2 in the arithmetic type
 
-// Traces of ZE, QX, QY and HB at one point from the six modes (state rows
+// The fourth modal row of element e in the arithmetic type: the bathymetry
+// mode HB_k (FP64 variants) or the depth mode ZE_k + HB_k summed in FP64 and
+// rounded (mixed), as the p=1 kernels' slots.
+__device__ __forceinline__ real fourth_mode(const double* __restrict__ q, const double* __restrict__ hb, int ne,
+                                            int e, int k) {
+#ifdef DGSWEM_MIXED
+  return (real)(q[(size_t)k * ne + e] + hb[(size_t)k * ne + e]);
+#else
+  return hb[(size_t)k * ne + e];
+#endif
+}
+
+// Traces of ZE, QX, QY and the fourth row (HB, or the depth in the mixed
+// variant; see trace_depth) at one point from the six modes (state rows
 // 6*var + k, bathymetry rows k), summed from mode 1 upwards as the
 // reference's trace loops are (mode 1 is 1 at every point).
 __device__ __forceinline__ void trace6(const double* __restrict__ q, const double* __restrict__ hb, int ne,
-                                       int e, const double* phi, double& z, double& u, double& v, double& h) {
-  z = q[e];
-  u = q[(size_t)6 * ne + e];
-  v = q[(size_t)12 * ne + e];
-  h = hb[e];
+                                       int e, const real* phi, real& z, real& u, real& v, real& h) {
+  z = (real)q[e];
+  u = (real)q[(size_t)6 * ne + e];
+  v = (real)q[(size_t)12 * ne + e];
+  h = fourth_mode(q, hb, ne, e, 0);
 #pragma unroll
   for (int k = 1; k < kP2Modes; ++k) {
-    z = z + q[(size_t)k * ne + e] * phi[k];
-    u = u + q[(size_t)(6 + k) * ne + e] * phi[k];
-    v = v + q[(size_t)(12 + k) * ne + e] * phi[k];
-    h = h + hb[(size_t)k * ne + e] * phi[k];
+    z = z + (real)q[(size_t)k * ne + e] * phi[k];
+    u = u + (real)q[(size_t)(6 + k) * ne + e] * phi[k];
+    v = v + (real)q[(size_t)(12 + k) * ne + e] * phi[k];
+    h = h + fourth_mode(q, hb, ne, e, k) * phi[k];
   }
 }
 
@@ -47,71 +63,95 @@ __global__ void __launch_bounds__(128) p2_edges(const __grid_constant__ P2Args A
   const int ed = (int)(w / kP2Egp), I = (int)(w - (long long)ed * kP2Egp);
   const MeshView& m = A.m;
   const Physics& P = A.ph;
-  const BasisP2& B = cB2;
+  const BasisP2T<real>& B = cB2R;
   const int ne = m.ne;
   const int e = A.edges[2 * ed], l = A.edges[2 * ed + 1];
   const unsigned info = m.einfo[e], kind = ei_kind(info, l);
-  const double nx = m.egeo[(size_t)(EGeo::kNx + l) * ne + e], ny = m.egeo[(size_t)(EGeo::kNy + l) * ne + e];
-  double zi, xi, yi, hi;
-  trace6(A.qin, m.hb, ne, e, B.phi_edge[l][I], zi, xi, yi, hi);
-  const double hti = depth<kNonlin>(P, zi, hi);
-  double* o = A.ef + ((size_t)(e * 3 + l) * kP2Egp + I) * 3;
+  const real* G = egeo_r(m);
+  const real nx = G[(size_t)(EGeo::kNx + l) * ne + e], ny = G[(size_t)(EGeo::kNy + l) * ne + e];
+  real* ef = reinterpret_cast<real*>(A.ef);
+  real zi, xi, yi, wi, hi, hti;
+  trace6(A.qin, m.hb, ne, e, B.phi_edge[l][I], zi, xi, yi, wi);
+  trace_depth<kNonlin>(P, zi, wi, hi, hti);
+  real* o = ef + ((size_t)(e * 3 + l) * kP2Egp + I) * 3;
   if (kind == kInterior) {
     const int ex = m.link[(size_t)l * ne + e], lx = (int)ei_nled(info, l), J = kP2Egp - 1 - I;
-    double zx, xx, yx, hx;
-    trace6(A.qin, m.hb, ne, ex, B.phi_edge[lx][J], zx, xx, yx, hx);
-    const double htx = depth<kNonlin>(P, zx, hx);
-    const Flux3 f = llf<kNonlin, double>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, 1.0, 1.0, nx, ny, P.g);
+    real zx, xx, yx, wx, hx, htx;
+    trace6(A.qin, m.hb, ne, ex, B.phi_edge[lx][J], zx, xx, yx, wx);
+    trace_depth<kNonlin>(P, zx, wx, hx, htx);
+    const Flux3T<real> f =
+        llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, real(1), real(1), nx, ny, real(P.g));
     o[0] = f.f; o[1] = f.g; o[2] = f.h;
-    double* ox = A.ef + ((size_t)(ex * 3 + lx) * kP2Egp + J) * 3;
+    real* ox = ef + ((size_t)(ex * 3 + lx) * kP2Egp + J) * 3;
     ox[0] = f.f; ox[1] = f.g; ox[2] = f.h;
     return;
   }
   // ghost state: land reflects the normal momentum (land_edge_hydro.F:201-218);
   // ocean takes the harmonic elevation with the depth-positivity fix
-  // (ocean_edge_hydro.F:148-177, 255-259) and the interior momentum
-  double zx = zi, xx = xi, yx = yi, htx = hti;
+  // (ocean_edge_hydro.F:148-177, 255-259; FP64 in every variant) and the
+  // interior momentum
+  real zx = zi, xx = xi, yx = yi, htx = hti;
   if (kind == kOcean) {
     const int list = m.link[(size_t)l * ne + e];
     double zsum = 0.0;
     for (int f = 0; f < m.nbfr; ++f) {
       const double* zg = A.ocean_zg + ((size_t)f * m.needs + list) * 2;
-      zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * B.xegp[I]);
+      zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * cB2.xegp[I]);
     }
-    if (zsum * P.ifnlfa + hi <= 0) zsum = fabs(hi) + P.h0;
-    zx = zsum;
+    const double hid = hi;
+    if (zsum * P.ifnlfa + hid <= 0) zsum = fabs(hid) + P.h0;
+    zx = (real)zsum;
     htx = depth<kNonlin>(P, zx, hi);
   } else {
-    const double tx = -ny, ty = nx;
-    const double qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
-    const double qne = -qn, qte = qt, den = 1.0 / (nx * ty - ny * tx);
+    const real tx = -ny, ty = nx;
+    const real qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
+    const real qne = -qn, qte = qt, den = real(1) / (nx * ty - ny * tx);
     xx = (ty * qne - ny * qte) * den;
     yx = (-tx * qne + nx * qte) * den;
   }
-  const Flux3 f = llf<kNonlin, double>(P, zi, zx, xi, xx, yi, yx, hi, hi, hti, htx, 1.0, 1.0, nx, ny, P.g);
+  const Flux3T<real> f =
+      llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hi, hti, htx, real(1), real(1), nx, ny, real(P.g));
   o[0] = f.f; o[1] = f.g; o[2] = f.h;
 }
 
 
+// Physics constants in the arithmetic type
+__device__ __forceinline__ PhysR phys_r(const P2Args& A) {
+#ifdef DGSWEM_MIXED
+  const PhysF& p = A.pf;
+#else
+  const Physics& p = A.ph;
+#endif
+  return PhysR{p.g, p.nleq, p.leq, p.nleqg, p.fg_l, p.tau_cap, p.cori, p.fric, p.cf};
+}
+
 // Volume fluxes and sources at area point i of element e (rhs_dg_hydro.F:58-470
 // with six modes): out = fx fy gx gy hx hy sx sy.  q: the element's 18 state
-// values (row 6*var + k), hbe: its six bathymetry modes.
+// values (row 6*var + k) and w its six fourth-row modes (fourth_mode: HB, or
+// the depth modes in the mixed variant), in the arithmetic type.
 template <bool kNonlin>
-__device__ __forceinline__ void p2_volume(const P2Args& A, const double* q, const double* hbe, double drdx,
-                                          double dsdx, double drdy, double dsdy, double hyb, int e, int i,
-                                          double out[8]) {
+__device__ __forceinline__ void p2_volume(const P2Args& A, const real* q, const real* w, real drdx, real dsdx,
+                                          real drdy, real dsdy, real hyb, int e, int i, real out[8]) {
   const MeshView& m = A.m;
   const Physics& P = A.ph;
-  const BasisP2& C = cB2;
+  const PhysR R = phys_r(A);
+  const BasisP2T<real>& C = cB2R;
   const int ne = m.ne;
-  const double NLEQ = kNonlin ? 1.0 : P.nleq, LEQ = kNonlin ? 0.0 : P.leq;
-  const double cori = m.cori ? m.cori[e] : P.cori;
-  double fric = m.fric ? m.fric[e] : P.fric;
-  double zq = q[0], uq = q[6], vq = q[12];
-  double hq = hbe[0] * C.phi_area[0][i];
+#ifdef DGSWEM_MIXED
+  real hbe[kP2Modes];
+#pragma unroll
+  for (int k = 0; k < kP2Modes; ++k) hbe[k] = w[k] - q[k];
+#else
+  const real* hbe = w;
+#endif
+  const real NLEQ = kNonlin ? real(1) : R.nleq, LEQ = kNonlin ? real(0) : R.leq;
+  const real cori = m.cori ? (real)m.cori[e] : R.cori;
+  real fric = m.fric ? (real)m.fric[e] : R.fric;
+  real zq = q[0], uq = q[6], vq = q[12];
+  real hq = hbe[0] * C.phi_area[0][i];
 #pragma unroll
   for (int k = 1; k < kP2Modes; ++k) hq = hq + hbe[k] * C.phi_area[k][i];
-  double dhx = 0, dhy = 0;
+  real dhx = 0, dhy = 0;
 #pragma unroll
   for (int k = 0; k < kP2Modes; ++k) {
     dhx = dhx + hbe[k] * (C.drphi[k][i] * drdx + C.dsphi[k][i] * dsdx);
@@ -123,49 +163,57 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const double* q, cons
     uq = uq + q[6 + k] * C.phi_area[k][i];
     vq = vq + q[12 + k] * C.phi_area[k][i];
   }
-  const double depth = zq + hq;
-  const double f1 = kNonlin ? 1.0 : NLEQ + LEQ * hq;
-  const double fx = uq * f1 * 1.0, fy = vq * f1;
-  const double fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
-  const double fg = P.nleqg * zq * 1;
-  const double fh = 1.0 / (kNonlin ? depth : NLEQ * depth + LEQ);
-  const double u = uq * fh, v = vq * fh;
-  const double huu = fu * u, hvv = fv * v, huv = fu * v;
-  const double gh2 = kNonlin ? fg * (0.5 * zq + hq) : fg * (0.5 * zq + hq) + P.fg_l * zq;
-  const double gx = (huu + gh2) * 1.0, gy = huv;
-  const double hx = huv * 1.0, hy = hvv + gh2;
+#ifdef DGSWEM_MIXED
+  // the depth from the depth modes (a thin column keeps FP32 relative accuracy)
+  real depth = w[0] * C.phi_area[0][i];
+#pragma unroll
+  for (int k = 1; k < kP2Modes; ++k) depth = depth + w[k] * C.phi_area[k][i];
+  if (!kNonlin) depth = zq + hq;
+#else
+  const real depth = zq + hq;
+#endif
+  const real f1 = kNonlin ? real(1) : NLEQ + LEQ * hq;
+  const real fx = uq * f1 * real(1), fy = vq * f1;
+  const real fu = kNonlin ? uq : NLEQ * uq, fv = kNonlin ? vq : NLEQ * vq;
+  const real fg = R.nleqg * zq * 1;
+  const real fh = real(1) / (kNonlin ? depth : NLEQ * depth + LEQ);
+  const real u = uq * fh, v = vq * fh;
+  const real huu = fu * u, hvv = fv * v, huv = fu * v;
+  const real gh2 = kNonlin ? fg * (real(0.5) * zq + hq) : fg * (real(0.5) * zq + hq) + R.fg_l * zq;
+  const real gx = (huu + gh2) * real(1), gy = huv;
+  const real hx = huv * real(1), hy = hvv + gh2;
   if (m.manning) {
-    const double nbar = m.egeo[(size_t)EGeo::kNbar * ne + e];
-    fric = P.g * (nbar * nbar) / cube_root(depth);
-    if (fric < P.cf) fric = P.cf;
+    const real nbar = egeo_r(m)[(size_t)EGeo::kNbar * ne + e];
+    fric = R.g * (nbar * nbar) / cube_root(depth);
+    if (fric < R.cf) fric = R.cf;
   }
-  double tau = fric;
+  real tau = fric;
   if (P.iflinbf == 0) {
-    const double umag = sqrt(u * u + v * v);
+    const real umag = sqrt(u * u + v * v);
     tau = tau * umag * fh;
     if (P.ifhybf == 1) tau = tau * hyb;
-    tau = fmin(tau, P.tau_cap);
+    tau = fmin(tau, R.tau_cap);
   }
-  double sx = -(tau * uq) + fg * dhx * 1.0 + cori * vq;
-  double sy = -(tau * vq) + fg * dhy - cori * uq;
+  real sx = -(tau * uq) + fg * dhx * real(1) + cori * vq;
+  real sy = -(tau * vq) + fg * dhy - cori * uq;
   if (P.nws != 0) {
     // met_forcing.F:49-66: the nodal fields scaled by the stage's ramp
-    const double drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
-    double dpsidx[3], dpsidy[3];
+    const real drpsi[3] = {-0.5, 0.5, 0.0}, dspsi[3] = {-0.5, 0.0, 0.5};
+    real dpsidx[3], dpsidy[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
       dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
     }
-    const double fw = 1.0 / f1, r = A.ramp ? *A.ramp : A.rampdg;
+    const real fw = real(1) / f1, r = (real)(A.ramp ? *A.ramp : A.rampdg);
     const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
-    const double wx0 = r * A.wsx[n0], wx1 = r * A.wsx[n1], wx2 = r * A.wsx[n2];
-    const double wy0 = r * A.wsy[n0], wy1 = r * A.wsy[n1], wy2 = r * A.wsy[n2];
-    const double p0 = r * A.pr[n0], p1 = r * A.pr[n1], p2 = r * A.pr[n2];
+    const real wx0 = r * (real)A.wsx[n0], wx1 = r * (real)A.wsx[n1], wx2 = r * (real)A.wsx[n2];
+    const real wy0 = r * (real)A.wsy[n0], wy1 = r * (real)A.wsy[n1], wy2 = r * (real)A.wsy[n2];
+    const real p0 = r * (real)A.pr[n0], p1 = r * (real)A.pr[n1], p2 = r * (real)A.pr[n2];
     sx = sx + fw * (wx0 * C.psi[0][i] + wx1 * C.psi[1][i] + wx2 * C.psi[2][i]) -
-         P.g * 1.0 * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
+         R.g * real(1) * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
     sy = sy + fw * (wy0 * C.psi[0][i] + wy1 * C.psi[1][i] + wy2 * C.psi[2][i]) -
-         P.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
+         R.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
   }
   out[0] = fx; out[1] = fy; out[2] = gx; out[3] = gy;
   out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
@@ -188,48 +236,54 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
   if (e >= A.ne_act) return;
   const MeshView& m = A.m;
   const Physics& P = A.ph;
-  const BasisP2& B = cB2;
+  const BasisP2T<real>& B = cB2R;
   const int ne = m.ne;
-  double q[3 * kP2Modes], hbe[kP2Modes];
+  const real* G = egeo_r(m);
+  const real* ef = reinterpret_cast<const real*>(A.ef);
+  real q[3 * kP2Modes], wm[kP2Modes];
 #pragma unroll
-  for (int c = 0; c < 3 * kP2Modes; ++c) q[c] = A.qin[(size_t)c * ne + e];
+  for (int c = 0; c < 3 * kP2Modes; ++c) q[c] = (real)A.qin[(size_t)c * ne + e];
 #pragma unroll
-  for (int k = 0; k < kP2Modes; ++k) hbe[k] = m.hb[(size_t)k * ne + e];
-  const double drdx = m.egeo[(size_t)EGeo::kDrdx * ne + e], dsdx = m.egeo[(size_t)EGeo::kDsdx * ne + e];
-  const double drdy = m.egeo[(size_t)EGeo::kDrdy * ne + e], dsdy = m.egeo[(size_t)EGeo::kDsdy * ne + e];
-  double hyb = 1.0;
+  for (int k = 0; k < kP2Modes; ++k) wm[k] = fourth_mode(A.qin, m.hb, ne, e, k);
+  const real drdx = G[(size_t)EGeo::kDrdx * ne + e], dsdx = G[(size_t)EGeo::kDsdx * ne + e];
+  const real drdy = G[(size_t)EGeo::kDrdy * ne + e], dsdy = G[(size_t)EGeo::kDsdy * ne + e];
+  real hyb = 1;
   if (P.iflinbf == 0 && P.ifhybf == 1) {
-    const double depth_c = hbe[0] + q[0];
-    const double fh_c = 1.0 / (kNonlin ? depth_c : P.nleq * depth_c + P.leq);
-    hyb = pow(1.0 + pow(P.hbreak * fh_c, P.ftheta), P.fgamma / P.ftheta);
+#ifdef DGSWEM_MIXED
+    const real depth_c = wm[0];  // depth mode 1
+#else
+    const real depth_c = wm[0] + q[0];
+#endif
+    const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
+    hyb = pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
   }
   // all three variables' sums at once (no per-point volume array): each
   // (variable, mode) sum takes the same terms in the same order as above
   const unsigned info = m.einfo[e];
-  double rhs[3][kP2Modes], isum[3][kP2Modes];
+  real rhs[3][kP2Modes], isum[3][kP2Modes];
 #pragma unroll
   for (int V = 0; V < 3; ++V)
 #pragma unroll
-    for (int k = 0; k < kP2Modes; ++k) { rhs[V][k] = 0.0; isum[V][k] = 0.0; }
+    for (int k = 0; k < kP2Modes; ++k) { rhs[V][k] = 0; isum[V][k] = 0; }
   for (int s = 0; s < 3; ++s) {
     const int l = ei_order(info, s);
     const unsigned kind = ei_kind(info, l);
     if (kind == kNone) continue;
-    const double* ef = A.ef + (size_t)(e * 3 + l) * kP2Egp * 3;
+    const real* efl = ef + (size_t)(e * 3 + l) * kP2Egp * 3;
     if (kind == kInterior) {
       const bool is_in = ei_flag(info, l) != 0;
-      const double edfac = m.egeo[(size_t)(EGeo::kEdfac + l) * ne + e];
-      double acc[3][kP2Modes];
+      const real edfac = G[(size_t)(EGeo::kEdfac + l) * ne + e];
+      real acc[3][kP2Modes];
 #pragma unroll
       for (int V = 0; V < 3; ++V)
 #pragma unroll
-        for (int k = 0; k < kP2Modes; ++k) acc[V][k] = 0.0;
+        for (int k = 0; k < kP2Modes; ++k) acc[V][k] = 0;
       for (int I = 0; I < kP2Egp; ++I) {
         const int j = is_in ? I : kP2Egp - 1 - I;
-        const double v0 = ef[j * 3], v1 = ef[j * 3 + 1], v2 = ef[j * 3 + 2];
+        const real v0 = efl[j * 3], v1 = efl[j * 3 + 1], v2 = efl[j * 3 + 2];
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) {
-          const double wk = edfac * B.edgeq[l][j][k];
+          const real wk = edfac * B.edgeq[l][j][k];
           if (is_in) {
             acc[0][k] = acc[0][k] - wk * v0;
             acc[1][k] = acc[1][k] - wk * v1;
@@ -246,13 +300,13 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) isum[V][k] = isum[V][k] + acc[V][k];
     } else {
-      const double areas = m.egeo[(size_t)EGeo::kAreas * ne + e];
-      const double xlen = m.egeo[(size_t)(EGeo::kXlen + l) * ne + e];
+      const real areas = G[(size_t)EGeo::kAreas * ne + e];
+      const real xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
       for (int I = 0; I < kP2Egp; ++I) {
-        const double v0 = ef[I * 3], v1 = ef[I * 3 + 1], v2 = ef[I * 3 + 2];
+        const real v0 = efl[I * 3], v1 = efl[I * 3 + 1], v2 = efl[I * 3 + 2];
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) {
-          const double wk = 2.0 * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
+          const real wk = real(2) * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
           rhs[0][k] = rhs[0][k] - wk * v0;
           rhs[1][k] = rhs[1][k] - wk * v1;
           rhs[2][k] = rhs[2][k] - wk * v2;
@@ -265,29 +319,30 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
 #pragma unroll
     for (int k = 0; k < kP2Modes; ++k) rhs[V][k] = rhs[V][k] + isum[V][k];  // add_internal_flux
   if (P.rainfall == 1) {
-    const double src = 7.0556e-6;
+    const real src = real(7.0556e-6);
     for (int i = 0; i < kP2Agp; ++i)
 #pragma unroll
       for (int k = 0; k < kP2Modes; ++k) rhs[0][k] = rhs[0][k] + B.srfac[k][i] * src;
   }
   for (int i = 0; i < kP2Agp; ++i) {
-    double vol[8];
-    p2_volume<kNonlin>(A, q, hbe, drdx, dsdx, drdy, dsdy, hyb, e, i, vol);
+    real vol[8];
+    p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, e, i, vol);
     rhs[1][0] = rhs[1][0] + B.srfac[0][i] * vol[6];
     rhs[2][0] = rhs[2][0] + B.srfac[0][i] * vol[7];
 #pragma unroll
     for (int k = 1; k < kP2Modes; ++k) {
-      const double dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
-      const double dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
-      const double xf = B.mw[k][i] * dpx;
-      const double yf = B.mw[k][i] * dpy;
-      const double sr = B.srfac[k][i];
+      const real dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
+      const real dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
+      const real xf = B.mw[k][i] * dpx;
+      const real yf = B.mw[k][i] * dpy;
+      const real sr = B.srfac[k][i];
       rhs[0][k] = rhs[0][k] + xf * vol[0] + yf * vol[1];
       rhs[1][k] = rhs[1][k] + xf * vol[2] + yf * vol[3] + sr * vol[6];
       rhs[2][k] = rhs[2][k] + xf * vol[4] + yf * vol[5] + sr * vol[7];
     }
   }
-  // SSP-RK combination (DG_hydro_timestep.F:238-290); zero coefficients skipped
+  // SSP-RK combination (DG_hydro_timestep.F:238-290) in FP64; zero
+  // coefficients skipped
   bool bad = false;
   const bool hist0 = A.irk > 1;
 #pragma unroll
@@ -295,9 +350,9 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
 #pragma unroll
     for (int k = 0; k < kP2Modes; ++k) {
       const int c = kP2Modes * V + k;
-      const double rk = rhs[V][k];
+      const double rk = (double)rhs[V][k];
       if (A.rout) A.rout[(size_t)c * ne + e] = rk;
-      const double qc = q[c];
+      const double qc = A.qin[(size_t)c * ne + e];
       double acc = 0.0;
       if (hist0) {
         if (A.a[0] != 0.0) acc = acc + A.a[0] * A.qhist[0][(size_t)c * ne + e];
@@ -379,7 +434,14 @@ __global__ void p2_soa_to_fortran(const double* __restrict__ q, double* __restri
   for (int k = 0; k < kP2Modes; ++k) f[(size_t)kP2Modes * e + k] = q[(size_t)(kP2Modes * var + k) * ne + i];
 }
 
-void set_basis_p2(const BasisP2& b) { cudaMemcpyToSymbol(cB2, &b, sizeof(b)); }
+void set_basis_p2(const BasisP2& b) {
+  cudaMemcpyToSymbol(cB2, &b, sizeof(b));
+  BasisP2T<real> r;
+  const double* src = reinterpret_cast<const double*>(&b);
+  real* dst = reinterpret_cast<real*>(&r);
+  for (size_t i = 0; i < sizeof(b) / sizeof(double); ++i) dst[i] = (real)src[i];
+  cudaMemcpyToSymbol(cB2R, &r, sizeof(r));
+}
 
 void launch_p2_stage(const P2Args& a, bool nonlin, cudaStream_t s) {
   const unsigned ge = (unsigned)(((long long)kP2Egp * a.nedge + 127) / 128);

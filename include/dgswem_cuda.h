@@ -124,7 +124,7 @@ typedef struct dgswem_cuda dgswem_cuda;
 
 /* Copies the setup to GPU `device` and builds the device layout.
  * Replaces the state the reference keeps in module arrays after PREP_DG
- * (src/dgswem.F:196).  DOFH = 6 makes a p=2 handle (FP64, fast or strict):
+ * (src/dgswem.F:196).  DOFH = 6 makes a p=2 handle (strict, fast or mixed):
  * no slope limiter and no wetting/drying (p=1 only in the reference), land,
  * ocean and interior edges, ICS=1, a whole-mesh handle; its interior-edge
  * sums run over all six modes (the reference's p=2 sums modes 1-3 only).

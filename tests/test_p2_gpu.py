@@ -1,7 +1,9 @@
 """The p=2 device path (GPU) against the oracle's p=2, which is checked by
 its convergence order (test_oracle_p2_convergence.py): the strict variant
-bit for bit, the fast one within 1e-10 relative; its own convergence order;
-and the p=1-only features rejected on a p=2 handle."""
+bit for bit, the fast one within 1e-10 relative, the mixed-precision one
+within the mixed form's elevation bar (1e-5 m) with water volume to
+round-off; its own convergence order; and the p=1-only features rejected on
+a p=2 handle."""
 import math
 
 import numpy as np
@@ -29,9 +31,9 @@ def standing_wave_state(path, nx):
     return orc, ze, np.zeros_like(ze), (px, wphys, phi)
 
 
-def run_pair(path, nsteps, strict, state=None, met=None):
+def run_pair(path, nsteps, strict, state=None, met=None, mixed=False):
     orc = Oracle(path)
-    with HydroStep(Deck(path), strict=strict) as hs:
+    with HydroStep(Deck(path), strict=None if mixed else strict, mixed=mixed) as hs:
         assert hs.dofh == 6
         if state is not None:
             wd = np.ones(hs.ne, np.int32)
@@ -87,6 +89,28 @@ def test_p2_fast_vs_oracle(built, scratch):
             assert np.abs(a - b).max() / scale <= 1e-10, f"{name}: {v}"
 
 
+def test_p2_mixed_vs_oracle(built, scratch):
+    """Mixed precision at p=2 (FP32 traces, fluxes, volume terms and sums;
+    FP64 state and SSP): nodal elevation within 1e-5 m of the FP64 oracle,
+    element means within 1e-5 m, water volume within 1e-12 relative."""
+    for name, path, n, state, met in decks_p2(scratch):
+        g, o, gn, on = run_pair(path, n, False, state, wind(path) if met else None, mixed=True)
+        d = Deck(path)
+        ne = d.s.ne
+        nm = d.int_array("nm", 3 * ne).reshape(3, ne) - 1
+        x, y = d.real_array("x", d.s.np), d.real_array("y", d.s.np)
+        hb = d.real_array("hb", 6 * ne).reshape(ne, 6)
+        a, b, c = nm
+        area = 0.5 * ((x[a] - x[c]) * (y[b] - y[c]) + (x[c] - x[b]) * (y[a] - y[c]))
+        d.close()
+        eta = np.abs(gn[0] - on[0]).max()
+        mean = np.abs(g[0][:, 0] - o[0][:, 0]).max()
+        vg, vo = np.sum((g[0][:, 0] + hb[:, 0]) * area), np.sum((o[0][:, 0] + hb[:, 0]) * area)
+        print(f"p=2 mixed, {name}: nodal eta {eta:.2e} m, mean {mean:.2e} m, volume {(vg - vo) / vo:.2e}")
+        assert eta <= 1e-5 and mean <= 1e-5, name
+        assert abs(vg - vo) <= 1e-12 * abs(vo), name
+
+
 def test_p2_convergence_order_on_device(built, scratch):
     errs = []
     for nx in (8, 16, 32):
@@ -110,8 +134,6 @@ def test_p2_rejects_p1_only_features(built, scratch):
                      lambda: _abi.check(hs._lib.dgswem_cuda_state_save(hs._h, 0))):
             with pytest.raises(DgswemError, match="p=1 only"):
                 call()
-    with pytest.raises(DgswemError, match="p=1 only"):
-        HydroStep(Deck(path), mixed=True)
     lim = decks.quarter_annulus(scratch / "p2_lim", nr=4, nth=8, nsteps=2, slopeflag=5, **P2)
     with pytest.raises(DgswemError, match="p = 1 only"):
         Deck(lim)
