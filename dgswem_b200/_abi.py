@@ -70,6 +70,8 @@ SIGNATURES = {
                                           C.POINTER(C.c_void_p)]),
     "dgswem_cuda_part_info": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     "dgswem_cuda_stage_rhs": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dgswem_cuda_stage_rhs_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "dgswem_cuda_tile_split": (C.c_int, [C.c_void_p, _ip, _ip]),
     "dgswem_cuda_stage_limit": (C.c_int, [C.c_void_p, C.c_int]),
     "dgswem_cuda_step_end": (C.c_int, [C.c_void_p]),
     "dgswem_cuda_halo_count": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _ip, _ip]),

@@ -346,6 +346,11 @@ struct dgswem_cuda {
   DevBuf<unsigned> einfo, eslot, tile_tasks;
   DevBuf<int> tile_elem_ptr, tile_task_ptr, tile_halo_ptr, tile_halo;
   int ntile = 0;
+  // tiles that read no ghost element and no internal-barrier side first
+  // (n_tile_interior of them), then the others: the stage can start on the
+  // former while the halo exchange that refreshes the ghosts is in flight
+  DevBuf<int> tile_order;
+  int n_tile_interior = 0;
   // shape of the stage tiles (kTileShapes) and of the limiter blocks
   // (kLimitBlocks): the defaults, or set / picked by dgswem_cuda_autotune
   int tile_shape = kDefaultTileShape, limit_shape = kDefaultLimitShape;
@@ -645,6 +650,19 @@ void build_tile_plan(dgswem_cuda* h, int n_tiled, int ne, const std::vector<int>
   for (int t = 0; t < ntile; ++t) {
     tasks.insert(tasks.end(), ttasks[t].begin(), ttasks[t].end());
     halo.insert(halo.end(), thalo[t].begin(), thalo[t].end());
+  }
+  {
+    std::vector<int> order, rest;
+    for (int t = 0; t < ntile; ++t) {
+      bool interior = true;
+      for (int g : thalo[t]) interior = interior && g < n_tiled;
+      for (size_t i = 0; i < ttasks[t].size(); i += 2)
+        interior = interior && (ttasks[t][i] & 7u) != kIBarrier;
+      (interior ? order : rest).push_back(t);
+    }
+    h->n_tile_interior = (int)order.size();
+    order.insert(order.end(), rest.begin(), rest.end());
+    h->tile_order.upload(order.empty() ? std::vector<int>(1, 0) : order);
   }
   h->ntile = ntile;
   h->tile_elem_ptr.upload(elem_ptr);
@@ -1087,7 +1105,12 @@ void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing, con
   t.done();
 }
 
-void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, const double* ramp = nullptr) {
+// Tiles of a stage launch (dgswem_cuda_stage_rhs_tiles): all, those that read
+// no ghost (interior), or the others (boundary)
+enum TileSet { kAllTiles = 0, kInteriorTiles = 1, kBoundaryTiles = 2 };
+
+void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, const double* ramp = nullptr,
+                      TileSet set = kAllTiles) {
   if (h->v2) {
     launch_stage_p2(h, it, irk, forcing, ramp);
     return;
@@ -1122,14 +1145,20 @@ void launch_stage_rhs(dgswem_cuda* h, int it, int irk, const double* forcing, co
   A.ib_rhs = h->ib_rhs.p;
   A.err = h->err.p;
   const bool nonlin = h->ph.nleq == 1.0 && h->ph.leq == 0.0;
-  if (h->mesh.nibseg > 0) {
+  if (h->mesh.nibseg > 0 && set != kInteriorTiles) {  // interior tiles have no barrier sides
     LaunchTimer t(h, 3);
     h->v->ibarrier(A, nonlin, h->stream);
     t.done();
   }
-  {
+  unsigned grid = (unsigned)h->ntile;
+  if (set != kAllTiles) {
+    A.tile_list = h->tile_order.p;
+    A.tile_off = set == kInteriorTiles ? 0 : h->n_tile_interior;
+    grid = set == kInteriorTiles ? (unsigned)h->n_tile_interior : (unsigned)(h->ntile - h->n_tile_interior);
+  }
+  if (grid > 0) {
     LaunchTimer t(h, 0);
-    h->v->stage(A, nonlin, h->tile_shape, (unsigned)h->ntile, h->stage_smem, h->stream);
+    h->v->stage(A, nonlin, h->tile_shape, grid, h->stage_smem, h->stream);
     t.done();
   }
 }
@@ -1896,12 +1925,19 @@ int dgswem_cuda_modal2nodal_noalloc(dgswem_cuda* h, double* eta2, double* uu2, d
   });
 }
 
-int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) {
+int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) { return dgswem_cuda_stage_rhs_tiles(h, it, irk, 0); }
+
+int dgswem_cuda_stage_rhs_tiles(dgswem_cuda* h, int it, int irk, int tiles) {
   return guarded([&]() {
     need_p1(h, "dgswem_cuda_stage_rhs");
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
     if (irk < 1 || irk > h->nrk) throw Failure(DGSWEM_ERR_ARG, "stage out of range");
+    if (tiles < 0 || tiles > 2) throw Failure(DGSWEM_ERR_ARG, "tiles must be 0 (all), 1 (interior) or 2 (boundary)");
     DG_CUDA(cudaSetDevice(h->device));
+    if (tiles == kBoundaryTiles) {  // the stage's forcing was uploaded by its interior launch
+      launch_stage_rhs(h, it, irk, h->forcing_per_stage ? h->forcing_dev.p : nullptr, nullptr, kBoundaryTiles);
+      return;
+    }
     const double* dev = nullptr;
     if (h->forcing_per_stage) {  // this stage's boundary forcing, host cos, one small copy
       if (h->forcing_copied) DG_CUDA(cudaEventSynchronize(h->forcing_copied));
@@ -1914,7 +1950,16 @@ int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk) {
       dev = h->forcing_dev.p;
     }
     if (h->met) met_stage(h);
-    launch_stage_rhs(h, it, irk, dev);
+    launch_stage_rhs(h, it, irk, dev, nullptr, (TileSet)tiles);
+  });
+}
+
+int dgswem_cuda_tile_split(const dgswem_cuda* h, int* n_interior, int* n_boundary) {
+  return guarded([&]() {
+    if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
+    need_p1(h, "dgswem_cuda_tile_split");
+    if (n_interior) *n_interior = h->n_tile_interior;
+    if (n_boundary) *n_boundary = h->ntile - h->n_tile_interior;
   });
 }
 

@@ -233,6 +233,10 @@ struct StageArgs {
   const double* __restrict__ pr;
   double* ib_rhs;                           // [(2*seg + side)*9 + c] internal-barrier terms
   unsigned* err;                            // device error word
+  // tiles of this launch: block b runs tile tile_list[tile_off + b], or
+  // tile b when tile_list is null (all tiles)
+  const int* __restrict__ tile_list;
+  int tile_off;
 };
 
 struct LimitArgs {

@@ -762,7 +762,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   const Physics& P = A.ph;
   const int ne = m.ne;
   const int tid = threadIdx.x;
-  const int tile = blockIdx.x;
+  const int tile = A.tile_list ? A.tile_list[A.tile_off + (int)blockIdx.x] : (int)blockIdx.x;
   const int tile0 = m.tile_elem_ptr[tile];
   const int n = m.tile_elem_ptr[tile + 1] - tile0;
   const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;

@@ -303,8 +303,19 @@ class HydroStep:
         _abi.check(self._lib.dgswem_cuda_part_info(self._h, *[C.byref(x) for x in v]))
         return dict(zip(("part", "nparts", "owned", "local"), (x.value for x in v)))
 
-    def stage_rhs(self, it: int, irk: int) -> None:
-        _abi.check(self._lib.dgswem_cuda_stage_rhs(self._h, int(it), int(irk)))
+    TILES = {"all": 0, "interior": 1, "boundary": 2}
+
+    def stage_rhs(self, it: int, irk: int, tiles: str = "all") -> None:
+        """One stage's right-hand side and SSP update of the owned elements;
+        tiles="interior" / "boundary" splits it in the two launches of
+        dgswem_cuda_stage_rhs_tiles (interior first, then boundary)."""
+        _abi.check(self._lib.dgswem_cuda_stage_rhs_tiles(self._h, int(it), int(irk), self.TILES[tiles]))
+
+    def tile_split(self) -> tuple[int, int]:
+        """(interior, boundary) tile counts of the stage launches."""
+        a, b = C.c_int(), C.c_int()
+        _abi.check(self._lib.dgswem_cuda_tile_split(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def stage_limit(self, irk: int) -> None:
         _abi.check(self._lib.dgswem_cuda_stage_limit(self._h, int(irk)))
@@ -366,9 +377,15 @@ class PartitionedRun:
 
     HALO_WIDTH = (3, 10)  # doubles per element of halo kinds 0 and 1
 
-    def __init__(self, setup, nparts: int, devices=None, strict: bool | None = None, mixed: bool = False):
+    def __init__(self, setup, nparts: int, devices=None, strict: bool | None = None, mixed: bool = False,
+                 overlap: bool = False):
+        """overlap=True runs each stage after the first as two launches around
+        the exchange that precedes it -- the tiles that read no ghost before
+        the halo moves, the others after -- the order DistributedPartition
+        uses to hide the transfer (bit-identical to the plain order)."""
         import torch
         self._torch = torch
+        self.overlap = bool(overlap)
         self.nparts = int(nparts)
         self.devices = list(devices) if devices is not None else [0] * self.nparts
         if len(self.devices) != self.nparts:
@@ -430,11 +447,15 @@ class PartitionedRun:
     def timestep(self, it: int) -> None:
         for irk in range(1, self.nrk + 1):
             for hs in self.parts:
-                hs.stage_rhs(it, irk)
+                hs.stage_rhs(it, irk, "boundary" if self.overlap and irk > 1 else "all")
             if self.slopeflag != 0:
                 self._exchange(0, irk)
             for hs in self.parts:
                 hs.stage_limit(irk)
+            if self.overlap and irk < self.nrk:
+                # the next stage's interior tiles before the halo moves
+                for hs in self.parts:
+                    hs.stage_rhs(it, irk + 1, "interior")
             self._exchange(1, irk)
         for hs in self.parts:
             hs.step_end()
@@ -477,13 +498,19 @@ class DistributedPartition:
     TRANSPORTS = ("nccl", "host")
 
     def __init__(self, setup, strict: bool | None = None, group=None, mixed: bool = False,
-                 transport: str = "nccl"):
+                 transport: str = "nccl", overlap: bool = True):
+        """overlap: each stage after the first runs its tiles that read no
+        ghost while the exchange before it is in flight (NCCL: on the stream,
+        concurrent with the transfer; host: on the GPU while the host sends
+        and receives), the others after the unpack; bit-identical to the
+        plain order."""
         import torch
         import torch.distributed as dist
         if transport not in self.TRANSPORTS:
             raise ValueError(f"transport must be one of {self.TRANSPORTS}")
         self._torch, self._dist, self._group = torch, dist, group
         self.transport = transport
+        self.overlap = bool(overlap)
         self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
         dev = torch.cuda.current_device()
         self.hs = HydroStep(setup, device=dev, strict=strict, part=self.rank, nparts=self.world, mixed=mixed)
@@ -514,7 +541,10 @@ class DistributedPartition:
     def __exit__(self, *exc):
         self.close()
 
-    def _exchange(self, kind: int, irk: int) -> None:
+    def _exchange(self, kind: int, irk: int, between=None) -> None:
+        """Pack, move and unpack halo kind ``kind`` of stage buffer ``irk``;
+        ``between()`` launches work that reads no ghost while the halo is in
+        flight."""
         dist = self._dist
         bufs = [(q, b) for (k, q), b in sorted(self.buf.items()) if k == kind]
         for q, (snd, _, ns, _, _, _) in bufs:
@@ -527,9 +557,11 @@ class DistributedPartition:
                     ops.append(dist.P2POp(dist.isend, snd, q, self._group))
                 if nr:
                     ops.append(dist.P2POp(dist.irecv, rcv, q, self._group))
-            if ops:
-                for req in dist.batch_isend_irecv(ops):
-                    req.wait()
+            reqs = dist.batch_isend_irecv(ops) if ops else []
+            if between is not None:
+                between()
+            for req in reqs:
+                req.wait()
         else:
             stream = self._torch.cuda.current_stream()
             for q, (snd, _, ns, _, hsnd, _) in bufs:
@@ -542,6 +574,8 @@ class DistributedPartition:
                     reqs.append(dist.isend(hsnd, q, self._group))
                 if nr:
                     reqs.append(dist.irecv(hrcv, q, self._group))
+            if between is not None:
+                between()
             for req in reqs:
                 req.wait()
             for q, (_, rcv, _, nr, _, hrcv) in bufs:
@@ -553,11 +587,14 @@ class DistributedPartition:
 
     def timestep(self, it: int) -> None:
         for irk in range(1, self.nrk + 1):
-            self.hs.stage_rhs(it, irk)
+            self.hs.stage_rhs(it, irk, "boundary" if self.overlap and irk > 1 else "all")
             if self.slopeflag != 0:
                 self._exchange(0, irk)
             self.hs.stage_limit(irk)
-            self._exchange(1, irk)
+            between = None
+            if self.overlap and irk < self.nrk:
+                between = (lambda nxt: lambda: self.hs.stage_rhs(it, nxt, "interior"))(irk + 1)
+            self._exchange(1, irk, between)
         self.hs.step_end()
 
     def run(self, it0: int, nsteps: int) -> None:

@@ -166,6 +166,19 @@ int dgswem_cuda_part_info(const dgswem_cuda* h, int* part, int* nparts, int* n_o
  * (stage buffer irk, 1..NRK), then the limiter and WETDRY of the same stage,
  * then the end of the step (the stage-NRK+1 state becomes the step state). */
 int dgswem_cuda_stage_rhs(dgswem_cuda* h, int it, int irk);
+/* dgswem_cuda_stage_rhs in two launches, so that a partition's stage can
+ * start while the halo exchange that refreshes its ghosts is in flight
+ * (the overlap of the reference's persistent MPI requests,
+ * src/messenger_elem.F:832-980): tiles = 1 runs the stage kernel on the tiles
+ * that read no ghost element and no internal-barrier side (valid as soon as
+ * the previous stage's limiter has run on this partition), tiles = 2 on the
+ * others (after the ghosts are unpacked); tiles = 0 runs all, the same as
+ * dgswem_cuda_stage_rhs.  A stage is either one call with 0 or a call with 1
+ * followed by one with 2; results are bit-identical either way.
+ * dgswem_cuda_tile_split gives the two tile counts.  No counterpart in the
+ * reference's C interface. */
+int dgswem_cuda_stage_rhs_tiles(dgswem_cuda* h, int it, int irk, int tiles);
+int dgswem_cuda_tile_split(const dgswem_cuda* h, int* n_interior, int* n_boundary);
 int dgswem_cuda_stage_limit(dgswem_cuda* h, int irk);
 int dgswem_cuda_step_end(dgswem_cuda* h);
 /* Elements this partition sends to / receives from `peer` for halo `kind`;

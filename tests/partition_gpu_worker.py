@@ -1,7 +1,8 @@
 """One rank of the world-size-2 partitioned run on one GPU (launched by
 test_partition_ranks_gpu.py): the rank steps its partition with
 DistributedPartition, halos staged through pinned host buffers and moved
-over gloo, and saves its owned rows."""
+over gloo (the next stage's ghost-free tiles launched while the host moves
+them, unless overlap is 0), and saves its owned rows."""
 import os
 import sys
 from datetime import timedelta
@@ -13,7 +14,8 @@ ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT))
 
 
-def main(rank: int, world: int, port: int, deck_dir: str, nsteps: int, strict: int, out: str) -> int:
+def main(rank: int, world: int, port: int, deck_dir: str, nsteps: int, strict: int, out: str,
+         overlap: int = 1) -> int:
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     import torch
     import torch.distributed as dist
@@ -21,7 +23,7 @@ def main(rank: int, world: int, port: int, deck_dir: str, nsteps: int, strict: i
     torch.cuda.set_device(0)
     from dgswem_b200 import Deck, DistributedPartition
     deck = Deck(deck_dir)
-    with DistributedPartition(deck, strict=bool(strict), transport="host") as dp:
+    with DistributedPartition(deck, strict=bool(strict), transport="host", overlap=bool(overlap)) as dp:
         info = dp.hs.part_info()
         dp.run(1, nsteps)
         dp.hs.synchronize()
@@ -34,4 +36,4 @@ def main(rank: int, world: int, port: int, deck_dir: str, nsteps: int, strict: i
 
 if __name__ == "__main__":
     sys.exit(main(int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]), sys.argv[4], int(sys.argv[5]),
-                  int(sys.argv[6]), sys.argv[7]))
+                  int(sys.argv[6]), sys.argv[7], int(sys.argv[8]) if len(sys.argv) > 8 else 1))

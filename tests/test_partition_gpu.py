@@ -11,12 +11,12 @@ from dgswem_b200 import Deck, HydroStep, PartitionedRun, decks
 pytestmark = pytest.mark.gpu
 
 
-def single_and_parts(path, nsteps, nparts, strict):
+def single_and_parts(path, nsteps, nparts, strict, overlap=False):
     deck = Deck(path)
     with HydroStep(deck, strict=strict) as hs:
         hs.run(1, nsteps)
         ref = hs.state()
-    with PartitionedRun(deck, nparts, strict=strict) as pr:
+    with PartitionedRun(deck, nparts, strict=strict, overlap=overlap) as pr:
         info = [hs.part_info() for hs in pr.parts]
         assert sum(i["owned"] for i in info) == deck.s.ne
         assert all(i["local"] > i["owned"] for i in info)
@@ -78,3 +78,21 @@ def test_partitions_with_other_tile_shapes(built):
         pr.run(1, 80)
         got = pr.state()
     check_equal(ref, got)
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_overlapped_stage_order(built, scratch, strict):
+    """Each stage after the first split around the exchange before it: the
+    tiles that read no ghost launched before the halo moves, the others
+    after the unpack (the order DistributedPartition uses to overlap the
+    transfer).  Bit-identical to the single handle; internal-barrier tiles
+    count as boundary tiles."""
+    from conftest import golden_dir
+    beach = decks.sloping_beach(scratch / "sb_overlap", nx=60, ny=12, lx=3000.0, ly=600.0, nsteps=100, dt=0.5)
+    for path, n in ((golden_dir("wetdry"), 100), (beach, 100)):
+        deck = Deck(path)
+        with PartitionedRun(deck, 3, strict=strict, overlap=True) as pr:
+            splits = [hs.tile_split() for hs in pr.parts]
+        assert sum(a for a, _ in splits) > 0 and all(b > 0 for _, b in splits), splits
+        ref, got = single_and_parts(path, n, 3, strict, overlap=True)
+        check_equal(ref, got)

@@ -26,12 +26,12 @@ def free_port() -> int:
         return sk.getsockname()[1]
 
 
-def run_two_ranks(path, nsteps, strict, tmp_path):
+def run_two_ranks(path, nsteps, strict, tmp_path, overlap=True):
     port = free_port()
     worker = ROOT / "tests" / "partition_gpu_worker.py"
     outs = [tmp_path / f"rank{r}.npz" for r in range(2)]
     procs = [subprocess.Popen([sys.executable, str(worker), str(r), "2", str(port), str(path), str(nsteps),
-                               str(int(strict)), str(outs[r])]) for r in range(2)]
+                               str(int(strict)), str(outs[r]), str(int(overlap))]) for r in range(2)]
     try:
         for p in procs:
             assert p.wait(timeout=600) == 0
@@ -57,10 +57,12 @@ def single(path, nsteps, strict):
         return hs.state()
 
 
+@pytest.mark.parametrize("overlap", [True, False])
 @pytest.mark.parametrize("case", ["wetdry_golden", "beach"])
-def test_two_ranks_host_transport_bitwise(built, scratch, tmp_path, case):
+def test_two_ranks_host_transport_bitwise(built, scratch, tmp_path, case, overlap):
     """Reference wetdry golden deck (barriers, hybrid friction, wet/dry) and
-    a limiter + Manning sloping beach, strict build."""
+    a limiter + Manning sloping beach, strict build; with and without the
+    overlapped stage order."""
     if case == "wetdry_golden":
         from conftest import golden_dir
         path, n = golden_dir("wetdry"), 100
@@ -68,7 +70,7 @@ def test_two_ranks_host_transport_bitwise(built, scratch, tmp_path, case):
         path, n = decks.sloping_beach(scratch / "sb_ranks", nx=60, ny=12, lx=3000.0, ly=600.0, nsteps=150,
                                       dt=0.5), 150
     ref = single(path, n, True)
-    got = run_two_ranks(path, n, True, tmp_path)
+    got = run_two_ranks(path, n, True, tmp_path, overlap)
     for a, b, name in zip(got, ref, ("ZE", "QX", "QY", "WDFLG")):
         np.testing.assert_array_equal(a, b, err_msg=f"{name} differs from the single-handle run")
     assert 0 < ref[3].sum() < len(ref[3])
