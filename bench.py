@@ -120,13 +120,18 @@ def rank0_first(rank: int, world: int, dist, fn):
 def config3_deck(workdir, nr: int, nth: int, p: int = 1, dramp: float | None = None) -> Path:
     """The config-3 quarter annulus (nr x nth cells, dt = 0.5 s, NWS=1, DG of
     degree p; the tide and wind ramp over ``dramp`` days, the generator's two
-    days by default) under workdir, written unless complete."""
+    days by default) under workdir, written unless complete.  p=1 steps with
+    SSP-RK(2,2); p=2 with SSP-RK(3,3): DG of degree 2 needs a third-order RK
+    for linear stability (with RK2 the p=2 run grows without bound, which
+    5000 steps of a quickly ramped tide show)."""
     from dgswem_b200 import decks
     path = Path(workdir) / (f"config3_{nr}x{nth}" + ("" if p == 1 else f"_p{p}") +
                             ("" if dramp is None else f"_ramp{dramp:g}"))
     done = path / ".complete"
     if not done.exists():
         kw = {} if dramp is None else {"dramp": dramp}
+        if p == 2:
+            kw.update(rk_stage=3, rk_order=3)
         decks.quarter_annulus(path, nr=nr, nth=nth, nsteps=5000, dt=0.5, nws=1, extra={"pl": p, "ph": p}, **kw)
         done.write_text("ok\n")
     return path
