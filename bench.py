@@ -64,11 +64,11 @@ STEP_BYTES_PER_ELEMENT_STAGE = STAGE_KERNEL_BYTES + 12 + 24
 # tasks of 8 bytes and 0.25 halo ids per element on the Morton-ordered mesh)
 # and the packed edge kinds / task slots
 STAGE_OVERHEAD_BYTES = {"geometry_rows_beyond_model": 112 - 48, "tile_plan": 14, "edge_info": 8}
-# DRAM bytes per element of one stage_p1 launch, dram__bytes_read.sum +
-# dram__bytes_write.sum from ncu on the same deck at 999,492 elements: the
-# mean of a stage-1 (291.6) and a stage-2 (364.0) launch; traffic grows with
-# the element count.
-STAGE_TRAFFIC_BYTES = 0.5 * (291.6 + 364.0)
+# DRAM bytes per element of one stage_p1 launch (strict build),
+# dram__bytes_read.sum + dram__bytes_write.sum from ncu on the same deck at
+# 999,492 elements: the mean of a stage-1 (292.0) and a stage-2 (367.4)
+# launch; traffic grows with the element count.
+STAGE_TRAFFIC_BYTES = 0.5 * (292.0 + 367.4)
 
 
 def rank_env():
