@@ -303,13 +303,19 @@ struct P2Variant {
   void (*modal2nodal)(const MeshView&, const double*, double, double, double*, double*, double*, int*,
                       cudaStream_t);
   void (*layout)(bool, const double*, double*, int, int, const int*, cudaStream_t);
+  size_t (*tile_smem)(int, int);
 };
 static const P2Variant kFastP2 = {fast_p2::set_basis_p2, fast_p2::launch_p2_stage, fast_p2::launch_p2_modal2nodal,
-                                  fast_p2::launch_p2_layout};
+                                  fast_p2::launch_p2_layout, fast_p2::p2_tile_smem};
 static const P2Variant kStrictP2 = {strict_p2::set_basis_p2, strict_p2::launch_p2_stage,
-                                    strict_p2::launch_p2_modal2nodal, strict_p2::launch_p2_layout};
+                                    strict_p2::launch_p2_modal2nodal, strict_p2::launch_p2_layout,
+                                    strict_p2::p2_tile_smem};
 static const P2Variant kMixedP2 = {mixed_p2::set_basis_p2, mixed_p2::launch_p2_stage,
-                                   mixed_p2::launch_p2_modal2nodal, mixed_p2::launch_p2_layout};
+                                   mixed_p2::launch_p2_modal2nodal, mixed_p2::launch_p2_layout,
+                                   mixed_p2::p2_tile_smem};
+// the tile plan a p=2 handle's tile kernel runs on: tiles of 64 elements
+// (kTileShapes[kP2PlanShape]), the p=2 kernel's tile
+constexpr int kP2PlanShape = 1;
 
 }  // namespace dgswem
 
@@ -362,6 +368,9 @@ struct dgswem_cuda {
   DevBuf<int> p2_edges;
   DevBuf<double> p2_ef;
   int p2_nedge = 0;
+  // the p=2 stage runs as the tile kernel (p2_tile) when its shared memory
+  // fits, else as the edge + element kernel pair through p2_ef
+  bool p2_tiled = false;
   DevBuf<double> emo_dg, efa_dg, qnam_dg, qnph_dg, ebht, ebcfsp, ibht, ibcfsb, ibcfsp;
   DevBuf<double> wsx, wsy, pr, minmax, staging;
   std::vector<DevBuf<double>> q;    // nrk+1 stage buffers, 9*NE each
@@ -1098,10 +1107,11 @@ void launch_stage_p2(dgswem_cuda* h, int it, int irk, const double* forcing, con
   A.nedge = h->p2_nedge;
   A.ne_act = h->n_own;
   A.err = h->err.p;
+  A.ntile = h->p2_tiled ? h->ntile : 0;
   const bool nonlin = h->ph.nleq == 1.0 && h->ph.leq == 0.0;
   LaunchTimer t(h, 0);
   h->v2->stage(A, nonlin, h->stream);
-  ++h->launches;  // two kernels
+  if (!A.ntile) ++h->launches;  // the edge + element kernel pair
   t.done();
 }
 
@@ -1582,8 +1592,10 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     // the strict kernels unless the fast or the mixed form is asked for
     h->v = (flags & DGSWEM_CUDA_FAST) ? &kFast : (flags & DGSWEM_CUDA_MIXED) ? &kMixed : &kStrict;
     h->dofh = s->dofh;
-    if (h->dofh == kP2Modes)
+    if (h->dofh == kP2Modes) {
       h->v2 = (flags & DGSWEM_CUDA_FAST) ? &kFastP2 : (flags & DGSWEM_CUDA_MIXED) ? &kMixedP2 : &kStrictP2;
+      h->tile_shape = kP2PlanShape;
+    }
     h->ne = s->ne;
     h->np = s->np;
     h->nrk = s->nrk;
@@ -1649,8 +1661,14 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
         }
       h->p2_nedge = (int)edges.size() / 2;
       h->p2_edges.upload(edges.empty() ? std::vector<int>(2, 0) : edges);
-      h->p2_ef.alloc((size_t)3 * kP2Egp * 3 * h->ne);  // slots of edges in no list stay zero
-      DG_CUDA(cudaMemset(h->p2_ef.p, 0, h->p2_ef.n * sizeof(double)));
+      int dev_smem = 0;
+      DG_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+      h->p2_tiled = h->ntile > 0 &&
+                    h->v2->tile_smem(h->mesh.max_halo, std::max(h->mesh.max_tasks, 1)) <= (size_t)dev_smem;
+      if (!h->p2_tiled) {  // the edge + element pair's flux slots (slots of edges in no list stay zero)
+        h->p2_ef.alloc((size_t)3 * kP2Egp * 3 * h->ne);
+        DG_CUDA(cudaMemset(h->p2_ef.p, 0, h->p2_ef.n * sizeof(double)));
+      }
     }
     const size_t nl = (size_t)h->ne, npl = (size_t)h->np;
     h->q.resize(s->nrk + 1);

@@ -320,6 +320,7 @@ struct P2Args {
   const int* __restrict__ edges;   // (element, local edge): interior edges from the in side, land and ocean edges
   int nedge, ne_act;
   unsigned* err;
+  int ntile;                       // tiles of the tile plan: > 0 runs the p=2 tile kernel (p2_tile)
 };
 #define DGSWEM_DECLARE_P2_LAUNCHERS(NS)                                                          \
   namespace NS {                                                                                 \
@@ -329,6 +330,7 @@ struct P2Args {
                              double* eta2, double* uu2, double* vv2, int* nodecode, cudaStream_t s); \
   void launch_p2_layout(bool to_device, const double* src, double* dst, int ne, int var,         \
                         const int* map, cudaStream_t s);                                         \
+  size_t p2_tile_smem(int max_halo, int max_tasks);                                              \
   }
 DGSWEM_DECLARE_P2_LAUNCHERS(fast_p2)
 DGSWEM_DECLARE_P2_LAUNCHERS(strict_p2)

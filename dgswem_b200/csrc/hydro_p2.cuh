@@ -373,6 +373,306 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
   if (bad) atomicOr(A.err, 1u);
 }
 
+// ---------------------------------------------------------------------------
+// p=2 tile kernel: the p=1 tile kernel's scheme at six modes.  Block b owns
+// tile b of the tile plan (consecutive elements of the Morton order, their
+// edge tasks, the out-of-tile neighbours those read), phases separated by
+// barriers:
+//   1. tile and halo elements' 24 slot values (18 modal values, six fourth-
+//      row modes: HB, or the depth modes in the mixed variant) and the
+//      tile's geometry rows, edge info and task words into shared memory;
+//   2. one thread per (edge task, Lobatto point): the LLF flux of the point
+//      in the reference's in/ex orientation, or the land / ocean ghost and
+//      its flux -> (F, G, H);
+//   3. one thread per (element, area point): volume fluxes and sources;
+//   4. one thread per (element, mode): the mode's right-hand side of the
+//      three variables in the order of p2_elements (boundary edges, interior
+//      edges as the slot sum, rain, area points), then the SSP combination.
+// Each interior edge point is evaluated once per tile (twice for an edge
+// between tiles) and its flux stays in shared memory: no flux slots in HBM.
+// Every sum has p2_elements' operands and order, so both give the same bits.
+// internal_edge_hydro.F, land_edge_hydro.F, ocean_edge_hydro.F,
+// rhs_dg_hydro.F, DG_hydro_timestep.F:238-290
+// ---------------------------------------------------------------------------
+constexpr int kP2Tile = 64, kP2TileThreads = 384;
+// slot stride in reals: 24 values and a pad keeping 16-byte loads by
+// consecutive slots off one bank group (13 or 7 16-byte units, odd)
+constexpr int kP2SlotStride = sizeof(real) == 8 ? 26 : 28;
+constexpr int kP2Vol = 8;  // fx fy gx gy hx hy sx sy
+
+struct P2Layout {
+  unsigned qs, geo, vol, res, info, tasks, bytes;
+};
+__host__ __device__ inline P2Layout p2_layout(int max_halo, int max_tasks) {
+  P2Layout L;
+  const unsigned S = (unsigned)(kP2Tile + max_halo), T = (unsigned)max_tasks, rb = (unsigned)sizeof(real);
+  L.qs = align16((unsigned)sizeof(BasisP2T<real>));
+  L.geo = align16(L.qs + S * kP2SlotStride * rb);
+  L.vol = align16(L.geo + kGeoRows * kP2Tile * rb);
+  L.res = align16(L.vol + kP2Vol * kP2Agp * kP2Tile * rb);
+  L.info = align16(L.res + T * kP2Egp * 3 * rb);
+  L.tasks = align16(L.info + 2u * kP2Tile * 4u);
+  L.bytes = align16(L.tasks + T * 8u);
+  return L;
+}
+
+// the 24 slot values of element g (device id) from global memory
+__device__ __forceinline__ void p2_slot_store(const P2Args& A, int g, real* dst) {
+  const int ne = A.m.ne;
+#pragma unroll
+  for (int c = 0; c < 3 * kP2Modes; ++c) dst[c] = (real)A.qin[(size_t)c * ne + g];
+#pragma unroll
+  for (int k = 0; k < kP2Modes; ++k) dst[3 * kP2Modes + k] = fourth_mode(A.qin, A.m.hb, ne, g, k);
+}
+
+// trace at point (led, gp) of the six modes at slot[off .. off+5], mode 1
+// first, as trace6 sums them
+__device__ __forceinline__ real p2_slot_trace(const BasisP2T<real>& B, const real* slot, int off, int led, int gp) {
+  const real* phi = B.phi_edge[led][gp];
+  real t = slot[off];
+#pragma unroll
+  for (int k = 1; k < kP2Modes; ++k) t = t + slot[off + k] * phi[k];
+  return t;
+}
+
+template <bool kNonlin>
+__global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_constant__ P2Args A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const MeshView& m = A.m;
+  const Physics& P = A.ph;
+  const int ne = m.ne;
+  const int tid = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int tile0 = m.tile_elem_ptr[tile];
+  const int n = m.tile_elem_ptr[tile + 1] - tile0;
+  const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
+  const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
+  const P2Layout L = p2_layout(m.max_halo, m.max_tasks);
+  BasisP2T<real>& B = *reinterpret_cast<BasisP2T<real>*>(smem_raw);
+  real* qs = reinterpret_cast<real*>(smem_raw + L.qs);
+  real* geo = reinterpret_cast<real*>(smem_raw + L.geo);
+  real* vol = reinterpret_cast<real*>(smem_raw + L.vol);
+  real* res = reinterpret_cast<real*>(smem_raw + L.res);
+  unsigned* sinfo = reinterpret_cast<unsigned*>(smem_raw + L.info);  // [einfo | eslot][kP2Tile]
+  uint2* stasks = reinterpret_cast<uint2*>(smem_raw + L.tasks);
+  const real* G = egeo_r(m);
+  {
+    const real* src = reinterpret_cast<const real*>(&cB2R);
+    real* dst = reinterpret_cast<real*>(&B);
+    for (int i = tid; i < (int)(sizeof(BasisP2T<real>) / sizeof(real)); i += kP2TileThreads) dst[i] = src[i];
+  }
+  // ---- phase 1: slots, geometry rows, edge info, task words ----
+  for (int j = tid; j < kP2Tile + nh; j += kP2TileThreads) {
+    if (j < kP2Tile) {
+      if (j < n) p2_slot_store(A, tile0 + j, qs + j * kP2SlotStride);
+    } else {
+      p2_slot_store(A, m.tile_halo[hbeg + j - kP2Tile], qs + j * kP2SlotStride);
+    }
+  }
+  for (int j = tid; j < EGeo::kSmemRows * kP2Tile; j += kP2TileThreads) {
+    const int r = j / kP2Tile, w = j - r * kP2Tile;
+    if (w < n && (r != EGeo::kNbar || m.manning)) geo[r * kP2Tile + w] = G[(size_t)r * ne + tile0 + w];
+  }
+  for (int j = tid; j < kP2Tile; j += kP2TileThreads)
+    if (j < n) {
+      sinfo[j] = m.einfo[tile0 + j];
+      sinfo[kP2Tile + j] = m.eslot[tile0 + j];
+    }
+  for (int j = tid; j < ntask; j += kP2TileThreads) stasks[j] = m.tile_tasks[tbeg + j];
+  __syncthreads();
+  // hybrid friction factor from the element-mean depth (phase 3 reads it)
+  if (P.iflinbf == 0 && P.ifhybf == 1) {
+    for (int el = tid; el < n; el += kP2TileThreads) {
+      const real* sl = qs + el * kP2SlotStride;
+#ifdef DGSWEM_MIXED
+      const real depth_c = sl[3 * kP2Modes];  // depth mode 1
+#else
+      const real depth_c = sl[3 * kP2Modes] + sl[0];
+#endif
+      const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
+      geo[SGeo::kHyb * kP2Tile + el] =
+          pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
+    }
+  }
+
+  // ---- phase 2: one thread per (edge task, Lobatto point) ----
+  for (int w = tid; w < kP2Egp * ntask; w += kP2TileThreads) {
+    const int ti = w / kP2Egp, I = w - kP2Egp * ti;
+    const uint2 tk = stasks[ti];
+    const unsigned fl = tk.x, kind = fl & 7u;
+    real* o = res + ((size_t)ti * kP2Egp + I) * 3;
+    const int sin = (fl >> TaskBits::kInSlot) & 511, sex = (fl >> TaskBits::kExSlot) & 511;
+    const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
+    const bool flip = (fl >> TaskBits::kFlip) & 1u;
+    const int owner = flip ? sex : sin, oled = flip ? led_ex : led_in;
+    real nx = geo[(EGeo::kNx + oled) * kP2Tile + owner], ny = geo[(EGeo::kNy + oled) * kP2Tile + owner];
+    if (flip) { nx = -nx; ny = -ny; }
+    const real* si = qs + sin * kP2SlotStride;
+    const real zi = p2_slot_trace(B, si, 0, led_in, I), xi = p2_slot_trace(B, si, kP2Modes, led_in, I);
+    const real yi = p2_slot_trace(B, si, 2 * kP2Modes, led_in, I);
+    const real wi = p2_slot_trace(B, si, 3 * kP2Modes, led_in, I);
+    real hi, hti;
+    trace_depth<kNonlin>(P, zi, wi, hi, hti);
+    if (kind == kInterior) {
+      const int J = kP2Egp - 1 - I;
+      const real* sx = qs + sex * kP2SlotStride;
+      const real zx = p2_slot_trace(B, sx, 0, led_ex, J), xx = p2_slot_trace(B, sx, kP2Modes, led_ex, J);
+      const real yx = p2_slot_trace(B, sx, 2 * kP2Modes, led_ex, J);
+      const real wx = p2_slot_trace(B, sx, 3 * kP2Modes, led_ex, J);
+      real hx, htx;
+      trace_depth<kNonlin>(P, zx, wx, hx, htx);
+      const Flux3T<real> f =
+          llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, real(1), real(1), nx, ny, real(P.g));
+      o[0] = f.f; o[1] = f.g; o[2] = f.h;
+      continue;
+    }
+    // ghost state: land reflects the normal momentum (land_edge_hydro.F:201-218);
+    // ocean takes the harmonic elevation with the depth-positivity fix
+    // (ocean_edge_hydro.F:148-177, 255-259; FP64 in every variant)
+    real zx = zi, xx = xi, yx = yi, htx = hti;
+    if (kind == kOcean) {
+      const int list = (int)tk.y;
+      double zsum = 0.0;
+      for (int f = 0; f < m.nbfr; ++f) {
+        const double* zg = A.ocean_zg + ((size_t)f * m.needs + list) * 2;
+        zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * cB2.xegp[I]);
+      }
+      const double hid = hi;
+      if (zsum * P.ifnlfa + hid <= 0) zsum = fabs(hid) + P.h0;
+      zx = (real)zsum;
+      htx = depth<kNonlin>(P, zx, hi);
+    } else {
+      const real tx = -ny, ty = nx;
+      const real qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
+      const real qne = -qn, qte = qt, den = real(1) / (nx * ty - ny * tx);
+      xx = (ty * qne - ny * qte) * den;
+      yx = (-tx * qne + nx * qte) * den;
+    }
+    const Flux3T<real> f =
+        llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hi, hti, htx, real(1), real(1), nx, ny, real(P.g));
+    o[0] = f.f; o[1] = f.g; o[2] = f.h;
+  }
+  __syncthreads();
+
+  // ---- phase 3: volume terms per (element, area point) ----
+  for (int w = tid; w < kP2Agp * kP2Tile; w += kP2TileThreads) {
+    const int i = w / kP2Tile, el = w - i * kP2Tile;
+    if (el >= n) continue;
+    const real* sl = qs + el * kP2SlotStride;
+    real q[3 * kP2Modes], wm[kP2Modes];
+#pragma unroll
+    for (int c = 0; c < 3 * kP2Modes; ++c) q[c] = sl[c];
+#pragma unroll
+    for (int k = 0; k < kP2Modes; ++k) wm[k] = sl[3 * kP2Modes + k];
+    const real drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
+    const real drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
+    const real hyb = (P.iflinbf == 0 && P.ifhybf == 1) ? geo[SGeo::kHyb * kP2Tile + el] : real(1);
+    real v[kP2Vol];
+    p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, tile0 + el, i, v);
+#pragma unroll
+    for (int r = 0; r < kP2Vol; ++r) vol[(r * kP2Agp + i) * kP2Tile + el] = v[r];
+  }
+  __syncthreads();
+
+  // ---- phase 4: per (element, mode) sums in p2_elements' order, SSP ----
+  for (int w = tid; w < kP2Modes * kP2Tile; w += kP2TileThreads) {
+    const int K = w / kP2Tile, el = w - K * kP2Tile;
+    if (el >= n) continue;
+    const int e = tile0 + el;
+    const unsigned info = sinfo[el], slots = sinfo[kP2Tile + el];
+    real rhs[3] = {0, 0, 0}, isum[3] = {0, 0, 0};
+    for (int s = 0; s < 3; ++s) {
+      const int l = ei_order(info, s);
+      const unsigned kind = ei_kind(info, l);
+      if (kind == kNone) continue;
+      const int ti = (slots >> (10 * l)) & kNoTask;
+      const real* r = res + (size_t)ti * kP2Egp * 3;
+      if (kind == kInterior) {
+        const bool is_in = ei_flag(info, l) != 0;
+        const real edfac = geo[(EGeo::kEdfac + l) * kP2Tile + el];
+        real acc[3] = {0, 0, 0};
+        for (int I = 0; I < kP2Egp; ++I) {
+          const int j = is_in ? I : kP2Egp - 1 - I;
+          const real wk = edfac * B.edgeq[l][j][K];
+          const real v0 = r[I * 3], v1 = r[I * 3 + 1], v2 = r[I * 3 + 2];
+          if (is_in) {
+            acc[0] = acc[0] - wk * v0;
+            acc[1] = acc[1] - wk * v1;
+            acc[2] = acc[2] - wk * v2;
+          } else {
+            acc[0] = acc[0] + wk * v0;
+            acc[1] = acc[1] + wk * v1;
+            acc[2] = acc[2] + wk * v2;
+          }
+        }
+#pragma unroll
+        for (int V = 0; V < 3; ++V) isum[V] = isum[V] + acc[V];
+      } else {
+        const real areas = G[(size_t)EGeo::kAreas * ne + e];
+        const real xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
+        for (int I = 0; I < kP2Egp; ++I) {
+          const real wk = real(2) * B.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * B.wegp[I];
+          rhs[0] = rhs[0] - wk * r[I * 3];
+          rhs[1] = rhs[1] - wk * r[I * 3 + 1];
+          rhs[2] = rhs[2] - wk * r[I * 3 + 2];
+        }
+      }
+    }
+#pragma unroll
+    for (int V = 0; V < 3; ++V) rhs[V] = rhs[V] + isum[V];  // add_internal_flux
+    if (P.rainfall == 1) {
+      const real src = real(7.0556e-6);
+      for (int i = 0; i < kP2Agp; ++i) rhs[0] = rhs[0] + B.srfac[K][i] * src;
+    }
+    const real drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
+    const real drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
+    for (int i = 0; i < kP2Agp; ++i) {
+      const real* vv = vol + i * kP2Tile + el;  // row r at vv[r * kP2Agp * kP2Tile]
+      const real sx = vv[6 * kP2Agp * kP2Tile], sy = vv[7 * kP2Agp * kP2Tile];
+      if (K == 0) {
+        rhs[1] = rhs[1] + B.srfac[0][i] * sx;
+        rhs[2] = rhs[2] + B.srfac[0][i] * sy;
+      } else {
+        const real dpx = B.drphi[K][i] * drdx + B.dsphi[K][i] * dsdx;
+        const real dpy = B.drphi[K][i] * drdy + B.dsphi[K][i] * dsdy;
+        const real xf = B.mw[K][i] * dpx;
+        const real yf = B.mw[K][i] * dpy;
+        const real sr = B.srfac[K][i];
+        rhs[0] = rhs[0] + xf * vv[0] + yf * vv[kP2Agp * kP2Tile];
+        rhs[1] = rhs[1] + xf * vv[2 * kP2Agp * kP2Tile] + yf * vv[3 * kP2Agp * kP2Tile] + sr * sx;
+        rhs[2] = rhs[2] + xf * vv[4 * kP2Agp * kP2Tile] + yf * vv[5 * kP2Agp * kP2Tile] + sr * sy;
+      }
+    }
+    // SSP-RK combination (DG_hydro_timestep.F:238-290) in FP64
+    bool bad = false;
+    const bool hist0 = A.irk > 1;
+#pragma unroll
+    for (int V = 0; V < 3; ++V) {
+      const int c = kP2Modes * V + K;
+      const double rk = (double)rhs[V];
+      if (A.rout) A.rout[(size_t)c * ne + e] = rk;
+      const double qc = A.qin[(size_t)c * ne + e];
+      double acc = 0.0;
+      if (hist0) {
+        if (A.a[0] != 0.0) acc = acc + A.a[0] * A.qhist[0][(size_t)c * ne + e];
+        if (A.b[0] != 0.0) acc = acc + A.b[0] * A.rhist[0][(size_t)c * ne + e];
+      }
+      for (int I = 1; I < A.irk; ++I) {
+        const bool cur = I == A.irk - 1;
+        if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc : A.qhist[I][(size_t)c * ne + e]);
+        if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rk : A.rhist[I][(size_t)c * ne + e]);
+      }
+      if (!hist0) {
+        if (A.a[0] != 0.0) acc = acc + A.a[0] * qc;
+        if (A.b[0] != 0.0) acc = acc + A.b[0] * rk;
+      }
+      bad = bad || isnan(acc);
+      A.qout[(size_t)c * ne + e] = acc;
+    }
+    if (bad) atomicOr(A.err, 1u);
+  }
+}
+
 // write_results.F:14-170 at p=2 (six modes at the element corners) + NODECODE
 __global__ void p2_modal2nodal(MeshView m, const double* __restrict__ q, double nleq, double leq, double* eta2,
                                double* uu2, double* vv2, int* nodecode) {
@@ -434,6 +734,8 @@ __global__ void p2_soa_to_fortran(const double* __restrict__ q, double* __restri
   for (int k = 0; k < kP2Modes; ++k) f[(size_t)kP2Modes * e + k] = q[(size_t)(kP2Modes * var + k) * ne + i];
 }
 
+size_t p2_tile_smem(int max_halo, int max_tasks) { return p2_layout(max_halo, max_tasks).bytes; }
+
 void set_basis_p2(const BasisP2& b) {
   cudaMemcpyToSymbol(cB2, &b, sizeof(b));
   BasisP2T<real> r;
@@ -444,6 +746,13 @@ void set_basis_p2(const BasisP2& b) {
 }
 
 void launch_p2_stage(const P2Args& a, bool nonlin, cudaStream_t s) {
+  if (a.ntile > 0) {  // the tile kernel
+    const size_t smem = p2_layout(a.m.max_halo, a.m.max_tasks).bytes;
+    auto* k = nonlin ? p2_tile<true> : p2_tile<false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<(unsigned)a.ntile, kP2TileThreads, smem, s>>>(a);
+    return;
+  }
   const unsigned ge = (unsigned)(((long long)kP2Egp * a.nedge + 127) / 128);
   const unsigned gl = (unsigned)((a.ne_act + 127) / 128);
   if (nonlin) {
