@@ -68,6 +68,9 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// all but the most recently committed group of this thread's copies complete
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void cp_async8_s(unsigned dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
@@ -380,12 +383,14 @@ __global__ void __launch_bounds__(128) ibarrier_sides(const __grid_constant__ St
 // kStageThreads threads:
 //   1. tile and halo elements: modal state, bathymetry modes and wet/dry flag
 //      into shared memory; tile elements also their geometry;
-//   2. one thread per (task, Lobatto point): the LLF flux of an edge point in
+//   2. one thread per (element, area point): volume fluxes and sources (tile
+//      elements only: in the FP64 variants the halo's copies are still in
+//      flight, waited for at the end of this phase);
+//   3. one thread per (task, Lobatto point): the LLF flux of an edge point in
 //      the reference's own in/ex orientation with its dry-side rules ->
 //      F, G_in, H_in, G_ex, H_ex (internal-barrier sides come from
 //      ibarrier_sides);
-//   3. one thread per (element, area point): volume fluxes and sources;
-//   4. one thread per (element, variable): the three modes of that variable
+//   4. one thread per (element, mode): that mode of the three variables
 //      summed in the reference's order (boundary edges, interior edges in
 //      edge-number order as the slot sum of add_internal_flux, rain, area
 //      points), then the SSP combination.
@@ -818,6 +823,13 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
 #pragma unroll
         for (int j = 0; j < 3; ++j)
           f[j] = make_float4((float)v[4 * j], (float)v[4 * j + 1], (float)v[4 * j + 2], (float)v[4 * j + 3]);
+        // hybrid friction factor from the element-mean depth (depth mode 1)
+        if (P.iflinbf == 0 && P.ifhybf == 1) {
+          const real depth_c = (real)v[9];
+          const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
+          geo[SGeo::kHyb * kTile + tid] =
+              pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
+        }
       }
     } else {
       constexpr int kU = kStageThreads - kTile, kStep = kU / kTile;
@@ -861,15 +873,12 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   }
   __syncthreads();
 #else
-  // Asynchronous global->shared copies (cp.async), no register staging:
-  // halo element j by thread j (one index load, then its 13 values), the
-  // tile's rows (state, bathymetry, geometry table, flags) by all threads,
-  // consecutive threads on consecutive elements of a row.
-  int hg = -1;
-  if (tid < nh) {
-    hg = m.tile_halo[hbeg + tid];
-    gid[tid] = hg;
-  }
+  // Asynchronous global->shared copies (cp.async), no register staging, in
+  // two groups: the tile's rows (state, bathymetry, geometry table, flags;
+  // consecutive threads on consecutive elements of a row) and task words,
+  // then the halo elements (thread j: halo element j's 13 values).  The
+  // volume phase needs only the first group; the halo lands meanwhile.
+  const int hg = tid < nh ? m.tile_halo[hbeg + tid] : -1;
   {
     // thread t: element t % kTile of every (kStageThreads / kTile)-th row;
     // shared addresses as 32-bit offsets, rows unrolled
@@ -910,9 +919,10 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
       }
     }
     for (int j = tid; j < ntask; j += kStageThreads) cp_async8(stasks + j, m.tile_tasks + tbeg + j);
+    cp_async_commit();
     for (int j = tid; j < nh; j += kStageThreads) {
       const int g = j == tid ? hg : m.tile_halo[hbeg + j];
-      if (j != tid) gid[j] = g;
+      gid[j] = g;
       const unsigned hdst = qs_s + (unsigned)((kTile + j) * kQStride) * 8u;
       const double* q0 = A.qin + g;
 #pragma unroll
@@ -922,27 +932,33 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
       for (int k = 0; k < 3; ++k) cp_async8_s(hdst + 72u + 8u * k, h0 + (size_t)k * ne);
       cp_async4(wds + kTile + j, A.wd + g);
     }
-    cp_async_wait_all();
+    cp_async_commit();
+    // hybrid friction factor of tile element tid from the element-mean depth
+    // (HB + ZE of mode 1, the operands the slot gets), for the volume phase
+    if (P.iflinbf == 0 && P.ifhybf == 1 && tid < n) {
+      const real depth_c = (real)(m.hb[tile0 + tid] + A.qin[tile0 + tid]);
+      const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
+      geo[SGeo::kHyb * kTile + tid] =
+          pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
+    }
+    cp_async_wait_prior();
   }
   __syncthreads();
 #endif
 
-  // hybrid friction factor from the element-mean depth, used by phase 3
-  // (visible after the next barrier)
-  if (P.iflinbf == 0 && P.ifhybf == 1) {
-    for (int el = tid; el < n; el += kStageThreads) {
-#ifdef DGSWEM_MIXED
-      const real depth_c = qt[el * kQfStride + 9];  // depth mode 1
-#else
-      const real depth_c = (real)(qs[el * kQStride + 9] + qs[el * kQStride]);
-#endif
-      const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
-      geo[SGeo::kHyb * kTile + el] =
-          pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
-    }
+  // ---- phase 2: volume fluxes and sources per (element, area point) ----
+  // (the point is the same for a whole warp: kTile is a multiple of 32)
+  for (int w = tid; w < 3 * kTile; w += kStageThreads) {
+    const int i = w / kTile, el = w - i * kTile;
+    if (el >= n || wds[el] == 0) continue;
+    volume_point<kNonlin, kSph, kTile>(A, B, qt, geo, vol, i, el, tile0 + el);
   }
+#ifndef DGSWEM_MIXED
+  cp_async_wait_all();  // the halo group
+#endif
+  __syncthreads();
 
-  // ---- phase 2: one thread per (edge task, Lobatto point) ----
+  // ---- phase 3: one thread per (edge task, Lobatto point) ----
   // (the three points of a task on adjacent lanes: same slots, broadcast loads)
   for (int w = tid; w < 3 * ntask; w += kStageThreads) {
     const int ti = w / 3, I = w - 3 * ti;
@@ -991,14 +1007,6 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   }
   __syncthreads();
 
-  // ---- phase 3: volume fluxes and sources per (element, area point) ----
-  // (the point is the same for a whole warp: kTile is a multiple of 32)
-  for (int w = tid; w < 3 * kTile; w += kStageThreads) {
-    const int i = w / kTile, el = w - i * kTile;
-    if (el >= n || wds[el] == 0) continue;
-    volume_point<kNonlin, kSph, kTile>(A, B, qt, geo, vol, i, el, tile0 + el);
-  }
-  __syncthreads();
 
   // ---- phase 4: per (element, mode) sums in the reference's order, SSP ----
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {

@@ -129,14 +129,45 @@ __device__ __forceinline__ PhysR phys_r(const P2Args& A) {
 // with six modes): out = fx fy gx gy hx hy sx sy.  q: the element's 18 state
 // values (row 6*var + k) and w its six fourth-row modes (fourth_mode: HB, or
 // the depth modes in the mixed variant), in the arithmetic type.
+// Per-element terms of the volume integral, in the arithmetic type: the
+// Coriolis parameter and the bottom friction coefficient (nodal arrays or the
+// constants), Manning's n, and the vertices' wind stress and pressure scaled
+// by the stage's ramp (met_forcing.F:49-66).
+struct P2Frc {
+  real cori, fric, nbar, wx[3], wy[3], pr[3];
+  // rows a tile keeps in shared memory: all but nbar (a geometry row)
+  static constexpr int kRows = 11;
+};
+__device__ __forceinline__ P2Frc p2_force(const P2Args& A, int e) {
+  const MeshView& m = A.m;
+  const PhysR R = phys_r(A);
+  const int ne = m.ne;
+  P2Frc F;
+  F.cori = m.cori ? (real)m.cori[e] : R.cori;
+  F.fric = m.fric ? (real)m.fric[e] : R.fric;
+  F.nbar = m.manning ? egeo_r(m)[(size_t)EGeo::kNbar * ne + e] : real(0);
+  if (A.ph.nws != 0) {
+    const real r = (real)(A.ramp ? *A.ramp : A.rampdg);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int n = m.nm[(size_t)a * ne + e];
+      F.wx[a] = r * (real)A.wsx[n];
+      F.wy[a] = r * (real)A.wsy[n];
+      F.pr[a] = r * (real)A.pr[n];
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) F.wx[a] = F.wy[a] = F.pr[a] = real(0);
+  }
+  return F;
+}
+
 template <bool kNonlin>
 __device__ __forceinline__ void p2_volume(const P2Args& A, const real* q, const real* w, real drdx, real dsdx,
-                                          real drdy, real dsdy, real hyb, int e, int i, real out[8]) {
-  const MeshView& m = A.m;
+                                          real drdy, real dsdy, real hyb, const P2Frc& F, int i, real out[8]) {
   const Physics& P = A.ph;
   const PhysR R = phys_r(A);
   const BasisP2T<real>& C = cB2R;
-  const int ne = m.ne;
 #ifdef DGSWEM_MIXED
   real hbe[kP2Modes];
 #pragma unroll
@@ -145,8 +176,8 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const real* q, const 
   const real* hbe = w;
 #endif
   const real NLEQ = kNonlin ? real(1) : R.nleq, LEQ = kNonlin ? real(0) : R.leq;
-  const real cori = m.cori ? (real)m.cori[e] : R.cori;
-  real fric = m.fric ? (real)m.fric[e] : R.fric;
+  const real cori = F.cori;
+  real fric = F.fric;
   real zq = q[0], uq = q[6], vq = q[12];
   real hq = hbe[0] * C.phi_area[0][i];
 #pragma unroll
@@ -182,8 +213,8 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const real* q, const 
   const real gh2 = kNonlin ? fg * (real(0.5) * zq + hq) : fg * (real(0.5) * zq + hq) + R.fg_l * zq;
   const real gx = (huu + gh2) * real(1), gy = huv;
   const real hx = huv * real(1), hy = hvv + gh2;
-  if (m.manning) {
-    const real nbar = egeo_r(m)[(size_t)EGeo::kNbar * ne + e];
+  if (A.m.manning) {
+    const real nbar = F.nbar;
     fric = R.g * (nbar * nbar) / cube_root(depth);
     if (fric < R.cf) fric = R.cf;
   }
@@ -205,15 +236,11 @@ __device__ __forceinline__ void p2_volume(const P2Args& A, const real* q, const 
       dpsidx[a] = drpsi[a] * drdx + dspsi[a] * dsdx;
       dpsidy[a] = drpsi[a] * drdy + dspsi[a] * dsdy;
     }
-    const real fw = real(1) / f1, r = (real)(A.ramp ? *A.ramp : A.rampdg);
-    const int n0 = m.nm[e], n1 = m.nm[(size_t)ne + e], n2 = m.nm[(size_t)2 * ne + e];
-    const real wx0 = r * (real)A.wsx[n0], wx1 = r * (real)A.wsx[n1], wx2 = r * (real)A.wsx[n2];
-    const real wy0 = r * (real)A.wsy[n0], wy1 = r * (real)A.wsy[n1], wy2 = r * (real)A.wsy[n2];
-    const real p0 = r * (real)A.pr[n0], p1 = r * (real)A.pr[n1], p2 = r * (real)A.pr[n2];
-    sx = sx + fw * (wx0 * C.psi[0][i] + wx1 * C.psi[1][i] + wx2 * C.psi[2][i]) -
-         R.g * real(1) * depth * (p0 * dpsidx[0] + p1 * dpsidx[1] + p2 * dpsidx[2]);
-    sy = sy + fw * (wy0 * C.psi[0][i] + wy1 * C.psi[1][i] + wy2 * C.psi[2][i]) -
-         R.g * depth * (p0 * dpsidy[0] + p1 * dpsidy[1] + p2 * dpsidy[2]);
+    const real fw = real(1) / f1;
+    sx = sx + fw * (F.wx[0] * C.psi[0][i] + F.wx[1] * C.psi[1][i] + F.wx[2] * C.psi[2][i]) -
+         R.g * real(1) * depth * (F.pr[0] * dpsidx[0] + F.pr[1] * dpsidx[1] + F.pr[2] * dpsidx[2]);
+    sy = sy + fw * (F.wy[0] * C.psi[0][i] + F.wy[1] * C.psi[1][i] + F.wy[2] * C.psi[2][i]) -
+         R.g * depth * (F.pr[0] * dpsidy[0] + F.pr[1] * dpsidy[1] + F.pr[2] * dpsidy[2]);
   }
   out[0] = fx; out[1] = fy; out[2] = gx; out[3] = gy;
   out[4] = hx; out[5] = hy; out[6] = sx; out[7] = sy;
@@ -326,7 +353,7 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
   }
   for (int i = 0; i < kP2Agp; ++i) {
     real vol[8];
-    p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, e, i, vol);
+    p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, p2_force(A, e), i, vol);
     rhs[1][0] = rhs[1][0] + B.srfac[0][i] * vol[6];
     rhs[2][0] = rhs[2][0] + B.srfac[0][i] * vol[7];
 #pragma unroll
@@ -379,15 +406,19 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
 // edge tasks, the out-of-tile neighbours those read), phases separated by
 // barriers:
 //   1. tile and halo elements' 24 slot values (18 modal values, six fourth-
-//      row modes: HB, or the depth modes in the mixed variant) and the
-//      tile's geometry rows, edge info and task words into shared memory;
-//   2. one thread per (edge task, Lobatto point): the LLF flux of the point
-//      in the reference's in/ex orientation, or the land / ocean ghost and
-//      its flux -> (F, G, H);
-//   3. one thread per (element, area point): volume fluxes and sources;
-//   4. one thread per (element, mode): the mode's right-hand side of the
+//      row modes: HB, or the depth modes in the mixed variant), the tile's
+//      geometry rows, edge info, task words and per-element forcing terms
+//      (P2Frc: Coriolis, friction, the vertices' wind and pressure) into
+//      shared memory, and the hybrid friction factor of each tile element;
+//   2. one work item per thread and round over the tile's edge points and
+//      then its area points: an edge point (edge task, Lobatto point) gives
+//      the LLF flux of the point in the reference's in/ex orientation, or the
+//      land / ocean ghost and its flux -> (F, G, H); an area point (element,
+//      point) gives its volume fluxes and sources;
+//   3. one thread per (element, mode): the mode's right-hand side of the
 //      three variables in the order of p2_elements (boundary edges, interior
-//      edges as the slot sum, rain, area points), then the SSP combination.
+//      edges as the slot sum, rain, area points), then the SSP combination,
+//      its state operands loaded before the sums.
 // Each interior edge point is evaluated once per tile (twice for an edge
 // between tiles) and its flux stays in shared memory: no flux slots in HBM.
 // Every sum has p2_elements' operands and order, so both give the same bits.
@@ -401,14 +432,15 @@ constexpr int kP2SlotStride = sizeof(real) == 8 ? 26 : 28;
 constexpr int kP2Vol = 8;  // fx fy gx gy hx hy sx sy
 
 struct P2Layout {
-  unsigned qs, geo, vol, res, info, tasks, bytes;
+  unsigned qs, geo, frc, vol, res, info, tasks, bytes;
 };
 __host__ __device__ inline P2Layout p2_layout(int max_halo, int max_tasks) {
   P2Layout L;
   const unsigned S = (unsigned)(kP2Tile + max_halo), T = (unsigned)max_tasks, rb = (unsigned)sizeof(real);
   L.qs = align16((unsigned)sizeof(BasisP2T<real>));
   L.geo = align16(L.qs + S * kP2SlotStride * rb);
-  L.vol = align16(L.geo + kGeoRows * kP2Tile * rb);
+  L.frc = align16(L.geo + kGeoRows * kP2Tile * rb);
+  L.vol = align16(L.frc + P2Frc::kRows * kP2Tile * rb);
   L.res = align16(L.vol + kP2Vol * kP2Agp * kP2Tile * rb);
   L.info = align16(L.res + T * kP2Egp * 3 * rb);
   L.tasks = align16(L.info + 2u * kP2Tile * 4u);
@@ -435,6 +467,79 @@ __device__ __forceinline__ real p2_slot_trace(const BasisP2T<real>& B, const rea
   return t;
 }
 
+// Hybrid friction factor from the element-mean depth of a slot
+template <bool kNonlin>
+__device__ __forceinline__ real p2_hybrid(const Physics& P, const real* sl) {
+#ifdef DGSWEM_MIXED
+  const real depth_c = sl[3 * kP2Modes];  // depth mode 1
+#else
+  const real depth_c = sl[3 * kP2Modes] + sl[0];
+#endif
+  const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
+  return pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
+}
+
+// Flux (F, G, H) at Lobatto point I of edge task tk into o[0..2]: the LLF
+// flux in the in/ex orientation for an interior edge, else the land / ocean
+// ghost state and its flux
+template <bool kNonlin>
+__device__ __forceinline__ void p2_tile_edge_point(const P2Args& A, const BasisP2T<real>& B, const real* qs,
+                                                   const real* geo, uint2 tk, int I, real* o) {
+  const MeshView& m = A.m;
+  const Physics& P = A.ph;
+  const unsigned fl = tk.x, kind = fl & 7u;
+  const int sin = (fl >> TaskBits::kInSlot) & 511, sex = (fl >> TaskBits::kExSlot) & 511;
+  const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
+  const bool flip = (fl >> TaskBits::kFlip) & 1u;
+  const int owner = flip ? sex : sin, oled = flip ? led_ex : led_in;
+  real nx = geo[(EGeo::kNx + oled) * kP2Tile + owner], ny = geo[(EGeo::kNy + oled) * kP2Tile + owner];
+  if (flip) { nx = -nx; ny = -ny; }
+  const real* si = qs + sin * kP2SlotStride;
+  const real zi = p2_slot_trace(B, si, 0, led_in, I), xi = p2_slot_trace(B, si, kP2Modes, led_in, I);
+  const real yi = p2_slot_trace(B, si, 2 * kP2Modes, led_in, I);
+  const real wi = p2_slot_trace(B, si, 3 * kP2Modes, led_in, I);
+  real hi, hti;
+  trace_depth<kNonlin>(P, zi, wi, hi, hti);
+  if (kind == kInterior) {
+    const int J = kP2Egp - 1 - I;
+    const real* sx = qs + sex * kP2SlotStride;
+    const real zx = p2_slot_trace(B, sx, 0, led_ex, J), xx = p2_slot_trace(B, sx, kP2Modes, led_ex, J);
+    const real yx = p2_slot_trace(B, sx, 2 * kP2Modes, led_ex, J);
+    const real wx = p2_slot_trace(B, sx, 3 * kP2Modes, led_ex, J);
+    real hx, htx;
+    trace_depth<kNonlin>(P, zx, wx, hx, htx);
+    const Flux3T<real> f =
+        llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, real(1), real(1), nx, ny, real(P.g));
+    o[0] = f.f; o[1] = f.g; o[2] = f.h;
+    return;
+  }
+  // ghost state: land reflects the normal momentum (land_edge_hydro.F:201-218);
+  // ocean takes the harmonic elevation with the depth-positivity fix
+  // (ocean_edge_hydro.F:148-177, 255-259; FP64 in every variant)
+  real zx = zi, xx = xi, yx = yi, htx = hti;
+  if (kind == kOcean) {
+    const int list = (int)tk.y;
+    double zsum = 0.0;
+    for (int f = 0; f < m.nbfr; ++f) {
+      const double* zg = A.ocean_zg + ((size_t)f * m.needs + list) * 2;
+      zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * cB2.xegp[I]);
+    }
+    const double hid = hi;
+    if (zsum * P.ifnlfa + hid <= 0) zsum = fabs(hid) + P.h0;
+    zx = (real)zsum;
+    htx = depth<kNonlin>(P, zx, hi);
+  } else {
+    const real tx = -ny, ty = nx;
+    const real qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
+    const real qne = -qn, qte = qt, den = real(1) / (nx * ty - ny * tx);
+    xx = (ty * qne - ny * qte) * den;
+    yx = (-tx * qne + nx * qte) * den;
+  }
+  const Flux3T<real> f =
+      llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hi, hti, htx, real(1), real(1), nx, ny, real(P.g));
+  o[0] = f.f; o[1] = f.g; o[2] = f.h;
+}
+
 template <bool kNonlin>
 __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_constant__ P2Args A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -451,112 +556,84 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
   BasisP2T<real>& B = *reinterpret_cast<BasisP2T<real>*>(smem_raw);
   real* qs = reinterpret_cast<real*>(smem_raw + L.qs);
   real* geo = reinterpret_cast<real*>(smem_raw + L.geo);
+  real* frc = reinterpret_cast<real*>(smem_raw + L.frc);  // cori, fric, wx[3], wy[3], pr[3]: [kRows][kP2Tile]
   real* vol = reinterpret_cast<real*>(smem_raw + L.vol);
   real* res = reinterpret_cast<real*>(smem_raw + L.res);
   unsigned* sinfo = reinterpret_cast<unsigned*>(smem_raw + L.info);  // [einfo | eslot][kP2Tile]
   uint2* stasks = reinterpret_cast<uint2*>(smem_raw + L.tasks);
   const real* G = egeo_r(m);
+  const bool hybrid = P.iflinbf == 0 && P.ifhybf == 1;
   {
     const real* src = reinterpret_cast<const real*>(&cB2R);
     real* dst = reinterpret_cast<real*>(&B);
     for (int i = tid; i < (int)(sizeof(BasisP2T<real>) / sizeof(real)); i += kP2TileThreads) dst[i] = src[i];
   }
-  // ---- phase 1: slots, geometry rows, edge info, task words ----
+  // ---- phase 1: slots, geometry rows, edge info, task words, forcing ----
+  // Exact copies go by cp.async (issued back to back, one wait); the halo
+  // ids are fetched first, the forcing gathers (node ids, then the nodal
+  // fields) last, so their round trips overlap the copies in flight.
+  const int hj = tid - kP2Tile;
+  const int hg = (hj >= 0 && hj < nh) ? m.tile_halo[hbeg + hj] : -1;
+  {
+    constexpr unsigned rb = sizeof(real);
+    const unsigned geo_s = smem_addr(geo);
+    for (int j = tid; j < EGeo::kSmemRows * kP2Tile; j += kP2TileThreads) {
+      const int r = j / kP2Tile, w = j - r * kP2Tile;
+      if (w < n && (r != EGeo::kNbar || m.manning)) {
+        if (rb == 8)
+          cp_async8_s(geo_s + (unsigned)(r * kP2Tile + w) * rb, G + (size_t)r * ne + tile0 + w);
+        else
+          cp_async4_s(geo_s + (unsigned)(r * kP2Tile + w) * rb, G + (size_t)r * ne + tile0 + w);
+      }
+    }
+  }
+  if (tid < n) {
+    cp_async4(sinfo + tid, m.einfo + tile0 + tid);
+    cp_async4(sinfo + kP2Tile + tid, m.eslot + tile0 + tid);
+  }
+  for (int j = tid; j < ntask; j += kP2TileThreads) cp_async8(stasks + j, m.tile_tasks + tbeg + j);
   for (int j = tid; j < kP2Tile + nh; j += kP2TileThreads) {
-    if (j < kP2Tile) {
-      if (j < n) p2_slot_store(A, tile0 + j, qs + j * kP2SlotStride);
-    } else {
-      p2_slot_store(A, m.tile_halo[hbeg + j - kP2Tile], qs + j * kP2SlotStride);
-    }
-  }
-  for (int j = tid; j < EGeo::kSmemRows * kP2Tile; j += kP2TileThreads) {
-    const int r = j / kP2Tile, w = j - r * kP2Tile;
-    if (w < n && (r != EGeo::kNbar || m.manning)) geo[r * kP2Tile + w] = G[(size_t)r * ne + tile0 + w];
-  }
-  for (int j = tid; j < kP2Tile; j += kP2TileThreads)
-    if (j < n) {
-      sinfo[j] = m.einfo[tile0 + j];
-      sinfo[kP2Tile + j] = m.eslot[tile0 + j];
-    }
-  for (int j = tid; j < ntask; j += kP2TileThreads) stasks[j] = m.tile_tasks[tbeg + j];
-  __syncthreads();
-  // hybrid friction factor from the element-mean depth (phase 3 reads it)
-  if (P.iflinbf == 0 && P.ifhybf == 1) {
-    for (int el = tid; el < n; el += kP2TileThreads) {
-      const real* sl = qs + el * kP2SlotStride;
+    if (j < kP2Tile && j >= n) continue;
+    const int g = j < kP2Tile ? tile0 + j : (j == tid ? hg : m.tile_halo[hbeg + j - kP2Tile]);
+    real* sl = qs + j * kP2SlotStride;
 #ifdef DGSWEM_MIXED
-      const real depth_c = sl[3 * kP2Modes];  // depth mode 1
+    p2_slot_store(A, g, sl);  // FP32 values and the depth modes: through registers
 #else
-      const real depth_c = sl[3 * kP2Modes] + sl[0];
+    const unsigned d = smem_addr(sl);
+#pragma unroll
+    for (int c = 0; c < 3 * kP2Modes; ++c) cp_async8_s(d + 8u * c, A.qin + (size_t)c * ne + g);
+#pragma unroll
+    for (int k = 0; k < kP2Modes; ++k) cp_async8_s(d + 8u * (3 * kP2Modes + k), m.hb + (size_t)k * ne + g);
 #endif
-      const real fh_c = real(1) / (kNonlin ? depth_c : real(P.nleq) * depth_c + real(P.leq));
-      geo[SGeo::kHyb * kP2Tile + el] =
-          pow(real(1) + pow(real(P.hbreak) * fh_c, real(P.ftheta)), real(P.fgamma / P.ftheta));
+  }
+  {  // the last kP2Tile threads: the forcing terms of the tile's elements
+    const int j = tid - (kP2TileThreads - kP2Tile);
+    if (j >= 0 && j < n) {
+      const P2Frc F = p2_force(A, tile0 + j);
+      frc[0 * kP2Tile + j] = F.cori;
+      frc[1 * kP2Tile + j] = F.fric;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        frc[(2 + a) * kP2Tile + j] = F.wx[a];
+        frc[(5 + a) * kP2Tile + j] = F.wy[a];
+        frc[(8 + a) * kP2Tile + j] = F.pr[a];
+      }
     }
   }
+  cp_async_wait_all();
+  // hybrid friction factor of tile element tid from the slot it copied
+  if (hybrid && tid < n) geo[SGeo::kHyb * kP2Tile + tid] = p2_hybrid<kNonlin>(P, qs + tid * kP2SlotStride);
+  __syncthreads();
 
-  // ---- phase 2: one thread per (edge task, Lobatto point) ----
-  for (int w = tid; w < kP2Egp * ntask; w += kP2TileThreads) {
-    const int ti = w / kP2Egp, I = w - kP2Egp * ti;
-    const uint2 tk = stasks[ti];
-    const unsigned fl = tk.x, kind = fl & 7u;
-    real* o = res + ((size_t)ti * kP2Egp + I) * 3;
-    const int sin = (fl >> TaskBits::kInSlot) & 511, sex = (fl >> TaskBits::kExSlot) & 511;
-    const int led_in = (fl >> TaskBits::kLedIn) & 3, led_ex = (fl >> TaskBits::kLedEx) & 3;
-    const bool flip = (fl >> TaskBits::kFlip) & 1u;
-    const int owner = flip ? sex : sin, oled = flip ? led_ex : led_in;
-    real nx = geo[(EGeo::kNx + oled) * kP2Tile + owner], ny = geo[(EGeo::kNy + oled) * kP2Tile + owner];
-    if (flip) { nx = -nx; ny = -ny; }
-    const real* si = qs + sin * kP2SlotStride;
-    const real zi = p2_slot_trace(B, si, 0, led_in, I), xi = p2_slot_trace(B, si, kP2Modes, led_in, I);
-    const real yi = p2_slot_trace(B, si, 2 * kP2Modes, led_in, I);
-    const real wi = p2_slot_trace(B, si, 3 * kP2Modes, led_in, I);
-    real hi, hti;
-    trace_depth<kNonlin>(P, zi, wi, hi, hti);
-    if (kind == kInterior) {
-      const int J = kP2Egp - 1 - I;
-      const real* sx = qs + sex * kP2SlotStride;
-      const real zx = p2_slot_trace(B, sx, 0, led_ex, J), xx = p2_slot_trace(B, sx, kP2Modes, led_ex, J);
-      const real yx = p2_slot_trace(B, sx, 2 * kP2Modes, led_ex, J);
-      const real wx = p2_slot_trace(B, sx, 3 * kP2Modes, led_ex, J);
-      real hx, htx;
-      trace_depth<kNonlin>(P, zx, wx, hx, htx);
-      const Flux3T<real> f =
-          llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hx, hti, htx, real(1), real(1), nx, ny, real(P.g));
-      o[0] = f.f; o[1] = f.g; o[2] = f.h;
+  // ---- phase 2: edge points (edge task, Lobatto point), then area points ----
+  const int nep = kP2Egp * ntask;
+  for (int w = tid; w < nep + kP2Agp * kP2Tile; w += kP2TileThreads) {
+    if (w < nep) {
+      const int ti = w / kP2Egp, I = w - kP2Egp * ti;
+      p2_tile_edge_point<kNonlin>(A, B, qs, geo, stasks[ti], I, res + ((size_t)ti * kP2Egp + I) * 3);
       continue;
     }
-    // ghost state: land reflects the normal momentum (land_edge_hydro.F:201-218);
-    // ocean takes the harmonic elevation with the depth-positivity fix
-    // (ocean_edge_hydro.F:148-177, 255-259; FP64 in every variant)
-    real zx = zi, xx = xi, yx = yi, htx = hti;
-    if (kind == kOcean) {
-      const int list = (int)tk.y;
-      double zsum = 0.0;
-      for (int f = 0; f < m.nbfr; ++f) {
-        const double* zg = A.ocean_zg + ((size_t)f * m.needs + list) * 2;
-        zsum = zsum + (0.5 * (zg[0] + zg[1]) + 0.5 * (zg[1] - zg[0]) * cB2.xegp[I]);
-      }
-      const double hid = hi;
-      if (zsum * P.ifnlfa + hid <= 0) zsum = fabs(hid) + P.h0;
-      zx = (real)zsum;
-      htx = depth<kNonlin>(P, zx, hi);
-    } else {
-      const real tx = -ny, ty = nx;
-      const real qn = xi * nx + yi * ny, qt = xi * tx + yi * ty;
-      const real qne = -qn, qte = qt, den = real(1) / (nx * ty - ny * tx);
-      xx = (ty * qne - ny * qte) * den;
-      yx = (-tx * qne + nx * qte) * den;
-    }
-    const Flux3T<real> f =
-        llf<kNonlin, real>(P, zi, zx, xi, xx, yi, yx, hi, hi, hti, htx, real(1), real(1), nx, ny, real(P.g));
-    o[0] = f.f; o[1] = f.g; o[2] = f.h;
-  }
-  __syncthreads();
-
-  // ---- phase 3: volume terms per (element, area point) ----
-  for (int w = tid; w < kP2Agp * kP2Tile; w += kP2TileThreads) {
-    const int i = w / kP2Tile, el = w - i * kP2Tile;
+    const int wa = w - nep, i = wa / kP2Tile, el = wa - i * kP2Tile;
     if (el >= n) continue;
     const real* sl = qs + el * kP2SlotStride;
     real q[3 * kP2Modes], wm[kP2Modes];
@@ -566,19 +643,44 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     for (int k = 0; k < kP2Modes; ++k) wm[k] = sl[3 * kP2Modes + k];
     const real drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
     const real drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
-    const real hyb = (P.iflinbf == 0 && P.ifhybf == 1) ? geo[SGeo::kHyb * kP2Tile + el] : real(1);
+    const real hyb = hybrid ? geo[SGeo::kHyb * kP2Tile + el] : real(1);
+    P2Frc F;
+    F.cori = frc[0 * kP2Tile + el];
+    F.fric = frc[1 * kP2Tile + el];
+    F.nbar = m.manning ? geo[EGeo::kNbar * kP2Tile + el] : real(0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const bool met = P.nws != 0;
+      F.wx[a] = met ? frc[(2 + a) * kP2Tile + el] : real(0);
+      F.wy[a] = met ? frc[(5 + a) * kP2Tile + el] : real(0);
+      F.pr[a] = met ? frc[(8 + a) * kP2Tile + el] : real(0);
+    }
     real v[kP2Vol];
-    p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, tile0 + el, i, v);
+    p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, F, i, v);
 #pragma unroll
     for (int r = 0; r < kP2Vol; ++r) vol[(r * kP2Agp + i) * kP2Tile + el] = v[r];
   }
   __syncthreads();
 
-  // ---- phase 4: per (element, mode) sums in p2_elements' order, SSP ----
+  // ---- phase 3: per (element, mode) sums in p2_elements' order, SSP ----
   for (int w = tid; w < kP2Modes * kP2Tile; w += kP2TileThreads) {
     const int K = w / kP2Tile, el = w - K * kP2Tile;
     if (el >= n) continue;
     const int e = tile0 + el;
+    // the SSP combination's state operands, loaded before the sums
+    const bool hist0 = A.irk > 1;
+    double qc[3], qh0[3], rh0[3];
+#pragma unroll
+    for (int V = 0; V < 3; ++V) {
+      const size_t c = (size_t)(kP2Modes * V + K) * ne + e;
+#ifdef DGSWEM_MIXED
+      qc[V] = A.qin[c];
+#else
+      qc[V] = qs[el * kP2SlotStride + kP2Modes * V + K];  // the slot holds qin exactly
+#endif
+      qh0[V] = (hist0 && A.a[0] != 0.0) ? A.qhist[0][c] : 0.0;
+      rh0[V] = (hist0 && A.b[0] != 0.0) ? A.rhist[0][c] : 0.0;
+    }
     const unsigned info = sinfo[el], slots = sinfo[kP2Tile + el];
     real rhs[3] = {0, 0, 0}, isum[3] = {0, 0, 0};
     for (int s = 0; s < 3; ++s) {
@@ -645,29 +747,27 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     }
     // SSP-RK combination (DG_hydro_timestep.F:238-290) in FP64
     bool bad = false;
-    const bool hist0 = A.irk > 1;
 #pragma unroll
     for (int V = 0; V < 3; ++V) {
-      const int c = kP2Modes * V + K;
+      const size_t c = (size_t)(kP2Modes * V + K) * ne + e;
       const double rk = (double)rhs[V];
-      if (A.rout) A.rout[(size_t)c * ne + e] = rk;
-      const double qc = A.qin[(size_t)c * ne + e];
+      if (A.rout) A.rout[c] = rk;
       double acc = 0.0;
       if (hist0) {
-        if (A.a[0] != 0.0) acc = acc + A.a[0] * A.qhist[0][(size_t)c * ne + e];
-        if (A.b[0] != 0.0) acc = acc + A.b[0] * A.rhist[0][(size_t)c * ne + e];
+        if (A.a[0] != 0.0) acc = acc + A.a[0] * qh0[V];
+        if (A.b[0] != 0.0) acc = acc + A.b[0] * rh0[V];
       }
       for (int I = 1; I < A.irk; ++I) {
         const bool cur = I == A.irk - 1;
-        if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc : A.qhist[I][(size_t)c * ne + e]);
-        if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rk : A.rhist[I][(size_t)c * ne + e]);
+        if (A.a[I] != 0.0) acc = acc + A.a[I] * (cur ? qc[V] : A.qhist[I][c]);
+        if (A.b[I] != 0.0) acc = acc + A.b[I] * (cur ? rk : A.rhist[I][c]);
       }
       if (!hist0) {
-        if (A.a[0] != 0.0) acc = acc + A.a[0] * qc;
+        if (A.a[0] != 0.0) acc = acc + A.a[0] * qc[V];
         if (A.b[0] != 0.0) acc = acc + A.b[0] * rk;
       }
       bad = bad || isnan(acc);
-      A.qout[(size_t)c * ne + e] = acc;
+      A.qout[c] = acc;
     }
     if (bad) atomicOr(A.err, 1u);
   }
