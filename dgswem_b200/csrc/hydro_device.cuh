@@ -191,7 +191,10 @@ __host__ __device__ inline StageLayout stage_layout(int tile, int max_halo, int 
   L.qf = L.geo + kGeoRows * nt * rb;           // geo[kGeoRows][tile] in the arithmetic type
   L.vol = L.qf + (rb == 8u ? 0u : kQfStride * S * 4u);  // qf[S][kQfStride] (mixed only)
   L.res = L.vol + kVolRows * 3u * nt * rb;     // vol[kVolRows][3][tile]
-  L.wd = L.res + 15u * T * rb;                 // res[task][point][5]
+  // res[task][point][5]; the mixed variant first stages the halo's FP64
+  // values there (12 doubles an element)
+  const unsigned res_bytes = 15u * T * rb, stage_bytes = rb == 8u ? 0u : 96u * (unsigned)max_halo;
+  L.wd = L.res + (res_bytes > stage_bytes ? res_bytes : stage_bytes);
   L.gid = align16(L.wd + S * 4u);              // wd[S]
   L.tdry = align16(L.gid + (unsigned)max_halo * 4u);
   L.info = align16(L.tdry + T * 4u);          // einfo, eslot of the tile's elements

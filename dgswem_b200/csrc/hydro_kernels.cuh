@@ -852,24 +852,23 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
         }
       }
       for (int j = u; j < ntask; j += kU) cp_async8(stasks + j, m.tile_tasks + tbeg + j);
+      cp_async_commit();
+      // halo element j: its 12 FP64 values staged by cp.async in the flux
+      // region (unused until the edge phase) and converted to its FP32 slot
+      // after the volume phase, so that the gather overlaps that phase
+      const unsigned hst = smem_addr(res);
       for (int j = u; j < nh; j += kU) {
         const int g = m.tile_halo[hbeg + j];
         gid[j] = g;
         cp_async4(wds + kTile + j, A.wd + g);
-        double d[12];
 #pragma unroll
-        for (int r = 0; r < 9; ++r) d[r] = A.qin[(size_t)r * ne + g];
+        for (int r = 0; r < 9; ++r) cp_async8_s(hst + 96u * j + 8u * r, A.qin + (size_t)r * ne + g);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) d[9 + k] = d[k] + m.hb[(size_t)k * ne + g];
-        float v[12];
-#pragma unroll
-        for (int r = 0; r < 12; ++r) v[r] = (float)d[r];
-        float4* f = reinterpret_cast<float4*>(qt + (kTile + j) * kQfStride);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) f[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        for (int k = 0; k < 3; ++k) cp_async8_s(hst + 96u * j + 72u + 8u * k, m.hb + (size_t)k * ne + g);
       }
+      cp_async_commit();
     }
-    cp_async_wait_all();
+    cp_async_wait_prior();
   }
   __syncthreads();
 #else
@@ -953,8 +952,19 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
     if (el >= n || wds[el] == 0) continue;
     volume_point<kNonlin, kSph, kTile>(A, B, qt, geo, vol, i, el, tile0 + el);
   }
-#ifndef DGSWEM_MIXED
   cp_async_wait_all();  // the halo group
+#ifdef DGSWEM_MIXED
+  for (int j = tid - kTile; j >= 0 && j < nh; j += kStageThreads - kTile) {
+    const double* d = reinterpret_cast<const double*>(res) + 12 * j;  // this thread's staged copies
+    float v[12];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) v[r] = (float)d[r];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) v[9 + k] = (float)(d[k] + d[9 + k]);
+    float4* f = reinterpret_cast<float4*>(qt + (kTile + j) * kQfStride);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) f[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  }
 #endif
   __syncthreads();
 
