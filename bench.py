@@ -275,8 +275,9 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     sin 30, PR2 = 0).  FP64 and mixed rates with the FP64 line's timing
     rules, and the mixed form's error against the FP64 form after
     ``--config3-err-steps`` steps from the same state.  With
-    ``--config3-p2-steps`` > 0 the same annulus at p=2 is timed too (FP64,
-    the p2_edges + p2_elements kernels): the "p2" object."""
+    ``--config3-p2-steps`` > 0 the same annulus at p=2 is timed too (the
+    FP64 build and the mixed form, with SSP-RK(3,3)): the "p2" and "p2_mixed"
+    objects."""
     import torch
     from dgswem_b200 import Deck, HydroStep
     nr, nth = args.config3_nr, args.config3_nth
@@ -331,7 +332,7 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     if args.config3_p2_steps > 0:
         # the p=2 half: the same annulus at p=2 (18 DOFs per element), the
-        # headline FP64 build and the mixed form (p2_edges + p2_elements)
+        # headline FP64 build and the mixed form
         path2 = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth, p=2))
         deck2 = Deck(path2)
         k2 = args.config3_p2_steps
@@ -355,11 +356,13 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
                 prof = h.profile_read()
                 h.profile(False)
                 h.synchronize()
+                tiled = h.get_shapes()[0] >= 0
             out[name] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
                          "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
                          "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
                          "dtype": "f64" if name == "p2" else "mixed (f32 traces/fluxes/volume/sums, f64 state/SSP)",
-                         "kernels": "p2_edges + p2_elements per RK stage"}
+                         "kernels": ("p2_tile (64-element tiles, edge fluxes in shared memory)" if tiled
+                                     else "p2_edges + p2_elements") + " per RK stage"}
         deck2.close()
         out["p2_mixed"]["speedup_vs_fp64"] = out["p2_mixed"]["value"] / out["p2"]["value"]
         if args.config3_p2_err_steps > 0:

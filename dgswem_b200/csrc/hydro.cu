@@ -2152,7 +2152,7 @@ int dgswem_cuda_set_shapes(dgswem_cuda* h, int tile_shape, int limit_shape) {
 int dgswem_cuda_get_shapes(const dgswem_cuda* h, int* tile_shape, int* limit_shape) {
   return guarded([&]() {
     if (!h) throw Failure(DGSWEM_ERR_ARG, "null handle");
-    if (tile_shape) *tile_shape = h->tile_shape;
+    if (tile_shape) *tile_shape = (h->dofh == 6 && !h->p2_tiled) ? -1 : h->tile_shape;
     if (limit_shape) *limit_shape = h->limit_shape;
   });
 }

@@ -295,7 +295,10 @@ int dgswem_cuda_set_graph(dgswem_cuda* h, int steps);
  * dgswem_cuda_set_shapes selects one of each by index (-1 keeps the current
  * one) and rebuilds the stage tile plan; DGSWEM_ERR_ARG if the tile shape's
  * plan does not fit the mesh (the current plan stays).  Captured CUDA graphs
- * are released.
+ * are released.  dgswem_cuda_get_shapes reports the current indices; for a
+ * p=2 handle the tile shape is that of the p=2 tile kernel's plan, or -1
+ * when the mesh's tiles do not fit shared memory and the p=2 edge + element
+ * kernel pair runs instead.
  *
  * dgswem_cuda_autotune times `steps` whole steps from step `it` (forcing of
  * steps it..it+steps-1), best of `reps`, with each tile shape, then with

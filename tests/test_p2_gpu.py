@@ -35,6 +35,7 @@ def run_pair(path, nsteps, strict, state=None, met=None, mixed=False):
     orc = Oracle(path)
     with HydroStep(Deck(path), strict=None if mixed else strict, mixed=mixed) as hs:
         assert hs.dofh == 6
+        assert hs.get_shapes()[0] >= 0  # the p=2 tile kernel runs (its tiles fit shared memory)
         if state is not None:
             wd = np.ones(hs.ne, np.int32)
             hs.set_state(state[0], state[1], state[1], wd)
