@@ -6,6 +6,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -1663,7 +1664,8 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
       h->p2_edges.upload(edges.empty() ? std::vector<int>(2, 0) : edges);
       int dev_smem = 0;
       DG_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-      h->p2_tiled = h->ntile > 0 &&
+      const char* pair = std::getenv("DGSWEM_CUDA_P2_PAIR");
+      h->p2_tiled = h->ntile > 0 && !(pair && std::atoi(pair) != 0) &&
                     h->v2->tile_smem(h->mesh.max_halo, std::max(h->mesh.max_tasks, 1)) <= (size_t)dev_smem;
       if (!h->p2_tiled) {  // the edge + element pair's flux slots (slots of edges in no list stay zero)
         h->p2_ef.alloc((size_t)3 * kP2Egp * 3 * h->ne);

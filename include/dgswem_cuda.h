@@ -129,7 +129,12 @@ typedef struct dgswem_cuda dgswem_cuda;
  * ocean and interior edges, ICS=1, a whole-mesh handle; its interior-edge
  * sums run over all six modes (the reference's p=2 sums modes 1-3 only).
  * State arrays are ZE/QX/QY(6, NE).  The adjoint, state slots, tile shapes
- * and partitions are p=1 only and return DGSWEM_ERR_ARG on a p=2 handle. */
+ * and partitions are p=1 only and return DGSWEM_ERR_ARG on a p=2 handle.
+ * A p=2 stage runs one tile kernel (edge fluxes kept in shared memory), or,
+ * where a tile does not fit the device's shared memory or the environment
+ * variable DGSWEM_CUDA_P2_PAIR is set to a non-zero integer at create, an
+ * edge kernel and an element kernel with the edge-point fluxes in device
+ * memory; the strict build gives the same bits with either. */
 int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
                        dgswem_cuda** out);
 

@@ -179,3 +179,34 @@ def test_p2_graphs_match_launches(built, scratch):
             out.append(hs.state())
     for a, b, v in zip(out[0], out[1], ("ZE", "QX", "QY", "WDFLG")):
         np.testing.assert_array_equal(a, b, err_msg=v)
+
+
+@pytest.mark.parametrize("variant", ["strict", "fast", "mixed"])
+def test_p2_pair_matches_tile_kernel(built, scratch, monkeypatch, variant):
+    """The edge + element kernel pair (DGSWEM_CUDA_P2_PAIR=1 at create, the
+    fallback for tiles that do not fit shared memory) against the tile
+    kernel on the same decks: the same bits in the strict build; within
+    the variant's own bar in the fast (contractions placed by the compiler
+    per kernel: 1e-10 of the field) and mixed (FP32 terms: 1e-5) builds."""
+    kw = {"strict": {"strict": True}, "fast": {"fast": True}, "mixed": {"mixed": True}}[variant]
+    for name, path, n, state, met in decks_p2(scratch):
+        out = []
+        for pair in ("0", "1"):
+            monkeypatch.setenv("DGSWEM_CUDA_P2_PAIR", pair)
+            with HydroStep(Deck(path), **kw) as hs:
+                assert (hs.get_shapes()[0] < 0) == (pair == "1")
+                if state is not None:
+                    hs.set_state(state[0], state[1], state[1], np.ones(hs.ne, np.int32))
+                if met is not None:
+                    hs.set_met(*wind(path))
+                hs.run(1, n)
+                hs.synchronize()
+                out.append(hs.state())
+        qscale = max(np.abs(out[1][1]).max(), np.abs(out[1][2]).max(), 1e-300)  # momentum scale
+        for a, b, v in zip(out[0][:3], out[1][:3], ("ZE", "QX", "QY")):
+            if variant == "strict":
+                np.testing.assert_array_equal(a, b, err_msg=f"{variant}, {name}: {v}")
+            else:
+                scale = max(np.abs(b).max(), 1e-300) if v == "ZE" else qscale
+                bar = 1e-10 if variant == "fast" else 1e-5
+                assert np.abs(a - b).max() <= bar * scale, f"{variant}, {name}: {v}"
