@@ -266,6 +266,93 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
             "tiles": tiles, "err_vs_fp64": err}
 
 
+def config3_met(npn: int):
+    """Config 3's uniform wind stress of 0.1 Pa at 30 degrees (NWS=1:
+    WSX2 = tau/rho0 cos 30, WSY2 = tau/rho0 sin 30, PR2 = 0) on npn nodes."""
+    tau_rho = 0.1 / 1000.0
+    return (np.full(npn, tau_rho * math.cos(math.radians(30.0))), np.full(npn, tau_rho * math.sin(math.radians(30.0))),
+            np.zeros(npn))
+
+
+def config3_p2(args, stream, device: int, world: int, dist, met=None) -> dict:
+    """Config 3 at p=2: the quarter annulus of config3_arm at p=2 (18 DOFs
+    per element, SSP-RK(3,3)), the headline FP64 build and the mixed form
+    timed over ``--config3-p2-steps`` steps (the "p2" and "p2_mixed"
+    objects), and with ``--config3-p2-err-steps`` > 0 the mixed form's error
+    against FP64 on the quickly ramped copy.  ``--p2-only`` runs this alone
+    (the profiling driver of the p=2 kernels)."""
+    import torch
+    from dgswem_b200 import Deck, HydroStep
+    nr, nth, w = args.config3_nr, args.config3_nth, args.warmup
+    out = {}
+    # the p=2 half: the same annulus at p=2 (18 DOFs per element), the
+    # headline FP64 build and the mixed form
+    path2 = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth, p=2))
+    deck2 = Deck(path2)
+    if met is None:
+        met = config3_met(deck2.s.np)
+    k2 = args.config3_p2_steps
+    dofs = 3 * deck2.s.dofh
+    for name, kw in (("p2", variant_kwargs(args.variant)), ("p2_mixed", {"mixed": True})):
+        with HydroStep(deck2, device=device, **kw) as h:
+            h.set_stream(stream.cuda_stream)
+            h.set_met(*met)
+            h.run(1, w)
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.run(w + 1, k2)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms2 = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+            h.profile(True)
+            h.run(w + 1 + k2, 4)
+            prof = h.profile_read()
+            h.profile(False)
+            h.synchronize()
+            tiled = h.get_shapes()[0] >= 0
+        out[name] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
+                     "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
+                     "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
+                     "dtype": "f64" if name == "p2" else "mixed (f32 traces/fluxes/volume/sums, f64 state/SSP)",
+                     "kernels": ("p2_tile (64-element tiles, edge fluxes in shared memory)" if tiled
+                                 else "p2_edges + p2_elements") + " per RK stage"}
+    deck2.close()
+    out["p2_mixed"]["speedup_vs_fp64"] = out["p2_mixed"]["value"] / out["p2"]["value"]
+    if args.config3_p2_err_steps > 0:
+        epath2 = rank0_first(rank_env()[0], world, dist,
+                             lambda: config3_deck(args.workdir, nr, nth, p=2, dramp=args.config3_err_dramp))
+        edeck2 = Deck(epath2)
+        st2 = {}
+        for name, kw in (("fp64", variant_kwargs(args.variant)), ("mixed", {"mixed": True})):
+            with HydroStep(edeck2, device=device, **kw) as h:
+                h.set_stream(stream.cuda_stream)
+                h.set_met(*met)
+                h.run(1, args.config3_p2_err_steps)
+                h.synchronize()
+                st2[name] = (h.state(), h.modal2nodal())
+        (pf_, pnf), (pm_, pnm) = st2["fp64"], st2["mixed"]
+        ne2 = edeck2.s.ne
+        nm2 = edeck2.int_array("nm", 3 * ne2).reshape(3, ne2) - 1
+        x2, y2 = edeck2.real_array("x", edeck2.s.np), edeck2.real_array("y", edeck2.s.np)
+        hb2 = edeck2.real_array("hb", 6 * ne2).reshape(ne2, 6)
+        a2, b2, c2 = nm2
+        ar2 = 0.5 * ((x2[a2] - x2[c2]) * (y2[b2] - y2[c2]) + (x2[c2] - x2[b2]) * (y2[a2] - y2[c2]))
+        vf, vm = np.sum((pf_[0][:, 0] + hb2[:, 0]) * ar2), np.sum((pm_[0][:, 0] + hb2[:, 0]) * ar2)
+        edeck2.close()
+        out["p2_mixed"]["err_vs_fp64"] = {
+            "steps": args.config3_p2_err_steps, "ramp_days": args.config3_err_dramp,
+            "fp64_eta_nodal_max_m": float(np.abs(pnf[0]).max()),
+            "fp64_vel_nodal_max_ms": float(max(np.abs(pnf[1]).max(), np.abs(pnf[2]).max())),
+            "eta_nodal_linf_m": float(np.abs(pnm[0] - pnf[0]).max()),
+            "ze_mean_linf_m": float(np.abs(pm_[0][:, 0] - pf_[0][:, 0]).max()),
+            "vel_nodal_linf_ms": float(max(np.abs(pnm[1] - pnf[1]).max(), np.abs(pnm[2] - pnf[2]).max())),
+            "mass_rel": (vm - vf) / vf}
+    return out
+
+
 def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     """Config 3 at p=1: the quarter annulus of config 1 refined to
     ``--config3-nr`` x ``--config3-nth`` cells (8M triangles by default),
@@ -286,9 +373,7 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     t_write = time.perf_counter() - t0
     deck = Deck(path)
     npn = deck.s.np
-    tau_rho = 0.1 / 1000.0
-    met = (np.full(npn, tau_rho * math.cos(math.radians(30.0))), np.full(npn, tau_rho * math.sin(math.radians(30.0))),
-           np.zeros(npn))
+    met = config3_met(npn)
     k, w = args.config3_steps, args.warmup
     out = {"workload": f"quarter annulus {nr}x{nth} cells, {deck.s.ne} elements, FP64/mixed DG p=1, SSP-RK(2,2), "
                        "linear friction, wind 0.1 Pa at 30 degrees (NWS=1), dt=0.5 s",
@@ -331,69 +416,7 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
     edeck.close()
     out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     if args.config3_p2_steps > 0:
-        # the p=2 half: the same annulus at p=2 (18 DOFs per element), the
-        # headline FP64 build and the mixed form
-        path2 = rank0_first(rank_env()[0], world, dist, lambda: config3_deck(args.workdir, nr, nth, p=2))
-        deck2 = Deck(path2)
-        k2 = args.config3_p2_steps
-        dofs = 3 * deck2.s.dofh
-        for name, kw in (("p2", variant_kwargs(args.variant)), ("p2_mixed", {"mixed": True})):
-            with HydroStep(deck2, device=device, **kw) as h:
-                h.set_stream(stream.cuda_stream)
-                h.set_met(*met)
-                h.run(1, w)
-                torch.cuda.synchronize()
-                if world > 1:
-                    dist.barrier()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                h.run(w + 1, k2)
-                e1.record(stream)
-                torch.cuda.synchronize()
-                ms2 = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
-                h.profile(True)
-                h.run(w + 1 + k2, 4)
-                prof = h.profile_read()
-                h.profile(False)
-                h.synchronize()
-                tiled = h.get_shapes()[0] >= 0
-            out[name] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
-                         "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
-                         "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
-                         "dtype": "f64" if name == "p2" else "mixed (f32 traces/fluxes/volume/sums, f64 state/SSP)",
-                         "kernels": ("p2_tile (64-element tiles, edge fluxes in shared memory)" if tiled
-                                     else "p2_edges + p2_elements") + " per RK stage"}
-        deck2.close()
-        out["p2_mixed"]["speedup_vs_fp64"] = out["p2_mixed"]["value"] / out["p2"]["value"]
-        if args.config3_p2_err_steps > 0:
-            epath2 = rank0_first(rank_env()[0], world, dist,
-                                 lambda: config3_deck(args.workdir, nr, nth, p=2, dramp=args.config3_err_dramp))
-            edeck2 = Deck(epath2)
-            st2 = {}
-            for name, kw in (("fp64", variant_kwargs(args.variant)), ("mixed", {"mixed": True})):
-                with HydroStep(edeck2, device=device, **kw) as h:
-                    h.set_stream(stream.cuda_stream)
-                    h.set_met(*met)
-                    h.run(1, args.config3_p2_err_steps)
-                    h.synchronize()
-                    st2[name] = (h.state(), h.modal2nodal())
-            (pf_, pnf), (pm_, pnm) = st2["fp64"], st2["mixed"]
-            ne2 = edeck2.s.ne
-            nm2 = edeck2.int_array("nm", 3 * ne2).reshape(3, ne2) - 1
-            x2, y2 = edeck2.real_array("x", edeck2.s.np), edeck2.real_array("y", edeck2.s.np)
-            hb2 = edeck2.real_array("hb", 6 * ne2).reshape(ne2, 6)
-            a2, b2, c2 = nm2
-            ar2 = 0.5 * ((x2[a2] - x2[c2]) * (y2[b2] - y2[c2]) + (x2[c2] - x2[b2]) * (y2[a2] - y2[c2]))
-            vf, vm = np.sum((pf_[0][:, 0] + hb2[:, 0]) * ar2), np.sum((pm_[0][:, 0] + hb2[:, 0]) * ar2)
-            edeck2.close()
-            out["p2_mixed"]["err_vs_fp64"] = {
-                "steps": args.config3_p2_err_steps, "ramp_days": args.config3_err_dramp,
-                "fp64_eta_nodal_max_m": float(np.abs(pnf[0]).max()),
-                "fp64_vel_nodal_max_ms": float(max(np.abs(pnf[1]).max(), np.abs(pnf[2]).max())),
-                "eta_nodal_linf_m": float(np.abs(pnm[0] - pnf[0]).max()),
-                "ze_mean_linf_m": float(np.abs(pm_[0][:, 0] - pf_[0][:, 0]).max()),
-                "vel_nodal_linf_ms": float(max(np.abs(pnm[1] - pnf[1]).max(), np.abs(pnm[2] - pnf[2]).max())),
-                "mass_rel": (vm - vf) / vf}
+        out.update(config3_p2(args, stream, device, world, dist, met))
     out["mixed"]["err_vs_fp64"] = {
         "steps": args.config3_err_steps, "ramp_days": args.config3_err_dramp,
         "fp64_eta_nodal_max_m": float(np.abs(nf[0]).max()),
@@ -784,6 +807,9 @@ def main(argv=None):
     ap.add_argument("--adjoint-ny", type=int, default=316, help="cells across the adjoint beach (y)")
     ap.add_argument("--adjoint-no-fd", action="store_true",
                     help="skip the adjoint arm's finite-difference check on the 10k-element basin")
+    ap.add_argument("--p2-only", action="store_true",
+                    help="only the config-3 p=2 timing (--config3-nr/-nth/-p2-steps/-p2-err-steps): the p=2 "
+                         "kernels' profiling driver")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="run only the adjoint arm (a driver for profiling its kernels) and print its object")
     ap.add_argument("--mixed-err-steps", type=int, default=200,
@@ -805,6 +831,13 @@ def main(argv=None):
         Path(args.workdir).mkdir(parents=True, exist_ok=True)
         if rank == 0:
             print(json.dumps({"adjoint": adjoint_arm(args, local)}), flush=True)
+        return 0
+    if args.p2_only:
+        Path(args.workdir).mkdir(parents=True, exist_ok=True)
+        if rank == 0:
+            stream = torch.cuda.Stream(device=local)
+            torch.cuda.set_stream(stream)
+            print(json.dumps({"config3_p2": config3_p2(args, stream, local, 1, None)}), flush=True)
         return 0
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))

@@ -626,14 +626,18 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
   __syncthreads();
 
   // ---- phase 2: edge points (edge task, Lobatto point), then area points ----
-  const int nep = kP2Egp * ntask;
-  for (int w = tid; w < nep + kP2Agp * kP2Tile; w += kP2TileThreads) {
-    if (w < nep) {
-      const int ti = w / kP2Egp, I = w - kP2Egp * ti;
-      p2_tile_edge_point<kNonlin>(A, B, qs, geo, stasks[ti], I, res + ((size_t)ti * kP2Egp + I) * 3);
+  // (the edge items padded to whole warps: a warp's area points share the
+  // point i, so its basis values are uniform constant-memory loads)
+  const int nep = kP2Egp * ntask, nep_pad = (nep + 31) & ~31;
+  for (int w = tid; w < nep_pad + kP2Agp * kP2Tile; w += kP2TileThreads) {
+    if (w < nep_pad) {
+      if (w < nep) {
+        const int ti = w / kP2Egp, I = w - kP2Egp * ti;
+        p2_tile_edge_point<kNonlin>(A, B, qs, geo, stasks[ti], I, res + ((size_t)ti * kP2Egp + I) * 3);
+      }
       continue;
     }
-    const int wa = w - nep, i = wa / kP2Tile, el = wa - i * kP2Tile;
+    const int wa = w - nep_pad, i = wa / kP2Tile, el = wa - i * kP2Tile;
     if (el >= n) continue;
     const real* sl = qs + el * kP2SlotStride;
     real q[3 * kP2Modes], wm[kP2Modes];
@@ -722,9 +726,13 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     }
 #pragma unroll
     for (int V = 0; V < 3; ++V) rhs[V] = rhs[V] + isum[V];  // add_internal_flux
+    // the mode K and point i are the same across a warp: basis values from
+    // constant memory (uniform loads), the shared-memory pipe kept for the
+    // per-element operands
+    const BasisP2T<real>& C = cB2R;
     if (P.rainfall == 1) {
       const real src = real(7.0556e-6);
-      for (int i = 0; i < kP2Agp; ++i) rhs[0] = rhs[0] + B.srfac[K][i] * src;
+      for (int i = 0; i < kP2Agp; ++i) rhs[0] = rhs[0] + C.srfac[K][i] * src;
     }
     const real drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
     const real drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
@@ -732,14 +740,14 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
       const real* vv = vol + i * kP2Tile + el;  // row r at vv[r * kP2Agp * kP2Tile]
       const real sx = vv[6 * kP2Agp * kP2Tile], sy = vv[7 * kP2Agp * kP2Tile];
       if (K == 0) {
-        rhs[1] = rhs[1] + B.srfac[0][i] * sx;
-        rhs[2] = rhs[2] + B.srfac[0][i] * sy;
+        rhs[1] = rhs[1] + C.srfac[0][i] * sx;
+        rhs[2] = rhs[2] + C.srfac[0][i] * sy;
       } else {
-        const real dpx = B.drphi[K][i] * drdx + B.dsphi[K][i] * dsdx;
-        const real dpy = B.drphi[K][i] * drdy + B.dsphi[K][i] * dsdy;
-        const real xf = B.mw[K][i] * dpx;
-        const real yf = B.mw[K][i] * dpy;
-        const real sr = B.srfac[K][i];
+        const real dpx = C.drphi[K][i] * drdx + C.dsphi[K][i] * dsdx;
+        const real dpy = C.drphi[K][i] * drdy + C.dsphi[K][i] * dsdy;
+        const real xf = C.mw[K][i] * dpx;
+        const real yf = C.mw[K][i] * dpy;
+        const real sr = C.srfac[K][i];
         rhs[0] = rhs[0] + xf * vv[0] + yf * vv[kP2Agp * kP2Tile];
         rhs[1] = rhs[1] + xf * vv[2 * kP2Agp * kP2Tile] + yf * vv[3 * kP2Agp * kP2Tile] + sr * sx;
         rhs[2] = rhs[2] + xf * vv[4 * kP2Agp * kP2Tile] + yf * vv[5 * kP2Agp * kP2Tile] + sr * sy;
