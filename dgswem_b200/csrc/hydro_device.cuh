@@ -20,6 +20,7 @@
 // doubles per element).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 #include <cuda_runtime.h>

@@ -430,6 +430,18 @@ constexpr int kP2Tile = 64, kP2TileThreads = 384;
 // consecutive slots off one bank group (13 or 7 16-byte units, odd)
 constexpr int kP2SlotStride = sizeof(real) == 8 ? 26 : 28;
 constexpr int kP2Vol = 8;  // fx fy gx gy hx hy sx sy
+// reals per edge task's flux slots (four points x F, G, H and a pad): an odd
+// stride spreads the tasks that a warp's elements read over the banks
+constexpr int kP2ResStride = 3 * kP2Egp + 1;
+
+// the basis values a tile reads with per-thread indices (local edge and
+// point vary across a warp), kept in shared memory: the leading members of
+// BasisP2T; the rest is read warp-uniformly from constant memory
+struct P2EdgeBasis {
+  real phi_edge[3][kP2Egp][kP2Modes];
+  real edgeq[3][kP2Egp][kP2Modes];
+};
+static_assert(sizeof(P2EdgeBasis) == offsetof(BasisP2T<real>, phi_area), "the leading members of BasisP2T");
 
 struct P2Layout {
   unsigned qs, geo, frc, vol, res, info, tasks, bytes;
@@ -437,12 +449,12 @@ struct P2Layout {
 __host__ __device__ inline P2Layout p2_layout(int max_halo, int max_tasks) {
   P2Layout L;
   const unsigned S = (unsigned)(kP2Tile + max_halo), T = (unsigned)max_tasks, rb = (unsigned)sizeof(real);
-  L.qs = align16((unsigned)sizeof(BasisP2T<real>));
+  L.qs = align16((unsigned)sizeof(P2EdgeBasis));
   L.geo = align16(L.qs + S * kP2SlotStride * rb);
   L.frc = align16(L.geo + kGeoRows * kP2Tile * rb);
   L.vol = align16(L.frc + P2Frc::kRows * kP2Tile * rb);
   L.res = align16(L.vol + kP2Vol * kP2Agp * kP2Tile * rb);
-  L.info = align16(L.res + T * kP2Egp * 3 * rb);
+  L.info = align16(L.res + T * kP2ResStride * rb);
   L.tasks = align16(L.info + 2u * kP2Tile * 4u);
   L.bytes = align16(L.tasks + T * 8u);
   return L;
@@ -459,7 +471,7 @@ __device__ __forceinline__ void p2_slot_store(const P2Args& A, int g, real* dst)
 
 // trace at point (led, gp) of the six modes at slot[off .. off+5], mode 1
 // first, as trace6 sums them
-__device__ __forceinline__ real p2_slot_trace(const BasisP2T<real>& B, const real* slot, int off, int led, int gp) {
+__device__ __forceinline__ real p2_slot_trace(const P2EdgeBasis& B, const real* slot, int off, int led, int gp) {
   const real* phi = B.phi_edge[led][gp];
   real t = slot[off];
 #pragma unroll
@@ -483,7 +495,7 @@ __device__ __forceinline__ real p2_hybrid(const Physics& P, const real* sl) {
 // flux in the in/ex orientation for an interior edge, else the land / ocean
 // ghost state and its flux
 template <bool kNonlin>
-__device__ __forceinline__ void p2_tile_edge_point(const P2Args& A, const BasisP2T<real>& B, const real* qs,
+__device__ __forceinline__ void p2_tile_edge_point(const P2Args& A, const P2EdgeBasis& B, const real* qs,
                                                    const real* geo, uint2 tk, int I, real* o) {
   const MeshView& m = A.m;
   const Physics& P = A.ph;
@@ -553,7 +565,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
   const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
   const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
   const P2Layout L = p2_layout(m.max_halo, m.max_tasks);
-  BasisP2T<real>& B = *reinterpret_cast<BasisP2T<real>*>(smem_raw);
+  P2EdgeBasis& B = *reinterpret_cast<P2EdgeBasis*>(smem_raw);
   real* qs = reinterpret_cast<real*>(smem_raw + L.qs);
   real* geo = reinterpret_cast<real*>(smem_raw + L.geo);
   real* frc = reinterpret_cast<real*>(smem_raw + L.frc);  // cori, fric, wx[3], wy[3], pr[3]: [kRows][kP2Tile]
@@ -566,7 +578,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
   {
     const real* src = reinterpret_cast<const real*>(&cB2R);
     real* dst = reinterpret_cast<real*>(&B);
-    for (int i = tid; i < (int)(sizeof(BasisP2T<real>) / sizeof(real)); i += kP2TileThreads) dst[i] = src[i];
+    for (int i = tid; i < (int)(sizeof(P2EdgeBasis) / sizeof(real)); i += kP2TileThreads) dst[i] = src[i];
   }
   // ---- phase 1: slots, geometry rows, edge info, task words, forcing ----
   // Exact copies go by cp.async (issued back to back, one wait); the halo
@@ -633,7 +645,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     if (w < nep_pad) {
       if (w < nep) {
         const int ti = w / kP2Egp, I = w - kP2Egp * ti;
-        p2_tile_edge_point<kNonlin>(A, B, qs, geo, stasks[ti], I, res + ((size_t)ti * kP2Egp + I) * 3);
+        p2_tile_edge_point<kNonlin>(A, B, qs, geo, stasks[ti], I, res + (size_t)ti * kP2ResStride + I * 3);
       }
       continue;
     }
@@ -692,7 +704,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
       const unsigned kind = ei_kind(info, l);
       if (kind == kNone) continue;
       const int ti = (slots >> (10 * l)) & kNoTask;
-      const real* r = res + (size_t)ti * kP2Egp * 3;
+      const real* r = res + (size_t)ti * kP2ResStride;
       if (kind == kInterior) {
         const bool is_in = ei_flag(info, l) != 0;
         const real edfac = geo[(EGeo::kEdfac + l) * kP2Tile + el];
@@ -717,7 +729,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
         const real areas = G[(size_t)EGeo::kAreas * ne + e];
         const real xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
         for (int I = 0; I < kP2Egp; ++I) {
-          const real wk = real(2) * B.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * B.wegp[I];
+          const real wk = real(2) * cB2R.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * cB2R.wegp[I];
           rhs[0] = rhs[0] - wk * r[I * 3];
           rhs[1] = rhs[1] - wk * r[I * 3 + 1];
           rhs[2] = rhs[2] - wk * r[I * 3 + 2];
