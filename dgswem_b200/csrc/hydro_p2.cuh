@@ -435,13 +435,14 @@ constexpr int kP2Vol = 8;  // fx fy gx gy hx hy sx sy
 constexpr int kP2ResStride = 3 * kP2Egp + 1;
 
 // the basis values a tile reads with per-thread indices (local edge and
-// point vary across a warp), kept in shared memory: the leading members of
-// BasisP2T; the rest is read warp-uniformly from constant memory
+// point vary across a warp), kept in shared memory with rows of seven (the
+// twelve (edge, point) rows a warp reads fall on distinct banks); the rest
+// of BasisP2T is read warp-uniformly from constant memory
+constexpr int kP2EbRow = kP2Modes + 1;
 struct P2EdgeBasis {
-  real phi_edge[3][kP2Egp][kP2Modes];
-  real edgeq[3][kP2Egp][kP2Modes];
+  real phi_edge[3][kP2Egp][kP2EbRow];
+  real edgeq[3][kP2Egp][kP2EbRow];
 };
-static_assert(sizeof(P2EdgeBasis) == offsetof(BasisP2T<real>, phi_area), "the leading members of BasisP2T");
 
 struct P2Layout {
   unsigned qs, geo, frc, vol, res, info, tasks, bytes;
@@ -575,10 +576,10 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
   uint2* stasks = reinterpret_cast<uint2*>(smem_raw + L.tasks);
   const real* G = egeo_r(m);
   const bool hybrid = P.iflinbf == 0 && P.ifhybf == 1;
-  {
-    const real* src = reinterpret_cast<const real*>(&cB2R);
-    real* dst = reinterpret_cast<real*>(&B);
-    for (int i = tid; i < (int)(sizeof(P2EdgeBasis) / sizeof(real)); i += kP2TileThreads) dst[i] = src[i];
+  for (int i = tid; i < 3 * kP2Egp * kP2Modes; i += kP2TileThreads) {
+    const int row = i / kP2Modes, k = i - row * kP2Modes;
+    (&B.phi_edge[0][0][0])[row * kP2EbRow + k] = (&cB2R.phi_edge[0][0][0])[i];
+    (&B.edgeq[0][0][0])[row * kP2EbRow + k] = (&cB2R.edgeq[0][0][0])[i];
   }
   // ---- phase 1: slots, geometry rows, edge info, task words, forcing ----
   // Exact copies go by cp.async (issued back to back, one wait); the halo
