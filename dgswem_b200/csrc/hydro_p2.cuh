@@ -700,6 +700,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     }
     const unsigned info = sinfo[el], slots = sinfo[kP2Tile + el];
     real rhs[3] = {0, 0, 0}, isum[3] = {0, 0, 0};
+#pragma unroll
     for (int s = 0; s < 3; ++s) {
       const int l = ei_order(info, s);
       const unsigned kind = ei_kind(info, l);
@@ -710,25 +711,23 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
         const bool is_in = ei_flag(info, l) != 0;
         const real edfac = geo[(EGeo::kEdfac + l) * kP2Tile + el];
         real acc[3] = {0, 0, 0};
+#pragma unroll
         for (int I = 0; I < kP2Egp; ++I) {
           const int j = is_in ? I : kP2Egp - 1 - I;
           const real wk = edfac * B.edgeq[l][j][K];
+          // the in side subtracts: acc + (-wk) * v equals acc - wk * v exactly
+          const real ws = is_in ? -wk : wk;
           const real v0 = r[I * 3], v1 = r[I * 3 + 1], v2 = r[I * 3 + 2];
-          if (is_in) {
-            acc[0] = acc[0] - wk * v0;
-            acc[1] = acc[1] - wk * v1;
-            acc[2] = acc[2] - wk * v2;
-          } else {
-            acc[0] = acc[0] + wk * v0;
-            acc[1] = acc[1] + wk * v1;
-            acc[2] = acc[2] + wk * v2;
-          }
+          acc[0] = acc[0] + ws * v0;
+          acc[1] = acc[1] + ws * v1;
+          acc[2] = acc[2] + ws * v2;
         }
 #pragma unroll
         for (int V = 0; V < 3; ++V) isum[V] = isum[V] + acc[V];
       } else {
         const real areas = G[(size_t)EGeo::kAreas * ne + e];
         const real xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
+#pragma unroll
         for (int I = 0; I < kP2Egp; ++I) {
           const real wk = real(2) * cB2R.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * cB2R.wegp[I];
           rhs[0] = rhs[0] - wk * r[I * 3];
@@ -749,6 +748,7 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     }
     const real drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
     const real drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
+#pragma unroll
     for (int i = 0; i < kP2Agp; ++i) {
       const real* vv = vol + i * kP2Tile + el;  // row r at vv[r * kP2Agp * kP2Tile]
       const real sx = vv[6 * kP2Agp * kP2Tile], sy = vv[7 * kP2Agp * kP2Tile];
