@@ -1088,6 +1088,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
   double q[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) q[c] = L.q[(size_t)c * ne + e];
+  // the element means (mode 1 of ZE, QX, QY) and WDFLG change only in
+  // WETDRY: values whose bits did not change are not stored again (modes
+  // 2-3 are rebuilt by the limiter and stored always)
+  const double m0 = q[0], m3 = q[3], m6 = q[6];
   if (L.slopeflag != 0) {
 #pragma unroll
     for (int var = 0; var < 3; ++var) {
@@ -1153,6 +1157,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
     for (int v = 0; v < 3; ++v) dpn[v] = L.m.dp[nd[v]];
     const double dpe_min = fmin(fmin(dpn[0], dpn[1]), dpn[2]);
     int wd = L.wd[e];
+    const int wd_read = wd;
     int ndry = 0, hmax_i = 0;
     double hmax = ZERO, ht[3], zn[3];
 #pragma unroll
@@ -1248,10 +1253,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
         wd = 0;
       }
     }
-    L.wd[e] = wd;
+    if (wd != wd_read) L.wd[e] = wd;
   }
+  auto same = [](double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); };
+  if (!same(q[0], m0)) L.q[e] = q[0];
+  if (!same(q[3], m3)) L.q[(size_t)3 * ne + e] = q[3];
+  if (!same(q[6], m6)) L.q[(size_t)6 * ne + e] = q[6];
 #pragma unroll
-  for (int c = 0; c < 9; ++c) L.q[(size_t)c * ne + e] = q[c];
+  for (int c = 0; c < 9; ++c)
+    if (c % 3 != 0) L.q[(size_t)c * ne + e] = q[c];
 }
 
 // write_results.F:14-170 (modal2nodal) + NODECODE from the wet flags; node n
