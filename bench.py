@@ -316,7 +316,7 @@ def config3_p2(args, stream, device: int, world: int, dist, met=None) -> dict:
         out[name] = {"value": world * dofs * deck2.s.ne * deck2.s.nrk * k2 / (ms2 / 1e3), "unit": "DOF-stage/s",
                      "dofs_per_element": dofs, "steps": k2, "ms_per_step": ms2 / k2,
                      "stage_ms": prof["stage_p1"][0] / max(prof["stage_p1"][1], 1),
-                     "dtype": "f64" if name == "p2" else "mixed (f32 traces/fluxes/volume/sums, f64 state/SSP)",
+                     "dtype": "f64" if name == "p2" else "mixed (f32 traces/fluxes/volume terms, f64 sums/state/SSP)",
                      "kernels": ("p2_tile (64-element tiles, edge fluxes in shared memory)" if tiled
                                  else "p2_edges + p2_elements") + " per RK stage"}
     deck2.close()

@@ -1,10 +1,12 @@
 // hydro_p2.cuh -- the p=2 stage (six modes per variable, four Gauss-Lobatto
-// points per edge, the six-point area rule): an edge kernel and an element
-// kernel per RK stage.  Included after hydro_kernels.cuh (its LLF flux,
-// depth, trace_depth, the arithmetic type `real`) by kernels_p2_fast.cu /
-// kernels_p2_strict.cu (FP64) and kernels_p2_mixed.cu (edge traces, fluxes,
-// volume terms and right-hand-side sums in FP32; state, SSP combination and
-// the ocean depth-positivity fix in FP64, as at p=1) with DGSWEM_VARIANT set.
+// points per edge, the six-point area rule): a tile kernel per RK stage, or
+// an edge kernel and an element kernel where a tile does not fit shared
+// memory.  Included after hydro_kernels.cuh (its LLF flux, depth,
+// trace_depth, the arithmetic type `real`) by kernels_p2_fast.cu /
+// kernels_p2_strict.cu (FP64) and kernels_p2_mixed.cu (edge traces, fluxes
+// and volume terms in FP32; the right-hand-side sums and their weights, the
+// state, the SSP combination and the ocean depth-positivity fix in FP64)
+// with DGSWEM_VARIANT set.
 // The arithmetic follows the p=1 kernels term for term, generalised over the
 // modes and points as the reference's p-generic boundary-edge code
 // (land_edge_hydro.F:144,273) is; the interior-edge sums run over every mode
@@ -286,8 +288,18 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
   }
   // all three variables' sums at once (no per-point volume array): each
   // (variable, mode) sum takes the same terms in the same order as above
+  // (the sums and their weights in FP64 in every variant, as p2_tile's)
+#ifdef DGSWEM_MIXED
+  using acc_t = double;
+  const BasisP2& W = cB2;
+  const acc_t drdxw = drdx, dsdxw = dsdx, drdyw = drdy, dsdyw = dsdy;
+#else
+  using acc_t = real;
+  const BasisP2T<real>& W = B;
+  const real drdxw = drdx, dsdxw = dsdx, drdyw = drdy, dsdyw = dsdy;
+#endif
   const unsigned info = m.einfo[e];
-  real rhs[3][kP2Modes], isum[3][kP2Modes];
+  acc_t rhs[3][kP2Modes], isum[3][kP2Modes];
 #pragma unroll
   for (int V = 0; V < 3; ++V)
 #pragma unroll
@@ -299,18 +311,18 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
     const real* efl = ef + (size_t)(e * 3 + l) * kP2Egp * 3;
     if (kind == kInterior) {
       const bool is_in = ei_flag(info, l) != 0;
-      const real edfac = G[(size_t)(EGeo::kEdfac + l) * ne + e];
-      real acc[3][kP2Modes];
+      const acc_t edfac = G[(size_t)(EGeo::kEdfac + l) * ne + e];
+      acc_t acc[3][kP2Modes];
 #pragma unroll
       for (int V = 0; V < 3; ++V)
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) acc[V][k] = 0;
       for (int I = 0; I < kP2Egp; ++I) {
         const int j = is_in ? I : kP2Egp - 1 - I;
-        const real v0 = efl[j * 3], v1 = efl[j * 3 + 1], v2 = efl[j * 3 + 2];
+        const acc_t v0 = efl[j * 3], v1 = efl[j * 3 + 1], v2 = efl[j * 3 + 2];
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) {
-          const real wk = edfac * B.edgeq[l][j][k];
+          const acc_t wk = edfac * W.edgeq[l][j][k];
           if (is_in) {
             acc[0][k] = acc[0][k] - wk * v0;
             acc[1][k] = acc[1][k] - wk * v1;
@@ -327,13 +339,13 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) isum[V][k] = isum[V][k] + acc[V][k];
     } else {
-      const real areas = G[(size_t)EGeo::kAreas * ne + e];
-      const real xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
+      const acc_t areas = G[(size_t)EGeo::kAreas * ne + e];
+      const acc_t xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
       for (int I = 0; I < kP2Egp; ++I) {
-        const real v0 = efl[I * 3], v1 = efl[I * 3 + 1], v2 = efl[I * 3 + 2];
+        const acc_t v0 = efl[I * 3], v1 = efl[I * 3 + 1], v2 = efl[I * 3 + 2];
 #pragma unroll
         for (int k = 0; k < kP2Modes; ++k) {
-          const real wk = real(2) * B.m_inv[k] / areas * xlen * B.phi_edge[l][I][k] * B.wegp[I];
+          const acc_t wk = acc_t(2) * W.m_inv[k] / areas * xlen * W.phi_edge[l][I][k] * W.wegp[I];
           rhs[0][k] = rhs[0][k] - wk * v0;
           rhs[1][k] = rhs[1][k] - wk * v1;
           rhs[2][k] = rhs[2][k] - wk * v2;
@@ -346,26 +358,29 @@ __global__ void __launch_bounds__(128, 4) p2_elements(const __grid_constant__ P2
 #pragma unroll
     for (int k = 0; k < kP2Modes; ++k) rhs[V][k] = rhs[V][k] + isum[V][k];  // add_internal_flux
   if (P.rainfall == 1) {
-    const real src = real(7.0556e-6);
+    const acc_t src = acc_t(7.0556e-6);
     for (int i = 0; i < kP2Agp; ++i)
 #pragma unroll
-      for (int k = 0; k < kP2Modes; ++k) rhs[0][k] = rhs[0][k] + B.srfac[k][i] * src;
+      for (int k = 0; k < kP2Modes; ++k) rhs[0][k] = rhs[0][k] + W.srfac[k][i] * src;
   }
   for (int i = 0; i < kP2Agp; ++i) {
     real vol[8];
     p2_volume<kNonlin>(A, q, wm, drdx, dsdx, drdy, dsdy, hyb, p2_force(A, e), i, vol);
-    rhs[1][0] = rhs[1][0] + B.srfac[0][i] * vol[6];
-    rhs[2][0] = rhs[2][0] + B.srfac[0][i] * vol[7];
+    acc_t vw[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) vw[r] = vol[r];
+    rhs[1][0] = rhs[1][0] + W.srfac[0][i] * vw[6];
+    rhs[2][0] = rhs[2][0] + W.srfac[0][i] * vw[7];
 #pragma unroll
     for (int k = 1; k < kP2Modes; ++k) {
-      const real dpx = B.drphi[k][i] * drdx + B.dsphi[k][i] * dsdx;
-      const real dpy = B.drphi[k][i] * drdy + B.dsphi[k][i] * dsdy;
-      const real xf = B.mw[k][i] * dpx;
-      const real yf = B.mw[k][i] * dpy;
-      const real sr = B.srfac[k][i];
-      rhs[0][k] = rhs[0][k] + xf * vol[0] + yf * vol[1];
-      rhs[1][k] = rhs[1][k] + xf * vol[2] + yf * vol[3] + sr * vol[6];
-      rhs[2][k] = rhs[2][k] + xf * vol[4] + yf * vol[5] + sr * vol[7];
+      const acc_t dpx = W.drphi[k][i] * drdxw + W.dsphi[k][i] * dsdxw;
+      const acc_t dpy = W.drphi[k][i] * drdyw + W.dsphi[k][i] * dsdyw;
+      const acc_t xf = W.mw[k][i] * dpx;
+      const acc_t yf = W.mw[k][i] * dpy;
+      const acc_t sr = W.srfac[k][i];
+      rhs[0][k] = rhs[0][k] + xf * vw[0] + yf * vw[1];
+      rhs[1][k] = rhs[1][k] + xf * vw[2] + yf * vw[3] + sr * vw[6];
+      rhs[2][k] = rhs[2][k] + xf * vw[4] + yf * vw[5] + sr * vw[7];
     }
   }
   // SSP-RK combination (DG_hydro_timestep.F:238-290) in FP64; zero
@@ -434,14 +449,14 @@ constexpr int kP2Vol = 8;  // fx fy gx gy hx hy sx sy
 // stride spreads the tasks that a warp's elements read over the banks
 constexpr int kP2ResStride = 3 * kP2Egp + 1;
 
-// the basis values a tile reads with per-thread indices (local edge and
-// point vary across a warp), kept in shared memory with rows of seven (the
-// twelve (edge, point) rows a warp reads fall on distinct banks); the rest
-// of BasisP2T is read warp-uniformly from constant memory
+// the edge traces' basis values, read with per-lane indices (local edge and
+// point vary across a warp) by the edge points, kept in shared memory with
+// rows of seven (the twelve (edge, point) rows a warp reads fall on
+// distinct banks); the sums read their edge weights from constant memory,
+// which takes that load off the shared-memory pipe
 constexpr int kP2EbRow = kP2Modes + 1;
 struct P2EdgeBasis {
   real phi_edge[3][kP2Egp][kP2EbRow];
-  real edgeq[3][kP2Egp][kP2EbRow];
 };
 
 struct P2Layout {
@@ -579,7 +594,6 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
   for (int i = tid; i < 3 * kP2Egp * kP2Modes; i += kP2TileThreads) {
     const int row = i / kP2Modes, k = i - row * kP2Modes;
     (&B.phi_edge[0][0][0])[row * kP2EbRow + k] = (&cB2R.phi_edge[0][0][0])[i];
-    (&B.edgeq[0][0][0])[row * kP2EbRow + k] = (&cB2R.edgeq[0][0][0])[i];
   }
   // ---- phase 1: slots, geometry rows, edge info, task words, forcing ----
   // Exact copies go by cp.async (issued back to back, one wait); the halo
@@ -699,7 +713,20 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
       rh0[V] = (hist0 && A.b[0] != 0.0) ? A.rhist[0][c] : 0.0;
     }
     const unsigned info = sinfo[el], slots = sinfo[kP2Tile + el];
-    real rhs[3] = {0, 0, 0}, isum[3] = {0, 0, 0};
+    // The sums and their weights in FP64 in every variant: the mixed form
+    // rounds only the operands (fluxes, volume terms) to FP32.  With FP32
+    // weights the hydrostatic pressure's edge and volume integrals no longer
+    // cancel to FP32 precision, and on a fine mesh the residual drives a
+    // spurious flow (config 3 at 8M elements after 5000 steps: 1.5e-5 m,
+    // against 3.5e-6 m with FP64 weights and sums).
+#ifdef DGSWEM_MIXED
+    using acc_t = double;
+    const BasisP2& CW = cB2;
+#else
+    using acc_t = real;
+    const BasisP2T<real>& CW = cB2R;
+#endif
+    acc_t rhs[3] = {0, 0, 0}, isum[3] = {0, 0, 0};
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
       const int l = ei_order(info, s);
@@ -709,15 +736,15 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
       const real* r = res + (size_t)ti * kP2ResStride;
       if (kind == kInterior) {
         const bool is_in = ei_flag(info, l) != 0;
-        const real edfac = geo[(EGeo::kEdfac + l) * kP2Tile + el];
-        real acc[3] = {0, 0, 0};
+        const acc_t edfac = geo[(EGeo::kEdfac + l) * kP2Tile + el];
+        acc_t acc[3] = {0, 0, 0};
 #pragma unroll
         for (int I = 0; I < kP2Egp; ++I) {
           const int j = is_in ? I : kP2Egp - 1 - I;
-          const real wk = edfac * B.edgeq[l][j][K];
+          const acc_t wk = edfac * (acc_t)CW.edgeq[l][j][K];
           // the in side subtracts: acc + (-wk) * v equals acc - wk * v exactly
-          const real ws = is_in ? -wk : wk;
-          const real v0 = r[I * 3], v1 = r[I * 3 + 1], v2 = r[I * 3 + 2];
+          const acc_t ws = is_in ? -wk : wk;
+          const acc_t v0 = r[I * 3], v1 = r[I * 3 + 1], v2 = r[I * 3 + 2];
           acc[0] = acc[0] + ws * v0;
           acc[1] = acc[1] + ws * v1;
           acc[2] = acc[2] + ws * v2;
@@ -725,14 +752,14 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
 #pragma unroll
         for (int V = 0; V < 3; ++V) isum[V] = isum[V] + acc[V];
       } else {
-        const real areas = G[(size_t)EGeo::kAreas * ne + e];
-        const real xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
+        const acc_t areas = G[(size_t)EGeo::kAreas * ne + e];
+        const acc_t xlen = G[(size_t)(EGeo::kXlen + l) * ne + e];
 #pragma unroll
         for (int I = 0; I < kP2Egp; ++I) {
-          const real wk = real(2) * cB2R.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * cB2R.wegp[I];
-          rhs[0] = rhs[0] - wk * r[I * 3];
-          rhs[1] = rhs[1] - wk * r[I * 3 + 1];
-          rhs[2] = rhs[2] - wk * r[I * 3 + 2];
+          const acc_t wk = acc_t(2) * CW.m_inv[K] / areas * xlen * CW.phi_edge[l][I][K] * CW.wegp[I];
+          rhs[0] = rhs[0] - wk * (acc_t)r[I * 3];
+          rhs[1] = rhs[1] - wk * (acc_t)r[I * 3 + 1];
+          rhs[2] = rhs[2] - wk * (acc_t)r[I * 3 + 2];
         }
       }
     }
@@ -741,29 +768,29 @@ __global__ void __launch_bounds__(kP2TileThreads, 2) p2_tile(const __grid_consta
     // the mode K and point i are the same across a warp: basis values from
     // constant memory (uniform loads), the shared-memory pipe kept for the
     // per-element operands
-    const BasisP2T<real>& C = cB2R;
+    const auto& C = CW;
     if (P.rainfall == 1) {
-      const real src = real(7.0556e-6);
+      const acc_t src = acc_t(7.0556e-6);
       for (int i = 0; i < kP2Agp; ++i) rhs[0] = rhs[0] + C.srfac[K][i] * src;
     }
-    const real drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
-    const real drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
+    const acc_t drdx = geo[EGeo::kDrdx * kP2Tile + el], dsdx = geo[EGeo::kDsdx * kP2Tile + el];
+    const acc_t drdy = geo[EGeo::kDrdy * kP2Tile + el], dsdy = geo[EGeo::kDsdy * kP2Tile + el];
 #pragma unroll
     for (int i = 0; i < kP2Agp; ++i) {
       const real* vv = vol + i * kP2Tile + el;  // row r at vv[r * kP2Agp * kP2Tile]
-      const real sx = vv[6 * kP2Agp * kP2Tile], sy = vv[7 * kP2Agp * kP2Tile];
+      const acc_t sx = vv[6 * kP2Agp * kP2Tile], sy = vv[7 * kP2Agp * kP2Tile];
       if (K == 0) {
         rhs[1] = rhs[1] + C.srfac[0][i] * sx;
         rhs[2] = rhs[2] + C.srfac[0][i] * sy;
       } else {
-        const real dpx = C.drphi[K][i] * drdx + C.dsphi[K][i] * dsdx;
-        const real dpy = C.drphi[K][i] * drdy + C.dsphi[K][i] * dsdy;
-        const real xf = C.mw[K][i] * dpx;
-        const real yf = C.mw[K][i] * dpy;
-        const real sr = C.srfac[K][i];
-        rhs[0] = rhs[0] + xf * vv[0] + yf * vv[kP2Agp * kP2Tile];
-        rhs[1] = rhs[1] + xf * vv[2 * kP2Agp * kP2Tile] + yf * vv[3 * kP2Agp * kP2Tile] + sr * sx;
-        rhs[2] = rhs[2] + xf * vv[4 * kP2Agp * kP2Tile] + yf * vv[5 * kP2Agp * kP2Tile] + sr * sy;
+        const acc_t dpx = C.drphi[K][i] * drdx + C.dsphi[K][i] * dsdx;
+        const acc_t dpy = C.drphi[K][i] * drdy + C.dsphi[K][i] * dsdy;
+        const acc_t xf = C.mw[K][i] * dpx;
+        const acc_t yf = C.mw[K][i] * dpy;
+        const acc_t sr = C.srfac[K][i];
+        rhs[0] = rhs[0] + xf * (acc_t)vv[0] + yf * (acc_t)vv[kP2Agp * kP2Tile];
+        rhs[1] = rhs[1] + xf * (acc_t)vv[2 * kP2Agp * kP2Tile] + yf * (acc_t)vv[3 * kP2Agp * kP2Tile] + sr * sx;
+        rhs[2] = rhs[2] + xf * (acc_t)vv[4 * kP2Agp * kP2Tile] + yf * (acc_t)vv[5 * kP2Agp * kP2Tile] + sr * sy;
       }
     }
     // SSP-RK combination (DG_hydro_timestep.F:238-290) in FP64

@@ -118,8 +118,11 @@ typedef struct dgswem_cuda dgswem_cuda;
  * sweeps (on deviations from the element mean) run in FP32; the state
  * (ZE/QX/QY modes), the SSP-RK combination (so the element-mean elevation
  * accumulates across stages in FP64), the ocean depth-positivity fix, the
- * node min/max and WETDRY stay FP64.  Results differ from the FP64 forms by
- * the FP32 rounding.  Excludes the other flags. */
+ * node min/max and WETDRY stay FP64; on a p=2 handle the right-hand-side
+ * sums and their weights stay FP64 too (the hydrostatic pressure's edge and
+ * volume integrals cancel to FP32 precision only with FP64 weights).
+ * Results differ from the FP64 forms by the FP32 rounding.  Excludes the
+ * other flags. */
 #define DGSWEM_CUDA_MIXED 2
 
 /* Copies the setup to GPU `device` and builds the device layout.
