@@ -673,7 +673,7 @@ __device__ __forceinline__ void sum_mode(const StageArgs& A, const BasisT<real>&
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
         const int j = is_in ? I : 2 - I;
-        const real wk = edfac * B.edgeq[l][j][K];
+        const real wk = edfac * C.edgeq[l][j][K];  // constant memory: off the shared-memory pipe
         const real* rv = r + 5 * I;
         const real val[3] = {rv[0], rv[c1], rv[c1 + 1]};
 #pragma unroll
@@ -692,7 +692,7 @@ __device__ __forceinline__ void sum_mode(const StageArgs& A, const BasisT<real>&
       const real xlen = egeo_r(m)[(size_t)(EGeo::kXlen + l) * ne + e];
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
-        const real wk = real(2) * C.m_inv[K] / areas * xlen * B.phi_edge[l][I][K] * C.wegp[I];
+        const real wk = real(2) * C.m_inv[K] / areas * xlen * C.phi_edge[l][I][K] * C.wegp[I];
 #pragma unroll
         for (int V = 0; V < 3; ++V) rhs[V] = rhs[V] - wk * r[5 * I + V];
       }
