@@ -994,8 +994,8 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
       const int gex = sex < kTile ? tile0 + sex : gid[sex - kTile];
       const int gp_in = I, gp_ex = 2 - I;
       real zi, xi, yi, wi, zx, xx, yx, wx, hi, hti, hx, htx;
-      slot_trace(B, qt, sin, led_in, gp_in, zi, xi, yi, wi);
-      slot_trace(B, qt, sex, led_ex, gp_ex, zx, xx, yx, wx);
+      slot_trace(cBasisR, qt, sin, led_in, gp_in, zi, xi, yi, wi);
+      slot_trace(cBasisR, qt, sex, led_ex, gp_ex, zx, xx, yx, wx);
       trace_depth<kNonlin>(P, zi, wi, hi, hti);
       trace_depth<kNonlin>(P, zx, wx, hx, htx);
       const real sfi = kSph ? (real)m.sfac_edge[(size_t)(led_in * 3 + gp_in) * ne + gin] : real(1);
@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
     } else {
       if (wd_in == 0) continue;
       real zi, xi, yi, wi, zx, xx, yx, hi, hti;
-      slot_trace(B, qt, sin, led_in, I, zi, xi, yi, wi);
+      slot_trace(cBasisR, qt, sin, led_in, I, zi, xi, yi, wi);
       trace_depth<kNonlin>(P, zi, wi, hi, hti);
       const real sfi = kSph ? (real)m.sfac_edge[(size_t)(led_in * 3 + I) * ne + gin] : real(1);
       ghost_state(A, kind, (int)tk.y, I, zi, xi, yi, hi, nx, ny, zx, xx, yx);

@@ -487,7 +487,8 @@ __device__ __forceinline__ void p2_slot_store(const P2Args& A, int g, real* dst)
 
 // trace at point (led, gp) of the six modes at slot[off .. off+5], mode 1
 // first, as trace6 sums them
-__device__ __forceinline__ real p2_slot_trace(const P2EdgeBasis& B, const real* slot, int off, int led, int gp) {
+template <class Basis>
+__device__ __forceinline__ real p2_slot_trace(const Basis& B, const real* slot, int off, int led, int gp) {
   const real* phi = B.phi_edge[led][gp];
   real t = slot[off];
 #pragma unroll
