@@ -185,7 +185,7 @@ __host__ __device__ inline StageLayout stage_layout(int tile, int max_halo, int 
   const unsigned nt = (unsigned)tile;
   const unsigned S = nt + (unsigned)max_halo;
   const unsigned T = (unsigned)max_tasks;
-  L.qs = align16(rb == 8u ? (unsigned)sizeof(BasisT<double>) : (unsigned)sizeof(BasisT<float>));
+  L.qs = 0;  // the basis tables are read from constant memory
   // qs[S][kQStride]: ZE, QX, QY, HB modes (mixed: the tile's own slots only,
   // for the FP64 SSP combination; the edge and volume terms read qf)
   L.geo = L.qs + kQStride * (rb == 8u ? S : nt) * 8u;

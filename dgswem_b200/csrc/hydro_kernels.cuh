@@ -621,14 +621,15 @@ __device__ __forceinline__ void volume_point(const StageArgs& A, const BasisT<re
 // reference's order -- boundary edges, interior edges in edge-number order
 // (the slot sum of add_internal_flux), rain, area points -- then the SSP
 // combination (DG_hydro_timestep.F:238-290) written to qout.  The edge and
-// area-point weights of mode K are formed once for the three variables.  B
-// is the shared-memory copy of the basis (runtime-indexed tables), cBasisR
-// the constant-memory one (K is the same for a whole warp, the point
-// indices are fixed by unrolled loops).  The sums are in the arithmetic
+// area-point weights of mode K are formed once for the three variables.  The
+// basis tables come from constant memory (cBasisR): K is the same for a
+// whole warp and the point indices are fixed by unrolled loops; the edge
+// weights' per-lane (edge, point) rows cost a few distinct addresses a warp
+// but keep the load off the shared-memory pipe.  The sums are in the arithmetic
 // type, the SSP combination in FP64 (in the mixed variant: the RHS rounded
 // to FP32, the stage states and their combination FP64).
 template <bool kNonlin, int kTile>
-__device__ __forceinline__ void sum_mode(const StageArgs& A, const BasisT<real>& B, const double* qs,
+__device__ __forceinline__ void sum_mode(const StageArgs& A, const double* qs,
                                          const real* geo, const real* vol, const real* res, const int* tdry,
                                          const unsigned* sinfo, const int* wds, const uint2* stasks, int K, int el,
                                          int e) {
@@ -773,7 +774,6 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   const int hbeg = m.tile_halo_ptr[tile], nh = m.tile_halo_ptr[tile + 1] - hbeg;
   const int tbeg = m.tile_task_ptr[tile], ntask = m.tile_task_ptr[tile + 1] - tbeg;
   const StageLayout L = stage_layout(kTile, m.max_halo, m.max_tasks, (unsigned)sizeof(real));
-  BasisT<real>& B = *reinterpret_cast<BasisT<real>*>(smem_raw);
   double* qs = reinterpret_cast<double*>(smem_raw + L.qs);
   real* geo = reinterpret_cast<real*>(smem_raw + L.geo);
 #ifdef DGSWEM_MIXED
@@ -788,11 +788,6 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   int* tdry = reinterpret_cast<int*>(smem_raw + L.tdry);
   unsigned* sinfo = reinterpret_cast<unsigned*>(smem_raw + L.info);  // [einfo | eslot][kTile]
   uint2* stasks = reinterpret_cast<uint2*>(smem_raw + L.tasks);      // the tile's edge-task words
-  {
-    const real* src = reinterpret_cast<const real*>(&cBasisR);
-    real* dst = reinterpret_cast<real*>(&B);
-    for (int i = tid; i < (int)(sizeof(BasisT<real>) / sizeof(real)); i += kStageThreads) dst[i] = src[i];
-  }
 
   // ---- phase 1: tile and halo elements into shared memory ----
 #ifdef DGSWEM_MIXED
@@ -950,7 +945,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int i = w / kTile, el = w - i * kTile;
     if (el >= n || wds[el] == 0) continue;
-    volume_point<kNonlin, kSph, kTile>(A, B, qt, geo, vol, i, el, tile0 + el);
+    volume_point<kNonlin, kSph, kTile>(A, cBasisR, qt, geo, vol, i, el, tile0 + el);
   }
   cp_async_wait_all();  // the halo group
 #ifdef DGSWEM_MIXED
@@ -1022,7 +1017,7 @@ __global__ void __launch_bounds__(kStageThreads, stage_min_blocks(kStageThreads)
   for (int w = tid; w < 3 * kTile; w += kStageThreads) {
     const int K = w / kTile, el = w - K * kTile;
     if (el >= n) continue;
-    sum_mode<kNonlin, kTile>(A, B, qs, geo, vol, res, tdry, sinfo, wds, stasks, K, el, tile0 + el);
+    sum_mode<kNonlin, kTile>(A, qs, geo, vol, res, tdry, sinfo, wds, stasks, K, el, tile0 + el);
   }
 }
 
