@@ -66,9 +66,9 @@ STEP_BYTES_PER_ELEMENT_STAGE = STAGE_KERNEL_BYTES + 12 + 24
 STAGE_OVERHEAD_BYTES = {"geometry_rows_beyond_model": 112 - 48, "tile_plan": 14, "edge_info": 8}
 # DRAM bytes per element of one stage_p1 launch (strict build),
 # dram__bytes_read.sum + dram__bytes_write.sum from ncu on the same deck at
-# 999,492 elements: the mean of a stage-1 (293.9) and a stage-2 (369.0)
+# 999,492 elements: the mean of a stage-1 (292.2) and a stage-2 (368.6)
 # launch; traffic grows with the element count.
-STAGE_TRAFFIC_BYTES = 0.5 * (293.9 + 369.0)
+STAGE_TRAFFIC_BYTES = 0.5 * (292.2 + 368.6)
 
 
 def rank_env():
