@@ -12,6 +12,8 @@ DG_HYDRO_TIMESTEP over the whole mesh.  The deck is generated (seeded) into
 
 Multi-GPU (torchrun): each rank steps its own replica of the basin; the path
 has no data exchange between independent meshes (weak scaling, replicas only).
+The "partitioned" object is the strong-scaling form: the one bench mesh split
+into one partition per rank, with the halo exchange over NCCL.
 
 Each handle's tile and limiter block shapes are picked after warm-up by the
 library's autotuner (whole steps with each shape, the state restored
@@ -21,8 +23,18 @@ afterwards; "tiles" objects give the picks and per-shape times);
 The line's "mixed" object is the mixed-precision form (FP32 edge, volume and
 limiter terms; FP64 state, SSP combination and wet/dry) on the same deck: its
 rate, its speed-up over the FP64 line and its error against the FP64 form.
-The "config3" object is the 8M-element quarter annulus with wind (config 3
-at p=1): FP64 and mixed rates and the mixed form's error against FP64.
+The "config3" object is the 8M-element quarter annulus with wind (config 3):
+at p=1 and at p=2 (SSP-RK(3,3)), FP64 and mixed rates and the mixed forms'
+errors against FP64 after 5000 steps of a quickly ramped copy.  The line's
+"other_variant" object is the opt-in FMA build on the bench deck, and
+"parity" the headline build against the FP64 oracle after the CPU sample's
+steps.
+
+    python bench.py --adjoint-only [--adjoint-nx NX --adjoint-ny NY --adjoint-steps K --adjoint-no-fd]
+    python bench.py --p2-only [--config3-nr NR --config3-nth NTH --config3-p2-steps K --config3-p2-err-steps K]
+
+run the adjoint object or the config-3 p=2 objects alone (the profiling
+drivers of those kernels).
 The "ensemble" object is the batched configuration: 256 seeded members of
 5k-200k elements (about 13.5M in all) advanced by one handle in mixed
 precision, with the batched-vs-one-at-a-time rate of its first 16 members.
