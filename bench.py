@@ -239,17 +239,19 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
     hm.set_stream(stream.cuda_stream)
     hm.run(1, args.warmup)
     tiles = autotune(hm, args, args.warmup + 1)
+    it = graphs_on(hm, args, args.warmup + 1)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    hm.run(args.warmup + 1, args.steps)
+    hm.run(it, args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+    hm.set_graph(0)
     hm.profile(True)
-    hm.run(args.warmup + 1 + args.steps, 20)
+    hm.run(it + args.steps, 20)
     prof = hm.profile_read()
     hm.profile(False)
     hm.close()
@@ -276,6 +278,17 @@ def mixed_arm(deck, stream, args, world: int, dist, device: int) -> dict:
             "dtype": "f32 edge/volume/limiter terms, f64 state, SSP, wet/dry",
             "per_kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items() if v[1]},
             "tiles": tiles, "err_vs_fp64": err}
+
+
+def graphs_on(h, args, it: int) -> int:
+    """With --graph-steps > 0: whole-step CUDA graphs for the handle's run
+    call (dgswem_cuda_set_graph), captured by running one chunk from step
+    ``it`` outside any timing; returns the next step."""
+    if not args.graph_steps:
+        return it
+    h.set_graph(args.graph_steps)
+    h.run(it, args.graph_steps)
+    return it + args.graph_steps
 
 
 def config3_met(npn: int):
@@ -310,17 +323,19 @@ def config3_p2(args, stream, device: int, world: int, dist, met=None) -> dict:
             h.set_stream(stream.cuda_stream)
             h.set_met(*met)
             h.run(1, w)
+            it = graphs_on(h, args, w + 1)
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            h.run(w + 1, k2)
+            h.run(it, k2)
             e1.record(stream)
             torch.cuda.synchronize()
             ms2 = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+            h.set_graph(0)
             h.profile(True)
-            h.run(w + 1 + k2, 4)
+            h.run(it + k2, 4)
             prof = h.profile_read()
             h.profile(False)
             h.synchronize()
@@ -397,12 +412,13 @@ def config3_arm(args, stream, device: int, world: int, dist) -> dict:
             h.set_met(*met)
             h.run(1, w)
             tiles = autotune(h, args, w + 1)
+            it = graphs_on(h, args, w + 1)
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            h.run(w + 1, k)
+            h.run(it, k)
             e1.record(stream)
             torch.cuda.synchronize()
             ms = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
@@ -709,18 +725,20 @@ def other_variant_arm(deck, stream, args, world: int, dist, device: int) -> dict
         h.set_stream(stream.cuda_stream)
         h.run(1, args.warmup)
         tiles = autotune(h, args, args.warmup + 1)
+        it = graphs_on(h, args, args.warmup + 1)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         k = args.other_variant_steps
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        h.run(args.warmup + 1, k)
+        h.run(it, k)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1), world, dist, "cuda")
+        h.set_graph(0)
         h.profile(True)
-        h.run(args.warmup + 1 + k, 10)
+        h.run(it + k, 10)
         prof = h.profile_read()
         h.profile(False)
     return {"variant": VARIANT_TEXT[other], "value": whole_job_rate(world, deck.s.ne, deck.s.nrk, k, ms),
@@ -812,6 +830,8 @@ def main(argv=None):
     ap.add_argument("--config3-p2-steps", type=int, default=50, help="timed steps of the p=2 config-3 annulus (0: skip)")
     ap.add_argument("--ensemble-members", type=int, default=256, help="members of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=2000)
+    ap.add_argument("--graph-steps", type=int, default=8,
+                    help="whole steps per CUDA graph in the headline arm (even; 0: plain launches)")
     ap.add_argument("--ensemble-graph-steps", type=int, default=8,
                     help="whole steps per CUDA graph in the ensemble arm (even; 0: plain launches)")
     ap.add_argument("--adjoint-steps", type=int, default=2000, help="steps of the adjoint arm (0: skip)")
@@ -876,6 +896,13 @@ def main(argv=None):
     tiles = autotune(hs, args, args.warmup + 1)
     torch.cuda.synchronize()
     it0 = args.warmup + 1
+    if args.graph_steps:
+        # whole-step CUDA graphs of the library's run call, captured outside
+        # the timing
+        hs.set_graph(args.graph_steps)
+        hs.run(it0, args.graph_steps)
+        it0 += args.graph_steps
+        torch.cuda.synchronize()
 
     sampler = ClockSampler(local)
     if world > 1:
@@ -892,6 +919,8 @@ def main(argv=None):
         dist.barrier()
     clocks = sampler.stop()
     launches = hs.kernel_launches - launches0
+    if args.graph_steps:
+        hs.set_graph(0)  # the per-kernel timing, the e2e and parity legs launch step by step
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world, dist if world > 1 else None, "cuda")
     hs.synchronize()
@@ -943,6 +972,7 @@ def main(argv=None):
         "data": "synthetic (seeded sloping-beach deck; no public dataset)",
         "config": workload_config(args, ne, nrk),
         "gpu_launches": int(launches),
+        "graph_steps": args.graph_steps,
         "setup_s": {"deck_read": t_setup1 - t_setup0, "device_create": t_setup2 - t_setup1},
         "tiles": tiles,
         "clocks": clocks,
