@@ -5,6 +5,7 @@ within the mixed form's bars (1e-5 m elevation, 1e-9 relative volume); its
 own convergence order; and the p=1-only features rejected on a p=2
 handle."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -35,7 +36,9 @@ def run_pair(path, nsteps, strict, state=None, met=None, mixed=False):
     orc = Oracle(path)
     with HydroStep(Deck(path), strict=None if mixed else strict, mixed=mixed) as hs:
         assert hs.dofh == 6
-        assert hs.get_shapes()[0] >= 0  # the p=2 tile kernel runs (its tiles fit shared memory)
+        # the p=2 tile kernel runs (its tiles fit shared memory) unless the pair is forced
+        forced_pair = os.environ.get("DGSWEM_CUDA_P2_PAIR", "0") not in ("", "0")
+        assert (hs.get_shapes()[0] < 0) == forced_pair
         if state is not None:
             wd = np.ones(hs.ne, np.int32)
             hs.set_state(state[0], state[1], state[1], wd)
@@ -210,3 +213,40 @@ def test_p2_pair_matches_tile_kernel(built, scratch, monkeypatch, variant):
                 scale = max(np.abs(b).max(), 1e-300) if v == "ZE" else qscale
                 bar = 1e-10 if variant == "fast" else 1e-5
                 assert np.abs(a - b).max() <= bar * scale, f"{variant}, {name}: {v}"
+
+
+def p2_rain_manning_deck(path):
+    """A p=2 rectangular basin (20 x 6 km, 10 m to 4 m deep) with a tide on
+    one short side, nodal Manning n (fort.13), rain (rainfall = 1) and
+    SSP-RK(3,3): the tile kernel's rain, Manning and boundary-weight
+    branches."""
+    nx, ny = 20, 6
+    xs, ys = np.linspace(0.0, 20e3, nx + 1), np.linspace(0.0, 6e3, ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    dp = 10.0 - 6.0 * X / 20e3
+    elems = decks._grid_triangles(nx, ny)
+    nid = lambda i, j: i * (ny + 1) + j + 1  # noqa: E731
+    ocean = [nid(0, j) for j in range(ny, -1, -1)]
+    land = [nid(i, 0) for i in range(0, nx + 1)] + [nid(nx, j) for j in range(1, ny + 1)] + \
+           [nid(i, ny) for i in range(nx - 1, -1, -1)]
+    rng = np.random.default_rng(7)
+    ctl = decks.Controls(title="p2 rain manning", nolibf=1, nolifa=1, cf=0.0025, dt=2.0, nsteps=100,
+                         rk_stage=3, rk_order=3, slopeflag=0, h0=0.01, nramp=1, dramp=0.01, manning=True,
+                         rainfall=1, extra={"pl": 2, "ph": 2})
+    return decks.write_deck(path, X.ravel(), Y.ravel(), dp.ravel(), elems, [ocean], [(land, 0)], ctl,
+                            emo=np.full(len(ocean), 0.5), efa=np.zeros(len(ocean)),
+                            manning=0.025 * rng.uniform(0.8, 1.2, X.size))
+
+
+@pytest.mark.parametrize("pair", ["0", "1"])
+def test_p2_rain_manning_strict_bitwise(built, scratch, monkeypatch, pair):
+    """Rain, nodal Manning n and SSP(3,3) at p=2: the strict tile kernel and
+    the edge + element pair each bit-identical to the oracle."""
+    monkeypatch.setenv("DGSWEM_CUDA_P2_PAIR", pair)
+    path = p2_rain_manning_deck(scratch / "p2_rain_manning")
+    g, o, gn, on = run_pair(path, 100, True)
+    assert np.abs(g[0]).max() > 0
+    for a, b, v in zip(g, o, ("ZE", "QX", "QY", "WDFLG")):
+        np.testing.assert_array_equal(a, b, err_msg=v)
+    for a, b, v in zip(gn, on, ("ETA2", "UU2", "VV2")):
+        np.testing.assert_array_equal(a, b, err_msg=v)
