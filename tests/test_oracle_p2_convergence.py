@@ -84,12 +84,10 @@ def test_standing_wave_convergence_order(built, tmp_path, p):
     assert all(r > p + 1 - 0.4 for r in rates), (errs, rates)
 
 
-@pytest.mark.parametrize("p", [1, 2])
-def test_closed_basin_mass_conserved(built, tmp_path, p):
-    """Nonlinear equations (NOLIFA=1) in the closed basin from a Gaussian
-    bump: the water volume sum_e (ZE_1 + HB_1) * area stays constant to
-    round-off over 400 steps (mode 1 is the element mean)."""
-    path = tmp_path / f"mass_p{p}"
+def bump_state(path, p):
+    """The closed basin with the full nonlinear equations (NOLIFA=1) and the
+    L2 projection of a Gaussian bump of elevation: (ZE modes, HB modes,
+    element areas), from the oracle's tables."""
     x, y, elems = basin(path, 16, p)
     f15 = (path / "fort.15").read_text()
     for key in ("NOLIFA", "NOLICA", "NOLICAT"):  # the full nonlinear equations
@@ -103,14 +101,29 @@ def test_closed_basin_mass_conserved(built, tmp_path, p):
     minv = orc.real_table("M_INV")
     bump = 0.5 * np.exp(-(((px - 0.4 * L) / 1500.0) ** 2 + ((py - 0.5 * W) / 800.0) ** 2))
     ze = (bump * wa[None, :]) @ phi.T * minv[None, :]
-    zero = np.zeros_like(ze)
-    orc.set_state(ze, zero, zero, np.ones(len(elems), np.int32))
-    area = np.sum(wphys, axis=1)
     hb = orc.real_table("HB").reshape(len(elems), orc.dofh)
-    vol0 = float(np.sum((ze[:, 0] + hb[:, 0]) * area))
+    orc.close()
+    return ze, hb, np.sum(wphys, axis=1)
+
+
+def water_volume(ze, hb, area) -> float:
+    """sum_e (ZE_1 + HB_1) * area (mode 1 is the element mean)."""
+    return float(np.sum((ze[:, 0] + hb[:, 0]) * area))
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_closed_basin_mass_conserved(built, tmp_path, p):
+    """Nonlinear equations (NOLIFA=1) in the closed basin from a Gaussian
+    bump: the water volume stays constant to round-off over 400 steps."""
+    path = tmp_path / f"mass_p{p}"
+    ze, hb, area = bump_state(path, p)
+    orc = Oracle(path)
+    zero = np.zeros_like(ze)
+    orc.set_state(ze, zero, zero, np.ones(len(ze), np.int32))
+    vol0 = water_volume(ze, hb, area)
     orc.run(1, NSTEPS)
     z, qx, _, _ = orc.state()
     orc.close()
-    vol1 = float(np.sum((z[:, 0] + hb[:, 0]) * area))
+    vol1 = water_volume(z, hb, area)
     assert np.abs(qx).max() > 1e-4  # the bump spread
     assert abs(vol1 - vol0) <= 1e-12 * vol0, (vol0, vol1)
