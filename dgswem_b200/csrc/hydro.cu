@@ -1583,6 +1583,7 @@ static dgswem_cuda* create_handle(const dgswem_cuda_setup* s, int part, int npar
     if (s->nws != 0 && s->nws != 1) throw Failure(DGSWEM_ERR_ARG, "only NWS=0/1 are supported");
     if (s->nramp == 3) throw Failure(DGSWEM_ERR_ARG, "NRAMP = 3 not supported");
     if (s->ics != 1 && s->ics != 2) throw Failure(DGSWEM_ERR_ARG, "ICS must be 1 or 2");
+    validate_mesh_ids(s);
     int ndev = 0;
     DG_CUDA(cudaGetDeviceCount(&ndev));
     (void)cudaGetLastError();  // drop an error left by other code on this thread

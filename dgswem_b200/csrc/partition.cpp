@@ -54,6 +54,32 @@ std::vector<int> morton_order(const std::vector<double>& px, const std::vector<d
   return perm;
 }
 
+void validate_mesh_ids(const dgswem_cuda_setup* s) {
+  auto need = [](bool ok, const char* what) {
+    if (!ok) throw Failure(DGSWEM_ERR_ARG, what);
+  };
+  need(s->nm && s->neled && s->nedel && s->nedsd, "setup lacks mesh arrays");
+  const size_t ne = (size_t)s->ne, ned = (size_t)s->nedges;
+  for (size_t i = 0; i < 3 * ne; ++i) {
+    need(s->nm[i] >= 1 && s->nm[i] <= s->np, "NM refers to a node outside 1..NP");
+    need(s->neled[i] >= 1 && (size_t)s->neled[i] <= ned, "NELED refers to an edge outside 1..NEDGES");
+  }
+  for (size_t k = 0; k < 2 * ned; ++k) {
+    need(s->nedel[k] >= 0 && s->nedel[k] <= s->ne, "NEDEL refers to an element outside 0..NE");
+    if (s->nedel[k] != 0) need(s->nedsd[k] >= 1 && s->nedsd[k] <= 3, "NEDSD is not a local edge number 1..3");
+  }
+  const struct { const int* list; int n; const char* what; } lists[] = {
+      {s->needn, s->needs, "NEEDN"}, {s->nledn, s->nleds, "NLEDN"}, {s->nfedn, s->nfeds, "NFEDN"},
+      {s->nredn, s->nreds, "NREDN"}, {s->nebsegn, s->nebseg, "NEBSEGN"}, {s->nibsegn, 2 * s->nibseg, "NIBSEGN"}};
+  for (const auto& L : lists) {
+    if (L.n <= 0) continue;
+    if (!L.list) throw Failure(DGSWEM_ERR_ARG, std::string("setup lacks ") + L.what);
+    for (int i = 0; i < L.n; ++i)  // NIBSEGN's opposite edge may be 0 (no partner)
+      if (!(L.list[i] >= 1 && (size_t)L.list[i] <= ned) && !(L.list == s->nibsegn && i % 2 == 1 && L.list[i] == 0))
+        throw Failure(DGSWEM_ERR_ARG, std::string(L.what) + " refers to an edge outside 1..NEDGES");
+  }
+}
+
 std::vector<int> mesh_components(const dgswem_cuda_setup* s, std::vector<int>* node_comp) {
   const int ne = s->ne, np = s->np;
   std::vector<int> parent(np);

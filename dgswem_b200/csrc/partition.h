@@ -16,6 +16,14 @@ namespace dgswem {
 std::vector<int> morton_order(const std::vector<double>& px, const std::vector<double>& py,
                               const std::vector<int>& group = {});
 
+// The setup's integer mesh tables checked against their ranges before any
+// of them indexes an array: NM in 1..NP, NELED in 1..NEDGES, NEDEL in
+// 0..NE (0: no element on that side), NEDSD in 1..3 where NEDEL names an
+// element, and the boundary lists' edge numbers in 1..NEDGES.  A host that
+// passes an inconsistent mesh gets DGSWEM_ERR_ARG (a Failure) instead of a
+// fault in the setup or the kernels.
+void validate_mesh_ids(const dgswem_cuda_setup* s);
+
 // Connected components of the mesh (elements joined by shared nodes),
 // numbered by their first element in input order: one id per element, and
 // per node in *node_comp when given.  A connected mesh is one component.

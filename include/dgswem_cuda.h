@@ -137,7 +137,11 @@ typedef struct dgswem_cuda dgswem_cuda;
  * where a tile does not fit the device's shared memory or the environment
  * variable DGSWEM_CUDA_P2_PAIR is set to a non-zero integer at create, an
  * edge kernel and an element kernel with the edge-point fluxes in device
- * memory; the strict build gives the same bits with either. */
+ * memory; the strict build gives the same bits with either.
+ * The integer mesh tables are range-checked on the host before the device
+ * is touched (NM in 1..NP, NELED and the boundary lists in 1..NEDGES, NEDEL
+ * in 0..NE, NEDSD in 1..3 where NEDEL names an element): an inconsistent
+ * mesh returns DGSWEM_ERR_ARG. */
 int dgswem_cuda_create(const dgswem_cuda_setup* setup, int device, int flags,
                        dgswem_cuda** out);
 

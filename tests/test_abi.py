@@ -56,3 +56,30 @@ def test_bad_arguments(built):
     h = C.c_void_p()
     assert lib.dgswem_cuda_create(None, 0, 0, C.byref(h)) == 1
     assert lib.dgswem_cuda_hydro_timestep(None, 1) == 1
+
+
+@pytest.mark.parametrize("table,index,value,message", [
+    ("nm", 5, 10**6, "NM refers to a node"),
+    ("nm", 0, 0, "NM refers to a node"),
+    ("neled", 7, -3, "NELED refers to an edge"),
+    ("nedel", 4, 10**7, "NEDEL refers to an element"),
+    ("nedsd", 0, 4, "NEDSD is not a local edge number"),
+])
+def test_inconsistent_mesh_is_an_argument_error(built, scratch, table, index, value, message):
+    """The drop-in create checks the host's integer mesh tables before any
+    of them indexes an array (on the host, before the device is touched):
+    an out-of-range id is DGSWEM_ERR_ARG with a message, not a fault."""
+    path = decks.quarter_annulus(scratch / "qa_badmesh", nr=2, nth=4, nsteps=1)
+    with Deck(path) as d:
+        arr = getattr(d.setup.contents, table)
+        old = arr[index]
+        arr[index] = value
+        try:
+            h = C.c_void_p()
+            rc = _abi.load().dgswem_cuda_create(d.setup, 0, 0, C.byref(h))
+            buf = C.create_string_buffer(256)
+            _abi.load().dgswem_cuda_last_error(buf, 256)
+        finally:
+            arr[index] = old
+        assert rc == 1 and not h.value, (rc, buf.value)
+        assert message in buf.value.decode()
