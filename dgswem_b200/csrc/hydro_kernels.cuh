@@ -1087,6 +1087,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
   // WETDRY: values whose bits did not change are not stored again (modes
   // 2-3 are rebuilt by the limiter and stored always)
   const double m0 = q[0], m3 = q[3], m6 = q[6];
+#ifdef DGSWEM_MIXED
+  // mixed variant: modes 2-3 of a variable are stored only where the
+  // limiter rebuilt them or WETDRY changed a mode
+  bool rebuilt[3] = {false, false, false}, wd_modes = false;
+#endif
   if (L.slopeflag != 0) {
 #pragma unroll
     for (int var = 0; var < 3; ++var) {
@@ -1096,17 +1101,25 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
       // mode 1 and bound - mode 1 (differences in FP64).  The sweeps and
       // the rebuild of modes 2-3 are the reference's with mode 1 = 0 (the
       // mean cancels exactly in both), so FP32 rounds only the small
-      // deviations, not the full vertex values.
+      // deviations, not the full vertex values.  A variable whose three
+      // vertex values lie within their bounds is left as it is: the clamp
+      // changes nothing, and the sweeps and the rebuild are the identity in
+      // exact arithmetic (the reference's FP64 rebuild returns the modes to
+      // rounding), so its FP64 modes are kept rather than rounded to FP32.
       const real z0 = 0;
       real vmin[3], vmax[3], vx[3];
+      bool clamped = false;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const double2 bd = node_bounds(L.minmax, np, nd[a], var);
         vmin[a] = (real)(bd.x - zc[0]);
         vmax[a] = (real)(bd.y - zc[0]);
-        vx[a] = (real)(B.phi_corner[a][1] * zc[1] + B.phi_corner[a][2] * zc[2]);
-        vx[a] = fmax(fmin(vx[a], vmax[a]), vmin[a]);
+        const real v = (real)(B.phi_corner[a][1] * zc[1] + B.phi_corner[a][2] * zc[2]);
+        vx[a] = fmax(fmin(v, vmax[a]), vmin[a]);
+        clamped = clamped || v > vmax[a] || v < vmin[a];
       }
+      if (!clamped) continue;
+      rebuilt[var] = true;
 #else
       const real z0 = zc[0];
       real vmin[3], vmax[3], vx[3];
@@ -1171,6 +1184,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
         check = true;
       }
     } else {
+#ifdef DGSWEM_MIXED
+      wd_modes = true;
+#endif
       const double ht_avg = q[0] + dp_avg;
       if (ndry == 3 || ht_avg <= H0 + ZERO) {  // cases 2 and 3A: flatten, stop flow
         q[0] = ht_avg - dp_avg;
@@ -1246,6 +1262,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
 #pragma unroll
         for (int c = 3; c < 9; ++c) q[c] = 0.0;
         wd = 0;
+#ifdef DGSWEM_MIXED
+        wd_modes = true;
+#endif
       }
     }
     if (wd != wd_read) L.wd[e] = wd;
@@ -1255,8 +1274,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
   if (!same(q[3], m3)) L.q[(size_t)3 * ne + e] = q[3];
   if (!same(q[6], m6)) L.q[(size_t)6 * ne + e] = q[6];
 #pragma unroll
-  for (int c = 0; c < 9; ++c)
-    if (c % 3 != 0) L.q[(size_t)c * ne + e] = q[c];
+  for (int c = 0; c < 9; ++c) {
+    if (c % 3 == 0) continue;
+#ifdef DGSWEM_MIXED
+    if (!rebuilt[c / 3] && !wd_modes) continue;
+#endif
+    L.q[(size_t)c * ne + e] = q[c];
+  }
 }
 
 // write_results.F:14-170 (modal2nodal) + NODECODE from the wet flags; node n
