@@ -1,9 +1,11 @@
 // kernels_mixed.cu -- the mixed-precision variant: the fast variant with the
 // stage kernel's edge traces, numerical fluxes, boundary ghost states,
-// volume fluxes and sources and the per-mode right-hand-side sums in FP32.
-// The state, the SSP-RK combination (so the element-mean elevation
-// accumulates across stages in FP64), the ocean depth-positivity fix, the
-// slope limiter and WETDRY stay FP64.
+// volume fluxes and sources and the per-mode right-hand-side sums in FP32,
+// and the slope limiter's sweeps in FP32 on deviations from the element
+// mean (a variable whose vertex values lie within their node bounds keeps
+// its FP64 modes).  The state, the SSP-RK combination (so the element-mean
+// elevation accumulates across stages in FP64), the node bounds, the ocean
+// depth-positivity fix and WETDRY stay FP64.
 #define DGSWEM_VARIANT mixed
 #define DGSWEM_FAST_MATH 1
 #define DGSWEM_MIXED 1

@@ -2,9 +2,10 @@
 
 The stage kernel's edge traces, numerical fluxes, boundary ghost states,
 volume terms and right-hand-side sums and the slope limiter's sweeps run in
-FP32; the state, the SSP-RK combination (so the element-mean elevation
-accumulates in FP64 across stages), the ocean depth-positivity fix and WETDRY
-stay FP64.  Bars, the precision targets of the mixed form:
+FP32 (a variable whose vertex values lie within their node bounds keeps its
+FP64 modes); the state, the SSP-RK combination (so the element-mean
+elevation accumulates in FP64 across stages), the ocean depth-positivity fix
+and WETDRY stay FP64.  Bars, the precision targets of the mixed form:
 * elevation within 1e-5 m of the FP64 result, as nodal ETA2 on wet nodes and
   as element means (ZE mode 1);
 * identical wet/dry flags and nodal wet/dry codes;
