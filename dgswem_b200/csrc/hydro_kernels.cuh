@@ -1136,6 +1136,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) limit_wetdry(const __grid_
       for (int sweep = 0; sweep < 3; ++sweep) {
         const real sumloc = third_of(vx[0] + vx[1] + vx[2]);
         real sumdif = (sumloc - z0) * real(3);
+        // A sweep that starts from sumdif == +0 with every vx - vmin free of
+        // a sign bit changes no bit: each redfac is +0 (the quotient of +0,
+        // or 0, capped by a non-negative redmax), so vx - redfac leaves vx
+        // (a -0 included) and the next sweep starts from the same values.
+        // Stopping there gives the bits of running all three sweeps.
+        if (!signbit(sumdif) && sumdif == real(0) && !signbit(vx[0] - vmin[0]) && !signbit(vx[1] - vmin[1]) &&
+            !signbit(vx[2] - vmin[2]))
+          break;
         const real signdif = copysign(real(1), sumdif);
         real dif[3];
 #pragma unroll
