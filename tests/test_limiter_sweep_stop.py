@@ -9,10 +9,11 @@ every vertex value's bits as they are.  This test runs the sweeps as the
 kernel writes them (IEEE double, round to nearest, no contraction; x / 3 is
 the correctly rounded quotient, which the kernel's div3 reproduces bit for
 bit) with and without the stop on a million elements drawn to hit ties,
-signed zeros, means on their bounds and clamped vertices, and compares the
-vertex values bit for bit.  The device build is checked against the oracle
-on real decks by the strict GPU tests; this pins the stop's argument on
-inputs no deck reaches.
+signed zeros, means on their bounds and clamped vertices (and, built by
+hand, -0 vertex values around a +0 mean, the case of the stop's sign
+guard), and compares the vertex values bit for bit.  The device build is
+checked against the oracle on real decks by the strict GPU tests; this pins
+the stop's argument on inputs no deck reaches.
 """
 import numpy as np
 
@@ -71,11 +72,22 @@ def elements(rng, n):
     return vx, vmin, vmax, z0
 
 
+def signed_zero_elements():
+    """Vertex values -0 around a mean +0: sumdif = (-0 - 0) * 3 = -0, the
+    sweep's signdif is -1 and vx - (+0)(-1) turns each -0 into +0.  A stop
+    at sumdif == -0 would keep the -0 bits."""
+    vx = np.full((4, 3), -0.0)
+    vx[1, 2] = 0.0
+    vmin = np.array([[-1.0] * 3, [-0.5] * 3, [-0.0] * 3, [-2.0, -0.0, -1.0]])
+    vmax = np.array([[1.0] * 3, [0.5] * 3, [0.0] * 3, [2.0, 0.0, 1.0]])
+    return vx, vmin, vmax, np.zeros(4)
+
+
 def test_sweep_stop_is_bit_exact():
     rng = np.random.default_rng(20261204)
     total_stopped = 0
-    for _ in range(4):
-        vx, vmin, vmax, z0 = elements(rng, 250_000)
+    for block in range(5):
+        vx, vmin, vmax, z0 = elements(rng, 250_000) if block < 4 else signed_zero_elements()
         full, _ = sweeps(vx, vmin, vmax, z0, stop=False)
         short, stopped = sweeps(vx, vmin, vmax, z0, stop=True)
         np.testing.assert_array_equal(full.view(np.int64), short.view(np.int64))
