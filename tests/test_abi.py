@@ -64,6 +64,8 @@ def test_bad_arguments(built):
     ("neled", 7, -3, "NELED refers to an edge"),
     ("nedel", 4, 10**7, "NEDEL refers to an element"),
     ("nedsd", 0, 4, "NEDSD is not a local edge number"),
+    ("needn", 0, 0, "NEEDN refers to an edge"),
+    ("nledn", 3, 10**6, "NLEDN refers to an edge"),
 ])
 def test_inconsistent_mesh_is_an_argument_error(built, scratch, table, index, value, message):
     """The drop-in create checks the host's integer mesh tables before any
