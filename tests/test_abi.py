@@ -85,3 +85,31 @@ def test_inconsistent_mesh_is_an_argument_error(built, scratch, table, index, va
             arr[index] = old
         assert rc == 1 and not h.value, (rc, buf.value)
         assert message in buf.value.decode()
+
+
+def test_valid_meshes_pass_the_mesh_check(built, scratch):
+    """create's range check accepts every kind of mesh the library reads:
+    barriers (the wetdry golden deck), flow and radiation edges, p=2, a
+    merged ensemble.  Without a GPU create then fails at the device query
+    (DGSWEM_ERR_CUDA), with one it succeeds; never DGSWEM_ERR_ARG."""
+    from conftest import golden_dir
+    specs = decks.ensemble_specs(3, seed=5, ne_min=200, ne_max=600)
+    members = [Deck(decks.ensemble_member(scratch / f"vm_m{i}", s["kind"], s["ne"], s["amp"], s["n_manning"],
+                                          s["seed"])) for i, s in enumerate(specs)]
+    paths = [golden_dir("wetdry"),
+             decks.quarter_annulus(scratch / "vm_flowrad", nr=4, nth=8, nsteps=1, flow_amp=0.05, radiation=True),
+             decks.quarter_annulus(scratch / "vm_p2", nr=4, nth=8, nsteps=1, rk_stage=3, rk_order=3,
+                                   extra={"pl": 2, "ph": 2})]
+    checked = [Deck(p) for p in paths] + [Deck.merge(members)]
+    lib = _abi.load()
+    for d in checked:
+        h = C.c_void_p()
+        rc = lib.dgswem_cuda_create(d.setup, 0, 0, C.byref(h))
+        buf = C.create_string_buffer(256)
+        lib.dgswem_cuda_last_error(buf, 256)
+        assert rc in (0, 2), (rc, buf.value)
+        if rc == 0:
+            lib.dgswem_cuda_destroy(h)
+        d.close()
+    for m in members:
+        m.close()
