@@ -33,6 +33,10 @@
 #include <unordered_map>
 #include <vector>
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 namespace {
 
 constexpr double kPi = 3.141592653589793;
@@ -53,15 +57,43 @@ class ListStream {
     in.seekg(0, std::ios::beg);
     buf_.resize(size > 0 ? (size_t)size : 0);
     if (size > 0) in.read(&buf_[0], size);
-    size_t i = 0, n = buf_.size();
-    while (i < n) {
-      size_t j = buf_.find('\n', i);
-      if (j == std::string::npos) j = n;
-      size_t len = j - i;
-      if (len > 0 && buf_[i + len - 1] == '\r') --len;
-      rec_.push_back({i, len});
-      i = j + 1;
+    // records: the text between line feeds (a trailing carriage return
+    // dropped; a last line without a line feed is a record too).  The line
+    // feeds are found in parallel, one contiguous chunk per thread, and the
+    // records assembled in order.
+    const size_t n = buf_.size();
+    int nchunk = 1;
+#ifdef _OPENMP
+    nchunk = std::max(1, omp_get_max_threads());
+#endif
+    const size_t chunk = (n + nchunk - 1) / std::max<size_t>(nchunk, 1);
+    std::vector<std::vector<size_t>> feeds(nchunk);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nchunk; ++c) {
+      const size_t b = std::min(n, (size_t)c * chunk), e = std::min(n, b + chunk);
+      for (size_t i = b; i < e;) {
+        const void* p = std::memchr(buf_.data() + i, '\n', e - i);
+        if (!p) break;
+        const size_t j = (size_t)(static_cast<const char*>(p) - buf_.data());
+        feeds[c].push_back(j);
+        i = j + 1;
+      }
     }
+    size_t total = 0;
+    for (const auto& f : feeds) total += f.size();
+    rec_.reserve(total + 1);
+    size_t start = 0;
+    auto add = [&](size_t end) {
+      size_t len = end - start;
+      if (len > 0 && buf_[start + len - 1] == '\r') --len;
+      rec_.push_back({start, len});
+    };
+    for (const auto& f : feeds)
+      for (size_t j : f) {
+        add(j);
+        start = j + 1;
+      }
+    if (start < n) add(n);
     return true;
   }
   const std::string& path() const { return path_; }

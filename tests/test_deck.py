@@ -92,3 +92,27 @@ def test_p2_deck(built, scratch):
         bad = decks.quarter_annulus(scratch / f"deck_p2_{next(iter(kw))}", nr=4, nth=8, nsteps=2, **kw, **p2)
         with pytest.raises(DgswemError, match="p = 1 only"):
             Deck(bad)
+
+
+def test_line_endings_do_not_change_the_deck(built, scratch):
+    """The reader splits its files into records at line feeds, in parallel
+    chunks: CRLF line endings, blank lines after the tables and a last line
+    without a line feed give the same deck as the plain files."""
+    import shutil
+    plain = decks.sloping_beach(scratch / "le_plain", nx=40, ny=8, nsteps=20)
+    crlf = scratch / "le_crlf"
+    shutil.rmtree(crlf, ignore_errors=True)
+    shutil.copytree(plain, crlf)
+    for name in ("fort.14", "fort.15", "fort.13"):
+        text = (plain / name).read_text()
+        (crlf / name).write_text(text.rstrip("\n").replace("\n", "\r\n") + ("\r\n\r\n" if name == "fort.14" else ""),
+                                 newline="")
+    a, b = Deck(plain), Deck(crlf)
+    s, t = a.s, b.s
+    assert (s.ne, s.np, s.nedges) == (t.ne, t.np, t.nedges)
+    for name, n in [("nm", 3 * s.ne), ("nedno", 2 * s.nedges), ("nedel", 2 * s.nedges), ("neled", 3 * s.ne)]:
+        np.testing.assert_array_equal(a.int_array(name, n), b.int_array(name, n), err_msg=name)
+    for name, n in [("x", s.np), ("y", s.np), ("dp", s.np)]:
+        np.testing.assert_array_equal(a.real_array(name, n), b.real_array(name, n), err_msg=name)
+    a.close()
+    b.close()
