@@ -279,3 +279,18 @@ def test_upload_download_roundtrip(built, scratch):
     np.testing.assert_array_equal(x2, qx)
     np.testing.assert_array_equal(y2, qy)
     np.testing.assert_array_equal(w2, wd)
+
+
+@pytest.mark.parametrize("rk", [(1, 1), (3, 3), (5, 2)])
+def test_strict_wetdry_other_rk_schemes(built, scratch, rk):
+    """Wet/dry, limiter 5 and nodal Manning n with the other SSP-RK schemes
+    of RK_TIME (forward Euler at a quarter of the step, SSP(3,3), the
+    tabulated SSP(5,2)): every stage's limiter and WETDRY pass and the
+    combinations over the stage history, bit for bit against the oracle."""
+    stages, order = rk
+    dt = 0.125 if stages == 1 else 0.5
+    path = decks.sloping_beach(scratch / f"sb_rk{stages}{order}", nx=40, ny=8, lx=2000.0, ly=400.0, nsteps=120,
+                               dt=dt, rk_stage=stages, rk_order=order)
+    _, _, g, o = run_both(path, 120, strict=True)
+    assert 0 < g[3].sum() < len(g[3])
+    check_bitwise(g, o)
